@@ -1,0 +1,219 @@
+/*
+ * w2d.h -- C-ABI of the B200 block-update library for Walicxe-2D.
+ *
+ * The library owns a device-resident pool of blocks (conserved variables u,
+ * the half-step copy up and, under DMC cooling, the primitives) indexed by
+ * the reference's own block ID.  A host that keeps the reference's Fortran
+ * main loop and its integer block tree (admesh, markref, locatebounds ...)
+ * calls these entry points in place of the Fortran subroutines named in each
+ * comment.  All entry points return an int status (W2D_OK == 0); no entry
+ * point keeps a host pointer after it returns.
+ *
+ * Array conventions follow the reference's Fortran globals
+ * (src/globals.f90:13-29):
+ *   - block IDs are 1-based (nbmin..nbmax);
+ *   - lp(nb,1:8), icoord(nb,1:2) and innerbounds(n,1:3) are column-major
+ *     with a caller-given leading dimension;
+ *   - Fortran LOGICAL arrays (leaf) are passed as 4-byte integers, any
+ *     nonzero value meaning .true.;
+ *   - a block's variables are u(nb, ieq, i, j) with ieq = 1..neq and
+ *     i, j = -1..nx+2.  The block-major entry points (w2d_put_blocks,
+ *     w2d_get_blocks) use [block][ieq][j][i] with i fastest, which is also
+ *     the device pool layout; the *_fortran variants read and write the
+ *     reference's own u(nbmin:nbmaxtot, neq, -1:18, -1:18) array directly.
+ */
+#ifndef W2D_H
+#define W2D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define W2D_OK              0
+#define W2D_ERR_ARG         1  /* bad argument or unsupported parameter      */
+#define W2D_ERR_CUDA        2  /* CUDA runtime error (message in last_error) */
+#define W2D_ERR_HLLC        3  /* NaN contact speed: src/hllcfluxes.f90:170  */
+#define W2D_ERR_CAPACITY    4  /* block pool exhausted: src/admesh.f90:44    */
+#define W2D_ERR_TOPOLOGY    5  /* innerbounds leaves a leaf face unfilled    */
+#define W2D_ERR_TIMEOUT     6  /* a bounded device wait gave up              */
+#define W2D_ERR_STATE       7  /* call out of order (e.g. no topology yet)   */
+#define W2D_ERR_NOMEM       8  /* device or host allocation failed           */
+
+/* ---- method selectors (JET/Makefile:27-62 compile-time flags) ----------- */
+#define W2D_HLLC        0   /* -DHLLC      src/hllcfluxes.f90     */
+#define W2D_HLL         1   /* -DHLL       src/hllfluxes.f90      */
+#define W2D_HLL_HLLC    2   /* -DHLL_HLLC  src/hll_hllcfluxes.f90 */
+
+#define W2D_ADIABATIC   0   /* -DADIABATIC  */
+#define W2D_COOLINGH    1   /* -DCOOLINGH   src/coolingh.f90  */
+#define W2D_COOLINGDMC  2   /* -DCOOLINGDMC src/coolingdmc.f90 */
+
+#define W2D_BC_OUTFLOW     0   /* -DOUTF*  */
+#define W2D_BC_REFLECTIVE  1   /* -DREF*   */
+
+#define W2D_USERBC_NONE 0
+#define W2D_USERBC_JET  1   /* -DOTHERB with impose_jet, src/jet.f90:41 */
+
+/* Reproduce the reference's known defects (default: both on).             */
+#define W2D_COMPAT_HLLC_STAR 1  /* primr(4)/(primr(4)*srmur): hllcfluxes.f90:157 */
+#define W2D_COMPAT_OUTFYB    2  /* u(nb,...) with nb the list index: boundaryI.f90:87 */
+
+/* ---- runtime parameters (src/parameters.f90 compile-time constants) ---- */
+typedef struct W2dParams {
+  int32_t neq;        /* equations incl. passive scalars (4..8)             */
+  int32_t npas;       /* passive scalars, neq == 4 + npas                   */
+  int32_t nx, ny;     /* interior cells per block side (16)                 */
+  int32_t nlevs;      /* refinement levels                                  */
+  int32_t nbroot_x;   /* root blocks in x                                   */
+  int32_t nbroot_y;   /* root blocks in y                                   */
+  int32_t nblocks;    /* pool capacity: largest block ID                    */
+  int32_t solver;     /* W2D_HLLC / W2D_HLL / W2D_HLL_HLLC                   */
+  int32_t limiter;    /* LIMITER, -1..6 (src/limiter.f90:30-85)              */
+  int32_t cooling;    /* W2D_ADIABATIC / W2D_COOLINGH / W2D_COOLINGDMC        */
+  int32_t bc_left, bc_right, bc_bottom, bc_top;  /* W2D_BC_*                 */
+  int32_t otherb;     /* W2D_USERBC_*                                        */
+  int32_t compat;     /* W2D_COMPAT_* bit set                                */
+  int32_t precision;  /* 64 (plain FP64 path) or 32 (FP32 state and fluxes)  */
+  int32_t pad_;
+  double cv, gamma, cfl, eta;      /* src/parameters.f90:39,61-63           */
+  double xmax, ymax;               /* box size, code units                   */
+  double tempsc, psc, tsc, rsc;    /* scalings, src/parameters.f90:50-54     */
+  double tol, tol2;                /* refinement tolerances, criteria.f90:11 */
+  /* jet source (src/jet.f90:14-33), code units */
+  double jet_rj, jet_lj, jet_posx, jet_posy;
+  double jet_den, jet_temp, jet_v0, jet_dv, jet_tau;
+} W2dParams;
+
+typedef struct W2dError {
+  int32_t code;       /* W2D_ERR_* of the first failure                     */
+  int32_t block;      /* block ID where the device saw it (0 if none)       */
+  int32_t i, j;       /* cell or interface index (reference numbering)      */
+  char message[240];
+} W2dError;
+
+typedef struct W2dCtx W2dCtx;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+/* Replaces the allocate() of u, up, primit in src/initmain.f90:76-81. */
+int w2d_create(const W2dParams* p, W2dCtx** out);
+int w2d_destroy(W2dCtx* ctx);
+/* Copies the first failure seen since the last call, then clears it. */
+int w2d_last_error(W2dCtx* ctx, W2dError* err);
+/* DMC table as read in src/initmain.f90:83-98: n rows of (log10 T, -log10 L). */
+int w2d_set_cooltab(W2dCtx* ctx, const double* log_t, const double* neg_log_l, int n);
+/* Library version string and the build's target architecture. */
+const char* w2d_version(void);
+
+/* ---- topology (produced on the host by basegrid/admesh/locatebounds) ---- */
+/* lp(nb,1:8), leaf(nb), icoord(nb,1:2) for nb = 1..nbmax, column-major with
+ * leading dimensions ld_lp / ld_icoord (rows are block IDs starting at 1).
+ * Mirrors the globals lp, leaf, icoord (src/globals.f90:19-24) and dx, dy
+ * (src/initmain.f90:58-62); dx and dy hold nlevs entries. */
+int w2d_set_topology(W2dCtx* ctx, const int32_t* lp, int ld_lp,
+                     const int32_t* leaf, const int32_t* icoord, int ld_icoord,
+                     int nbmax, const double* dx, const double* dy);
+/* innerbounds(1:ninternal,1:3) as built by locatebounds
+ * (src/locatebounds.f90:29-540), column-major with leading dimension ld. */
+int w2d_set_bounds(W2dCtx* ctx, const int32_t* innerbounds, int ld, int ninternal);
+
+/* ---- block data (host <-> pool) ----------------------------------------- */
+/* u of the n blocks ids[0..n-1], block-major [n][neq][nx+4][nx+4], i fastest.
+ * put also recomputes the stored primitives and the CFL partials of those
+ * blocks, as calcprim does after the reference sets u (basegrid.f90:38-41). */
+int w2d_put_blocks(W2dCtx* ctx, const int32_t* ids, int n, const double* u);
+int w2d_get_blocks(W2dCtx* ctx, const int32_t* ids, int n, double* u);
+/* Same, on the reference's Fortran array u(nbmin:nbmaxtot,neq,-1:18,-1:18)
+ * with leading dimension ld (= nbmaxtot-nbmin+1); only the listed IDs move. */
+int w2d_put_u_fortran(W2dCtx* ctx, const double* u, int ld, int nbmin,
+                      const int32_t* ids, int n);
+int w2d_get_u_fortran(W2dCtx* ctx, double* u, int ld, int nbmin,
+                      const int32_t* ids, int n);
+/* primit (block-major, like w2d_get_blocks) as the reference holds it. */
+int w2d_get_primit(W2dCtx* ctx, const int32_t* ids, int n, double* prim);
+
+/* ---- the per-step block update (src/main.f90:87-98) --------------------- */
+/* timestep(dt), src/timestep.f90:7-61: CFL minimum over interior leaf cells
+ * (and the DMC cooling-time limit).  Writes dt to *dt. */
+int w2d_timestep(W2dCtx* ctx, double* dt);
+/* tstep(time,dt), src/tstep.f90:4-126, after w2d_set_bounds has received the
+ * list that locatebounds(time) builds: half step, boundaryII, full step,
+ * viscosity, u=up, boundaryI, then calcprim / coolingh / coolingdmc. */
+int w2d_tstep(W2dCtx* ctx, double time, double dt);
+/* criteria(nb,...), src/criteria.f90:16-50: the per-leaf maximum relative
+ * jump of p and rho.  grad[nb-1] for nb = 1..nbmax (non-leaves get -1). The
+ * flags follow on the host: grad >= tol -> refine (level < nlevs), else
+ * grad <= tol2 -> coarsen. */
+int w2d_criteria(W2dCtx* ctx, double* grad);
+/* The u motion of refine (src/refine.f90:30-38, 227-258): quads[k*5+0] is
+ * the parent, quads[k*5+1..4] the four sons (BL, BR, TL, TR). */
+int w2d_refine(W2dCtx* ctx, const int32_t* quads, int n);
+/* The u motion of coarse (src/coarse.f90:29-180): quads[k*5+0] is the new
+ * leaf (dad), quads[k*5+1..4] its four sons. */
+int w2d_coarse(W2dCtx* ctx, const int32_t* quads, int n);
+/* Standalone ghost fills and source terms, each equal to the reference
+ * routine applied to the current pool (used by hosts that split tstep). */
+int w2d_boundaryI(W2dCtx* ctx, double time);    /* src/boundaryI.f90:4   */
+int w2d_boundaryII(W2dCtx* ctx, double time);   /* src/boundaryII.f90:4  */
+int w2d_calcprim(W2dCtx* ctx);                  /* src/calcprim.f90:5, every leaf */
+int w2d_coolingh(W2dCtx* ctx, double dt_s);     /* src/coolingh.f90:5    */
+int w2d_coolingdmc(W2dCtx* ctx, double dt_s);   /* src/coolingdmc.f90:6  */
+
+/* ---- measurement --------------------------------------------------------- */
+/* Turns per-kernel CUDA-event timing on (1) or off (0) and resets it. */
+int w2d_profile(W2dCtx* ctx, int on);
+/* Kernel timing totals since w2d_profile(ctx,1): names[k] (NUL-separated,
+ * up to cap bytes), launches[k], total_ms[k]; returns the number of kernels
+ * in *nk (at most maxk). */
+int w2d_profile_read(W2dCtx* ctx, char* names, int cap, int32_t* launches,
+                     double* total_ms, int maxk, int* nk);
+/* Number of the library's own kernel launches since creation. */
+int w2d_launch_count(W2dCtx* ctx, int64_t* n);
+/* Blocks until all queued work of the context is done. */
+int w2d_sync(W2dCtx* ctx);
+
+/* ---- whole-run driver ----------------------------------------------------
+ * A C++ restatement of the reference's host side (main.f90 loop, basegrid,
+ * admesh, markref, critneighup/down, updatelpup/down, locatebounds) driving
+ * the entry points above.  It exists so that the block update can be run and
+ * measured without the Fortran host; it makes the same calls a Fortran host
+ * would. */
+typedef struct W2dInit {
+  int32_t kind;          /* W2D_IC_* */
+  int32_t init_levels;   /* uniform pre-refinement (1 = roots only)          */
+  int32_t startup_admesh;/* admesh passes before the loop (main.f90:60-63)   */
+  int32_t pad_;
+  double rho0, p0;       /* ambient density and pressure (code units)       */
+  double e_dep;          /* energy density in the deposit region            */
+  double xc, yc, rb;     /* deposit centre and radius (code units)          */
+  double xh0;            /* neutral fraction of the ambient (COOLINGH)       */
+  double extra[8];       /* kind-specific (SN: rho_in, vmax, eth_in, rsn)    */
+} W2dInit;
+
+#define W2D_IC_SEDOV 0   /* uniform ambient + energy deposit (Sedov blast)  */
+#define W2D_IC_SNR   1   /* impose_sn-style remnant, src/sn.f90:19-62       */
+#define W2D_IC_JET   2   /* ambient + impose_jet, src/user_mod.f90:39-62     */
+
+typedef struct W2dSim W2dSim;
+int w2d_sim_create(const W2dParams* p, const W2dInit* ic, W2dSim** out);
+int w2d_sim_destroy(W2dSim* sim);
+/* Advances nsteps steps of the main loop: timestep, tstep, admesh. */
+int w2d_sim_run(W2dSim* sim, int nsteps);
+/* time, last dt, steps taken, nbmax, leaf count, zone-updates so far */
+int w2d_sim_status(W2dSim* sim, double* time, double* dt, int64_t* steps,
+                   int32_t* nbmax, int32_t* nleaf, int64_t* zone_updates);
+/* The context the driver uses (for w2d_get_blocks, w2d_profile ...). */
+W2dCtx* w2d_sim_ctx(W2dSim* sim);
+/* Host block tree: copies lp (column-major, ld = nblocks), leaf, icoord and
+ * the current innerbounds (column-major, ld = *ninternal) when non-NULL. */
+int w2d_sim_tree(W2dSim* sim, int32_t* lp, int32_t* leaf, int32_t* icoord,
+                 int32_t* innerbounds, int32_t* ninternal);
+/* Enables/disables AMR (admesh after each step); on by default if nlevs>1. */
+int w2d_sim_set_amr(W2dSim* sim, int on);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* W2D_H */

@@ -1,0 +1,152 @@
+"""Runtime parameters of the block update (ctypes mirror of ``include/w2d.h``).
+
+The reference fixes all of these at compile time (``src/parameters.f90`` and
+the ``-D`` flags of ``JET/Makefile:27-62``); here they are fields of
+``W2dParams`` so one build serves every configuration.  ``W2dInit`` selects
+the initial conditions of the whole-run driver.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+# method selectors (JET/Makefile:27-62)
+HLLC, HLL, HLL_HLLC = 0, 1, 2
+ADIABATIC, COOLINGH, COOLINGDMC = 0, 1, 2
+BC_OUTFLOW, BC_REFLECTIVE = 0, 1
+USERBC_NONE, USERBC_JET = 0, 1
+COMPAT_HLLC_STAR = 1   # src/hllcfluxes.f90:157
+COMPAT_OUTFYB = 2      # src/boundaryI.f90:87
+IC_SEDOV, IC_SNR, IC_JET = 0, 1, 2
+
+# physical constants of src/parameters.f90:28-34 (cgs)
+PC = 3.0857e18
+AU = 1.496e13
+MSUN = 1.99e33
+AMH = 1.66e-24
+KB = 1.38e-16
+RG = 8.3145e7
+YR = 3.156e7
+
+
+class W2dParams(C.Structure):
+    _fields_ = [
+        ("neq", C.c_int32), ("npas", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32),
+        ("nlevs", C.c_int32), ("nbroot_x", C.c_int32), ("nbroot_y", C.c_int32),
+        ("nblocks", C.c_int32), ("solver", C.c_int32), ("limiter", C.c_int32),
+        ("cooling", C.c_int32), ("bc_left", C.c_int32), ("bc_right", C.c_int32),
+        ("bc_bottom", C.c_int32), ("bc_top", C.c_int32), ("otherb", C.c_int32),
+        ("compat", C.c_int32), ("precision", C.c_int32), ("pad_", C.c_int32),
+        ("cv", C.c_double), ("gamma", C.c_double), ("cfl", C.c_double), ("eta", C.c_double),
+        ("xmax", C.c_double), ("ymax", C.c_double),
+        ("tempsc", C.c_double), ("psc", C.c_double), ("tsc", C.c_double), ("rsc", C.c_double),
+        ("tol", C.c_double), ("tol2", C.c_double),
+        ("jet_rj", C.c_double), ("jet_lj", C.c_double), ("jet_posx", C.c_double),
+        ("jet_posy", C.c_double), ("jet_den", C.c_double), ("jet_temp", C.c_double),
+        ("jet_v0", C.c_double), ("jet_dv", C.c_double), ("jet_tau", C.c_double),
+    ]
+
+    def copy(self) -> "W2dParams":
+        q = W2dParams()
+        C.pointer(q)[0] = self
+        return q
+
+    def as_dict(self) -> dict:
+        return {f[0]: getattr(self, f[0]) for f in self._fields_ if f[0] != "pad_"}
+
+
+class W2dInit(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("init_levels", C.c_int32), ("startup_admesh", C.c_int32),
+        ("pad_", C.c_int32),
+        ("rho0", C.c_double), ("p0", C.c_double), ("e_dep", C.c_double),
+        ("xc", C.c_double), ("yc", C.c_double), ("rb", C.c_double), ("xh0", C.c_double),
+        ("extra", C.c_double * 8),
+    ]
+
+
+class W2dError(C.Structure):
+    _fields_ = [("code", C.c_int32), ("block", C.c_int32), ("i", C.c_int32),
+                ("j", C.c_int32), ("message", C.c_char * 240)]
+
+
+def scalings(xphys: float, xmax: float, cv: float = 1.5, t0: float = 1.0e4,
+             amol: float = 0.6) -> dict:
+    """Scaling factors of src/parameters.f90:39-54, evaluated left to right."""
+    gamma = (cv + 1.0) / cv
+    rsc = xphys / xmax
+    tempsc = t0 * gamma
+    psc = gamma * AMH * RG * t0
+    vsc2 = gamma * t0 * RG / amol
+    tsc = rsc / math.sqrt(vsc2)
+    return dict(gamma=gamma, rsc=rsc, rhosc=AMH * amol, tempsc=tempsc, psc=psc,
+                vsc2=vsc2, tsc=tsc)
+
+
+def base_params(**kw) -> W2dParams:
+    """Defaults of src/parameters.f90 with the serial build's flag set."""
+    p = W2dParams()
+    p.neq, p.npas, p.nx, p.ny = 4, 0, 16, 16
+    p.nlevs, p.nbroot_x, p.nbroot_y, p.nblocks = 1, 4, 4, 64
+    p.solver, p.limiter, p.cooling = HLLC, 1, ADIABATIC
+    p.bc_left = p.bc_right = p.bc_bottom = p.bc_top = BC_OUTFLOW
+    p.otherb = USERBC_NONE
+    p.compat = COMPAT_HLLC_STAR | COMPAT_OUTFYB
+    p.precision = 64
+    p.cv = 1.5
+    sc = scalings(3.0e17, 1.0, p.cv)
+    p.gamma = sc["gamma"]
+    p.cfl, p.eta = 0.4, 0.001
+    p.xmax, p.ymax = 1.0, 1.0
+    p.tempsc, p.psc, p.tsc, p.rsc = sc["tempsc"], sc["psc"], sc["tsc"], sc["rsc"]
+    p.tol, p.tol2 = 0.05, 1.0          # src/criteria.f90:11
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def sedov(nbroot: int = 4, nlevs: int = 1, tol: float = 0.1, nblocks: int | None = None,
+          rb_cells: float = 3.0, e0: float = 1.0, p0: float = 1.0e-5, rho0: float = 1.0,
+          startup_admesh: int | None = None, **kw):
+    """2D Sedov blast: ambient rho0, p0 and energy e0 deposited as a uniform
+    energy density in the cells (of the root level) whose centres lie within
+    rb_cells root cells of the domain centre.
+
+    nbroot=4, nlevs=1 is the CPU-runnable 4x4-block case; nbroot=8, nlevs=5,
+    tol=0.1 is the AMR case (about 1,500-4,000 leaves once the blast grows).
+    """
+    if nblocks is None:
+        nblocks = nbroot * nbroot if nlevs == 1 else 40000
+    p = base_params(nlevs=nlevs, nbroot_x=nbroot, nbroot_y=nbroot, nblocks=nblocks,
+                    tol=tol, **kw)
+    dx1 = p.xmax / p.nx / nbroot
+    dy1 = p.ymax / p.ny / nbroot
+    # count of root-level cell centres inside the deposit radius (32 for 3 cells)
+    n_in = 0
+    half = int(rb_cells) + 2
+    for a in range(-half, half):
+        for b in range(-half, half):
+            if (a + 0.5) ** 2 + (b + 0.5) ** 2 < rb_cells ** 2:
+                n_in += 1
+    ic = W2dInit()
+    ic.kind = IC_SEDOV
+    ic.init_levels = 1
+    ic.startup_admesh = 4 if (startup_admesh is None and nlevs > 1) else (startup_admesh or 0)
+    ic.rho0, ic.p0 = rho0, p0
+    ic.xc, ic.yc = 0.5 * p.xmax, 0.5 * p.ymax
+    ic.rb = rb_cells * dx1
+    ic.e_dep = e0 / (n_in * dx1 * dy1)
+    ic.xh0 = 0.0
+    return p, ic
+
+
+def config(name: str):
+    """Named workloads: 'sedov64' (4x4 roots, no AMR), 'sedov_amr' (8x8
+    roots, 5 levels, tol 0.1) and small test variants."""
+    if name == "sedov64":
+        return sedov(nbroot=4, nlevs=1)
+    if name == "sedov_amr":
+        return sedov(nbroot=8, nlevs=5, tol=0.1)
+    if name == "sedov_amr_small":
+        return sedov(nbroot=4, nlevs=3, tol=0.1, nblocks=4000)
+    raise KeyError(name)
