@@ -1,0 +1,85 @@
+"""ctypes binding of libw2d.so (the C-ABI declared in include/w2d.h).
+
+The library is built in-tree (``walicxe2d_b200/libw2d.so``).  There is no
+CPU fallback: if the library or a CUDA device is missing, loading fails
+with an exception.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .params import W2dError, W2dInit, W2dParams
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libw2d.so")
+
+# Every entry point of include/w2d.h: name -> (restype, argtypes)
+_vp = C.c_void_p
+_I = C.c_int
+_D = C.c_double
+_PI32 = C.POINTER(C.c_int32)
+_PD = C.POINTER(C.c_double)
+SIGNATURES = {
+    "w2d_version": (C.c_char_p, []),
+    "w2d_create": (_I, [C.POINTER(W2dParams), C.POINTER(_vp)]),
+    "w2d_destroy": (_I, [_vp]),
+    "w2d_last_error": (_I, [_vp, C.POINTER(W2dError)]),
+    "w2d_set_cooltab": (_I, [_vp, _PD, _PD, _I]),
+    "w2d_set_topology": (_I, [_vp, _PI32, _I, _PI32, _PI32, _I, _I, _PD, _PD]),
+    "w2d_set_bounds": (_I, [_vp, _PI32, _I, _I]),
+    "w2d_put_blocks": (_I, [_vp, _PI32, _I, _PD]),
+    "w2d_get_blocks": (_I, [_vp, _PI32, _I, _PD]),
+    "w2d_put_u_fortran": (_I, [_vp, _PD, _I, _I, _PI32, _I]),
+    "w2d_get_u_fortran": (_I, [_vp, _PD, _I, _I, _PI32, _I]),
+    "w2d_get_primit": (_I, [_vp, _PI32, _I, _PD]),
+    "w2d_timestep": (_I, [_vp, _PD]),
+    "w2d_tstep": (_I, [_vp, _D, _D]),
+    "w2d_criteria": (_I, [_vp, _PD]),
+    "w2d_refine": (_I, [_vp, _PI32, _I]),
+    "w2d_coarse": (_I, [_vp, _PI32, _I]),
+    "w2d_boundaryI": (_I, [_vp, _D]),
+    "w2d_boundaryII": (_I, [_vp, _D]),
+    "w2d_calcprim": (_I, [_vp]),
+    "w2d_coolingh": (_I, [_vp, _D]),
+    "w2d_coolingdmc": (_I, [_vp, _D]),
+    "w2d_profile": (_I, [_vp, _I]),
+    "w2d_profile_read": (_I, [_vp, C.c_char_p, _I, _PI32, _PD, _I, C.POINTER(_I)]),
+    "w2d_launch_count": (_I, [_vp, C.POINTER(C.c_int64)]),
+    "w2d_sync": (_I, [_vp]),
+    "w2d_sim_create": (_I, [C.POINTER(W2dParams), C.POINTER(W2dInit), C.POINTER(_vp)]),
+    "w2d_sim_destroy": (_I, [_vp]),
+    "w2d_sim_run": (_I, [_vp, _I]),
+    "w2d_sim_status": (_I, [_vp, _PD, _PD, C.POINTER(C.c_int64), _PI32, _PI32, C.POINTER(C.c_int64)]),
+    "w2d_sim_ctx": (_vp, [_vp]),
+    "w2d_sim_tree": (_I, [_vp, _PI32, _PI32, _PI32, _PI32, _PI32]),
+    "w2d_sim_set_amr": (_I, [_vp, _I]),
+}
+
+_LIB = None
+
+
+def load(path: str = LIBPATH):
+    """Loads libw2d.so and declares every entry point; raises if absent."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with walicxe2d_b200.build.build()")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+class W2dException(RuntimeError):
+    def __init__(self, code: int, err: W2dError | None = None, what: str = ""):
+        msg = f"{what}: status {code}"
+        if err is not None and err.code:
+            msg += f" ({err.message.decode(errors='replace')}; block {err.block}, i {err.i}, j {err.j})"
+        super().__init__(msg)
+        self.code = code
+        self.block = err.block if err is not None else 0

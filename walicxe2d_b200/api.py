@@ -1,0 +1,241 @@
+"""Python mirror of the reference's routines over the C-ABI.
+
+``Context`` is one device pool; its methods carry the names of the Fortran
+subroutines they replace (``timestep``, ``tstep``, ``boundaryI`` ...).
+``Simulation`` is the whole-run driver (the reference's ``main`` loop with
+its host block tree restated in C++), used for runs and measurements.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .params import W2dError, W2dInit, W2dParams
+
+W = 20  # block side with ghosts
+
+
+def _pi32(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _pd(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Context:
+    """A device block pool (w2d_create).  Block IDs are 1-based."""
+
+    def __init__(self, p: W2dParams | None = None, handle=None, owner=None):
+        self.L = _lib.load()
+        self._owner = owner
+        if handle is not None:
+            self.h = C.c_void_p(handle)
+            self._own = False
+            self.p = p
+        else:
+            self.p = p.copy()
+            h = C.c_void_p()
+            rc = self.L.w2d_create(C.byref(self.p), C.byref(h))
+            if rc:
+                raise _lib.W2dException(rc, None, "w2d_create")
+            self.h = h
+            self._own = True
+        self.neq = self.p.neq
+
+    def close(self):
+        if getattr(self, "_own", False) and self.h:
+            self.L.w2d_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc:
+            e = W2dError()
+            self.L.w2d_last_error(self.h, C.byref(e))
+            raise _lib.W2dException(rc, e, what)
+
+    # ---- set-up ------------------------------------------------------------
+    def set_cooltab(self, log_t, neg_log_l):
+        a = np.ascontiguousarray(log_t, np.float64)
+        b = np.ascontiguousarray(neg_log_l, np.float64)
+        self._check(self.L.w2d_set_cooltab(self.h, _pd(a), _pd(b), a.size), "w2d_set_cooltab")
+
+    def set_topology(self, lp: np.ndarray, leaf: np.ndarray, icoord: np.ndarray, nbmax: int,
+                     dx: np.ndarray, dy: np.ndarray):
+        """lp: (nbmax, 8) rows of lp(nb,1:8); leaf: (nbmax,); icoord: (nbmax, 2);
+        dx, dy: (nlevs,) spacings of levels 1..nlevs."""
+        lpf = np.ascontiguousarray(np.asarray(lp, np.int32)[:nbmax].T)        # column-major
+        icf = np.ascontiguousarray(np.asarray(icoord, np.int32)[:nbmax].T)
+        lf = np.ascontiguousarray(np.asarray(leaf, np.int32)[:nbmax])
+        dxa = np.ascontiguousarray(dx, np.float64)
+        dya = np.ascontiguousarray(dy, np.float64)
+        self._check(self.L.w2d_set_topology(self.h, _pi32(lpf), max(nbmax, 1), _pi32(lf), _pi32(icf),
+                                            max(nbmax, 1), nbmax, _pd(dxa), _pd(dya)), "w2d_set_topology")
+
+    def set_bounds(self, innerbounds: np.ndarray):
+        """innerbounds: (n, 3) rows (source ID, neighbour ID, type) in list order."""
+        ib = np.asarray(innerbounds, np.int32).reshape(-1, 3)
+        n = ib.shape[0]
+        ibf = np.ascontiguousarray(ib.T)
+        self._check(self.L.w2d_set_bounds(self.h, _pi32(ibf), max(n, 1), n), "w2d_set_bounds")
+
+    def put_blocks(self, ids, u: np.ndarray):
+        ids = np.ascontiguousarray(ids, np.int32)
+        u = np.ascontiguousarray(u, np.float64)
+        assert u.shape == (ids.size, self.neq, W, W)
+        self._check(self.L.w2d_put_blocks(self.h, _pi32(ids), ids.size, _pd(u)), "w2d_put_blocks")
+
+    def get_blocks(self, ids) -> np.ndarray:
+        ids = np.ascontiguousarray(ids, np.int32)
+        u = np.zeros((ids.size, self.neq, W, W))
+        self._check(self.L.w2d_get_blocks(self.h, _pi32(ids), ids.size, _pd(u)), "w2d_get_blocks")
+        return u
+
+    def get_primit(self, ids) -> np.ndarray:
+        ids = np.ascontiguousarray(ids, np.int32)
+        u = np.zeros((ids.size, self.neq, W, W))
+        self._check(self.L.w2d_get_primit(self.h, _pi32(ids), ids.size, _pd(u)), "w2d_get_primit")
+        return u
+
+    # ---- the reference's routines -------------------------------------------
+    def timestep(self) -> float:
+        dt = C.c_double()
+        self._check(self.L.w2d_timestep(self.h, C.byref(dt)), "w2d_timestep")
+        return dt.value
+
+    def tstep(self, time: float, dt: float):
+        self._check(self.L.w2d_tstep(self.h, time, dt), "w2d_tstep")
+
+    def boundaryI(self, time: float = 0.0):
+        self._check(self.L.w2d_boundaryI(self.h, time), "w2d_boundaryI")
+
+    def boundaryII(self, time: float = 0.0):
+        self._check(self.L.w2d_boundaryII(self.h, time), "w2d_boundaryII")
+
+    def calcprim(self):
+        self._check(self.L.w2d_calcprim(self.h), "w2d_calcprim")
+
+    def coolingh(self, dt_s: float):
+        self._check(self.L.w2d_coolingh(self.h, dt_s), "w2d_coolingh")
+
+    def coolingdmc(self, dt_s: float):
+        self._check(self.L.w2d_coolingdmc(self.h, dt_s), "w2d_coolingdmc")
+
+    def criteria(self, nbmax: int) -> np.ndarray:
+        g = np.zeros(max(nbmax, 1))
+        self._check(self.L.w2d_criteria(self.h, _pd(g)), "w2d_criteria")
+        return g[:nbmax]
+
+    def refine(self, quads):
+        q = np.ascontiguousarray(quads, np.int32).reshape(-1, 5)
+        self._check(self.L.w2d_refine(self.h, _pi32(q), q.shape[0]), "w2d_refine")
+
+    def coarse(self, quads):
+        q = np.ascontiguousarray(quads, np.int32).reshape(-1, 5)
+        self._check(self.L.w2d_coarse(self.h, _pi32(q), q.shape[0]), "w2d_coarse")
+
+    def sync(self):
+        self._check(self.L.w2d_sync(self.h), "w2d_sync")
+
+    # ---- measurement --------------------------------------------------------
+    def profile(self, on: bool = True):
+        self._check(self.L.w2d_profile(self.h, 1 if on else 0), "w2d_profile")
+
+    def profile_read(self) -> dict:
+        names = C.create_string_buffer(4096)
+        la = np.zeros(64, np.int32)
+        ms = np.zeros(64)
+        nk = C.c_int()
+        self._check(self.L.w2d_profile_read(self.h, names, 4096, _pi32(la), _pd(ms), 64, C.byref(nk)),
+                    "w2d_profile_read")
+        out, pos = {}, 0
+        raw = names.raw
+        for k in range(nk.value):
+            end = raw.index(b"\0", pos)
+            out[raw[pos:end].decode()] = (int(la[k]), float(ms[k]))
+            pos = end + 1
+        return out
+
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        self._check(self.L.w2d_launch_count(self.h, C.byref(n)), "w2d_launch_count")
+        return n.value
+
+
+class Simulation:
+    """The main loop of the reference (timestep, tstep, admesh) on the device."""
+
+    def __init__(self, p: W2dParams, ic: W2dInit):
+        self.L = _lib.load()
+        self.p = p.copy()
+        self.ic = ic
+        h = C.c_void_p()
+        rc = self.L.w2d_sim_create(C.byref(self.p), C.byref(self.ic), C.byref(h))
+        if rc:
+            raise _lib.W2dException(rc, None, "w2d_sim_create")
+        self.h = h
+        self.ctx = Context(self.p, handle=self.L.w2d_sim_ctx(self.h), owner=self)
+
+    def close(self):
+        if self.h:
+            self.L.w2d_sim_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, nsteps: int):
+        rc = self.L.w2d_sim_run(self.h, nsteps)
+        if rc:
+            self.ctx._check(rc, "w2d_sim_run")
+
+    def set_amr(self, on: bool):
+        self.L.w2d_sim_set_amr(self.h, 1 if on else 0)
+
+    def status(self) -> dict:
+        t, dt = C.c_double(), C.c_double()
+        steps, zu = C.c_int64(), C.c_int64()
+        nbmax, nleaf = C.c_int32(), C.c_int32()
+        self.L.w2d_sim_status(self.h, C.byref(t), C.byref(dt), C.byref(steps), C.byref(nbmax),
+                              C.byref(nleaf), C.byref(zu))
+        return dict(time=t.value, dt=dt.value, steps=steps.value, nbmax=nbmax.value,
+                    nleaf=nleaf.value, zone_updates=zu.value)
+
+    def tree(self):
+        """lp (cap+1, 8), leaf (cap+1,), icoord (cap+1, 2) with row 0 unused,
+        as the oracle holds them, plus innerbounds (n, 3)."""
+        cap = self.p.nblocks
+        lp = np.zeros(8 * cap, np.int32)
+        lf = np.zeros(cap, np.int32)
+        ic = np.zeros(2 * cap, np.int32)
+        n = C.c_int32()
+        self.L.w2d_sim_tree(self.h, None, None, None, None, C.byref(n))
+        ib = np.zeros(3 * max(n.value, 1), np.int32)
+        self.L.w2d_sim_tree(self.h, _pi32(lp), _pi32(lf), _pi32(ic), _pi32(ib), C.byref(n))
+        lp2 = np.zeros((cap + 1, 8), np.int32)
+        lp2[1:] = lp.reshape(8, cap).T
+        ic2 = np.zeros((cap + 1, 2), np.int32)
+        ic2[1:] = ic.reshape(2, cap).T
+        lf2 = np.zeros(cap + 1, np.int32)
+        lf2[1:] = lf
+        nib = n.value
+        ibr = ib[: 3 * nib].reshape(3, nib).T.copy() if nib else np.zeros((0, 3), np.int32)
+        return lp2, lf2, ic2, ibr
+
+    def blocks(self, ids=None) -> tuple[np.ndarray, np.ndarray]:
+        """u of the given (default: all leaf) blocks, block-major."""
+        if ids is None:
+            _, lf, _, _ = self.tree()
+            ids = np.nonzero(lf)[0].astype(np.int32)
+        return np.asarray(ids, np.int32), self.ctx.get_blocks(ids)

@@ -1,0 +1,749 @@
+// w2d_api.cu -- the C-ABI of include/w2d.h: context, device pool, the
+// per-step plan built from innerbounds, and the entry points that replace
+// the reference's Fortran subroutines.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "w2d_ctx.h"
+
+using namespace w2d;
+
+namespace {
+
+int set_error(W2dCtx* c, int code, int block, int i, int j, const char* fmt, ...)
+{
+  if (c && c->err.code == 0) {
+    c->err.code = code;
+    c->err.block = block;
+    c->err.i = i;
+    c->err.j = j;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(c->err.message, sizeof(c->err.message), fmt, ap);
+    va_end(ap);
+  }
+  return code;
+}
+
+#define CK(call)                                                                    \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess)                                                          \
+      return set_error(c, W2D_ERR_CUDA, 0, 0, 0, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+int kid(W2dCtx* c, const char* name)
+{
+  for (size_t k = 0; k < c->kname.size(); ++k)
+    if (c->kname[k] == name) return (int)k;
+  c->kname.push_back(name);
+  c->klaunch.push_back(0);
+  c->kms.push_back(0.0);
+  return (int)c->kname.size() - 1;
+}
+
+cudaEvent_t get_event(W2dCtx* c)
+{
+  if (!c->evpool.empty()) {
+    cudaEvent_t e = c->evpool.back();
+    c->evpool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+void drain_profile(W2dCtx* c)
+{
+  for (auto& q : c->pending) {
+    float ms = 0.f;
+    cudaEventSynchronize(q.b);
+    cudaEventElapsedTime(&ms, q.a, q.b);
+    c->kms[q.id] += ms;
+    c->klaunch[q.id] += 1;
+    c->evpool.push_back(q.a);
+    c->evpool.push_back(q.b);
+  }
+  c->pending.clear();
+}
+
+// Launches fn on the context stream, counting it and timing it with CUDA
+// events on that stream when profiling is on.
+template <class F>
+int launch(W2dCtx* c, const char* name, F fn)
+{
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (c->prof) {
+    a = get_event(c);
+    b = get_event(c);
+    cudaEventRecord(a, c->st);
+  }
+  cudaError_t e = fn();
+  if (e != cudaSuccess)
+    return set_error(c, W2D_ERR_CUDA, 0, 0, 0, "launch %s: %s", name, cudaGetErrorString(e));
+  c->nlaunch++;
+  if (c->prof) {
+    cudaEventRecord(b, c->st);
+    c->pending.push_back({kid(c, name), a, b});
+    if (c->pending.size() > 4096) drain_profile(c);
+  }
+  return W2D_OK;
+}
+
+KArgs kargs(W2dCtx* c, const int2* fd)
+{
+  KArgs a;
+  memset(&a, 0, sizeof(a));
+  a.u = c->d_u;
+  a.up = c->d_up;
+  a.prim = c->d_prim;
+  a.leaves = c->d_leaves;
+  a.nleaf = (int)c->leaves.size();
+  a.lev = c->d_lev;
+  a.icoord = c->d_icoord;
+  a.fd = fd;
+  a.cfl = c->d_cfl;
+  a.dtcool = c->d_dtcool;
+  a.grad = c->d_grad;
+  a.err = c->d_err;
+  a.cooltab = c->d_cooltab;
+  a.nlevs = c->p.nlevs;
+  a.eta = c->p.eta;
+  a.psc = c->p.psc;
+  a.tempsc_d = c->p.tempsc;
+  for (int l = 0; l <= W2D_MAXLEV; ++l) {
+    a.dx[l] = c->dx[l];
+    a.dy[l] = c->dy[l];
+  }
+  return a;
+}
+
+PhysArgs pargs(W2dCtx* c)
+{
+  PhysArgs pa;
+  pa.cv = c->p.cv;
+  pa.gamma = c->p.gamma;
+  pa.tempsc = c->p.tempsc;
+  pa.cooling = c->p.cooling;
+  pa.hllc_compat = (c->p.compat & W2D_COMPAT_HLLC_STAR) ? 1 : 0;
+  pa.solver = c->p.solver;
+  pa.limiter = c->p.limiter;
+  return pa;
+}
+
+int ensure_ids(W2dCtx* c, int n)
+{
+  if (n <= c->ids_cap) return W2D_OK;
+  if (c->d_ids) cudaFree(c->d_ids);
+  c->d_ids = nullptr;
+  int cap = std::max(n, 1024);
+  CK(cudaMalloc(&c->d_ids, sizeof(int) * (size_t)cap));
+  c->ids_cap = cap;
+  return W2D_OK;
+}
+
+int ensure_stage(W2dCtx* c, size_t bytes)
+{
+  if (bytes > c->stage_bytes) {
+    CK(cudaStreamSynchronize(c->st));
+    if (c->d_stage) cudaFree(c->d_stage);
+    c->d_stage = nullptr;
+    CK(cudaMalloc(&c->d_stage, bytes));
+    c->stage_bytes = bytes;
+  }
+  if (bytes > c->h_stage_bytes) {
+    CK(cudaStreamSynchronize(c->st));
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    c->h_stage = nullptr;
+    CK(cudaMallocHost(&c->h_stage, bytes));
+    c->h_stage_bytes = bytes;
+  }
+  return W2D_OK;
+}
+
+// Checks the device error word (the queue must have drained).
+int check_device(W2dCtx* c)
+{
+  if (c->h_err[0] != 0) {
+    int code = c->h_err[0];
+    int rc = set_error(c, code, c->h_err[1], c->h_err[2], c->h_err[3],
+                       code == W2D_ERR_HLLC ? "Error in hllc: NaN contact speed" : "device error");
+    c->h_err[0] = 0;
+    cudaMemsetAsync(c->d_err, 0, 4 * sizeof(int), c->st);
+    return rc;
+  }
+  return W2D_OK;
+}
+
+int sync_and_check(W2dCtx* c)
+{
+  CK(cudaMemcpyAsync(c->h_err, c->d_err, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return check_device(c);
+}
+
+int valid_ids(W2dCtx* c, const int32_t* ids, int n)
+{
+  for (int k = 0; k < n; ++k)
+    if (ids[k] < 1 || ids[k] > c->cap)
+      return set_error(c, W2D_ERR_ARG, ids[k], 0, 0, "block ID %d outside 1..%d", ids[k], c->cap);
+  return W2D_OK;
+}
+
+// per-block primitives/CFL/criteria of the listed slots (device list)
+int stats_for(W2dCtx* c, const int* d_list, int n)
+{
+  if (!c->have_topology || n == 0) return W2D_OK;
+  KArgs a = kargs(c, c->d_fd1);
+  PhysArgs pa = pargs(c);
+  return launch(c, "calcprim", [&] { return c->L->calcprim(c->neq, a, pa, d_list, n, c->st); });
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char* w2d_version(void) { return "walicxe2d-b200 1.0 (sm_100a)"; }
+
+int w2d_create(const W2dParams* p, W2dCtx** out)
+{
+  if (!p || !out) return W2D_ERR_ARG;
+  *out = nullptr;
+  if (p->neq < 4 || p->neq > 6 || p->npas != p->neq - 4 || p->nx != W2D_NX || p->ny != W2D_NX ||
+      p->nlevs < 1 || p->nlevs > W2D_MAXLEV || p->nblocks < 1 || p->solver < 0 || p->solver > 2 ||
+      p->limiter < -1 || p->limiter > 6 || p->cooling < 0 || p->cooling > 2 ||
+      (p->cooling == W2D_COOLINGH && p->neq < 5) || (p->precision != 64 && p->precision != 32) ||
+      p->otherb != W2D_USERBC_NONE)
+    return W2D_ERR_ARG;
+  W2dCtx* c = new W2dCtx();
+  c->p = *p;
+  c->cap = p->nblocks;
+  c->neq = p->neq;
+  c->bs = (size_t)p->neq * W2D_CELLS;
+  c->L = (p->precision == 64) ? &launchers64() : &launchers32();
+  c->elem = c->L->elem;
+  cudaGetDevice(&c->device);
+  const size_t slots = (size_t)c->cap + 1;
+  const size_t pool = slots * c->bs * c->elem;
+#define CKC(call)                          \
+  do {                                     \
+    if ((call) != cudaSuccess) {           \
+      w2d_destroy(c);                      \
+      return W2D_ERR_NOMEM;                \
+    }                                      \
+  } while (0)
+  CKC(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  CKC(cudaMalloc(&c->d_u, pool));
+  CKC(cudaMalloc(&c->d_up, pool));
+  CKC(cudaMemsetAsync(c->d_u, 0, pool, c->st));
+  CKC(cudaMemsetAsync(c->d_up, 0, pool, c->st));
+  if (p->cooling == W2D_COOLINGDMC) {
+    CKC(cudaMalloc(&c->d_prim, pool));
+    CKC(cudaMemsetAsync(c->d_prim, 0, pool, c->st));
+  }
+  CKC(cudaMalloc(&c->d_lev, sizeof(int) * slots));
+  CKC(cudaMalloc(&c->d_icoord, sizeof(int) * 2 * slots));
+  CKC(cudaMalloc(&c->d_cfl, sizeof(double) * slots));
+  CKC(cudaMalloc(&c->d_dtcool, sizeof(double) * slots));
+  CKC(cudaMalloc(&c->d_grad, sizeof(double) * slots));
+  CKC(cudaMalloc(&c->d_err, sizeof(int) * 4));
+  CKC(cudaMalloc(&c->d_dt, sizeof(double) * 4));
+  CKC(cudaMalloc(&c->d_cooltab, sizeof(double) * 82));
+  CKC(cudaMemsetAsync(c->d_lev, 0, sizeof(int) * slots, c->st));
+  CKC(cudaMemsetAsync(c->d_icoord, 0, sizeof(int) * 2 * slots, c->st));
+  CKC(cudaMemsetAsync(c->d_err, 0, sizeof(int) * 4, c->st));
+  CKC(cudaMemsetAsync(c->d_cooltab, 0, sizeof(double) * 82, c->st));
+  {
+    std::vector<double> big(slots, 1e30);
+    CKC(cudaMemcpy(c->d_cfl, big.data(), sizeof(double) * slots, cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(c->d_dtcool, big.data(), sizeof(double) * slots, cudaMemcpyHostToDevice));
+    std::vector<double> neg(slots, -1.0);
+    CKC(cudaMemcpy(c->d_grad, neg.data(), sizeof(double) * slots, cudaMemcpyHostToDevice));
+  }
+  CKC(cudaMallocHost(&c->h_small, sizeof(double) * 8));
+  CKC(cudaMallocHost(&c->h_err, sizeof(int) * 4));
+  CKC(cudaMallocHost(&c->h_grad, sizeof(double) * slots));
+  memset(c->h_err, 0, sizeof(int) * 4);
+#undef CKC
+  c->lev.assign(slots, 0);
+  c->leaf.assign(slots, 0);
+  c->icoord.assign(2 * slots, 0);
+  c->leaf_index.assign(slots, -1);
+  if (cudaStreamSynchronize(c->st) != cudaSuccess) {
+    w2d_destroy(c);
+    return W2D_ERR_CUDA;
+  }
+  *out = c;
+  return W2D_OK;
+}
+
+int w2d_destroy(W2dCtx* c)
+{
+  if (!c) return W2D_ERR_ARG;
+  if (c->st) cudaStreamSynchronize(c->st);
+  for (auto& q : c->pending) { cudaEventDestroy(q.a); cudaEventDestroy(q.b); }
+  for (auto e : c->evpool) cudaEventDestroy(e);
+  void* dev[] = {c->d_u, c->d_up, c->d_prim, c->d_lev, c->d_icoord, c->d_cfl, c->d_dtcool, c->d_grad,
+                 c->d_err, c->d_dt, c->d_cooltab, c->d_leaves, c->d_fd1, c->d_fd2, c->d_stage, c->d_ids};
+  for (void* d : dev)
+    if (d) cudaFree(d);
+  void* host[] = {c->h_stage, c->h_small, c->h_grad, c->h_err, c->h_fd1, c->h_fd2, c->h_leaves};
+  for (void* h : host)
+    if (h) cudaFreeHost(h);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return W2D_OK;
+}
+
+int w2d_last_error(W2dCtx* c, W2dError* e)
+{
+  if (!c || !e) return W2D_ERR_ARG;
+  *e = c->err;
+  memset(&c->err, 0, sizeof(c->err));
+  return W2D_OK;
+}
+
+int w2d_set_cooltab(W2dCtx* c, const double* log_t, const double* neg_log_l, int n)
+{
+  if (!c || !log_t || !neg_log_l || n != 41) return W2D_ERR_ARG;
+  double tab[82];
+  for (int i = 0; i < 41; ++i) {  // src/initmain.f90:89-93, host libm as the reference
+    tab[i] = pow(10.e0, (log_t[i]));
+    tab[41 + i] = pow(10.e0, (-neg_log_l[i]));
+  }
+  CK(cudaMemcpyAsync(c->d_cooltab, tab, sizeof(tab), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->have_cooltab = true;
+  return W2D_OK;
+}
+
+int w2d_set_topology(W2dCtx* c, const int32_t* lp, int ld_lp, const int32_t* leaf, const int32_t* icoord,
+                     int ld_icoord, int nbmax, const double* dx, const double* dy)
+{
+  if (!c || !lp || !leaf || !icoord || !dx || !dy) return W2D_ERR_ARG;
+  if (nbmax < 0 || nbmax > c->cap || ld_lp < nbmax || ld_icoord < nbmax)
+    return set_error(c, W2D_ERR_ARG, 0, 0, 0, "nbmax %d outside the pool (capacity %d)", nbmax, c->cap);
+  c->nbmax = nbmax;
+  c->leaves.clear();
+  std::fill(c->leaf_index.begin(), c->leaf_index.end(), -1);
+  for (int nb = 1; nb <= nbmax; ++nb) {
+    c->lev[nb] = lp[nb - 1];                       // lp(nb,1)
+    c->leaf[nb] = leaf[nb - 1] != 0;
+    c->icoord[2 * nb] = icoord[nb - 1];
+    c->icoord[2 * nb + 1] = icoord[(size_t)ld_icoord + nb - 1];
+    if (c->leaf[nb]) {
+      if (c->lev[nb] < 1 || c->lev[nb] > c->p.nlevs)
+        return set_error(c, W2D_ERR_TOPOLOGY, nb, 0, 0, "leaf %d has level %d", nb, c->lev[nb]);
+      c->leaf_index[nb] = (int)c->leaves.size();
+      c->leaves.push_back(nb);
+    }
+  }
+  for (int l = 1; l <= c->p.nlevs; ++l) {
+    c->dx[l] = dx[l - 1];
+    c->dy[l] = dy[l - 1];
+  }
+  CK(cudaMemcpyAsync(c->d_lev, c->lev.data(), sizeof(int) * (size_t)(nbmax + 1), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_icoord, c->icoord.data(), sizeof(int) * 2 * (size_t)(nbmax + 1),
+                     cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));  // host vectors are pageable
+  c->have_topology = true;
+  c->have_bounds = false;
+  return W2D_OK;
+}
+
+// Builds the two fill plans from the list (src/locatebounds.f90:29-540
+// output) in list order: for every leaf face the last entry that writes it
+// wins, as in the sequential walks of boundaryI/II.
+int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
+{
+  if (!c || (!ib && n > 0) || n < 0 || ld < n) return W2D_ERR_ARG;
+  if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
+  const int nl = (int)c->leaves.size();
+  if (nl > c->h_plan_cap) {
+    CK(cudaStreamSynchronize(c->st));
+    if (c->h_fd1) cudaFreeHost(c->h_fd1);
+    if (c->h_fd2) cudaFreeHost(c->h_fd2);
+    if (c->h_leaves) cudaFreeHost(c->h_leaves);
+    if (c->d_fd1) cudaFree(c->d_fd1);
+    if (c->d_fd2) cudaFree(c->d_fd2);
+    if (c->d_leaves) cudaFree(c->d_leaves);
+    c->h_fd1 = c->h_fd2 = nullptr;
+    c->h_leaves = nullptr;
+    c->d_fd1 = c->d_fd2 = nullptr;
+    c->d_leaves = nullptr;
+    int cap = std::max(nl + nl / 2, 256);
+    CK(cudaMallocHost(&c->h_fd1, sizeof(int2) * 4 * (size_t)cap));
+    CK(cudaMallocHost(&c->h_fd2, sizeof(int2) * 4 * (size_t)cap));
+    CK(cudaMallocHost(&c->h_leaves, sizeof(int) * (size_t)cap));
+    CK(cudaMalloc(&c->d_fd1, sizeof(int2) * 4 * (size_t)cap));
+    CK(cudaMalloc(&c->d_fd2, sizeof(int2) * 4 * (size_t)cap));
+    CK(cudaMalloc(&c->d_leaves, sizeof(int) * (size_t)cap));
+    c->h_plan_cap = cap;
+  } else {
+    CK(cudaStreamSynchronize(c->st));  // previous plan upload may still read the pinned buffers
+  }
+  for (int k = 0; k < 4 * nl; ++k) c->h_fd1[k] = c->h_fd2[k] = make_int2(0, FK_KEEP);
+  for (int k = 0; k < nl; ++k) c->h_leaves[k] = c->leaves[k];
+  auto put = [&](int2* fd, int blk, int face, int nbr, int kind, int off) {
+    if (blk < 1 || blk > c->nbmax) return;
+    const int li = c->leaf_index[blk];
+    if (li < 0) return;  // non-leaf targets are never read before being rewritten
+    fd[li * 4 + face] = make_int2(nbr, kind | (off << 8));
+  };
+  auto both = [&](int blk, int face, int nbr, int kind, int off) {
+    put(c->h_fd1, blk, face, nbr, kind, off);
+    put(c->h_fd2, blk, face, nbr, kind, off);
+  };
+  const int H = W2D_NX / 2;
+  const int bc[4] = {c->p.bc_left, c->p.bc_right, c->p.bc_bottom, c->p.bc_top};
+  const bool f6b = (c->p.compat & W2D_COMPAT_OUTFYB) != 0;
+  for (int e = 1; e <= n; ++e) {
+    const int nbs = ib[e - 1], n1 = ib[(size_t)ld + e - 1], t = ib[2 * (size_t)ld + e - 1];
+    if (nbs < 1 || nbs > c->nbmax || (t > 0 && (n1 < 1 || n1 > c->nbmax)))
+      return set_error(c, W2D_ERR_TOPOLOGY, nbs, e, t, "innerbounds entry %d (%d,%d,%d) out of range", e, nbs, n1, t);
+    switch (t) {
+      case -1: case -2: case -4: {
+        const int f = (t == -1) ? 0 : (t == -2) ? 1 : 3;
+        both(nbs, f, nbs, bc[f] == W2D_BC_REFLECTIVE ? FK_REFLECT : FK_MIRROR, 0);
+        break;
+      }
+      case -3:
+        if (bc[2] == W2D_BC_REFLECTIVE) {
+          both(nbs, 2, nbs, FK_REFLECT, 0);
+        } else {
+          put(c->h_fd2, nbs, 2, nbs, FK_MIRROR, 0);
+          // src/boundaryI.f90:87 fills block "nb" (the list index e)
+          const int tb = f6b ? e : nbs;
+          put(c->h_fd1, tb, 2, tb, FK_MIRROR, 0);
+        }
+        break;
+      case 1:  both(nbs, 0, n1, FK_SAME, 0);  both(n1, 1, nbs, FK_SAME, 0); break;
+      case 4:  both(nbs, 1, n1, FK_SAME, 0);  both(n1, 0, nbs, FK_SAME, 0); break;
+      case 7:  both(nbs, 2, n1, FK_SAME, 0);  both(n1, 3, nbs, FK_SAME, 0); break;
+      case 10: both(nbs, 3, n1, FK_SAME, 0);  both(n1, 2, nbs, FK_SAME, 0); break;
+      case 2:
+        both(nbs, 0, n1, FK_RESTRICT, 0);
+        both(n1, 1, nbs, FK_INJECT, 0);
+        both(n1 + 2, 1, nbs, FK_INJECT, H);
+        break;
+      case 5:
+        both(nbs, 1, n1, FK_RESTRICT, 0);
+        both(n1, 0, nbs, FK_INJECT, 0);
+        both(n1 + 2, 0, nbs, FK_INJECT, H);
+        break;
+      case 8:
+        both(nbs, 2, n1, FK_RESTRICT, 0);
+        both(n1, 3, nbs, FK_INJECT, 0);
+        both(n1 + 1, 3, nbs, FK_INJECT, H);
+        break;
+      case 11:
+        both(nbs, 3, n1, FK_RESTRICT, 0);
+        both(n1, 2, nbs, FK_INJECT, 0);
+        both(n1 + 1, 2, nbs, FK_INJECT, H);
+        break;
+      default:
+        return set_error(c, W2D_ERR_TOPOLOGY, nbs, e, t, "innerbounds type %d not in the serial list", t);
+    }
+  }
+  if (nl > 0) {
+    CK(cudaMemcpyAsync(c->d_fd1, c->h_fd1, sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_fd2, c->h_fd2, sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_leaves, c->h_leaves, sizeof(int) * (size_t)nl, cudaMemcpyHostToDevice, c->st));
+  }
+  c->have_bounds = true;
+  return W2D_OK;
+}
+
+int w2d_put_blocks(W2dCtx* c, const int32_t* ids, int n, const double* u)
+{
+  if (!c || (n > 0 && (!ids || !u)) || n < 0) return W2D_ERR_ARG;
+  if (n == 0) return W2D_OK;
+  int rc = valid_ids(c, ids, n);
+  if (rc) return rc;
+  if ((rc = ensure_stage(c, (size_t)n * c->bs * c->elem)) || (rc = ensure_ids(c, n))) return rc;
+  CK(cudaStreamSynchronize(c->st));
+  if (c->elem == sizeof(double)) {
+    memcpy(c->h_stage, u, (size_t)n * c->bs * sizeof(double));
+  } else {
+    float* h = (float*)c->h_stage;
+    for (size_t k = 0; k < (size_t)n * c->bs; ++k) h[k] = (float)u[k];
+  }
+  CK(cudaMemcpyAsync(c->d_stage, c->h_stage, (size_t)n * c->bs * c->elem, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_ids, ids, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st));
+  if ((rc = launch(c, "scatter", [&] { return c->L->scatter(c->d_u, c->d_stage, c->d_ids, n, c->bs, c->st); })))
+    return rc;
+  if ((rc = stats_for(c, c->d_ids, n))) return rc;
+  CK(cudaStreamSynchronize(c->st));
+  return W2D_OK;
+}
+
+static int get_pool(W2dCtx* c, void* pool, const int32_t* ids, int n, double* u)
+{
+  int rc = valid_ids(c, ids, n);
+  if (rc) return rc;
+  if ((rc = ensure_stage(c, (size_t)n * c->bs * c->elem)) || (rc = ensure_ids(c, n))) return rc;
+  CK(cudaMemcpyAsync(c->d_ids, ids, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st));
+  if (pool) {
+    if ((rc = launch(c, "gather", [&] { return c->L->gather(pool, c->d_stage, c->d_ids, n, c->bs, c->st); })))
+      return rc;
+  } else {
+    PhysArgs pa = pargs(c);
+    if ((rc = launch(c, "to_prim", [&] { return c->L->to_prim(c->neq, pa, c->d_u, c->d_stage, c->d_ids, n, c->st); })))
+      return rc;
+  }
+  CK(cudaMemcpyAsync(c->h_stage, c->d_stage, (size_t)n * c->bs * c->elem, cudaMemcpyDeviceToHost, c->st));
+  if ((rc = sync_and_check(c))) return rc;
+  if (c->elem == sizeof(double)) {
+    memcpy(u, c->h_stage, (size_t)n * c->bs * sizeof(double));
+  } else {
+    const float* h = (const float*)c->h_stage;
+    for (size_t k = 0; k < (size_t)n * c->bs; ++k) u[k] = (double)h[k];
+  }
+  return W2D_OK;
+}
+
+int w2d_get_blocks(W2dCtx* c, const int32_t* ids, int n, double* u)
+{
+  if (!c || n < 0 || (n > 0 && (!ids || !u))) return W2D_ERR_ARG;
+  if (n == 0) return W2D_OK;
+  return get_pool(c, c->d_u, ids, n, u);
+}
+
+int w2d_get_primit(W2dCtx* c, const int32_t* ids, int n, double* prim)
+{
+  if (!c || n < 0 || (n > 0 && (!ids || !prim))) return W2D_ERR_ARG;
+  if (n == 0) return W2D_OK;
+  return get_pool(c, c->d_prim, ids, n, prim);  // nullptr pool: derived from u
+}
+
+// Fortran layout u(nbmin:nbmaxtot, neq, -1:18, -1:18): element (nb,k,i,j)
+// at ((j+1)*20 + (i+1))*neq*ld + k*ld + (nb-nbmin).
+int w2d_put_u_fortran(W2dCtx* c, const double* u, int ld, int nbmin, const int32_t* ids, int n)
+{
+  if (!c || !u || n < 0 || (n > 0 && !ids) || ld < 1) return W2D_ERR_ARG;
+  std::vector<double> blk((size_t)n * c->bs);
+  for (int q = 0; q < n; ++q) {
+    const size_t r = (size_t)(ids[q] - nbmin);
+    if (ids[q] < nbmin || r >= (size_t)ld) return W2D_ERR_ARG;
+    for (int k = 0; k < c->neq; ++k)
+      for (int cc = 0; cc < W2D_CELLS; ++cc)
+        blk[(size_t)q * c->bs + (size_t)k * W2D_CELLS + cc] = u[((size_t)cc * c->neq + k) * ld + r];
+  }
+  return w2d_put_blocks(c, ids, n, blk.data());
+}
+
+int w2d_get_u_fortran(W2dCtx* c, double* u, int ld, int nbmin, const int32_t* ids, int n)
+{
+  if (!c || !u || n < 0 || (n > 0 && !ids) || ld < 1) return W2D_ERR_ARG;
+  std::vector<double> blk((size_t)n * c->bs);
+  int rc = w2d_get_blocks(c, ids, n, blk.data());
+  if (rc) return rc;
+  for (int q = 0; q < n; ++q) {
+    const size_t r = (size_t)(ids[q] - nbmin);
+    if (ids[q] < nbmin || r >= (size_t)ld) return W2D_ERR_ARG;
+    for (int k = 0; k < c->neq; ++k)
+      for (int cc = 0; cc < W2D_CELLS; ++cc)
+        u[((size_t)cc * c->neq + k) * ld + r] = blk[(size_t)q * c->bs + (size_t)k * W2D_CELLS + cc];
+  }
+  return W2D_OK;
+}
+
+int w2d_timestep(W2dCtx* c, double* dt)
+{
+  if (!c || !dt) return W2D_ERR_ARG;
+  if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
+  const int nl = (int)c->leaves.size();
+  if (!c->have_bounds) {  // the leaf list lives with the plan
+    int rc = w2d_set_bounds(c, nullptr, 0, 0);
+    if (rc) return rc;
+    c->have_bounds = false;
+  }
+  int rc = launch(c, "timestep", [&] {
+    return launch_dt(c->d_leaves, nl, c->d_cfl, c->d_dtcool, c->p.cooling == W2D_COOLINGDMC, c->p.cfl,
+                     c->p.psc, c->p.tsc, c->d_dt, c->st);
+  });
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(c->h_small, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  if ((rc = sync_and_check(c))) return rc;
+  *dt = c->h_small[0];
+  return W2D_OK;
+}
+
+int w2d_tstep(W2dCtx* c, double time, double dt)
+{
+  (void)time;
+  if (!c) return W2D_ERR_ARG;
+  if (!c->have_topology || !c->have_bounds)
+    return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology and w2d_set_bounds first");
+  if (c->p.cooling == W2D_COOLINGDMC && !c->have_cooltab)
+    return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_cooltab first (COOLINGDMC)");
+  PhysArgs pa = pargs(c);
+  KArgs a2 = kargs(c, c->d_fd2);
+  KArgs a1 = kargs(c, c->d_fd1);
+  int rc;
+  if ((rc = launch(c, "half_step", [&] { return c->L->half(c->neq, a2, pa, dt, c->st); }))) return rc;
+  if ((rc = launch(c, "full_step", [&] { return c->L->full(c->neq, a2, pa, dt, c->st); }))) return rc;
+  const int stats = c->p.cooling == W2D_ADIABATIC;
+  if ((rc = launch(c, "fill_I", [&] { return c->L->fill1(c->neq, a1, pa, stats, c->st); }))) return rc;
+  if (c->p.cooling != W2D_ADIABATIC) {
+    const double dts = dt * c->p.tsc;
+    if ((rc = launch(c, "cooling", [&] { return c->L->cool(c->neq, a1, pa, dts, c->st); }))) return rc;
+  }
+  return W2D_OK;
+}
+
+int w2d_criteria(W2dCtx* c, double* grad)
+{
+  if (!c || !grad) return W2D_ERR_ARG;
+  if (c->nbmax > 0)
+    CK(cudaMemcpyAsync(c->h_grad, c->d_grad + 1, sizeof(double) * (size_t)c->nbmax, cudaMemcpyDeviceToHost, c->st));
+  int rc = sync_and_check(c);
+  if (rc) return rc;
+  for (int nb = 1; nb <= c->nbmax; ++nb) grad[nb - 1] = c->leaf[nb] ? c->h_grad[nb - 1] : -1.0;
+  return W2D_OK;
+}
+
+static int amr_ops(W2dCtx* c, const int32_t* quads, int n, bool refine)
+{
+  if (!c || n < 0 || (n > 0 && !quads)) return W2D_ERR_ARG;
+  if (n == 0) return W2D_OK;
+  if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
+  int rc = valid_ids(c, quads, 5 * n);
+  if (rc) return rc;
+  if ((rc = ensure_ids(c, 5 * n + 4 * n))) return rc;
+  // the new leaves: levels and icoord as refine/coarse set them
+  std::vector<int> newl;
+  newl.reserve(4 * n);
+  const int NX = W2D_NX;
+  for (int q = 0; q < n; ++q) {
+    const int* o = quads + 5 * q;
+    if (refine) {
+      const int l2 = c->lev[o[0]] + 1;
+      const int nx0 = c->icoord[2 * o[0]] * 2, ny0 = c->icoord[2 * o[0] + 1] * 2;  // refine.f90:42-43
+      for (int s = 0; s < 4; ++s) {
+        const int son = o[1 + s];
+        c->lev[son] = l2;
+        c->icoord[2 * son] = nx0 + ((s & 1) ? NX : 0);
+        c->icoord[2 * son + 1] = ny0 + ((s & 2) ? NX : 0);
+        newl.push_back(son);
+      }
+    } else {
+      newl.push_back(o[0]);
+    }
+  }
+  std::vector<int> buf(quads, quads + 5 * n);
+  buf.insert(buf.end(), newl.begin(), newl.end());
+  CK(cudaMemcpyAsync(c->d_ids, buf.data(), sizeof(int) * buf.size(), cudaMemcpyHostToDevice, c->st));
+  {
+    const int lo = *std::min_element(newl.begin(), newl.end());
+    const int hi = *std::max_element(newl.begin(), newl.end());
+    const size_t cnt = (size_t)(hi - lo + 1);
+    CK(cudaMemcpyAsync(c->d_lev + lo, &c->lev[lo], sizeof(int) * cnt, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_icoord + 2 * lo, &c->icoord[2 * lo], 2 * sizeof(int) * cnt,
+                       cudaMemcpyHostToDevice, c->st));
+  }
+  if (refine)
+    rc = launch(c, "refine", [&] { return c->L->refine(c->neq, c->d_u, c->d_ids, n, c->st); });
+  else
+    rc = launch(c, "coarse", [&] { return c->L->coarse(c->neq, c->d_u, c->d_ids, n, c->st); });
+  if (rc) return rc;
+  if ((rc = stats_for(c, c->d_ids + 5 * n, (int)newl.size()))) return rc;
+  CK(cudaStreamSynchronize(c->st));  // pageable sources above
+  return W2D_OK;
+}
+
+int w2d_refine(W2dCtx* c, const int32_t* quads, int n) { return amr_ops(c, quads, n, true); }
+int w2d_coarse(W2dCtx* c, const int32_t* quads, int n) { return amr_ops(c, quads, n, false); }
+
+int w2d_boundaryI(W2dCtx* c, double time)
+{
+  (void)time;
+  if (!c) return W2D_ERR_ARG;
+  if (!c->have_bounds) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_bounds first");
+  KArgs a = kargs(c, c->d_fd1);
+  return launch(c, "fill_I_only", [&] { return c->L->fill_only(c->neq, a, c->d_u, 1, c->st); });
+}
+
+int w2d_boundaryII(W2dCtx* c, double time)
+{
+  (void)time;
+  if (!c) return W2D_ERR_ARG;
+  if (!c->have_bounds) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_bounds first");
+  KArgs a = kargs(c, c->d_fd2);
+  return launch(c, "fill_II_only", [&] { return c->L->fill_only(c->neq, a, c->d_up, 2, c->st); });
+}
+
+int w2d_calcprim(W2dCtx* c)
+{
+  if (!c) return W2D_ERR_ARG;
+  if (!c->have_bounds) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_bounds first");
+  return stats_for(c, c->d_leaves, (int)c->leaves.size());
+}
+
+static int cooling_only(W2dCtx* c, double dt_s, int mode)
+{
+  if (!c) return W2D_ERR_ARG;
+  if (c->p.cooling != mode) return set_error(c, W2D_ERR_ARG, 0, 0, 0, "context built for another cooling mode");
+  if (!c->have_bounds) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_bounds first");
+  KArgs a = kargs(c, c->d_fd1);
+  PhysArgs pa = pargs(c);
+  return launch(c, "cooling", [&] { return c->L->cool(c->neq, a, pa, dt_s, c->st); });
+}
+
+int w2d_coolingh(W2dCtx* c, double dt_s) { return cooling_only(c, dt_s, W2D_COOLINGH); }
+int w2d_coolingdmc(W2dCtx* c, double dt_s) { return cooling_only(c, dt_s, W2D_COOLINGDMC); }
+
+int w2d_profile(W2dCtx* c, int on)
+{
+  if (!c) return W2D_ERR_ARG;
+  CK(cudaStreamSynchronize(c->st));
+  drain_profile(c);
+  c->prof = on != 0;
+  std::fill(c->klaunch.begin(), c->klaunch.end(), 0);
+  std::fill(c->kms.begin(), c->kms.end(), 0.0);
+  return W2D_OK;
+}
+
+int w2d_profile_read(W2dCtx* c, char* names, int cap, int32_t* launches, double* total_ms, int maxk, int* nk)
+{
+  if (!c || !nk) return W2D_ERR_ARG;
+  CK(cudaStreamSynchronize(c->st));
+  drain_profile(c);
+  int k = 0, pos = 0;
+  for (size_t q = 0; q < c->kname.size() && k < maxk; ++q) {
+    if (c->klaunch[q] == 0) continue;
+    const std::string& s = c->kname[q];
+    if (names) {
+      if (pos + (int)s.size() + 1 > cap) break;
+      memcpy(names + pos, s.c_str(), s.size() + 1);
+    }
+    pos += (int)s.size() + 1;
+    if (launches) launches[k] = c->klaunch[q];
+    if (total_ms) total_ms[k] = c->kms[q];
+    ++k;
+  }
+  *nk = k;
+  return W2D_OK;
+}
+
+int w2d_launch_count(W2dCtx* c, int64_t* n)
+{
+  if (!c || !n) return W2D_ERR_ARG;
+  *n = c->nlaunch;
+  return W2D_OK;
+}
+
+int w2d_sync(W2dCtx* c)
+{
+  if (!c) return W2D_ERR_ARG;
+  return sync_and_check(c);
+}
+
+}  // extern "C"

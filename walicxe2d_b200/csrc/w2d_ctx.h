@@ -1,0 +1,76 @@
+// w2d_ctx.h -- the context behind the C-ABI (device pool, plans, streams).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/w2d.h"
+#include "w2d_launch.h"
+
+struct W2dCtx {
+  W2dParams p{};
+  int cap = 0;            // largest block ID
+  int neq = 4;
+  size_t bs = 0;          // elements per block
+  size_t elem = 8;        // sizeof(R)
+  const w2d::Launchers* L = nullptr;
+  int device = 0;
+  cudaStream_t st = nullptr;
+
+  // device pool and per-slot arrays (slot = block ID, slot 0 unused)
+  void* d_u = nullptr;
+  void* d_up = nullptr;
+  void* d_prim = nullptr;
+  int* d_lev = nullptr;
+  int* d_icoord = nullptr;
+  double* d_cfl = nullptr;
+  double* d_dtcool = nullptr;
+  double* d_grad = nullptr;
+  int* d_err = nullptr;
+  double* d_dt = nullptr;
+  double* d_cooltab = nullptr;
+  // per-step plan
+  int* d_leaves = nullptr;
+  int2* d_fd1 = nullptr;   // boundaryI (layer 0 of u)
+  int2* d_fd2 = nullptr;   // boundaryII (two layers of up)
+  int plan_cap = 0;
+  // scratch for host transfers
+  void* d_stage = nullptr;
+  size_t stage_bytes = 0;
+  int* d_ids = nullptr;
+  int ids_cap = 0;
+  void* h_stage = nullptr;   // pinned
+  size_t h_stage_bytes = 0;
+  double* h_small = nullptr; // pinned scalars (dt, ...)
+  double* h_grad = nullptr;  // pinned, one per leaf
+  int* h_err = nullptr;      // pinned error word
+  int2* h_fd1 = nullptr;     // pinned plan staging
+  int2* h_fd2 = nullptr;
+  int* h_leaves = nullptr;
+  int h_plan_cap = 0;
+
+  // host copy of the topology
+  std::vector<int> lev, leaf, icoord;  // per slot
+  std::vector<int> leaves;             // leaf slots, ascending
+  std::vector<int> leaf_index;         // slot -> position in leaves, -1
+  int nbmax = 0;
+  double dx[W2D_MAXLEV + 1] = {0}, dy[W2D_MAXLEV + 1] = {0};
+  bool have_topology = false;
+  bool have_bounds = false;
+  bool have_cooltab = false;
+
+  // measurement
+  bool prof = false;
+  std::vector<std::string> kname;
+  std::vector<int> klaunch;
+  std::vector<double> kms;
+  struct Pending { int id; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> evpool;
+  int64_t nlaunch = 0;
+
+  W2dError err{};
+};

@@ -1,0 +1,436 @@
+// w2d_host.cpp -- whole-run driver: the reference's host side restated in
+// C++ (serial build) on top of the C-ABI.
+//
+//   main loop        src/main.f90:69-107 (timestep, tstep, admesh; no output)
+//   basegrid         src/basegrid.f90:26-165, generalized to nbx x nby roots
+//   admesh           src/admesh.f90:4-111
+//   markref/criteria src/markref.f90:4-85, src/criteria.f90:36-50 (flags)
+//   critneighup      src/critneighup.f90:5-61
+//   critneighdown    src/critneighdown.f90:5-55
+//   updatelpup       src/updatelpup.f90:4-190
+//   updatelpdown     src/updatelpdown.f90:4-59
+//   locatebounds     src/locatebounds.f90:29-540
+//
+// The integer arrays use the reference's Fortran layout (column-major,
+// 1-based block IDs) so they can be handed to w2d_set_topology as they are.
+// The per-cell work of refine/coarse/criteria/calcprim runs on the device
+// through the C-ABI; only integer bookkeeping happens here.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/w2d.h"
+
+struct W2dSim {
+  W2dParams p{};
+  W2dInit ic{};
+  W2dCtx* ctx = nullptr;
+  int cap = 0, nbmax = 0, nbleafs = 0;
+  std::vector<int32_t> lp, leaf, icoord;  // column-major, ld = cap
+  std::vector<double> dx, dy;             // nlevs entries
+  std::vector<int32_t> ib;                // innerbounds, column-major, ld = nib
+  int nib = 0;
+  double time = 0.0, dt = 0.0;
+  int64_t steps = 0, zone_updates = 0;
+  bool amr = true;
+  bool dirty = true;
+  std::vector<unsigned char> irefup, irefdown, bounds;
+  std::vector<double> grad;
+  std::vector<int32_t> rops, cops;
+  std::vector<int32_t> ib1, ib2, ib3;
+
+  int32_t& LP(int nb, int k) { return lp[(size_t)(k - 1) * cap + (nb - 1)]; }
+  int32_t& LEAF(int nb) { return leaf[(size_t)nb - 1]; }
+  int32_t& IC(int nb, int k) { return icoord[(size_t)(k - 1) * cap + (nb - 1)]; }
+};
+
+namespace {
+
+// Initial conditions of one block at its own resolution (the Sedov set-up,
+// or src/user_mod.f90:39-62 with impose_jet, src/jet.f90:41-78, at t = 0).
+void initial_block(W2dSim* s, int nb, double* ub)
+{
+  const W2dParams& p = s->p;
+  const W2dInit& ic = s->ic;
+  const int W = p.nx + 4, neq = p.neq;
+  const int lev = s->LP(nb, 1);
+  const double dxl = s->dx[lev - 1], dyl = s->dy[lev - 1];
+  auto at = [&](int k, int i, int j) -> double& { return ub[((size_t)k * W + (j + 1)) * W + (i + 1)]; };
+  const double pi = std::acos(-1.);
+  const double vjet = p.jet_v0 + p.jet_dv * std::sin(2. * pi * 0.0 / p.jet_tau);
+  for (int i = -1; i <= p.nx + 2; ++i)
+    for (int j = -1; j <= p.ny + 2; ++j) {
+      for (int k = 0; k < neq; ++k) at(k, i, j) = 0.;
+      const double x = ((double)(i + s->IC(nb, 1)) - 0.5) * dxl;
+      const double y = ((double)(j + s->IC(nb, 2)) - 0.5) * dyl;
+      if (ic.kind == W2D_IC_JET) {
+        at(0, i, j) = ic.rho0;
+        at(3, i, j) = p.cv * 1.0001 * ic.rho0 * ic.p0 / p.tempsc;
+        if (neq > 4) at(4, i, j) = ic.rho0 * 0.9999;
+        if (neq > 5) at(5, i, j) = -ic.rho0;
+        if ((std::fabs(x - p.jet_posx) <= p.jet_lj) && (std::fabs(y - p.jet_posy) <= p.jet_rj)) {
+          at(0, i, j) = p.jet_den;
+          at(1, i, j) = p.jet_den * vjet;
+          at(2, i, j) = 0.;
+          at(3, i, j) = 0.5 * p.jet_den * (vjet * vjet) + p.cv * p.jet_den * 1.0001 * p.jet_temp;
+          if (neq > 4) at(4, i, j) = p.jet_den * 0.9999;
+          if (neq > 5) at(5, i, j) = p.jet_den;
+        }
+        continue;
+      }
+      const double r2 = (x - ic.xc) * (x - ic.xc) + (y - ic.yc) * (y - ic.yc);
+      at(0, i, j) = ic.rho0;
+      at(3, i, j) = p.cv * ic.p0;
+      if (neq > 4) at(4, i, j) = ic.xh0 * ic.rho0;
+      if (r2 < ic.rb * ic.rb) at(3, i, j) = ic.e_dep;
+    }
+}
+
+// src/updatelpup.f90:4-190 (serial build; nbleafs kept as the MPI build does)
+void updatelpup(W2dSim* s, int nb, int s1, int s2, int s3, int s4)
+{
+  auto& L = *s;
+  const int nlev2 = L.LP(nb, 1) + 1;
+  int nsr;
+  s->nbleafs += 3;
+  L.LP(s1, 1) = nlev2; L.LP(s1, 2) = nb; L.LP(s1, 4) = 1; L.LP(s1, 6) = s2; L.LP(s1, 8) = s3;
+  if (L.LP(nb, 5) == -1 || L.LEAF(L.LP(nb, 5))) L.LP(s1, 5) = L.LP(nb, 5);
+  else { nsr = L.LP(L.LP(nb, 5), 3) + 1; L.LP(s1, 5) = nsr; L.LP(nsr, 6) = s1; }
+  if (L.LP(nb, 7) == -1 || L.LEAF(L.LP(nb, 7))) L.LP(s1, 7) = L.LP(nb, 7);
+  else { nsr = L.LP(L.LP(nb, 7), 3) + 2; L.LP(s1, 7) = nsr; L.LP(nsr, 8) = s1; }
+
+  L.LP(s2, 1) = nlev2; L.LP(s2, 2) = nb; L.LP(s2, 4) = 2; L.LP(s2, 5) = s1; L.LP(s2, 8) = s4;
+  if (L.LP(nb, 6) == -1 || L.LEAF(L.LP(nb, 6))) L.LP(s2, 6) = L.LP(nb, 6);
+  else { nsr = L.LP(L.LP(nb, 6), 3); L.LP(s2, 6) = nsr; L.LP(nsr, 5) = s2; }
+  if (L.LP(nb, 7) == -1 || L.LEAF(L.LP(nb, 7))) L.LP(s2, 7) = L.LP(nb, 7);
+  else { nsr = L.LP(L.LP(nb, 7), 3) + 3; L.LP(s2, 7) = nsr; L.LP(nsr, 8) = s2; }
+
+  L.LP(s3, 1) = nlev2; L.LP(s3, 2) = nb; L.LP(s3, 4) = 3; L.LP(s3, 6) = s4; L.LP(s3, 7) = s1;
+  if (L.LP(nb, 5) == -1 || L.LEAF(L.LP(nb, 5))) L.LP(s3, 5) = L.LP(nb, 5);
+  else { nsr = L.LP(L.LP(nb, 5), 3) + 3; L.LP(s3, 5) = nsr; L.LP(nsr, 6) = s3; }
+  if (L.LP(nb, 8) == -1 || L.LEAF(L.LP(nb, 8))) L.LP(s3, 8) = L.LP(nb, 8);
+  else { nsr = L.LP(L.LP(nb, 8), 3); L.LP(s3, 8) = nsr; L.LP(nsr, 7) = s3; }
+
+  L.LP(s4, 1) = nlev2; L.LP(s4, 2) = nb; L.LP(s4, 4) = 4; L.LP(s4, 5) = s3; L.LP(s4, 7) = s2;
+  if (L.LP(nb, 6) == -1 || L.LEAF(L.LP(nb, 6))) L.LP(s4, 6) = L.LP(nb, 6);
+  else { nsr = L.LP(L.LP(nb, 6), 3) + 2; L.LP(s4, 6) = nsr; L.LP(nsr, 5) = s4; }
+  if (L.LP(nb, 8) == -1 || L.LEAF(L.LP(nb, 8))) L.LP(s4, 8) = L.LP(nb, 8);
+  else { nsr = L.LP(L.LP(nb, 8), 3) + 1; L.LP(s4, 8) = nsr; L.LP(nsr, 7) = s4; }
+
+  L.LEAF(nb) = 0;
+  L.LEAF(s1) = L.LEAF(s2) = L.LEAF(s3) = L.LEAF(s4) = 1;
+  s->irefup[nb] = 0;
+  s->irefdown[nb] = 0;
+  s->irefdown[s1] = s->irefdown[s2] = s->irefdown[s3] = s->irefdown[s4] = 0;
+  // icoord of the sons, src/refine.f90:42-43,247-256
+  const int nx0 = L.IC(nb, 1) * 2, ny0 = L.IC(nb, 2) * 2;
+  L.IC(s1, 1) = nx0;            L.IC(s1, 2) = ny0;
+  L.IC(s2, 1) = nx0 + s->p.nx;  L.IC(s2, 2) = ny0;
+  L.IC(s3, 1) = nx0;            L.IC(s3, 2) = ny0 + s->p.ny;
+  L.IC(s4, 1) = nx0 + s->p.nx;  L.IC(s4, 2) = ny0 + s->p.ny;
+}
+
+// src/updatelpdown.f90:4-59
+void updatelpdown(W2dSim* s, int dad, int s1, int s2, int s3, int s4)
+{
+  auto& L = *s;
+  L.LEAF(dad) = 1;
+  L.LEAF(s1) = L.LEAF(s2) = L.LEAF(s3) = L.LEAF(s4) = 0;
+  s->nbleafs -= 3;
+  int nb1 = L.LP(dad, 5);
+  if (nb1 != -1 && !L.LEAF(nb1)) { nb1 = L.LP(L.LP(nb1, 3), 6); L.LP(nb1, 6) = dad; L.LP(L.LP(nb1, 8), 6) = dad; }
+  nb1 = L.LP(dad, 6);
+  if (nb1 != -1 && !L.LEAF(nb1)) { nb1 = L.LP(nb1, 3); L.LP(nb1, 5) = dad; L.LP(L.LP(nb1, 8), 5) = dad; }
+  nb1 = L.LP(dad, 7);
+  if (nb1 != -1 && !L.LEAF(nb1)) { nb1 = L.LP(L.LP(nb1, 3), 8); L.LP(nb1, 8) = dad; L.LP(L.LP(nb1, 6), 8) = dad; }
+  nb1 = L.LP(dad, 8);
+  if (nb1 != -1 && !L.LEAF(nb1)) { nb1 = L.LP(nb1, 3); L.LP(nb1, 7) = dad; L.LP(L.LP(nb1, 6), 7) = dad; }
+}
+
+int push_topology(W2dSim* s)
+{
+  return w2d_set_topology(s->ctx, s->lp.data(), s->cap, s->leaf.data(), s->icoord.data(), s->cap,
+                          s->nbmax, s->dx.data(), s->dy.data());
+}
+
+// src/locatebounds.f90:29-540 (serial build)
+void locatebounds(W2dSim* s)
+{
+  auto& L = *s;
+  std::fill(s->bounds.begin(), s->bounds.end(), 0);
+  auto BND = [&](int nb, int k) -> unsigned char& { return s->bounds[(size_t)nb * 4 + k - 1]; };
+  s->ib1.clear(); s->ib2.clear(); s->ib3.clear();
+  auto push = [&](int a, int b, int t) { s->ib1.push_back(a); s->ib2.push_back(b); s->ib3.push_back(t); };
+  for (int nb = 1; nb <= s->nbmax; ++nb) {
+    if (!L.LEAF(nb)) continue;
+    if (!BND(nb, 1)) {
+      if (L.LP(nb, 5) == -1) { BND(nb, 1) = 1; push(nb, 0, -1); }
+      else if (L.LP(L.LP(nb, 5), 1) >= L.LP(nb, 1)) {
+        int n1 = L.LP(nb, 5);
+        if (L.LEAF(n1)) { push(nb, n1, 1); BND(nb, 1) = 1; BND(n1, 2) = 1; }
+        else { BND(nb, 1) = 1; n1 = L.LP(n1, 3) + 1; push(nb, n1, 2); BND(n1, 2) = 1; BND(n1 + 2, 2) = 1; }
+      }
+    }
+    if (!BND(nb, 2)) {
+      if (L.LP(nb, 6) == -1) { BND(nb, 2) = 1; push(nb, 0, -2); }
+      else if (L.LP(L.LP(nb, 6), 1) >= L.LP(nb, 1)) {
+        int n1 = L.LP(nb, 6);
+        if (L.LEAF(n1)) { push(nb, n1, 4); BND(nb, 2) = 1; BND(n1, 1) = 1; }
+        else { BND(nb, 2) = 1; n1 = L.LP(n1, 3); push(nb, n1, 5); BND(n1, 1) = 1; BND(n1 + 2, 1) = 1; }
+      }
+    }
+    if (!BND(nb, 3)) {
+      if (L.LP(nb, 7) == -1) { BND(nb, 3) = 1; push(nb, 0, -3); }
+      else if (L.LP(L.LP(nb, 7), 1) >= L.LP(nb, 1)) {
+        int n1 = L.LP(nb, 7);
+        if (L.LEAF(n1)) { push(nb, n1, 7); BND(nb, 3) = 1; BND(n1, 4) = 1; }
+        else { BND(nb, 3) = 1; n1 = L.LP(n1, 3) + 2; push(nb, n1, 8); BND(n1, 4) = 1; BND(n1 + 1, 4) = 1; }
+      }
+    }
+    if (!BND(nb, 4)) {
+      if (L.LP(nb, 8) == -1) { BND(nb, 4) = 1; push(nb, 0, -4); }
+      else if (L.LP(L.LP(nb, 8), 1) >= L.LP(nb, 1)) {
+        int n1 = L.LP(nb, 8);
+        if (L.LEAF(n1)) { push(nb, n1, 10); BND(nb, 4) = 1; BND(n1, 3) = 1; }
+        else { BND(nb, 4) = 1; n1 = L.LP(n1, 3); push(nb, n1, 11); BND(n1, 3) = 1; BND(n1 + 1, 3) = 1; }
+      }
+    }
+  }
+  s->nib = (int)s->ib1.size();
+  s->ib.resize((size_t)3 * s->nib);
+  std::copy(s->ib1.begin(), s->ib1.end(), s->ib.begin());
+  std::copy(s->ib2.begin(), s->ib2.end(), s->ib.begin() + s->nib);
+  std::copy(s->ib3.begin(), s->ib3.end(), s->ib.begin() + 2 * (size_t)s->nib);
+}
+
+int refresh_plan(W2dSim* s)
+{
+  int rc = push_topology(s);
+  if (rc) return rc;
+  locatebounds(s);
+  rc = w2d_set_bounds(s->ctx, s->ib.data(), s->nib, s->nib);
+  if (rc) return rc;
+  s->dirty = false;
+  return W2D_OK;
+}
+
+// src/admesh.f90:4-111 (np = 1).  The u motion of every refine and coarse
+// of the pass is batched into one device call each: within a pass no refine
+// or coarse reads a block that another one writes.
+int admesh(W2dSim* s)
+{
+  auto& L = *s;
+  const int nlevs = s->p.nlevs;
+  int rc;
+  if (s->dirty && (rc = refresh_plan(s))) return rc;
+  // markref + criteria flags (criteria.f90:36-50 on the device maximum)
+  rc = w2d_criteria(s->ctx, s->grad.data());
+  if (rc) return rc;
+  std::fill(s->irefup.begin(), s->irefup.end(), 0);
+  std::fill(s->irefdown.begin(), s->irefdown.end(), 0);
+  for (int nb = 1; nb <= s->nbmax; ++nb) {
+    if (!(L.LEAF(nb) && L.LP(nb, 1) >= 1)) continue;
+    const double g = s->grad[nb - 1];
+    if (g >= s->p.tol) {
+      if (L.LP(nb, 1) < nlevs) { s->irefup[nb] = 1; s->irefdown[nb] = 0; }
+    } else if (g <= s->p.tol2) {
+      s->irefdown[nb] = 1;
+    }
+  }
+  // critneighup
+  for (int nl = nlevs - 1; nl >= 1; --nl)
+    for (int nb = 1; nb <= s->nbmax; ++nb)
+      if (s->irefup[nb] && L.LP(nb, 1) == nl)
+        for (int k = 5; k <= 8; ++k) {
+          const int n1 = L.LP(nb, k);
+          if (n1 != -1 && L.LP(n1, 1) < L.LP(nb, 1)) s->irefup[n1] = 1;
+        }
+  int nbmaxp = s->nbmax;
+  const int nbmaxp1 = s->nbmax;
+  s->rops.clear();
+  s->cops.clear();
+  for (int nl = 1; nl <= nlevs - 1; ++nl)
+    for (int nb = 1; nb <= nbmaxp1; ++nb) {
+      if (!(L.LP(nb, 1) == nl && s->irefup[nb])) continue;
+      int s1, s2, s3, s4;
+      if (L.LP(nb, 3) == 0) {
+        s1 = nbmaxp + 1; s2 = s1 + 1; s3 = s1 + 2; s4 = s1 + 3;
+        if (s4 > s->cap) return W2D_ERR_CAPACITY;   // admesh.f90:44-47
+        L.LP(nb, 3) = s1;
+        nbmaxp += 4;
+      } else {
+        s1 = L.LP(nb, 3); s2 = L.LP(s1, 6); s3 = L.LP(s1, 8); s4 = L.LP(s3, 6);
+      }
+      s->nbmax = nbmaxp;
+      const int q[5] = {nb, s1, s2, s3, s4};
+      s->rops.insert(s->rops.end(), q, q + 5);
+      updatelpup(s, nb, s1, s2, s3, s4);
+    }
+  // critneighdown
+  for (int nb = 1; nb <= s->nbmax; ++nb)
+    if (s->irefdown[nb])
+      for (int k = 5; k <= 8; ++k) {
+        const int n1 = L.LP(nb, k);
+        if (n1 != -1 && !L.LEAF(n1)) s->irefdown[nb] = 0;
+      }
+  for (int nl = nlevs; nl >= 2; --nl)
+    for (int nb = 1; nb <= nbmaxp1; ++nb) {
+      if (!(s->irefdown[nb] && L.LP(nb, 4) == 1 && L.LP(nb, 1) == nl)) continue;
+      const int dad = L.LP(nb, 2), s1 = nb, s2 = L.LP(nb, 6), s3 = L.LP(nb, 8);
+      const int s4 = L.LP(L.LP(nb, 6), 8);
+      if (s->irefdown[s2] && s->irefdown[s3] && s->irefdown[s4]) {
+        const int q[5] = {dad, s1, s2, s3, s4};
+        s->cops.insert(s->cops.end(), q, q + 5);
+        updatelpdown(s, dad, s1, s2, s3, s4);
+      }
+    }
+  const int nr = (int)s->rops.size() / 5, nc = (int)s->cops.size() / 5;
+  if (nr && (rc = w2d_refine(s->ctx, s->rops.data(), nr))) return rc;
+  if (nc && (rc = w2d_coarse(s->ctx, s->cops.data(), nc))) return rc;
+  if (nr || nc) s->dirty = true;
+  return W2D_OK;
+}
+
+// basegrid, generalized (see w2d.h); the initial conditions of every leaf
+// are uploaded in one w2d_put_blocks.
+int basegrid(W2dSim* s)
+{
+  auto& L = *s;
+  const int nbx = s->p.nbroot_x, nby = s->p.nbroot_y;
+  if (nbx * nby > s->cap) return W2D_ERR_CAPACITY;
+  for (int iy = 0; iy < nby; ++iy)
+    for (int ix = 0; ix < nbx; ++ix) {
+      const int nb = 1 + ix + iy * nbx;
+      L.LP(nb, 1) = 1; L.LP(nb, 2) = 0; L.LP(nb, 3) = 0; L.LP(nb, 4) = 1;
+      L.LP(nb, 5) = ix > 0 ? nb - 1 : -1;
+      L.LP(nb, 6) = ix < nbx - 1 ? nb + 1 : -1;
+      L.LP(nb, 7) = iy > 0 ? nb - nbx : -1;
+      L.LP(nb, 8) = iy < nby - 1 ? nb + nbx : -1;
+      L.IC(nb, 1) = ix * s->p.nx;
+      L.IC(nb, 2) = iy * s->p.ny;
+      L.LEAF(nb) = 1;
+    }
+  s->nbmax = nbx * nby;
+  s->nbleafs = nbx * nby;
+  const int lmax = s->ic.init_levels < s->p.nlevs ? s->ic.init_levels : s->p.nlevs;
+  for (int lev = 1; lev < lmax; ++lev) {
+    const int nb0 = s->nbmax;
+    for (int nb = 1; nb <= nb0; ++nb) {
+      if (!(L.LEAF(nb) && L.LP(nb, 1) == lev)) continue;
+      const int s1 = s->nbmax + 1;
+      if (s1 + 3 > s->cap) return W2D_ERR_CAPACITY;
+      L.LP(nb, 3) = s1;
+      updatelpup(s, nb, s1, s1 + 1, s1 + 2, s1 + 3);
+      s->nbmax += 4;
+    }
+  }
+  int rc = push_topology(s);
+  if (rc) return rc;
+  std::vector<int32_t> ids;
+  for (int nb = 1; nb <= s->nbmax; ++nb)
+    if (L.LEAF(nb)) ids.push_back(nb);
+  const size_t bs = (size_t)s->p.neq * (s->p.nx + 4) * (s->p.nx + 4);
+  std::vector<double> blocks(bs * ids.size());
+  for (size_t q = 0; q < ids.size(); ++q) initial_block(s, ids[q], blocks.data() + q * bs);
+  rc = w2d_put_blocks(s->ctx, ids.data(), (int)ids.size(), blocks.data());
+  if (rc) return rc;
+  s->dirty = true;
+  return W2D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int w2d_sim_create(const W2dParams* p, const W2dInit* ic, W2dSim** out)
+{
+  if (!p || !ic || !out) return W2D_ERR_ARG;
+  *out = nullptr;
+  W2dSim* s = new W2dSim();
+  s->p = *p;
+  s->ic = *ic;
+  s->cap = p->nblocks;
+  int rc = w2d_create(p, &s->ctx);
+  if (rc) { delete s; return rc; }
+  s->lp.assign((size_t)8 * s->cap, 0);
+  s->leaf.assign((size_t)s->cap, 0);
+  s->icoord.assign((size_t)2 * s->cap, 0);
+  s->irefup.assign((size_t)s->cap + 1, 0);
+  s->irefdown.assign((size_t)s->cap + 1, 0);
+  s->bounds.assign(((size_t)s->cap + 1) * 4, 0);
+  s->grad.assign((size_t)s->cap, -1.0);
+  s->dx.resize(p->nlevs);
+  s->dy.resize(p->nlevs);
+  for (int l = 1; l <= p->nlevs; ++l) {  // src/initmain.f90:58-62, generalized
+    s->dx[l - 1] = p->xmax / p->nx / (std::pow(2., (double)(l - 1))) / (double)(p->nbroot_x);
+    s->dy[l - 1] = p->ymax / p->ny / (std::pow(2., (double)(l - 1))) / (double)(p->nbroot_y);
+  }
+  s->amr = p->nlevs > 1;
+  if ((rc = basegrid(s))) { w2d_sim_destroy(s); return rc; }
+  for (int k = 0; k < ic->startup_admesh && p->nlevs > 1; ++k)   // src/main.f90:60-63
+    if ((rc = admesh(s))) { w2d_sim_destroy(s); return rc; }
+  *out = s;
+  return W2D_OK;
+}
+
+int w2d_sim_destroy(W2dSim* s)
+{
+  if (!s) return W2D_ERR_ARG;
+  if (s->ctx) w2d_destroy(s->ctx);
+  delete s;
+  return W2D_OK;
+}
+
+int w2d_sim_run(W2dSim* s, int nsteps)
+{
+  if (!s || nsteps < 0) return W2D_ERR_ARG;
+  int rc;
+  for (int n = 0; n < nsteps; ++n) {
+    if (s->dirty && (rc = refresh_plan(s))) return rc;
+    double dt = 0.0;
+    if ((rc = w2d_timestep(s->ctx, &dt))) return rc;       // src/main.f90:87
+    s->dt = dt;
+    s->time = s->time + dt;                                 // src/main.f90:88
+    if ((rc = w2d_tstep(s->ctx, s->time, dt))) return rc;   // src/main.f90:95
+    s->zone_updates += (int64_t)s->nbleafs * s->p.nx * s->p.ny;
+    if (s->amr && (rc = admesh(s))) return rc;              // src/main.f90:98
+    s->steps++;
+  }
+  return W2D_OK;
+}
+
+int w2d_sim_status(W2dSim* s, double* time, double* dt, int64_t* steps, int32_t* nbmax, int32_t* nleaf,
+                   int64_t* zone_updates)
+{
+  if (!s) return W2D_ERR_ARG;
+  if (time) *time = s->time;
+  if (dt) *dt = s->dt;
+  if (steps) *steps = s->steps;
+  if (nbmax) *nbmax = s->nbmax;
+  if (nleaf) *nleaf = s->nbleafs;
+  if (zone_updates) *zone_updates = s->zone_updates;
+  return W2D_OK;
+}
+
+W2dCtx* w2d_sim_ctx(W2dSim* s) { return s ? s->ctx : nullptr; }
+
+int w2d_sim_tree(W2dSim* s, int32_t* lp, int32_t* leaf, int32_t* icoord, int32_t* innerbounds, int32_t* ninternal)
+{
+  if (!s) return W2D_ERR_ARG;
+  if (lp) memcpy(lp, s->lp.data(), sizeof(int32_t) * s->lp.size());
+  if (leaf) memcpy(leaf, s->leaf.data(), sizeof(int32_t) * s->leaf.size());
+  if (icoord) memcpy(icoord, s->icoord.data(), sizeof(int32_t) * s->icoord.size());
+  if (s->dirty) locatebounds(s);
+  if (innerbounds) memcpy(innerbounds, s->ib.data(), sizeof(int32_t) * s->ib.size());
+  if (ninternal) *ninternal = s->nib;
+  return W2D_OK;
+}
+
+int w2d_sim_set_amr(W2dSim* s, int on)
+{
+  if (!s) return W2D_ERR_ARG;
+  s->amr = on != 0 && s->p.nlevs > 1;
+  return W2D_OK;
+}
+
+}  // extern "C"

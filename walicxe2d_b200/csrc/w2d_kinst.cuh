@@ -1,0 +1,106 @@
+// w2d_kinst.cuh -- launcher table for one arithmetic type R.  Included once
+// by w2d_k64.cu (R = double, built with --fmad=false) and once by
+// w2d_k32.cu (R = float).
+#pragma once
+
+#include "w2d_cool.cuh"
+#include "w2d_launch.h"
+
+namespace w2d {
+namespace W2D_INST_NS {
+
+using R = W2D_INST_REAL;
+
+#define W2D_NEQ_SWITCH(neq, CALL)             \
+  switch (neq) {                              \
+    case 4: { constexpr int NEQ = 4; CALL; } break; \
+    case 5: { constexpr int NEQ = 5; CALL; } break; \
+    case 6: { constexpr int NEQ = 6; CALL; } break; \
+    default: return cudaErrorInvalidValue;    \
+  }
+
+static cudaError_t half(int neq, const KArgs& a, const PhysArgs& pa, double dt, cudaStream_t st)
+{
+  if (a.nleaf == 0) return cudaSuccess;
+  W2D_NEQ_SWITCH(neq, (k_half<R, NEQ><<<a.nleaf, W2D_THREADS, 0, st>>>(a, pa, dt)));
+  return cudaGetLastError();
+}
+
+static cudaError_t full(int neq, const KArgs& a, const PhysArgs& pa, double dt, cudaStream_t st)
+{
+  if (a.nleaf == 0) return cudaSuccess;
+  W2D_NEQ_SWITCH(neq, (k_full<R, NEQ><<<a.nleaf, W2D_THREADS, 0, st>>>(a, pa, dt)));
+  return cudaGetLastError();
+}
+
+static cudaError_t fill1(int neq, const KArgs& a, const PhysArgs& pa, int stats, cudaStream_t st)
+{
+  if (a.nleaf == 0) return cudaSuccess;
+  W2D_NEQ_SWITCH(neq, (k_fill1<R, NEQ><<<a.nleaf, W2D_THREADS, 0, st>>>(a, pa, stats)));
+  return cudaGetLastError();
+}
+
+static cudaError_t fill_only(int neq, const KArgs& a, void* pool, int layers, cudaStream_t st)
+{
+  if (a.nleaf == 0) return cudaSuccess;
+  W2D_NEQ_SWITCH(neq, (k_fill_only<R, NEQ><<<a.nleaf, 128, 0, st>>>(a, (R*)pool, layers)));
+  return cudaGetLastError();
+}
+
+static cudaError_t calcprim(int neq, const KArgs& a, const PhysArgs& pa, const int* list, int n,
+                            cudaStream_t st)
+{
+  if (n == 0) return cudaSuccess;
+  W2D_NEQ_SWITCH(neq, (k_calcprim<R, NEQ><<<n, W2D_THREADS, 0, st>>>(a, pa, list, n)));
+  return cudaGetLastError();
+}
+
+static cudaError_t refine(int neq, void* u, const int* quads, int n, cudaStream_t st)
+{
+  if (n == 0) return cudaSuccess;
+  W2D_NEQ_SWITCH(neq, (k_refine<R, NEQ><<<4 * n, 256, 0, st>>>((R*)u, quads)));
+  return cudaGetLastError();
+}
+
+static cudaError_t coarse(int neq, void* u, const int* quads, int n, cudaStream_t st)
+{
+  if (n == 0) return cudaSuccess;
+  W2D_NEQ_SWITCH(neq, (k_coarse<R, NEQ><<<n, 256, 0, st>>>((R*)u, quads)));
+  return cudaGetLastError();
+}
+
+static cudaError_t cool(int neq, const KArgs& a, const PhysArgs& pa, double dt_s, cudaStream_t st)
+{
+  if (a.nleaf == 0) return cudaSuccess;
+  if (neq < 5 && pa.cooling == COOL_H) return cudaErrorInvalidValue;
+  W2D_NEQ_SWITCH(neq, (k_cool<R, NEQ><<<a.nleaf, W2D_THREADS, 0, st>>>(a, pa, dt_s)));
+  return cudaGetLastError();
+}
+
+static cudaError_t scatter(void* pool, const void* stage, const int* ids, int n, size_t bs, cudaStream_t st)
+{
+  if (n == 0) return cudaSuccess;
+  k_scatter<R><<<n, 256, 0, st>>>((R*)pool, (const R*)stage, ids, bs);
+  return cudaGetLastError();
+}
+
+static cudaError_t gather(const void* pool, void* stage, const int* ids, int n, size_t bs, cudaStream_t st)
+{
+  if (n == 0) return cudaSuccess;
+  k_gather<R><<<n, 256, 0, st>>>((const R*)pool, (R*)stage, ids, bs);
+  return cudaGetLastError();
+}
+
+static cudaError_t to_prim(int neq, const PhysArgs& pa, const void* u, void* out, const int* ids, int n,
+                           cudaStream_t st)
+{
+  if (n == 0) return cudaSuccess;
+  W2D_NEQ_SWITCH(neq, (k_to_prim<R, NEQ><<<n, 256, 0, st>>>(pa, (const R*)u, (R*)out, ids)));
+  return cudaGetLastError();
+}
+
+static const Launchers table = {half, full, fill1, fill_only, calcprim, refine,
+                                coarse, cool, scatter, gather, to_prim, sizeof(R)};
+
+}  // namespace W2D_INST_NS
+}  // namespace w2d

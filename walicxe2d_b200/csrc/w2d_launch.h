@@ -1,0 +1,32 @@
+// w2d_launch.h -- host-side launchers of the device kernels (one set per
+// arithmetic type; the FP64 set lives in w2d_k64.cu, built without FMA
+// contraction, the FP32 set in w2d_k32.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include "w2d_kernels.cuh"
+
+namespace w2d {
+
+struct Launchers {
+  cudaError_t (*half)(int neq, const KArgs&, const PhysArgs&, double dt, cudaStream_t);
+  cudaError_t (*full)(int neq, const KArgs&, const PhysArgs&, double dt, cudaStream_t);
+  cudaError_t (*fill1)(int neq, const KArgs&, const PhysArgs&, int stats, cudaStream_t);
+  cudaError_t (*fill_only)(int neq, const KArgs&, void* pool, int layers, cudaStream_t);
+  cudaError_t (*calcprim)(int neq, const KArgs&, const PhysArgs&, const int* list, int n, cudaStream_t);
+  cudaError_t (*refine)(int neq, void* u, const int* quads, int n, cudaStream_t);
+  cudaError_t (*coarse)(int neq, void* u, const int* quads, int n, cudaStream_t);
+  cudaError_t (*cool)(int neq, const KArgs&, const PhysArgs&, double dt_s, cudaStream_t);
+  cudaError_t (*scatter)(void* pool, const void* stage, const int* ids, int n, size_t bs, cudaStream_t);
+  cudaError_t (*gather)(const void* pool, void* stage, const int* ids, int n, size_t bs, cudaStream_t);
+  cudaError_t (*to_prim)(int neq, const PhysArgs&, const void* u, void* out, const int* ids, int n, cudaStream_t);
+  size_t elem;  // sizeof(R)
+};
+
+const Launchers& launchers64();
+const Launchers& launchers32();
+
+cudaError_t launch_dt(const int* leaves, int n, const double* cfl, const double* dtcool, int use_cool,
+                      double courant, double psc, double tsc, double* dt_out, cudaStream_t st);
+
+}  // namespace w2d

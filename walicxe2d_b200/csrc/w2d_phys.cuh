@@ -1,0 +1,232 @@
+// w2d_phys.cuh -- per-cell and per-interface physics of the block update.
+//
+// Each function restates one routine of the reference (file:line in the
+// comment) with the same operation order, so that the FP64 instantiation,
+// compiled with --fmad=false, rounds exactly as the reference does (IEEE
+// division and square root, no contraction).  The FP32 instantiation uses
+// the same code with float arithmetic.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define W2D_NX 16               // interior cells per block side
+#define W2D_W 20                // with two ghost layers
+#define W2D_CELLS (W2D_W * W2D_W)
+
+namespace w2d {
+
+// Fortran MAX/MIN of two reals: compare and select (no NaN operands).
+template <typename R> __device__ __forceinline__ R fmaxr(R a, R b) { return (a > b) ? a : b; }
+template <typename R> __device__ __forceinline__ R fminr(R a, R b) { return (a < b) ? a : b; }
+__device__ __forceinline__ double sqrtr(double x) { return sqrt(x); }
+__device__ __forceinline__ float sqrtr(float x) { return sqrtf(x); }
+__device__ __forceinline__ double absr(double x) { return fabs(x); }
+__device__ __forceinline__ float absr(float x) { return fabsf(x); }
+__device__ __forceinline__ double signr(double a) { return copysign(1.0, a); }
+__device__ __forceinline__ float signr(float a) { return copysignf(1.0f, a); }
+
+enum { SOLVER_HLLC = 0, SOLVER_HLL = 1, SOLVER_HLL_HLLC = 2 };
+enum { COOL_NONE = 0, COOL_H = 1, COOL_DMC = 2 };
+
+// Constants the point functions need, in the arithmetic type R.
+template <typename R>
+struct Phys {
+  R cv, gamma, tempsc;
+  int cooling;
+  int hllc_compat;     // primr(4)/(primr(4)*srmur), src/hllcfluxes.f90:157
+  int solver;
+  int limiter;
+};
+
+// src/uprim.f90:5-63 -- prim from u; T is returned for the cooling modes.
+template <int NEQ, typename R>
+__device__ __forceinline__ void uprim(const Phys<R>& ph, R* prim, const R* uu, R& T)
+{
+  const R tiny = R(1e-15);
+  R r = uu[0] > tiny ? uu[0] : tiny;
+  prim[0] = r;
+  prim[1] = uu[1] / r;
+  prim[2] = uu[2] / r;
+#pragma unroll
+  for (int k = 4; k < NEQ; ++k) prim[k] = uu[k];
+  prim[3] = (uu[3] - R(0.5) * r * (prim[1] * prim[1] + prim[2] * prim[2])) / ph.cv;
+  prim[3] = fmaxr(prim[3], tiny);
+  if (ph.cooling == COOL_NONE) {
+    T = prim[3] / r;
+  } else if (ph.cooling == COOL_H) {
+    R dentot = (R(2.) * r - prim[NEQ > 4 ? 4 : 0]);
+    dentot = fmaxr(dentot, tiny);
+    T = fmaxr(R(1.), (prim[3] / dentot) * ph.tempsc);
+    prim[3] = dentot * T / ph.tempsc;
+  } else {
+    r = fmaxr(r, tiny);
+    T = fmaxr(R(1.), (prim[3] / (r)) * ph.tempsc);
+    prim[3] = r * T / ph.tempsc;
+  }
+}
+
+// src/primu.f90:4-19
+template <int NEQ, typename R>
+__device__ __forceinline__ void primu(const Phys<R>& ph, const R* p, R* uu)
+{
+  uu[0] = p[0];
+  uu[1] = p[0] * p[1];
+  uu[2] = p[0] * p[2];
+  uu[3] = R(0.5) * p[0] * (p[1] * p[1] + p[2] * p[2]) + ph.cv * p[3];
+#pragma unroll
+  for (int k = 4; k < NEQ; ++k) uu[k] = p[k];
+}
+
+// src/primf.f90:5-23 (x-flux of one state; y uses the swapped state)
+template <int NEQ, typename R>
+__device__ __forceinline__ void primf(const Phys<R>& ph, const R* p, R* ff)
+{
+  R etot = R(0.5) * p[0] * (p[1] * p[1] + p[2] * p[2]) + ph.cv * p[3];
+  ff[0] = p[0] * p[1];
+  ff[1] = p[0] * p[1] * p[1] + p[3];
+  ff[2] = p[0] * p[1] * p[2];
+  ff[3] = p[1] * (etot + p[3]);
+#pragma unroll
+  for (int k = 4; k < NEQ; ++k) ff[k] = p[k] * p[1];
+}
+
+// src/sound.f90:4-13
+template <typename R>
+__device__ __forceinline__ R sound(const Phys<R>& ph, R p, R d) { return sqrtr(ph.gamma * p / d); }
+
+// Star-region state of HLLC, src/hllcfluxes.f90:127-160, for the side
+// "s" (left: s = sl, smus = sl - u_l; right: s = sr, smus = sr - u_r).
+template <int NEQ, typename R>
+__device__ __forceinline__ void hllc_star(const Phys<R>& ph, const R* q, R s, R smus, R sst,
+                                          R den, R* ff)
+{
+  R uu[NEQ], uuk[NEQ];
+  R rhost = q[0] * (smus) / (s - sst);
+  R ek = R(0.5) * q[0] * (q[1] * q[1] + q[2] * q[2]) + ph.cv * q[3];
+  uuk[0] = rhost;
+  uuk[1] = rhost * sst;
+  uuk[2] = rhost * q[2];
+  uuk[3] = rhost * (ek / q[0] + (sst - q[1]) * (sst + q[3] / (den * smus)));
+#pragma unroll
+  for (int k = 4; k < NEQ; ++k) uuk[k] = rhost * q[k] / q[0];
+  primf<NEQ>(ph, q, ff);
+  primu<NEQ>(ph, q, uu);
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k) ff[k] = ff[k] + s * (uuk[k] - uu[k]);
+}
+
+// HLL flux between ql and qr, src/hllfluxes.f90:118-124
+template <int NEQ, typename R>
+__device__ __forceinline__ void hll_flux(const Phys<R>& ph, const R* ql, const R* qr, R sl, R sr,
+                                         R* ff)
+{
+  R fl[NEQ], fr[NEQ], ul[NEQ], ur[NEQ];
+  primf<NEQ>(ph, ql, fl);
+  primf<NEQ>(ph, qr, fr);
+  primu<NEQ>(ph, ql, ul);
+  primu<NEQ>(ph, qr, ur);
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k)
+    ff[k] = (sr * fl[k] - sl * fr[k] + sl * sr * (ur[k] - ul[k])) / (sr - sl);
+}
+
+// Riemann flux of the selected solver:
+//   HLLC      src/hllcfluxes.f90:98-173
+//   HLL       src/hllfluxes.f90:98-132
+//   HLL-HLLC  src/hll_hllcfluxes.f90:98-210
+// csl/csr are the sound speeds of the two states (callers that reuse a
+// cell's sound speed pass it in; the value is the one sound() returns).
+// Returns false on the NaN contact speed that stops the reference.
+template <int NEQ, typename R>
+__device__ __forceinline__ bool riemann(const Phys<R>& ph, const R* pl, const R* pr, R csl, R csr,
+                                        R* ff)
+{
+  R beta1 = R(1.), beta2 = R(0.);
+  if (ph.solver == SOLVER_HLL_HLLC) {              // hll_hllcfluxes.f90:110-129
+    R dq1 = pr[1] - pl[1];
+    R dq2 = pr[2] - pl[2];
+    R mag = sqrtr(dq1 * dq1 + dq2 * dq2);
+    if (mag <= R(1e-6)) {
+      beta1 = R(1.0);
+      beta2 = R(0.0);
+    } else {
+      R alpha1 = absr(dq1) / mag;
+      beta1 = sqrtr(alpha1);
+      beta2 = R(1.) - beta1;
+    }
+  }
+  R sr = fmaxr(pl[1] + csl, pr[1] + csr);
+  R sl = fminr(pl[1] - csl, pr[1] - csr);
+  if (sl > R(0)) { primf<NEQ>(ph, pl, ff); return true; }
+  if (sr < R(0)) { primf<NEQ>(ph, pr, ff); return true; }
+  if (ph.solver == SOLVER_HLL) { hll_flux<NEQ>(ph, pl, pr, sl, sr, ff); return true; }
+  R slmul = sl - pl[1];
+  R srmur = sr - pr[1];
+  R rholul = pl[0] * pl[1];
+  R rhorur = pr[0] * pr[1];
+  R sst = (srmur * rhorur - slmul * rholul - pr[3] + pl[3]) / (srmur * pr[0] - slmul * pl[0]);
+  bool left = sst >= R(0.);
+  if (!left && !(sst <= R(0.))) return false;
+  if (left) hllc_star<NEQ>(ph, pl, sl, slmul, sst, pl[0], ff);
+  else      hllc_star<NEQ>(ph, pr, sr, srmur, sst, ph.hllc_compat ? pr[3] : pr[0], ff);
+  if (ph.solver == SOLVER_HLL_HLLC) {
+    R fh[NEQ];
+    hll_flux<NEQ>(ph, pl, pr, sl, sr, fh);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) ff[k] = beta1 * (ff[k]) + beta2 * (fh[k]);
+  }
+  return true;
+}
+
+// average(a,b) of src/limiter.f90:24-86 for LIMITER = -1..6
+template <typename R>
+__device__ __forceinline__ R average(int limiter, R a, R b)
+{
+  switch (limiter) {
+    case -1: return R(0.);
+    case 0: return R(0.5) * (a + b);
+    case 1: { R s = signr(a); return s * fmaxr(R(0.), fminr(absr(a), s * b)); }
+    case 2:
+      if (a * b <= R(0.)) return R(0.);
+      return a * b * (a + b) / (a * a + b * b);
+    case 3: {
+      const R delta = R(1.e-7);
+      return (a * (b * b + delta) + b * (a * a + delta)) / (a * a + b * b + delta);
+    }
+    case 4: {
+      R s = signr(a);
+      R c = R(0.25) * a + R(0.75) * b;
+      R d = R(0.75) * a + R(0.25) * b;
+      R av = fminr(fminr(fminr(R(2.) * absr(a), R(2.) * s * b), s * c), s * d);
+      return s * fmaxr(R(0.), av);
+    }
+    case 5: {
+      R s = signr(a);
+      R c = R(0.5) * (a + b);
+      R av = fminr(fminr(R(2.) * absr(a), R(2.) * s * b), s * c);
+      return s * fmaxr(R(0.), av);
+    }
+    default: {
+      R s = signr(b);
+      R av1 = fminr(R(2.) * absr(b), s * a);
+      R av2 = fminr(absr(b), R(2.) * s * a);
+      return s * fmaxr(fmaxr(R(0.), av1), av2);
+    }
+  }
+}
+
+// src/limiter.f90:7-22 on one equation
+template <typename R>
+__device__ __forceinline__ void limit1(int limiter, R pll, R& pl, R& pr, R prr)
+{
+  R dl = pl - pll;
+  R dm = pr - pl;
+  R dr = prr - pr;
+  R al = average<R>(limiter, dl, dm);
+  R ar = average<R>(limiter, dm, dr);
+  pl = pl + al * R(0.5);
+  pr = pr - ar * R(0.5);
+}
+
+}  // namespace w2d
