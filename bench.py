@@ -1,0 +1,343 @@
+"""Benchmark of the Walicxe-2D block update on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: 2D Sedov blast with AMR -- 8x8 root blocks of 16x16 cells, up to
+5 levels, refinement where the relative jump of p or rho reaches 0.1, HLLC
+fluxes with the minmod limiter, gamma 5/3, CFL 0.4, outflow boundaries,
+plain FP64.  The blast is first advanced (untimed) until it covers about
+2,500 leaf blocks (~0.65M zones); then W untimed and K timed steps follow.
+A step is one iteration of the reference's main loop: timestep, tstep and
+admesh (criteria on the device, integer block tree on the host, refine and
+coarse data motion on the device).
+
+Metric: zone-updates/s = sum over steps of (leaf blocks x 256) / time.
+  value      pool resident in HBM; every step timed with CUDA events on the
+             library's stream, L2 flushed (a 256 MB write) between steps
+  e2e        through the public C-ABI from host memory: upload of the state
+             (w2d_put_blocks), K steps, download of every leaf
+             (w2d_get_blocks); host wall clock around all of it
+  roofline   the dominant kernel's achieved GB/s (algorithmic bytes per
+             launch / mean launch time, CUDA events) against the measured
+             HBM copy bandwidth
+  cpu_baseline  the CPU oracle (C restatement of the reference; the
+             reference is Fortran and no Fortran compiler exists here) on
+             the host cores, a bounded sample of the same workload
+
+--impl reference times that CPU implementation alone (rank 0 only).
+Several GPUs run independent replicas (the single AMR run does not shard):
+value = all ranks' zone-updates / the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "zone-updates/s on 1 B200, plain FP64 vs batched FP32+NN-cooling at L1≤1e-3"
+UNIT = "zone-updates/s"
+PRE_STEPS = 250          # untimed evolution to a developed blast
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _pin_device(local: int, ws: int):
+    """One process per GPU: each rank sees only its own device."""
+    if ws > 1:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        devs = vis.split(",") if vis else [str(k) for k in range(64)]
+        os.environ["CUDA_VISIBLE_DEVICES"] = devs[local]
+
+
+def _measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int = 0):
+        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+        self.gpu = gpu_index
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)], stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        self.tmp.flush()
+        try:
+            rows = [r.split(",") for r in open(self.tmp.name).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        os.unlink(self.tmp.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def _traffic_per_zone(kernel: str):
+    """DRAM bytes per zone of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)[kernel]["dram_bytes_per_zone"]
+    except Exception:
+        return None
+
+
+def cpu_baseline(threads: int, target_s: float = 12.0, max_steps: int = 400):
+    """The oracle on the host cores: a bounded sample of the same workload."""
+    from oracle.oracle import Oracle, build
+    from walicxe2d_b200.params import config
+    build()
+    p, ic = config("sedov_amr")
+    o = Oracle(p, ic, threads=threads)
+    o.startup()
+    o.run(PRE_STEPS)
+    leaves0 = o.nbleafs
+    t0 = time.perf_counter()
+    zu, n = 0, 0
+    while True:
+        zu += o.nbleafs * 256
+        o.run(1)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > target_s or n >= max_steps:
+            break
+    return {"value": zu / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} main-loop steps of the same AMR Sedov workload after {PRE_STEPS} untimed "
+                      f"steps ({leaves0} leaves), oracle C restatement with {threads} OpenMP threads, "
+                      f"{el:.1f} s"}
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    res = []
+    from oracle.oracle import Oracle, build
+    from walicxe2d_b200.params import config
+    build()
+    p, ic = config("sedov_amr")
+    o = Oracle(p, ic, threads=threads)
+    o.startup()
+    o.run(PRE_STEPS)
+    o.run(max(args.warmup, 0))
+    sample = max(1, min(args.steps, 40))
+    zu = 0
+    t0 = time.perf_counter()
+    for _ in range(sample):
+        zu += o.nbleafs * 256
+        o.run(1)
+    el = time.perf_counter() - t0
+    value = zu / el
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": sample,
+        "warmup": args.warmup, "ms_per_step": 1000 * el / sample, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": "sedov_amr: 2D Sedov blast, 8x8 roots of 16x16, 5 levels, tol 0.1, "
+                               "HLLC+minmod, FP64", "leaves": o.nbleafs, "pre_steps": PRE_STEPS},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{sample} steps after {PRE_STEPS}+{args.warmup} untimed steps; "
+                                   "oracle C restatement (the Fortran reference cannot be built: "
+                                   "no Fortran compiler)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, ws, rank, local):
+    from walicxe2d_b200.api import Simulation
+    from walicxe2d_b200.params import config
+
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(0)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = (torch, td)
+
+    p, ic = config("sedov_amr")
+    p.precision = args.precision
+    sim = Simulation(p, ic)
+    ctx = sim.ctx
+    sim.run(PRE_STEPS)
+    sim.run(max(args.warmup, 3))
+
+    def barrier():
+        if dist:
+            dist[1].barrier()
+
+    # ---- value: device-resident, CUDA events per step, L2 flushed between -------------
+    barrier()
+    ctx.sync()
+    st0 = sim.status()
+    n0 = ctx.launch_count()
+    ctx.profile(True)
+    step_ms = []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            ctx.flush_l2()
+            ctx.event_record(0)
+            sim.run(1)
+            ctx.event_record(1)
+            step_ms.append(ctx.event_elapsed(0, 1))
+    ctx.sync()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    launches = ctx.launch_count() - n0
+    st1 = sim.status()
+    barrier()
+    zu = st1["zone_updates"] - st0["zone_updates"]
+    t_ms = sum(step_ms)
+    if dist:
+        torch, td = dist
+        tt = torch.tensor([t_ms, float(zu)], dtype=torch.float64, device="cuda")
+        tmax = tt[:1].clone()
+        td.all_reduce(tmax, op=td.ReduceOp.MAX)
+        tsum = tt[1:].clone()
+        td.all_reduce(tsum, op=td.ReduceOp.SUM)
+        t_all, zu_all = float(tmax.item()), float(tsum.item())
+    else:
+        t_all, zu_all = t_ms, float(zu)
+    value = zu_all / (t_all / 1000.0)
+
+    # ---- roofline of the dominant kernel ----------------------------------------------
+    flush_names = {"scatter", "gather"}
+    dom = max((k for k in prof if k not in flush_names), key=lambda k: prof[k][1])
+    nl, tot_ms = prof[dom]
+    elem = 8 if args.precision == 64 else 4
+    bytes_per_zone = 2.5625 * p.neq * elem          # halo tile read + block write
+    per_launch_zones = zu / max(nl, 1) if dom in ("half_step", "full_step") else zu / max(nl, 1)
+    achieved = bytes_per_zone * per_launch_zones / (tot_ms / nl / 1000.0) / 1e9
+    peak, peak_kind = _measured_peaks()
+    tpz = _traffic_per_zone(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": (tpz * per_launch_zones) if tpz is not None else None,
+                "algorithmic_bytes_per_launch": bytes_per_zone * per_launch_zones,
+                "mean_launch_us": 1000.0 * tot_ms / nl,
+                "kernels": {k: {"launches": v[0], "total_ms": v[1]} for k, v in prof.items()}}
+
+    # ---- e2e: host state in, K steps, host state out, through the C-ABI ----------------
+    ids, state = sim.blocks()
+    import numpy as np
+    state = np.ascontiguousarray(state)
+    barrier()
+    ctx.sync()
+    t0 = time.perf_counter()
+    ctx.put_blocks(ids, state)
+    e0 = sim.status()
+    sim.run(args.steps)
+    e1 = sim.status()
+    ids2, out = sim.blocks()
+    e2e_s = time.perf_counter() - t0
+    e2e_zu = e1["zone_updates"] - e0["zone_updates"]
+    h2d = state.nbytes / args.steps * (elem / 8)
+    d2h = out.nbytes / args.steps * (elem / 8) + 8 * (1 + e1["nbmax"])
+    e2e = {"value": e2e_zu / e2e_s * ws, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h),
+           "how": "w2d_put_blocks of every leaf from host memory, K main-loop steps (topology and "
+                  "plans uploaded, dt and criteria read back each step), w2d_get_blocks of every "
+                  "leaf; host wall clock"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline(os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_all / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == 64 else "f32", "data": "synthetic",
+            "config": {"workload": "sedov_amr: 2D Sedov blast, 8x8 roots of 16x16, 5 levels, tol 0.1, "
+                                   "HLLC+minmod, outflow, plain path",
+                       "leaves_at_start": st0["nleaf"], "leaves_at_end": st1["nleaf"],
+                       "pre_steps": PRE_STEPS, "l2": "flushed (256 MB write) before every timed step",
+                       "parallelism": f"replicas x{ws}"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clk.summary(),
+            "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist[1].destroy_process_group()
+    sim.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", type=int, default=64, choices=[64, 32])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    ws, rank, local = _dist_env()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank)
+    _pin_device(local, ws)
+    return run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -173,6 +173,13 @@ int w2d_profile_read(W2dCtx* ctx, char* names, int cap, int32_t* launches,
 int w2d_launch_count(W2dCtx* ctx, int64_t* n);
 /* Blocks until all queued work of the context is done. */
 int w2d_sync(W2dCtx* ctx);
+/* Records CUDA event `slot` (0..63) on the context's stream. */
+int w2d_event_record(W2dCtx* ctx, int slot);
+/* Milliseconds between two recorded events (waits for the later one). */
+int w2d_event_elapsed(W2dCtx* ctx, int slot_a, int slot_b, double* ms);
+/* Overwrites a scratch buffer larger than the L2 cache on the context's
+ * stream, so that the next call starts with a cold L2. */
+int w2d_flush_l2(W2dCtx* ctx);
 
 /* ---- whole-run driver ----------------------------------------------------
  * A C++ restatement of the reference's host side (main.f90 loop, basegrid,

@@ -47,6 +47,9 @@ SIGNATURES = {
     "w2d_profile_read": (_I, [_vp, C.c_char_p, _I, _PI32, _PD, _I, C.POINTER(_I)]),
     "w2d_launch_count": (_I, [_vp, C.POINTER(C.c_int64)]),
     "w2d_sync": (_I, [_vp]),
+    "w2d_event_record": (_I, [_vp, _I]),
+    "w2d_event_elapsed": (_I, [_vp, _I, _I, _PD]),
+    "w2d_flush_l2": (_I, [_vp]),
     "w2d_sim_create": (_I, [C.POINTER(W2dParams), C.POINTER(W2dInit), C.POINTER(_vp)]),
     "w2d_sim_destroy": (_I, [_vp]),
     "w2d_sim_run": (_I, [_vp, _I]),

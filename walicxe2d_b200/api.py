@@ -164,6 +164,17 @@ class Context:
             pos = end + 1
         return out
 
+    def event_record(self, slot: int):
+        self._check(self.L.w2d_event_record(self.h, slot), "w2d_event_record")
+
+    def event_elapsed(self, a: int, b: int) -> float:
+        ms = C.c_double()
+        self._check(self.L.w2d_event_elapsed(self.h, a, b, C.byref(ms)), "w2d_event_elapsed")
+        return ms.value
+
+    def flush_l2(self):
+        self._check(self.L.w2d_flush_l2(self.h), "w2d_flush_l2")
+
     def launch_count(self) -> int:
         n = C.c_int64()
         self._check(self.L.w2d_launch_count(self.h, C.byref(n)), "w2d_launch_count")

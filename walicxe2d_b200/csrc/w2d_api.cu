@@ -290,8 +290,11 @@ int w2d_destroy(W2dCtx* c)
   if (c->st) cudaStreamSynchronize(c->st);
   for (auto& q : c->pending) { cudaEventDestroy(q.a); cudaEventDestroy(q.b); }
   for (auto e : c->evpool) cudaEventDestroy(e);
+  for (auto e : c->ev)
+    if (e) cudaEventDestroy(e);
   void* dev[] = {c->d_u, c->d_up, c->d_prim, c->d_lev, c->d_icoord, c->d_cfl, c->d_dtcool, c->d_grad,
-                 c->d_err, c->d_dt, c->d_cooltab, c->d_leaves, c->d_fd1, c->d_fd2, c->d_stage, c->d_ids};
+                 c->d_err, c->d_dt, c->d_cooltab, c->d_leaves, c->d_fd1, c->d_fd2, c->d_stage, c->d_ids,
+                 c->d_flush};
   for (void* d : dev)
     if (d) cudaFree(d);
   void* host[] = {c->h_stage, c->h_small, c->h_grad, c->h_err, c->h_fd1, c->h_fd2, c->h_leaves};
@@ -744,6 +747,37 @@ int w2d_sync(W2dCtx* c)
 {
   if (!c) return W2D_ERR_ARG;
   return sync_and_check(c);
+}
+
+int w2d_event_record(W2dCtx* c, int slot)
+{
+  if (!c || slot < 0 || slot >= 64) return W2D_ERR_ARG;
+  if (!c->ev[slot]) CK(cudaEventCreate(&c->ev[slot]));
+  CK(cudaEventRecord(c->ev[slot], c->st));
+  return W2D_OK;
+}
+
+int w2d_event_elapsed(W2dCtx* c, int a, int b, double* ms)
+{
+  if (!c || !ms || a < 0 || b < 0 || a >= 64 || b >= 64 || !c->ev[a] || !c->ev[b]) return W2D_ERR_ARG;
+  CK(cudaEventSynchronize(c->ev[b]));
+  float f = 0.f;
+  CK(cudaEventElapsedTime(&f, c->ev[a], c->ev[b]));
+  *ms = f;
+  return W2D_OK;
+}
+
+int w2d_flush_l2(W2dCtx* c)
+{
+  if (!c) return W2D_ERR_ARG;
+  if (!c->d_flush) {
+    int l2 = 0;
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, c->device);
+    c->flush_bytes = std::max<size_t>((size_t)l2 * 2, (size_t)256 << 20);
+    CK(cudaMalloc(&c->d_flush, c->flush_bytes));
+  }
+  CK(cudaMemsetAsync(c->d_flush, (int)(c->nlaunch & 0xff), c->flush_bytes, c->st));
+  return W2D_OK;
 }
 
 }  // extern "C"

@@ -71,6 +71,9 @@ struct W2dCtx {
   std::vector<Pending> pending;
   std::vector<cudaEvent_t> evpool;
   int64_t nlaunch = 0;
+  cudaEvent_t ev[64] = {nullptr};
+  void* d_flush = nullptr;
+  size_t flush_bytes = 0;
 
   W2dError err{};
 };

@@ -328,7 +328,9 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
   }
   __syncthreads();
 
-  // u ghosts = up ghosts (u = up, src/tstep.f90:85), then calcprim(up)
+  // u ghosts = up ghosts (u = up, src/tstep.f90:85), then calcprim(up).
+  // Only the outer layer is stored here: layer 0 of u still feeds the
+  // viscosity below and is stored after it.
   R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;
   for (int c = tid; c < W2D_CELLS; c += W2D_THREADS) {
     const int ti = c % W2D_W, tj = c / W2D_W;
@@ -337,7 +339,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
     R uu[NEQ], q[NEQ], T;
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) uu[k] = st[k][tj][ti];
-    if (gx || gy) {
+    if (ti == 0 || ti == 19 || tj == 0 || tj == 19) {
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) u[k * W2D_CELLS + c] = uu[k];
     }
@@ -408,6 +410,17 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
     const int i = 1 + tid % 16, j = 1 + tid / 16;
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) u[k * W2D_CELLS + cidx(i, j)] = unew[k];
+  }
+  if (tid < 64) {  // layer 0 of u = layer 0 of the filled up (u = up)
+    const int f = tid / 16, m = 1 + tid % 16;
+    int i, j;
+    ghost_ij(f, 0, m, i, j);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) {
+      R v;
+      if (!face_value<R>(upool, bs, b, dface[f], f, 0, m, k, v)) v = upb[k * W2D_CELLS + cidx(i, j)];
+      u[k * W2D_CELLS + cidx(i, j)] = v;
+    }
   }
 }
 
