@@ -215,7 +215,7 @@ def run_ours(args, ws, rank, local):
     p.precision = args.precision
     sim = Simulation(p, ic)
     ctx = sim.ctx
-    sim.run(PRE_STEPS)
+    sim.run(args.pre_steps)
     sim.run(max(args.warmup, 3))
 
     def barrier():
@@ -308,7 +308,7 @@ def run_ours(args, ws, rank, local):
             "config": {"workload": "sedov_amr: 2D Sedov blast, 8x8 roots of 16x16, 5 levels, tol 0.1, "
                                    "HLLC+minmod, outflow, plain path",
                        "leaves_at_start": st0["nleaf"], "leaves_at_end": st1["nleaf"],
-                       "pre_steps": PRE_STEPS, "l2": "flushed (256 MB write) before every timed step",
+                       "pre_steps": args.pre_steps, "l2": "flushed (256 MB write) before every timed step",
                        "parallelism": f"replicas x{ws}"},
             "roofline": roofline,
             "cpu_baseline": cpu,
@@ -331,6 +331,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", type=int, default=64, choices=[64, 32])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--pre-steps", type=int, default=PRE_STEPS,
+                    help="untimed steps before warm-up (smaller cases for profiling)")
     args = ap.parse_args()
     ws, rank, local = _dist_env()
     if args.impl == "reference":
