@@ -181,6 +181,30 @@ int w2d_event_elapsed(W2dCtx* ctx, int slot_a, int slot_b, double* ms);
  * stream, so that the next call starts with a cold L2. */
 int w2d_flush_l2(W2dCtx* ctx);
 
+/* ---- allocation-free time step -------------------------------------------
+ * No counterpart in the reference.  For hosts that cannot allocate device
+ * memory: a Fortran code whose device arrays belong to an OpenACC or
+ * OpenMP-offload runtime, or a code whose memory manager forbids
+ * cudaMalloc/cudaFree inside its time loop.  Such a host owns its blocks on
+ * the device and cannot create a context (w2d_create allocates the pool).
+ *
+ * Computes what w2d_timestep computes for the nblocks blocks at u (device
+ * pointer, block-major [nblocks][neq][20][20], i fastest) whose levels are
+ * lev (device pointer, nblocks ints, 1..nlevs); dx, dy are host arrays of
+ * nlevs spacings; dt (host) receives the CFL time step.  FP64 only, not for
+ * COOLINGDMC.  Nothing is allocated: the per-block partials live in a
+ * file-scope device array of W2D_NOALLOC_MAX_BLOCKS doubles that every GPU
+ * loading the library keeps until exit; nblocks above that is rejected with
+ * W2D_ERR_CAPACITY.  The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress) with the device current; make that first
+ * call before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race.  Work is queued on the legacy default stream and
+ * the call returns once dt has been copied back. */
+#define W2D_NOALLOC_MAX_BLOCKS 65536
+#define W2D_MAXLEV_NOALLOC 16
+int w2d_timestep_noalloc(const W2dParams* p, const double* u, const int32_t* lev, int nblocks,
+                         const double* dx, const double* dy, double* dt);
+
 /* ---- whole-run driver ----------------------------------------------------
  * A C++ restatement of the reference's host side (main.f90 loop, basegrid,
  * admesh, markref, critneighup/down, updatelpup/down, locatebounds) driving

@@ -50,6 +50,7 @@ SIGNATURES = {
     "w2d_event_record": (_I, [_vp, _I]),
     "w2d_event_elapsed": (_I, [_vp, _I, _I, _PD]),
     "w2d_flush_l2": (_I, [_vp]),
+    "w2d_timestep_noalloc": (_I, [C.POINTER(W2dParams), _vp, _vp, _I, _PD, _PD, _PD]),
     "w2d_sim_create": (_I, [C.POINTER(W2dParams), C.POINTER(W2dInit), C.POINTER(_vp)]),
     "w2d_sim_destroy": (_I, [_vp]),
     "w2d_sim_run": (_I, [_vp, _I]),
