@@ -89,10 +89,23 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.gpu)], stdout=self.tmp, stderr=subprocess.DEVNULL)
+                 "-lms", "50", "-i", str(self.gpu)], stdout=self.tmp, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        # wait for the first sample so that the timed region is covered
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < 5.0:
+            self.tmp.flush()
+            if os.path.getsize(self.tmp.name) > 0:
+                break
+            time.sleep(0.05)
+        self.start = time.time()
         return self
+
+    def mark_start(self):
+        """Samples taken before this call are dropped from the summary."""
+        self.start = time.time()
+        self.skip = sum(1 for _ in open(self.tmp.name)) if os.path.exists(self.tmp.name) else 0
 
     def __exit__(self, *a):
         if self.proc is not None:
@@ -109,6 +122,9 @@ class ClockSampler:
         except Exception:
             rows = []
         os.unlink(self.tmp.name)
+        skip = getattr(self, "skip", 0)
+        if len(rows) > skip + 1:
+            rows = rows[max(skip - 1, 0):]   # keep the sample just before the region too
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
@@ -216,11 +232,14 @@ def run_ours(args, ws, rank, local):
     sim = Simulation(p, ic)
     ctx = sim.ctx
     sim.run(args.pre_steps)
-    sim.run(max(args.warmup, 3))
 
     def barrier():
         if dist:
             dist[1].barrier()
+            dist[0].cuda.synchronize()
+
+    clk = ClockSampler(0).__enter__()      # sampling runs from the warm-up on
+    sim.run(max(args.warmup, 3))
 
     # ---- value: device-resident, CUDA events per step, L2 flushed between -------------
     barrier()
@@ -229,14 +248,16 @@ def run_ours(args, ws, rank, local):
     n0 = ctx.launch_count()
     ctx.profile(True)
     step_ms = []
-    with ClockSampler(0) as clk:
-        for _ in range(args.steps):
-            ctx.flush_l2()
-            ctx.event_record(0)
-            sim.run(1)
-            ctx.event_record(1)
-            step_ms.append(ctx.event_elapsed(0, 1))
+    clk.mark_start()
+    for _ in range(args.steps):
+        ctx.flush_l2()
+        ctx.event_record(0)
+        sim.run(1)
+        ctx.event_record(1)
+        step_ms.append(ctx.event_elapsed(0, 1))
     ctx.sync()
+    time.sleep(0.06)                       # one more clock sample after the region
+    clk.__exit__()
     prof = ctx.profile_read()
     ctx.profile(False)
     launches = ctx.launch_count() - n0
@@ -326,7 +347,7 @@ def run_ours(args, ws, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", type=int, default=64, choices=[64, 32])

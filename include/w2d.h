@@ -243,6 +243,9 @@ int w2d_sim_tree(W2dSim* sim, int32_t* lp, int32_t* leaf, int32_t* icoord,
                  int32_t* innerbounds, int32_t* ninternal);
 /* Enables/disables AMR (admesh after each step); on by default if nlevs>1. */
 int w2d_sim_set_amr(W2dSim* sim, int on);
+/* DMC table for the driver's context (as w2d_set_cooltab), then the
+ * primitives and per-block partials of every leaf are recomputed with it. */
+int w2d_sim_set_cooltab(W2dSim* sim, const double* log_t, const double* neg_log_l, int n);
 
 #ifdef __cplusplus
 }

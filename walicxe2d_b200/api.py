@@ -214,6 +214,15 @@ class Simulation:
     def set_amr(self, on: bool):
         self.L.w2d_sim_set_amr(self.h, 1 if on else 0)
 
+    def set_cooltab(self, log_t, neg_log_l):
+        """DMC table (src/DMClib/coolingDMC.tab rows); recomputes the leaves'
+        primitives and time-step partials with it."""
+        a = np.ascontiguousarray(log_t, np.float64)
+        b = np.ascontiguousarray(neg_log_l, np.float64)
+        rc = self.L.w2d_sim_set_cooltab(self.h, _pd(a), _pd(b), a.size)
+        if rc:
+            self.ctx._check(rc, "w2d_sim_set_cooltab")
+
     def status(self) -> dict:
         t, dt = C.c_double(), C.c_double()
         steps, zu = C.c_int64(), C.c_int64()

@@ -267,14 +267,30 @@ int w2d_create(const W2dParams* p, W2dCtx** out)
     std::vector<double> neg(slots, -1.0);
     CKC(cudaMemcpy(c->d_grad, neg.data(), sizeof(double) * slots, cudaMemcpyHostToDevice));
   }
+  CKC(cudaMalloc(&c->d_dtwork, sizeof(unsigned long long) * 2));
+  CKC(cudaMalloc(&c->d_dtcount, sizeof(unsigned int)));
+  CKC(cudaMemsetAsync(c->d_dtcount, 0, sizeof(unsigned int), c->st));
+  {
+    const double big = 1e30;
+    unsigned long long bits;
+    memcpy(&bits, &big, sizeof(bits));
+    const unsigned long long w2[2] = {bits, bits};
+    CKC(cudaMemcpy(c->d_dtwork, w2, sizeof(w2), cudaMemcpyHostToDevice));
+  }
   CKC(cudaMallocHost(&c->h_small, sizeof(double) * 8));
   CKC(cudaMallocHost(&c->h_err, sizeof(int) * 4));
   CKC(cudaMallocHost(&c->h_grad, sizeof(double) * slots));
+  CKC(cudaMallocHost(&c->lev, sizeof(int) * slots));
+  CKC(cudaMallocHost(&c->icoord, sizeof(int) * 2 * slots));
+  CKC(cudaEventCreateWithFlags(&c->ev_topo, cudaEventDisableTiming));
+  CKC(cudaEventCreateWithFlags(&c->ev_ops, cudaEventDisableTiming));
+  CKC(cudaEventCreateWithFlags(&c->ev_plan[0], cudaEventDisableTiming));
+  CKC(cudaEventCreateWithFlags(&c->ev_plan[1], cudaEventDisableTiming));
   memset(c->h_err, 0, sizeof(int) * 4);
+  memset(c->lev, 0, sizeof(int) * slots);
+  memset(c->icoord, 0, sizeof(int) * 2 * slots);
 #undef CKC
-  c->lev.assign(slots, 0);
   c->leaf.assign(slots, 0);
-  c->icoord.assign(2 * slots, 0);
   c->leaf_index.assign(slots, -1);
   if (cudaStreamSynchronize(c->st) != cudaSuccess) {
     w2d_destroy(c);
@@ -292,12 +308,16 @@ int w2d_destroy(W2dCtx* c)
   for (auto e : c->evpool) cudaEventDestroy(e);
   for (auto e : c->ev)
     if (e) cudaEventDestroy(e);
+  cudaEvent_t evs[] = {c->ev_topo, c->ev_ops, c->ev_plan[0], c->ev_plan[1]};
+  for (auto e : evs)
+    if (e) cudaEventDestroy(e);
   void* dev[] = {c->d_u, c->d_up, c->d_prim, c->d_lev, c->d_icoord, c->d_cfl, c->d_dtcool, c->d_grad,
                  c->d_err, c->d_dt, c->d_cooltab, c->d_leaves, c->d_fd1, c->d_fd2, c->d_stage, c->d_ids,
-                 c->d_flush};
+                 c->d_flush, c->d_dtwork, c->d_dtcount};
   for (void* d : dev)
     if (d) cudaFree(d);
-  void* host[] = {c->h_stage, c->h_small, c->h_grad, c->h_err, c->h_fd1, c->h_fd2, c->h_leaves};
+  void* host[] = {c->h_stage, c->h_small, c->h_grad, c->h_err, c->h_fd1[0], c->h_fd2[0], c->h_leaves[0],
+                  c->h_fd1[1], c->h_fd2[1], c->h_leaves[1], c->h_ops, c->lev, c->icoord};
   for (void* h : host)
     if (h) cudaFreeHost(h);
   if (c->st) cudaStreamDestroy(c->st);
@@ -333,9 +353,10 @@ int w2d_set_topology(W2dCtx* c, const int32_t* lp, int ld_lp, const int32_t* lea
   if (!c || !lp || !leaf || !icoord || !dx || !dy) return W2D_ERR_ARG;
   if (nbmax < 0 || nbmax > c->cap || ld_lp < nbmax || ld_icoord < nbmax)
     return set_error(c, W2D_ERR_ARG, 0, 0, 0, "nbmax %d outside the pool (capacity %d)", nbmax, c->cap);
+  CK(cudaEventSynchronize(c->ev_topo));  // the previous upload has left the pinned arrays
+  for (int b : c->leaves) c->leaf_index[b] = -1;  // only the old leaves are set
   c->nbmax = nbmax;
   c->leaves.clear();
-  std::fill(c->leaf_index.begin(), c->leaf_index.end(), -1);
   for (int nb = 1; nb <= nbmax; ++nb) {
     c->lev[nb] = lp[nb - 1];                       // lp(nb,1)
     c->leaf[nb] = leaf[nb - 1] != 0;
@@ -352,10 +373,10 @@ int w2d_set_topology(W2dCtx* c, const int32_t* lp, int ld_lp, const int32_t* lea
     c->dx[l] = dx[l - 1];
     c->dy[l] = dy[l - 1];
   }
-  CK(cudaMemcpyAsync(c->d_lev, c->lev.data(), sizeof(int) * (size_t)(nbmax + 1), cudaMemcpyHostToDevice, c->st));
-  CK(cudaMemcpyAsync(c->d_icoord, c->icoord.data(), sizeof(int) * 2 * (size_t)(nbmax + 1),
+  CK(cudaMemcpyAsync(c->d_lev, c->lev, sizeof(int) * (size_t)(nbmax + 1), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_icoord, c->icoord, sizeof(int) * 2 * (size_t)(nbmax + 1),
                      cudaMemcpyHostToDevice, c->st));
-  CK(cudaStreamSynchronize(c->st));  // host vectors are pageable
+  CK(cudaEventRecord(c->ev_topo, c->st));
   c->have_topology = true;
   c->have_bounds = false;
   return W2D_OK;
@@ -371,29 +392,38 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
   const int nl = (int)c->leaves.size();
   if (nl > c->h_plan_cap) {
     CK(cudaStreamSynchronize(c->st));
-    if (c->h_fd1) cudaFreeHost(c->h_fd1);
-    if (c->h_fd2) cudaFreeHost(c->h_fd2);
-    if (c->h_leaves) cudaFreeHost(c->h_leaves);
+    for (int q = 0; q < 2; ++q) {
+      if (c->h_fd1[q]) cudaFreeHost(c->h_fd1[q]);
+      if (c->h_fd2[q]) cudaFreeHost(c->h_fd2[q]);
+      if (c->h_leaves[q]) cudaFreeHost(c->h_leaves[q]);
+      c->h_fd1[q] = c->h_fd2[q] = nullptr;
+      c->h_leaves[q] = nullptr;
+    }
     if (c->d_fd1) cudaFree(c->d_fd1);
     if (c->d_fd2) cudaFree(c->d_fd2);
     if (c->d_leaves) cudaFree(c->d_leaves);
-    c->h_fd1 = c->h_fd2 = nullptr;
-    c->h_leaves = nullptr;
     c->d_fd1 = c->d_fd2 = nullptr;
     c->d_leaves = nullptr;
     int cap = std::max(nl + nl / 2, 256);
-    CK(cudaMallocHost(&c->h_fd1, sizeof(int2) * 4 * (size_t)cap));
-    CK(cudaMallocHost(&c->h_fd2, sizeof(int2) * 4 * (size_t)cap));
-    CK(cudaMallocHost(&c->h_leaves, sizeof(int) * (size_t)cap));
+    for (int q = 0; q < 2; ++q) {
+      CK(cudaMallocHost(&c->h_fd1[q], sizeof(int2) * 4 * (size_t)cap));
+      CK(cudaMallocHost(&c->h_fd2[q], sizeof(int2) * 4 * (size_t)cap));
+      CK(cudaMallocHost(&c->h_leaves[q], sizeof(int) * (size_t)cap));
+    }
     CK(cudaMalloc(&c->d_fd1, sizeof(int2) * 4 * (size_t)cap));
     CK(cudaMalloc(&c->d_fd2, sizeof(int2) * 4 * (size_t)cap));
     CK(cudaMalloc(&c->d_leaves, sizeof(int) * (size_t)cap));
     c->h_plan_cap = cap;
-  } else {
-    CK(cudaStreamSynchronize(c->st));  // previous plan upload may still read the pinned buffers
   }
-  for (int k = 0; k < 4 * nl; ++k) c->h_fd1[k] = c->h_fd2[k] = make_int2(0, FK_KEEP);
-  for (int k = 0; k < nl; ++k) c->h_leaves[k] = c->leaves[k];
+  // alternate pinned buffers; wait only for the upload that last used this one
+  const int q = c->plan_buf;
+  c->plan_buf ^= 1;
+  CK(cudaEventSynchronize(c->ev_plan[q]));
+  int2* hf1 = c->h_fd1[q];
+  int2* hf2 = c->h_fd2[q];
+  int* hl = c->h_leaves[q];
+  for (int k = 0; k < 4 * nl; ++k) hf1[k] = hf2[k] = make_int2(0, FK_KEEP);
+  for (int k = 0; k < nl; ++k) hl[k] = c->leaves[k];
   auto put = [&](int2* fd, int blk, int face, int nbr, int kind, int off) {
     if (blk < 1 || blk > c->nbmax) return;
     const int li = c->leaf_index[blk];
@@ -401,8 +431,8 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
     fd[li * 4 + face] = make_int2(nbr, kind | (off << 8));
   };
   auto both = [&](int blk, int face, int nbr, int kind, int off) {
-    put(c->h_fd1, blk, face, nbr, kind, off);
-    put(c->h_fd2, blk, face, nbr, kind, off);
+    put(hf1, blk, face, nbr, kind, off);
+    put(hf2, blk, face, nbr, kind, off);
   };
   const int H = W2D_NX / 2;
   const int bc[4] = {c->p.bc_left, c->p.bc_right, c->p.bc_bottom, c->p.bc_top};
@@ -421,10 +451,10 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
         if (bc[2] == W2D_BC_REFLECTIVE) {
           both(nbs, 2, nbs, FK_REFLECT, 0);
         } else {
-          put(c->h_fd2, nbs, 2, nbs, FK_MIRROR, 0);
+          put(hf2, nbs, 2, nbs, FK_MIRROR, 0);
           // src/boundaryI.f90:87 fills block "nb" (the list index e)
           const int tb = f6b ? e : nbs;
-          put(c->h_fd1, tb, 2, tb, FK_MIRROR, 0);
+          put(hf1, tb, 2, tb, FK_MIRROR, 0);
         }
         break;
       case 1:  both(nbs, 0, n1, FK_SAME, 0);  both(n1, 1, nbs, FK_SAME, 0); break;
@@ -456,10 +486,11 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
     }
   }
   if (nl > 0) {
-    CK(cudaMemcpyAsync(c->d_fd1, c->h_fd1, sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->d_fd2, c->h_fd2, sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->d_leaves, c->h_leaves, sizeof(int) * (size_t)nl, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_fd1, hf1, sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_fd2, hf2, sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_leaves, hl, sizeof(int) * (size_t)nl, cudaMemcpyHostToDevice, c->st));
   }
+  CK(cudaEventRecord(c->ev_plan[q], c->st));
   c->have_bounds = true;
   return W2D_OK;
 }
@@ -570,7 +601,7 @@ int w2d_timestep(W2dCtx* c, double* dt)
   }
   int rc = launch(c, "timestep", [&] {
     return launch_dt(c->d_leaves, nl, c->d_cfl, c->d_dtcool, c->p.cooling == W2D_COOLINGDMC, c->p.cfl,
-                     c->p.psc, c->p.tsc, c->d_dt, c->st);
+                     c->p.psc, c->p.tsc, c->d_dtwork, c->d_dtcount, c->d_dt, c->st);
   });
   if (rc) return rc;
   CK(cudaMemcpyAsync(c->h_small, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -620,7 +651,19 @@ static int amr_ops(W2dCtx* c, const int32_t* quads, int n, bool refine)
   if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
   int rc = valid_ids(c, quads, 5 * n);
   if (rc) return rc;
-  if ((rc = ensure_ids(c, 5 * n + 4 * n))) return rc;
+  // staging layout: quads (5n), new leaves (<= 4n), (slot, level, ix, iy)
+  // of the new leaves (<= 16n); pinned, sent asynchronously, reused only
+  // once the previous send has completed
+  if ((rc = ensure_ids(c, 25 * n))) return rc;
+  if (25 * n > c->h_ops_cap) {
+    CK(cudaEventSynchronize(c->ev_ops));
+    if (c->h_ops) cudaFreeHost(c->h_ops);
+    c->h_ops = nullptr;
+    c->h_ops_cap = std::max(25 * n, 8192);
+    CK(cudaMallocHost(&c->h_ops, sizeof(int) * (size_t)c->h_ops_cap));
+  }
+  CK(cudaEventSynchronize(c->ev_ops));
+  CK(cudaEventSynchronize(c->ev_topo));   // host lev/icoord are not being uploaded
   // the new leaves: levels and icoord as refine/coarse set them
   std::vector<int> newl;
   newl.reserve(4 * n);
@@ -641,24 +684,32 @@ static int amr_ops(W2dCtx* c, const int32_t* quads, int n, bool refine)
       newl.push_back(o[0]);
     }
   }
-  std::vector<int> buf(quads, quads + 5 * n);
-  buf.insert(buf.end(), newl.begin(), newl.end());
-  CK(cudaMemcpyAsync(c->d_ids, buf.data(), sizeof(int) * buf.size(), cudaMemcpyHostToDevice, c->st));
-  {
-    const int lo = *std::min_element(newl.begin(), newl.end());
-    const int hi = *std::max_element(newl.begin(), newl.end());
-    const size_t cnt = (size_t)(hi - lo + 1);
-    CK(cudaMemcpyAsync(c->d_lev + lo, &c->lev[lo], sizeof(int) * cnt, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->d_icoord + 2 * lo, &c->icoord[2 * lo], 2 * sizeof(int) * cnt,
-                       cudaMemcpyHostToDevice, c->st));
+  const int nn = (int)newl.size();
+  int* h = c->h_ops;
+  memcpy(h, quads, sizeof(int) * 5 * (size_t)n);
+  memcpy(h + 5 * n, newl.data(), sizeof(int) * (size_t)nn);
+  int* tup = h + 5 * n + nn;
+  for (int k = 0; k < nn; ++k) {
+    const int b = newl[k];
+    tup[4 * k] = b;
+    tup[4 * k + 1] = c->lev[b];
+    tup[4 * k + 2] = c->icoord[2 * b];
+    tup[4 * k + 3] = c->icoord[2 * b + 1];
   }
+  const size_t nops = 5 * (size_t)n + 5 * (size_t)nn;
+  CK(cudaMemcpyAsync(c->d_ids, h, sizeof(int) * nops, cudaMemcpyHostToDevice, c->st));
+  CK(cudaEventRecord(c->ev_ops, c->st));
+  if ((rc = launch(c, "set_slots", [&] {
+         return launch_set_slots(c->d_ids + 5 * n + nn, nn, c->d_lev, c->d_icoord, c->st);
+       })))
+    return rc;
   if (refine)
     rc = launch(c, "refine", [&] { return c->L->refine(c->neq, c->d_u, c->d_ids, n, c->st); });
   else
     rc = launch(c, "coarse", [&] { return c->L->coarse(c->neq, c->d_u, c->d_ids, n, c->st); });
   if (rc) return rc;
+  // d_ids is reused by the next call only after this call's kernels (stream order)
   if ((rc = stats_for(c, c->d_ids + 5 * n, (int)newl.size()))) return rc;
-  CK(cudaStreamSynchronize(c->st));  // pageable sources above
   return W2D_OK;
 }
 

@@ -3,9 +3,9 @@
 //   coolingh   src/coolingh.f90:5-259 (atomic, ALOSS, alpha, colf, betah)
 //   coolingdmc src/coolingdmc.f90:6-54 with cooldmc, src/dmc_module.f90:14-32
 //
-// Same operation order as the reference; exp/pow/log/log10 are CUDA's own
-// (they differ from glibc by a few ulp), so these kernels agree with the
-// reference to a relative tolerance, not bit for bit.
+// Same operation order as the reference, always in FP64; exp/pow/log/log10
+// are CUDA's own (they differ from glibc by a few ulp), so these kernels
+// agree with the reference to a relative tolerance, not bit for bit.
 #pragma once
 
 #include "w2d_kernels.cuh"
@@ -96,41 +96,36 @@ __device__ __forceinline__ void d_atomic(const Phys<double>& ph, double dt, doub
   uu[3] = ph.cv * (2. * uu[0] - uu[4]) * t1 / ph.tempsc + 0.5 * prim[0] * (prim[1] * prim[1] + prim[2] * prim[2]);
 }
 
-// src/dmc_module.f90:14-32; the index is clamped to the table (the
-// reference reads row 42 at T == 1e8 exactly).
-__device__ __forceinline__ double d_cooldmc(const double* __restrict__ tab, double T)
+// Cooling of cells 0..17 of every leaf (after the fill of layer 0), then
+// the per-block CFL partial, DMC cooling-time limit and criteria maximum of
+// the cooled state.  pa.cooling selects coolingh or coolingdmc.
+template <typename R, int NEQ>
+__host__ __device__ constexpr size_t smem_cool()
 {
-  if (T > 1e8) return 0.21e-26 * sqrt(T);
-  int if1 = (int)(log10(T) * 10) - 39;
-  if1 = if1 > 40 ? 40 : (if1 < 1 ? 1 : if1);
-  double T0 = tab[if1 - 1], c0 = tab[41 + if1 - 1];
-  double T1 = tab[if1], c1 = tab[41 + if1];
-  return (c1 - c0) * (T - T0) / (T1 - T0) + c0;
+  return 128 + sizeof(R) * NEQ * W2D_CELLS + 64 * sizeof(double);
 }
 
-// Cooling of cells 0..17 of every leaf (after the fill of layer 0), then
-// the per-block CFL partial, DMC cooling-time limit and criteria maximum
-// of the cooled state.  mode: COOL_H or COOL_DMC.
 template <typename R, int NEQ>
 __global__ void __launch_bounds__(W2D_THREADS) k_cool(KArgs a, PhysArgs pa, double dt_s)
 {
-  __shared__ R sp[NEQ][18][18];
-  __shared__ double sred[3][W2D_THREADS / 32];
-  const Phys<R> ph = make_phys<R>(pa.cv, pa.gamma, pa.tempsc, pa.cooling, pa.hllc_compat,
-                                  pa.solver, pa.limiter);
-  const Phys<double> phd = make_phys<double>(pa.cv, pa.gamma, pa.tempsc, pa.cooling, pa.hllc_compat,
-                                             pa.solver, pa.limiter);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
+  R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
+  double* sred = reinterpret_cast<double*>(w2d_smem + 128 + sizeof(R) * NEQ * W2D_CELLS);
+  const Phys<R> ph = make_phys<R, -1, -1>(pa);
+  const Phys<double> phd = make_phys<double, -1, -1>(pa);
   const int b = a.leaves[blockIdx.x];
   const int tid = threadIdx.x;
   const size_t bs = (size_t)NEQ * W2D_CELLS;
   R* __restrict__ u = (R*)a.u + (size_t)b * bs;
   R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;
+  load_tile<R, NEQ>(&st[0][0][0], u, bar, a.err, b);
+  if (!wait_tiles(bar, a.err, b)) return;
   for (int c = tid; c < 18 * 18; c += W2D_THREADS) {
     const int i = c % 18, j = c / 18;
     if ((i == 0 || i == 17) && (j == 0 || j == 17)) continue;
     double uu[NEQ];
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) uu[k] = (double)u[k * W2D_CELLS + cidx(i, j)];
+    for (int k = 0; k < NEQ; ++k) uu[k] = (double)st[k][j + 1][i + 1];
     if (pa.cooling == COOL_H) {
       d_atomic<NEQ>(phd, dt_s, uu);
       u[3 * W2D_CELLS + cidx(i, j)] = R(uu[3]);
@@ -140,7 +135,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_cool(KArgs a, PhysArgs pa, doub
       for (int k = 0; k < NEQ; ++k) ur[k] = R(uu[k]);
       uprim<NEQ>(ph, q, ur, T);
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) sp[k][j][i] = q[k];
+      for (int k = 0; k < NEQ; ++k) st[k][j + 1][i + 1] = q[k];
     } else {
       double q[NEQ], T;
       uprim<NEQ>(phd, q, uu, T);
@@ -155,57 +150,12 @@ __global__ void __launch_bounds__(W2D_THREADS) k_cool(KArgs a, PhysArgs pa, doub
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) {
         pb[k * W2D_CELLS + cidx(i, j)] = R(q[k]);
-        sp[k][j][i] = R(q[k]);
+        st[k][j + 1][i + 1] = R(q[k]);
       }
     }
   }
   __syncthreads();
-  const int lev = a.lev[b];
-  double dtp = 1e30, grad = 0., dtc = 1e30;
-  if (tid < 256) {
-    const int i = 1 + tid % 16, j = 1 + tid / 16;
-    const R rho = sp[0][j][i], vx = sp[1][j][i], vy = sp[2][j][i], p = sp[3][j][i];
-    const R cs = sound(ph, p, rho);
-    R t1 = R(a.dx[lev]) / (absr(vx) + cs);
-    R t2 = R(a.dy[lev]) / (absr(vy) + cs);
-    dtp = (double)fminr(t1, t2);
-    const R fl = R(1e-15);
-    const R am = fmaxr(fl, absr(p)), am2 = fmaxr(fl, absr(rho));
-    R gr = R(0.);
-    gr = fmaxr(gr, absr(sp[3][j][i + 1] - p) / am);
-    gr = fmaxr(gr, absr(sp[3][j][i - 1] - p) / am);
-    gr = fmaxr(gr, absr(sp[3][j + 1][i] - p) / am);
-    gr = fmaxr(gr, absr(sp[3][j - 1][i] - p) / am);
-    gr = fmaxr(gr, absr(sp[0][j][i + 1] - rho) / am2);
-    gr = fmaxr(gr, absr(sp[0][j][i - 1] - rho) / am2);
-    gr = fmaxr(gr, absr(sp[0][j + 1][i] - rho) / am2);
-    gr = fmaxr(gr, absr(sp[0][j - 1][i] - rho) / am2);
-    grad = (double)gr;
-    if (pa.cooling == COOL_DMC) {                      // timestep.f90:34-41
-      double T = ((double)p / (double)rho) * pa.tempsc;
-      if (T > 1e4) {
-        double aloss = d_cooldmc(a.cooltab, T) * ((double)rho * (double)rho);
-        dtc = pa.cv * (double)p / aloss;
-      }
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    dtp = fmin(dtp, __shfl_xor_sync(0xffffffffu, dtp, o));
-    grad = fmax(grad, __shfl_xor_sync(0xffffffffu, grad, o));
-    dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
-  }
-  if ((tid & 31) == 0) { sred[0][tid >> 5] = dtp; sred[1][tid >> 5] = grad; sred[2][tid >> 5] = dtc; }
-  __syncthreads();
-  if (tid == 0) {
-    double m0 = sred[0][0], m1 = sred[1][0], m2 = sred[2][0];
-    for (int w = 1; w < W2D_THREADS / 32; ++w) {
-      m0 = fmin(m0, sred[0][w]); m1 = fmax(m1, sred[1][w]); m2 = fmin(m2, sred[2][w]);
-    }
-    a.cfl[b] = m0;
-    a.grad[b] = m1;
-    a.dtcool[b] = m2;
-  }
+  block_stats<R, NEQ>(st, ph, a, pa, b, sred);
 }
 
 // primitives of whole blocks into a staging buffer (w2d_get_primit when
@@ -214,8 +164,7 @@ template <typename R, int NEQ>
 __global__ void k_to_prim(PhysArgs pa, const R* __restrict__ u, R* __restrict__ out,
                           const int* __restrict__ ids)
 {
-  const Phys<R> ph = make_phys<R>(pa.cv, pa.gamma, pa.tempsc, pa.cooling, pa.hllc_compat,
-                                  pa.solver, pa.limiter);
+  const Phys<R> ph = make_phys<R, -1, -1>(pa);
   const size_t bs = (size_t)NEQ * W2D_CELLS;
   const R* ub = u + (size_t)ids[blockIdx.x] * bs;
   R* ob = out + (size_t)blockIdx.x * bs;

@@ -31,6 +31,8 @@ struct W2dCtx {
   double* d_grad = nullptr;
   int* d_err = nullptr;
   double* d_dt = nullptr;
+  unsigned long long* d_dtwork = nullptr;  // k_dt minima (bit patterns)
+  unsigned int* d_dtcount = nullptr;       // k_dt CTA counter
   double* d_cooltab = nullptr;
   // per-step plan
   int* d_leaves = nullptr;
@@ -45,15 +47,27 @@ struct W2dCtx {
   void* h_stage = nullptr;   // pinned
   size_t h_stage_bytes = 0;
   double* h_small = nullptr; // pinned scalars (dt, ...)
-  double* h_grad = nullptr;  // pinned, one per leaf
+  double* h_grad = nullptr;  // pinned, one per slot
   int* h_err = nullptr;      // pinned error word
-  int2* h_fd1 = nullptr;     // pinned plan staging
-  int2* h_fd2 = nullptr;
-  int* h_leaves = nullptr;
+  // pinned plan staging, double-buffered; an event marks when the upload
+  // from each buffer has been consumed
+  int2* h_fd1[2] = {nullptr, nullptr};
+  int2* h_fd2[2] = {nullptr, nullptr};
+  int* h_leaves[2] = {nullptr, nullptr};
+  cudaEvent_t ev_plan[2] = {nullptr, nullptr};
+  int plan_buf = 0;
   int h_plan_cap = 0;
+  // pinned staging of refine/coarse lists
+  int* h_ops = nullptr;
+  int h_ops_cap = 0;
+  cudaEvent_t ev_ops = nullptr;
 
-  // host copy of the topology
-  std::vector<int> lev, leaf, icoord;  // per slot
+  // host copy of the topology; lev and icoord are pinned and uploaded
+  // asynchronously (ev_topo marks the last upload)
+  int* lev = nullptr;                  // per slot
+  int* icoord = nullptr;               // 2 per slot
+  cudaEvent_t ev_topo = nullptr;
+  std::vector<int> leaf;               // per slot
   std::vector<int> leaves;             // leaf slots, ascending
   std::vector<int> leaf_index;         // slot -> position in leaves, -1
   int nbmax = 0;

@@ -11,10 +11,17 @@
 //   updatelpdown     src/updatelpdown.f90:4-59
 //   locatebounds     src/locatebounds.f90:29-540
 //
-// The integer arrays use the reference's Fortran layout (column-major,
-// 1-based block IDs) so they can be handed to w2d_set_topology as they are.
-// The per-cell work of refine/coarse/criteria/calcprim runs on the device
-// through the C-ABI; only integer bookkeeping happens here.
+// Block IDs are 1-based as in the reference.  lp(nb,1:8) is kept row by row
+// (the eight pointers of a block side by side); leaf and icoord are kept in
+// the reference's Fortran layout so they can be handed to w2d_set_topology
+// as they are.  The per-cell work of refine/coarse/criteria/calcprim runs on
+// the device through the C-ABI; only integer bookkeeping happens here.
+//
+// Every loop of the reference that scans all blocks once per level visits
+// here only the leaves of that level, in ascending ID: only leaves ever carry
+// the refine/coarsen flags (markref sets them on leaves, critneighup on the
+// coarser leaves its pointers reach), so the same blocks are visited in the
+// same order and the decisions are identical.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -26,7 +33,9 @@ struct W2dSim {
   W2dInit ic{};
   W2dCtx* ctx = nullptr;
   int cap = 0, nbmax = 0, nbleafs = 0;
-  std::vector<int32_t> lp, leaf, icoord;  // column-major, ld = cap
+  std::vector<int32_t> lp;                // row-major [(cap+1)][8]
+  std::vector<int32_t> leaf, icoord;      // column-major, ld = cap
+  std::vector<int32_t> levbuf;            // lp(:,1) as one column, for w2d_set_topology
   std::vector<double> dx, dy;             // nlevs entries
   std::vector<int32_t> ib;                // innerbounds, column-major, ld = nib
   int nib = 0;
@@ -34,12 +43,15 @@ struct W2dSim {
   int64_t steps = 0, zone_updates = 0;
   bool amr = true;
   bool dirty = true;
-  std::vector<unsigned char> irefup, irefdown, bounds;
+  std::vector<unsigned char> irefup, irefdown;
+  std::vector<uint32_t> bounds;           // locatebounds flags, valid when == gen
+  uint32_t gen = 0;
+  std::vector<std::vector<int32_t>> bucket;  // leaves per level, ascending ID
   std::vector<double> grad;
   std::vector<int32_t> rops, cops;
   std::vector<int32_t> ib1, ib2, ib3;
 
-  int32_t& LP(int nb, int k) { return lp[(size_t)(k - 1) * cap + (nb - 1)]; }
+  int32_t& LP(int nb, int k) { return lp[(size_t)nb * 8 + (k - 1)]; }
   int32_t& LEAF(int nb) { return leaf[(size_t)nb - 1]; }
   int32_t& IC(int nb, int k) { return icoord[(size_t)(k - 1) * cap + (nb - 1)]; }
 };
@@ -147,9 +159,12 @@ void updatelpdown(W2dSim* s, int dad, int s1, int s2, int s3, int s4)
   if (nb1 != -1 && !L.LEAF(nb1)) { nb1 = L.LP(nb1, 3); L.LP(nb1, 7) = dad; L.LP(L.LP(nb1, 6), 7) = dad; }
 }
 
+// w2d_set_topology reads only lp(:,1) of the lp argument, so the level
+// column is passed on its own.
 int push_topology(W2dSim* s)
 {
-  return w2d_set_topology(s->ctx, s->lp.data(), s->cap, s->leaf.data(), s->icoord.data(), s->cap,
+  for (int nb = 1; nb <= s->nbmax; ++nb) s->levbuf[nb - 1] = s->LP(nb, 1);
+  return w2d_set_topology(s->ctx, s->levbuf.data(), s->cap, s->leaf.data(), s->icoord.data(), s->cap,
                           s->nbmax, s->dx.data(), s->dy.data());
 }
 
@@ -157,8 +172,19 @@ int push_topology(W2dSim* s)
 void locatebounds(W2dSim* s)
 {
   auto& L = *s;
-  std::fill(s->bounds.begin(), s->bounds.end(), 0);
-  auto BND = [&](int nb, int k) -> unsigned char& { return s->bounds[(size_t)nb * 4 + k - 1]; };
+  // bounds(nb,k) is "set" when it holds the current generation number
+  if (++s->gen == 0) {
+    std::fill(s->bounds.begin(), s->bounds.end(), 0u);
+    s->gen = 1;
+  }
+  const uint32_t g = s->gen;
+  struct Flag {
+    uint32_t* v;
+    uint32_t g;
+    operator bool() const { return *v == g; }
+    Flag& operator=(int on) { *v = on ? g : 0u; return *this; }
+  };
+  auto BND = [&](int nb, int k) { return Flag{&s->bounds[(size_t)nb * 4 + k - 1], g}; };
   s->ib1.clear(); s->ib2.clear(); s->ib3.clear();
   auto push = [&](int a, int b, int t) { s->ib1.push_back(a); s->ib2.push_back(b); s->ib3.push_back(t); };
   for (int nb = 1; nb <= s->nbmax; ++nb) {
@@ -228,30 +254,33 @@ int admesh(W2dSim* s)
   if (rc) return rc;
   std::fill(s->irefup.begin(), s->irefup.end(), 0);
   std::fill(s->irefdown.begin(), s->irefdown.end(), 0);
-  for (int nb = 1; nb <= s->nbmax; ++nb) {
-    if (!(L.LEAF(nb) && L.LP(nb, 1) >= 1)) continue;
-    const double g = s->grad[nb - 1];
-    if (g >= s->p.tol) {
-      if (L.LP(nb, 1) < nlevs) { s->irefup[nb] = 1; s->irefdown[nb] = 0; }
-    } else if (g <= s->p.tol2) {
-      s->irefdown[nb] = 1;
+  // leaves per level in ascending ID (the only blocks that get flags)
+  for (auto& v : s->bucket) v.clear();
+  for (int nb = 1; nb <= s->nbmax; ++nb)
+    if (L.LEAF(nb) && L.LP(nb, 1) >= 1) s->bucket[L.LP(nb, 1)].push_back(nb);
+  for (int nl = 1; nl <= nlevs; ++nl)
+    for (int nb : s->bucket[nl]) {
+      const double g = s->grad[nb - 1];
+      if (g >= s->p.tol) {
+        if (L.LP(nb, 1) < nlevs) { s->irefup[nb] = 1; s->irefdown[nb] = 0; }
+      } else if (g <= s->p.tol2) {
+        s->irefdown[nb] = 1;
+      }
     }
-  }
-  // critneighup
+  // critneighup: flags reach coarser leaves, visited at their own level later
   for (int nl = nlevs - 1; nl >= 1; --nl)
-    for (int nb = 1; nb <= s->nbmax; ++nb)
-      if (s->irefup[nb] && L.LP(nb, 1) == nl)
+    for (int nb : s->bucket[nl])
+      if (s->irefup[nb])
         for (int k = 5; k <= 8; ++k) {
           const int n1 = L.LP(nb, k);
           if (n1 != -1 && L.LP(n1, 1) < L.LP(nb, 1)) s->irefup[n1] = 1;
         }
   int nbmaxp = s->nbmax;
-  const int nbmaxp1 = s->nbmax;
   s->rops.clear();
   s->cops.clear();
   for (int nl = 1; nl <= nlevs - 1; ++nl)
-    for (int nb = 1; nb <= nbmaxp1; ++nb) {
-      if (!(L.LP(nb, 1) == nl && s->irefup[nb])) continue;
+    for (int nb : s->bucket[nl]) {
+      if (!s->irefup[nb]) continue;
       int s1, s2, s3, s4;
       if (L.LP(nb, 3) == 0) {
         s1 = nbmaxp + 1; s2 = s1 + 1; s3 = s1 + 2; s4 = s1 + 3;
@@ -266,16 +295,17 @@ int admesh(W2dSim* s)
       s->rops.insert(s->rops.end(), q, q + 5);
       updatelpup(s, nb, s1, s2, s3, s4);
     }
-  // critneighdown
-  for (int nb = 1; nb <= s->nbmax; ++nb)
-    if (s->irefdown[nb])
-      for (int k = 5; k <= 8; ++k) {
-        const int n1 = L.LP(nb, k);
-        if (n1 != -1 && !L.LEAF(n1)) s->irefdown[nb] = 0;
-      }
+  // critneighdown (only the leaves of the pass carry irefdown)
+  for (int nl = 1; nl <= nlevs; ++nl)
+    for (int nb : s->bucket[nl])
+      if (s->irefdown[nb])
+        for (int k = 5; k <= 8; ++k) {
+          const int n1 = L.LP(nb, k);
+          if (n1 != -1 && !L.LEAF(n1)) s->irefdown[nb] = 0;
+        }
   for (int nl = nlevs; nl >= 2; --nl)
-    for (int nb = 1; nb <= nbmaxp1; ++nb) {
-      if (!(s->irefdown[nb] && L.LP(nb, 4) == 1 && L.LP(nb, 1) == nl)) continue;
+    for (int nb : s->bucket[nl]) {
+      if (!(s->irefdown[nb] && L.LP(nb, 4) == 1)) continue;
       const int dad = L.LP(nb, 2), s1 = nb, s2 = L.LP(nb, 6), s3 = L.LP(nb, 8);
       const int s4 = L.LP(L.LP(nb, 6), 8);
       if (s->irefdown[s2] && s->irefdown[s3] && s->irefdown[s4]) {
@@ -352,7 +382,9 @@ int w2d_sim_create(const W2dParams* p, const W2dInit* ic, W2dSim** out)
   s->cap = p->nblocks;
   int rc = w2d_create(p, &s->ctx);
   if (rc) { delete s; return rc; }
-  s->lp.assign((size_t)8 * s->cap, 0);
+  s->lp.assign((size_t)8 * (s->cap + 1), 0);
+  s->levbuf.assign((size_t)s->cap, 0);
+  s->bucket.assign((size_t)p->nlevs + 1, std::vector<int32_t>());
   s->leaf.assign((size_t)s->cap, 0);
   s->icoord.assign((size_t)2 * s->cap, 0);
   s->irefup.assign((size_t)s->cap + 1, 0);
@@ -417,7 +449,9 @@ W2dCtx* w2d_sim_ctx(W2dSim* s) { return s ? s->ctx : nullptr; }
 int w2d_sim_tree(W2dSim* s, int32_t* lp, int32_t* leaf, int32_t* icoord, int32_t* innerbounds, int32_t* ninternal)
 {
   if (!s) return W2D_ERR_ARG;
-  if (lp) memcpy(lp, s->lp.data(), sizeof(int32_t) * s->lp.size());
+  if (lp)  // column-major, ld = cap, as the reference's lp(nblocks, 8)
+    for (int k = 1; k <= 8; ++k)
+      for (int nb = 1; nb <= s->cap; ++nb) lp[(size_t)(k - 1) * s->cap + (nb - 1)] = s->LP(nb, k);
   if (leaf) memcpy(leaf, s->leaf.data(), sizeof(int32_t) * s->leaf.size());
   if (icoord) memcpy(icoord, s->icoord.data(), sizeof(int32_t) * s->icoord.size());
   if (s->dirty) locatebounds(s);
@@ -431,6 +465,15 @@ int w2d_sim_set_amr(W2dSim* s, int on)
   if (!s) return W2D_ERR_ARG;
   s->amr = on != 0 && s->p.nlevs > 1;
   return W2D_OK;
+}
+
+int w2d_sim_set_cooltab(W2dSim* s, const double* log_t, const double* neg_log_l, int n)
+{
+  if (!s) return W2D_ERR_ARG;
+  int rc = w2d_set_cooltab(s->ctx, log_t, neg_log_l, n);
+  if (rc) return rc;
+  if (s->dirty && (rc = refresh_plan(s))) return rc;
+  return w2d_calcprim(s->ctx);
 }
 
 }  // extern "C"

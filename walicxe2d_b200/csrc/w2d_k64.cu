@@ -8,19 +8,26 @@ namespace w2d {
 
 const Launchers& launchers64() { return k64::table; }
 
-// src/timestep.f90:48: dt = min(cfl*dtp, 0.4*dtcool*Psc/tsc) over the leaves
-__global__ void __launch_bounds__(1024) k_dt(const int* __restrict__ leaves, int n,
-                                             const double* __restrict__ cfl,
-                                             const double* __restrict__ dtcool, int use_cool,
-                                             double courant, double psc, double tsc,
-                                             double* __restrict__ dt_out)
+// src/timestep.f90:48: dt = min(cfl*dtp, 0.4*dtcool*Psc/tsc), dtp and dtcool
+// the minima of the per-block partials over the leaves.  Each CTA reduces
+// 256 leaves and folds its minima into work[0..1] with 64-bit atomicMin on
+// the bit patterns (for non-negative doubles the integer order is the
+// numeric order); the last CTA to finish forms dt and resets work/count.
+__global__ void __launch_bounds__(256) k_dt(const int* __restrict__ leaves, int n,
+                                            const double* __restrict__ cfl,
+                                            const double* __restrict__ dtcool, int use_cool,
+                                            double courant, double psc, double tsc,
+                                            unsigned long long* __restrict__ work,
+                                            unsigned int* __restrict__ count, double* __restrict__ dt_out)
 {
-  __shared__ double s0[32], s1[32];
+  __shared__ double s0[8], s1[8];
+  __shared__ bool last;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
   double m0 = 1.e30, m1 = 1e30;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+  if (k < n) {
     const int b = leaves[k];
-    m0 = fmin(m0, cfl[b]);
-    if (use_cool) m1 = fmin(m1, dtcool[b]);
+    m0 = cfl[b];
+    if (use_cool) m1 = dtcool[b];
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -30,19 +37,52 @@ __global__ void __launch_bounds__(1024) k_dt(const int* __restrict__ leaves, int
   if ((threadIdx.x & 31) == 0) { s0[threadIdx.x >> 5] = m0; s1[threadIdx.x >> 5] = m1; }
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) { m0 = fmin(m0, s0[w]); m1 = fmin(m1, s1[w]); }
-    m0 = s0[0]; m1 = s1[0];
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) { m0 = fmin(m0, s0[w]); m1 = fmin(m1, s1[w]); }
-    const double a = courant * m0;
-    const double c = 0.4 * m1 * psc / tsc;
+    m0 = s0[0];
+    m1 = s1[0];
+    for (int w = 1; w < 8; ++w) { m0 = fmin(m0, s0[w]); m1 = fmin(m1, s1[w]); }
+    atomicMin(&work[0], (unsigned long long)__double_as_longlong(m0));
+    atomicMin(&work[1], (unsigned long long)__double_as_longlong(m1));
+    __threadfence();
+    last = (atomicAdd(count, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    const double d0 = __longlong_as_double((long long)atomicAdd(&work[0], 0ull));
+    const double d1 = __longlong_as_double((long long)atomicAdd(&work[1], 0ull));
+    const double a = courant * d0;
+    const double c = 0.4 * d1 * psc / tsc;
     dt_out[0] = (a < c) ? a : c;
+    work[0] = work[1] = (unsigned long long)__double_as_longlong(1.e30);
+    *count = 0u;
   }
 }
 
-cudaError_t launch_dt(const int* leaves, int n, const double* cfl, const double* dtcool, int use_cool,
-                      double courant, double psc, double tsc, double* dt_out, cudaStream_t st)
+// level and icoord of new leaves from (slot, level, ix, iy) tuples
+__global__ void k_set_slots(const int* __restrict__ t, int n, int* __restrict__ lev, int* __restrict__ icoord)
 {
-  k_dt<<<1, 1024, 0, st>>>(leaves, n, cfl, dtcool, use_cool, courant, psc, tsc, dt_out);
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) {
+    const int b = t[4 * k];
+    lev[b] = t[4 * k + 1];
+    icoord[2 * b] = t[4 * k + 2];
+    icoord[2 * b + 1] = t[4 * k + 3];
+  }
+}
+
+cudaError_t launch_set_slots(const int* tuples, int n, int* lev, int* icoord, cudaStream_t st)
+{
+  if (n == 0) return cudaSuccess;
+  k_set_slots<<<(n + 127) / 128, 128, 0, st>>>(tuples, n, lev, icoord);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dt(const int* leaves, int n, const double* cfl, const double* dtcool, int use_cool,
+                      double courant, double psc, double tsc, unsigned long long* work, unsigned int* count,
+                      double* dt_out, cudaStream_t st)
+{
+  const int grid = n > 0 ? (n + 255) / 256 : 1;
+  k_dt<<<grid, 256, 0, st>>>(leaves, n, cfl, dtcool, use_cool, courant, psc, tsc, work, count, dt_out);
   return cudaGetLastError();
 }
 

@@ -1,24 +1,30 @@
 // w2d_kernels.cuh -- device kernels of the block update, templated on the
-// arithmetic type R (double: the plain path; float: the FP32 path) and on
-// the number of equations NEQ.
+// arithmetic type R (double: the plain path; float: the FP32 path), on the
+// number of equations NEQ and, for the flux kernels, on the Riemann solver
+// and slope limiter (-1 / -99: chosen at run time from PhysArgs).
 //
 // Pool layout (HBM): block slot b (= the reference's block ID) holds
 // [NEQ][20][20] values, i fastest; cell (i,j), i,j = -1..18, sits at
-// (j+1)*20 + (i+1).  One CTA works on one leaf block per launch.
+// (j+1)*20 + (i+1).  A block is one contiguous 16-byte aligned run, so a
+// CTA pulls its own block into shared memory with one TMA bulk copy.  One
+// CTA works on one leaf block per launch.
 //
 // Ghost cells are addressed by face f (0 left, 1 right, 2 bottom, 3 top),
 // layer g (0 = next to the interior, 1 = outer) and position m = 1..16.
 // The 16 corner cells of each block (both ghost layers in both directions)
-// are neither read nor written by these kernels: no interior or edge-ghost
-// value of the reference depends on them.
+// are neither gathered nor relied on: no interior or edge-ghost value of the
+// reference depends on them.
 #pragma once
 
 #include "w2d_phys.cuh"
+#include "w2d_tma.cuh"
 
 namespace w2d {
 
 #define W2D_MAXLEV 16
 #define W2D_THREADS 288   // 9 warps: 272 interfaces per direction
+
+extern __shared__ __align__(128) unsigned char w2d_smem[];
 
 // face-descriptor kinds (what fills a ghost face in a walk of innerbounds)
 enum FaceKind {
@@ -29,6 +35,8 @@ enum FaceKind {
   FK_RESTRICT = 4,  // two finer neighbours: 2x2 means of their interior
   FK_INJECT = 5,    // coarser neighbour: 0th-order injection
 };
+
+enum { ERR_HLLC = 3, ERR_TIMEOUT = 6 };
 
 struct KArgs {
   void* u;            // R*, pool of conserved variables
@@ -45,9 +53,14 @@ struct KArgs {
   int* err;           // device error word {code, block, i, j}
   const double* cooltab;  // [2][41] DMC table (T, Lambda)
   int nlevs;
-  int bc_lr_reflect;  // unused by kernels (descriptors carry it)
+  int pad_;
   double eta, psc, tempsc_d;
   double dx[W2D_MAXLEV + 1], dy[W2D_MAXLEV + 1];
+};
+
+struct PhysArgs {
+  double cv, gamma, tempsc;
+  int cooling, hllc_compat, solver, limiter;
 };
 
 __device__ __forceinline__ int cidx(int i, int j) { return (j + 1) * W2D_W + (i + 1); }
@@ -60,6 +73,17 @@ __device__ __forceinline__ void ghost_ij(int f, int g, int m, int& i, int& j)
     case 1: i = W2D_NX + 1 + g; j = m; break;
     case 2: i = m; j = -g; break;
     default: i = m; j = W2D_NX + 1 + g; break;
+  }
+}
+
+// Interior source cell of a box face (MIRROR/REFLECT).
+__device__ __forceinline__ void mirror_ij(int f, int g, int m, int& si, int& sj)
+{
+  switch (f) {
+    case 0: si = 1 + g; sj = m; break;
+    case 1: si = W2D_NX - g; sj = m; break;
+    case 2: si = m; sj = 1 + g; break;
+    default: si = m; sj = W2D_NX - g; break;
   }
 }
 
@@ -92,12 +116,7 @@ __device__ __forceinline__ bool face_value(const R* __restrict__ arr, size_t bst
     case FK_MIRROR:
     case FK_REFLECT: {
       int si, sj;
-      switch (f) {
-        case 0: si = 1 + g; sj = m; break;
-        case 1: si = NX - g; sj = m; break;
-        case 2: si = m; sj = 1 + g; break;
-        default: si = m; sj = NX - g; break;
-      }
+      mirror_ij(f, g, m, si, sj);
       R v = arr[(size_t)b * bstride + (size_t)k * W2D_CELLS + cidx(si, sj)];
       if (kind == FK_REFLECT && k == ((f < 2) ? 1 : 2)) v = -v;
       out = v;
@@ -152,25 +171,144 @@ __device__ __forceinline__ bool face_value(const R* __restrict__ arr, size_t bst
   }
 }
 
-template <typename R>
-__device__ __forceinline__ Phys<R> make_phys(const double cv, const double gamma, const double tempsc,
-                                             int cooling, int compat, int solver, int limiter)
+template <typename R, int SOLVER, int LIMITER>
+__device__ __forceinline__ Phys<R> make_phys(const PhysArgs& pa)
 {
   Phys<R> ph;
-  ph.cv = R(cv);
-  ph.gamma = R(gamma);
-  ph.tempsc = R(tempsc);
-  ph.cooling = cooling;
-  ph.hllc_compat = compat;
-  ph.solver = solver;
-  ph.limiter = limiter;
+  ph.cv = R(pa.cv);
+  ph.gamma = R(pa.gamma);
+  ph.tempsc = R(pa.tempsc);
+  ph.cooling = pa.cooling;
+  ph.hllc_compat = pa.hllc_compat;
+  ph.solver = (SOLVER >= 0) ? SOLVER : pa.solver;
+  ph.limiter = (LIMITER >= -1) ? LIMITER : pa.limiter;
   return ph;
 }
 
-struct PhysArgs {
-  double cv, gamma, tempsc;
-  int cooling, hllc_compat, solver, limiter;
-};
+// Pulls block b of pool src (NEQ*400 values) into shared tile dst; every
+// thread returns whether the copy completed (false: timeout recorded).
+template <typename R, int NEQ>
+__device__ __forceinline__ bool load_tile(R* dst, const R* src_block, uint64_t* bar, int* err, int b)
+{
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+  }
+  __syncthreads();
+  constexpr uint32_t bytes = (uint32_t)(NEQ * W2D_CELLS * sizeof(R));
+  if (threadIdx.x == 0) {
+    mbar_arrive_expect(bar, bytes);
+    bulk_g2s(dst, src_block, bytes, bar);
+  }
+  return true;
+}
+
+template <typename R, int NEQ>
+__device__ __forceinline__ bool load_two_tiles(R* d1, const R* s1, R* d2, const R* s2, uint64_t* bar)
+{
+  if (threadIdx.x == 0) mbar_init(bar, 1);
+  __syncthreads();
+  constexpr uint32_t bytes = (uint32_t)(NEQ * W2D_CELLS * sizeof(R));
+  if (threadIdx.x == 0) {
+    mbar_arrive_expect(bar, 2 * bytes);
+    bulk_g2s(d1, s1, bytes, bar);
+    bulk_g2s(d2, s2, bytes, bar);
+  }
+  return true;
+}
+
+// Waits for the tile copies; on timeout records the error and waits once
+// more (bounded) so that no copy is still landing when the CTA exits.
+__device__ __forceinline__ bool wait_tiles(uint64_t* bar, int* err, int b)
+{
+  if (mbar_wait(bar, 0)) return true;
+  if (threadIdx.x == 0) set_err(err, ERR_TIMEOUT, b, -1, -1);
+  mbar_wait(bar, 0);
+  return false;
+}
+
+// src/dmc_module.f90:14-32 on the table cooltab(1:2,1:41) (T row then
+// Lambda row); the index is clamped to the table (the reference reads row 42
+// at T == 1e8 exactly).
+__device__ __forceinline__ double d_cooldmc(const double* __restrict__ tab, double T)
+{
+  if (T > 1e8) return 0.21e-26 * sqrt(T);
+  int if1 = (int)(log10(T) * 10) - 39;
+  if1 = if1 > 40 ? 40 : (if1 < 1 ? 1 : if1);
+  double T0 = tab[if1 - 1], c0 = tab[41 + if1 - 1];
+  double T1 = tab[if1], c1 = tab[41 + if1];
+  return (c1 - c0) * (T - T0) / (T1 - T0) + c0;
+}
+
+// Per-block statistics of a primitive tile (cells 0..17 valid): the CFL
+// partial of timestep (src/timestep.f90:21-47), the criteria maximum
+// (src/criteria.f90:16-50) and, under DMC, the cooling-time limit.  Both
+// reductions divide once per block or per cell instead of per neighbour:
+// for x, y > 0, RN(x/y) is monotone in x and in y, so
+//   min_c RN(dx/(|u|+cs)_c) = RN(dx / max_c (|u|+cs)_c)
+//   max_n RN(|dp_n|/am)     = RN(max_n |dp_n| / am)
+// exactly, and the results equal the reference's.
+template <typename R, int NEQ>
+__device__ __forceinline__ void block_stats(const R (*sp)[W2D_W][W2D_W], const Phys<R>& ph, const KArgs& a,
+                                            const PhysArgs& pa, int b, double* sred)
+{
+  const int tid = threadIdx.x;
+  double au = 0., av = 0., grad = 0., dtc = 1e30;
+  if (tid < 256) {
+    const int i = 1 + tid % 16, j = 1 + tid / 16;
+    const int ti = i + 1, tj = j + 1;
+    const R rho = sp[0][tj][ti], vx = sp[1][tj][ti], vy = sp[2][tj][ti], p = sp[3][tj][ti];
+    const R cs = sound(ph, p, rho);
+    au = (double)(absr(vx) + cs);
+    av = (double)(absr(vy) + cs);
+    const R fl = R(1e-15);
+    const R am = fmaxr(fl, absr(p)), am2 = fmaxr(fl, absr(rho));
+    R dp = absr(sp[3][tj][ti + 1] - p);
+    dp = fmaxr(dp, absr(sp[3][tj][ti - 1] - p));
+    dp = fmaxr(dp, absr(sp[3][tj + 1][ti] - p));
+    dp = fmaxr(dp, absr(sp[3][tj - 1][ti] - p));
+    R dr = absr(sp[0][tj][ti + 1] - rho);
+    dr = fmaxr(dr, absr(sp[0][tj][ti - 1] - rho));
+    dr = fmaxr(dr, absr(sp[0][tj + 1][ti] - rho));
+    dr = fmaxr(dr, absr(sp[0][tj - 1][ti] - rho));
+    grad = (double)fmaxr(dp / am, dr / am2);
+    if (pa.cooling == COOL_DMC) {                    // src/timestep.f90:34-41
+      const double T = ((double)p / (double)rho) * pa.tempsc;
+      if (T > 1e4) {
+        const double aloss = d_cooldmc(a.cooltab, T) * ((double)rho * (double)rho);
+        dtc = pa.cv * (double)p / aloss;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    au = fmax(au, __shfl_xor_sync(0xffffffffu, au, o));
+    av = fmax(av, __shfl_xor_sync(0xffffffffu, av, o));
+    grad = fmax(grad, __shfl_xor_sync(0xffffffffu, grad, o));
+    dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
+  }
+  if ((tid & 31) == 0) {
+    sred[tid >> 5] = au;
+    sred[16 + (tid >> 5)] = av;
+    sred[32 + (tid >> 5)] = grad;
+    sred[48 + (tid >> 5)] = dtc;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double m0 = sred[0], m1 = sred[16], m2 = sred[32], m3 = sred[48];
+    for (int w = 1; w < W2D_THREADS / 32; ++w) {
+      m0 = fmax(m0, sred[w]);
+      m1 = fmax(m1, sred[16 + w]);
+      m2 = fmax(m2, sred[32 + w]);
+      m3 = fmin(m3, sred[48 + w]);
+    }
+    const int lev = a.lev[b];
+    const R t1 = R(a.dx[lev]) / R(m0);
+    const R t2 = R(a.dy[lev]) / R(m1);
+    a.cfl[b] = (double)fminr(t1, t2);
+    a.grad[b] = m2;
+    if (pa.cooling == COOL_DMC) a.dtcool[b] = m3;
+  }
+}
 
 // ---------------------------------------------------------------------------
 // Half step: src/tstep.f90:22-46 -- hllcfluxes(nb,1) from primit (cells
@@ -178,42 +316,49 @@ struct PhysArgs {
 // COOLINGH, where primit == calcprim(u) at step start) or from the stored
 // primit (COOLINGDMC).
 template <typename R, int NEQ>
+__host__ __device__ constexpr size_t smem_half()
+{
+  return 128 + sizeof(R) * (NEQ * W2D_CELLS + W2D_CELLS + 2 * NEQ * 272);
+}
+
+template <typename R, int NEQ, int SOLVER>
 __global__ void __launch_bounds__(W2D_THREADS) k_half(KArgs a, PhysArgs pa, double dt)
 {
-  __shared__ R sp[NEQ][18][18];
-  __shared__ R scs[18][18];
-  __shared__ R sf[NEQ][16][17];
-  __shared__ R sg[NEQ][17][16];
-  const Phys<R> ph = make_phys<R>(pa.cv, pa.gamma, pa.tempsc, pa.cooling, pa.hllc_compat,
-                                  pa.solver, pa.limiter);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
+  R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
+  R(*scs)[W2D_W] = reinterpret_cast<R(*)[W2D_W]>(w2d_smem + 128 + sizeof(R) * NEQ * W2D_CELLS);
+  R(*sf)[16][17] = reinterpret_cast<R(*)[16][17]>(w2d_smem + 128 + sizeof(R) * (NEQ + 1) * W2D_CELLS);
+  R(*sg)[17][16] = reinterpret_cast<R(*)[17][16]>(w2d_smem + 128 + sizeof(R) * ((NEQ + 1) * W2D_CELLS + NEQ * 272));
+  const Phys<R> ph = make_phys<R, SOLVER, -1>(pa);
   const int b = a.leaves[blockIdx.x];
   const int tid = threadIdx.x;
   const size_t bs = (size_t)NEQ * W2D_CELLS;
   const R* __restrict__ u = (const R*)a.u + (size_t)b * bs;
   R* __restrict__ up = (R*)a.up + (size_t)b * bs;
+  const bool dmc = pa.cooling == COOL_DMC;
+  load_tile<R, NEQ>(&st[0][0][0], dmc ? (const R*)a.prim + (size_t)b * bs : u, bar, a.err, b);
   const int lev = a.lev[b];
   const double dtm = dt / 2.;
   const R dtdx = R(dtm / a.dx[lev]);
   const R dtdy = R(dtm / a.dy[lev]);
+  if (!wait_tiles(bar, a.err, b)) return;
 
-  // primitives and sound speed of cells 0..17 (corners skipped)
-  const R* __restrict__ src = (pa.cooling == COOL_DMC) ? (const R*)a.prim + (size_t)b * bs : u;
+  // primitives (in place) and sound speed of cells 0..17 (corners skipped)
   for (int c = tid; c < 18 * 18; c += W2D_THREADS) {
-    const int wi = c % 18, wj = c / 18;
-    if ((wi == 0 || wi == 17) && (wj == 0 || wj == 17)) continue;
+    const int ti = 1 + c % 18, tj = 1 + c / 18;
+    if ((ti == 1 || ti == 18) && (tj == 1 || tj == 18)) continue;
     R q[NEQ];
-    if (pa.cooling == COOL_DMC) {
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) q[k] = src[k * W2D_CELLS + cidx(wi, wj)];
-    } else {
+    for (int k = 0; k < NEQ; ++k) q[k] = st[k][tj][ti];
+    if (!dmc) {
       R uu[NEQ], T;
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) uu[k] = src[k * W2D_CELLS + cidx(wi, wj)];
+      for (int k = 0; k < NEQ; ++k) uu[k] = q[k];
       uprim<NEQ>(ph, q, uu, T);
-    }
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) sp[k][wj][wi] = q[k];
-    scs[wj][wi] = sound(ph, q[3], q[0]);
+      for (int k = 0; k < NEQ; ++k) st[k][tj][ti] = q[k];
+    }
+    scs[tj][ti] = sound(ph, q[3], q[0]);
   }
   __syncthreads();
 
@@ -222,18 +367,18 @@ __global__ void __launch_bounds__(W2D_THREADS) k_half(KArgs a, PhysArgs pa, doub
     {  // x interface between (i,j) and (i+1,j)
       const int i = tid % 17, j = 1 + tid / 17;
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) { pl[k] = sp[k][j][i]; pr[k] = sp[k][j][i + 1]; }
-      if (!riemann<NEQ>(ph, pl, pr, scs[j][i], scs[j][i + 1], ff)) set_err(a.err, 3, b, i, j);
+      for (int k = 0; k < NEQ; ++k) { pl[k] = st[k][j + 1][i + 1]; pr[k] = st[k][j + 1][i + 2]; }
+      if (!riemann<NEQ>(ph, pl, pr, scs[j + 1][i + 1], scs[j + 1][i + 2], ff)) set_err(a.err, ERR_HLLC, b, i, j);
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) sf[k][j - 1][i] = ff[k];
     }
     {  // y interface between (i,j) and (i,j+1), states swapped (swapy)
       const int i = 1 + tid % 16, j = tid / 16;
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) { pl[k] = sp[k][j][i]; pr[k] = sp[k][j + 1][i]; }
+      for (int k = 0; k < NEQ; ++k) { pl[k] = st[k][j + 1][i + 1]; pr[k] = st[k][j + 2][i + 1]; }
       R t = pl[1]; pl[1] = pl[2]; pl[2] = t;
       t = pr[1]; pr[1] = pr[2]; pr[2] = t;
-      if (!riemann<NEQ>(ph, pl, pr, scs[j][i], scs[j + 1][i], ff)) set_err(a.err, 3, b, i, j);
+      if (!riemann<NEQ>(ph, pl, pr, scs[j + 1][i + 1], scs[j + 2][i + 1], ff)) set_err(a.err, ERR_HLLC, b, i, j);
       t = ff[1]; ff[1] = ff[2]; ff[2] = t;
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) sg[k][j][i - 1] = ff[k];
@@ -258,79 +403,70 @@ __global__ void __launch_bounds__(W2D_THREADS) k_half(KArgs a, PhysArgs pa, doub
 // fluxes of hllcfluxes(nb,2), step(nb,dt), viscosity and u(interior) = up:
 // src/tstep.f90:53-88.
 template <typename R, int NEQ>
+__host__ __device__ constexpr size_t smem_full()
+{
+  return 128 + sizeof(R) * (2 * NEQ * W2D_CELLS + 2 * NEQ * 272);
+}
+
+template <typename R, int NEQ, int SOLVER, int LIMITER>
 __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, double dt)
 {
-  __shared__ R st[NEQ][W2D_W][W2D_W];   // up tile, then primitives
-  __shared__ R sf[NEQ][16][17];
-  __shared__ R sg[NEQ][17][16];
-  const Phys<R> ph = make_phys<R>(pa.cv, pa.gamma, pa.tempsc, pa.cooling, pa.hllc_compat,
-                                  pa.solver, pa.limiter);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
+  R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
+  R(*so)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128 + sizeof(R) * NEQ * W2D_CELLS);
+  R(*sf)[16][17] = reinterpret_cast<R(*)[16][17]>(w2d_smem + 128 + sizeof(R) * 2 * NEQ * W2D_CELLS);
+  R(*sg)[17][16] = reinterpret_cast<R(*)[17][16]>(w2d_smem + 128 + sizeof(R) * (2 * NEQ * W2D_CELLS + NEQ * 272));
+  const Phys<R> ph = make_phys<R, SOLVER, LIMITER>(pa);
   const int li = blockIdx.x;
   const int b = a.leaves[li];
   const int tid = threadIdx.x;
   const size_t bs = (size_t)NEQ * W2D_CELLS;
   const R* __restrict__ upool = (const R*)a.up;
   R* __restrict__ u = (R*)a.u + (size_t)b * bs;
-  const R* __restrict__ upb = upool + (size_t)b * bs;
+  load_two_tiles<R, NEQ>(&st[0][0][0], upool + (size_t)b * bs, &so[0][0][0], u, bar);
   const int lev = a.lev[b];
   const R dtdx = R(dt / a.dx[lev]);
   const R dtdy = R(dt / a.dy[lev]);
   const bool visc = lev >= (a.nlevs - 1);
   const R eta = R(a.eta);
 
-  // interior of up
-  for (int c = tid; c < NEQ * 256; c += W2D_THREADS) {
-    const int k = c / 256, r = c % 256, i = 1 + r % 16, j = 1 + r / 16;
-    st[k][j + 1][i + 1] = upb[k * W2D_CELLS + cidx(i, j)];
-  }
-  // ghosts from the neighbours (remote kinds)
+  // ghosts gathered from the neighbours while the tiles land
   int2 dface[4];
 #pragma unroll
   for (int f = 0; f < 4; ++f) dface[f] = a.fd[li * 4 + f];
+  R gv[NEQ];
+  const int gf = tid / 32, gg = (tid / 16) % 2, gm = 1 + tid % 16;
+  int gkind = FK_KEEP;
   if (tid < 128) {
-    const int f = tid / 32, g = (tid / 16) % 2, m = 1 + tid % 16;
-    int i, j;
-    ghost_ij(f, g, m, i, j);
-    const int kind = dface[f].y & 0xff;
-    if (kind >= FK_SAME) {
+    gkind = dface[gf].y & 0xff;
+    if (gkind >= FK_SAME) {
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) {
-        R v;
-        face_value<R>(upool, bs, b, dface[f], f, g, m, k, v);
-        st[k][j + 1][i + 1] = v;
-      }
-    } else if (kind == FK_KEEP) {
-#pragma unroll
-      for (int k = 0; k < NEQ; ++k) st[k][j + 1][i + 1] = upb[k * W2D_CELLS + cidx(i, j)];
+      for (int k = 0; k < NEQ; ++k) face_value<R>(upool, bs, b, dface[gf], gf, gg, gm, k, gv[k]);
     }
   }
-  __syncthreads();
-  if (tid < 128) {  // box faces read the block's own interior
-    const int f = tid / 32, g = (tid / 16) % 2, m = 1 + tid % 16;
+  if (!wait_tiles(bar, a.err, b)) return;
+  if (tid < 128 && gkind >= FK_SAME) {
     int i, j;
-    ghost_ij(f, g, m, i, j);
-    const int kind = dface[f].y & 0xff;
-    if (kind == FK_MIRROR || kind == FK_REFLECT) {
-      int si, sj;
-      switch (f) {
-        case 0: si = 1 + g; sj = m; break;
-        case 1: si = W2D_NX - g; sj = m; break;
-        case 2: si = m; sj = 1 + g; break;
-        default: si = m; sj = W2D_NX - g; break;
-      }
+    ghost_ij(gf, gg, gm, i, j);
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) {
-        R v = st[k][sj + 1][si + 1];
-        if (kind == FK_REFLECT && k == ((f < 2) ? 1 : 2)) v = -v;
-        st[k][j + 1][i + 1] = v;
-      }
+    for (int k = 0; k < NEQ; ++k) st[k][j + 1][i + 1] = gv[k];
+  }
+  __syncthreads();
+  if (tid < 128 && (gkind == FK_MIRROR || gkind == FK_REFLECT)) {  // box faces: own interior
+    int i, j, si, sj;
+    ghost_ij(gf, gg, gm, i, j);
+    mirror_ij(gf, gg, gm, si, sj);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) {
+      R v = st[k][sj + 1][si + 1];
+      if (gkind == FK_REFLECT && k == ((gf < 2) ? 1 : 2)) v = -v;
+      st[k][j + 1][i + 1] = v;
     }
   }
   __syncthreads();
 
-  // u ghosts = up ghosts (u = up, src/tstep.f90:85), then calcprim(up).
-  // Only the outer layer is stored here: layer 0 of u still feeds the
-  // viscosity below and is stored after it.
+  // u ghosts = up ghosts (u = up, src/tstep.f90:85; the old u stays in so),
+  // then calcprim(up) in place
   R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;
   for (int c = tid; c < W2D_CELLS; c += W2D_THREADS) {
     const int ti = c % W2D_W, tj = c / W2D_W;
@@ -339,7 +475,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
     R uu[NEQ], q[NEQ], T;
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) uu[k] = st[k][tj][ti];
-    if (ti == 0 || ti == 19 || tj == 0 || tj == 19) {
+    if (gx || gy) {
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) u[k * W2D_CELLS + c] = uu[k];
     }
@@ -366,7 +502,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
         limit1<R>(ph.limiter, pll[k], pl[k], pr[k], prr[k]);
       }
       R csl = sound(ph, pl[3], pl[0]), csr = sound(ph, pr[3], pr[0]);
-      if (!riemann<NEQ>(ph, pl, pr, csl, csr, ff)) set_err(a.err, 3, b, i, j);
+      if (!riemann<NEQ>(ph, pl, pr, csl, csr, ff)) set_err(a.err, ERR_HLLC, b, i, j);
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) sf[k][j - 1][i] = ff[k];
     }
@@ -383,7 +519,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
       R t = pl[1]; pl[1] = pl[2]; pl[2] = t;
       t = pr[1]; pr[1] = pr[2]; pr[2] = t;
       R csl = sound(ph, pl[3], pl[0]), csr = sound(ph, pr[3], pr[0]);
-      if (!riemann<NEQ>(ph, pl, pr, csl, csr, ff)) set_err(a.err, 3, b, i, j);
+      if (!riemann<NEQ>(ph, pl, pr, csl, csr, ff)) set_err(a.err, ERR_HLLC, b, i, j);
       t = ff[1]; ff[1] = ff[2]; ff[2] = t;
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) sg[k][j][i - 1] = ff[k];
@@ -391,34 +527,16 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
   }
   __syncthreads();
 
-  // step(nb,dt) + viscosity, src/step.f90:31-32, src/viscosity.f90:15-21
-  R unew[NEQ];
+  // step(nb,dt) + viscosity from the old u, src/step.f90:31-32, src/viscosity.f90:15-21
   if (tid < 256) {
     const int i = 1 + tid % 16, j = 1 + tid / 16;
+    const int ti = i + 1, tj = j + 1;
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) {
-      const R* uk = u + k * W2D_CELLS;
-      const R uo = uk[cidx(i, j)];
+      const R uo = so[k][tj][ti];
       R v = uo - dtdx * (sf[k][j - 1][i] - sf[k][j - 1][i - 1]) - dtdy * (sg[k][j][i - 1] - sg[k][j - 1][i - 1]);
       if (visc)
-        v = v + eta * (uk[cidx(i + 1, j)] + uk[cidx(i - 1, j)] + uk[cidx(i, j + 1)] + uk[cidx(i, j - 1)] - R(4.) * uo);
-      unew[k] = v;
-    }
-  }
-  __syncthreads();
-  if (tid < 256) {
-    const int i = 1 + tid % 16, j = 1 + tid / 16;
-#pragma unroll
-    for (int k = 0; k < NEQ; ++k) u[k * W2D_CELLS + cidx(i, j)] = unew[k];
-  }
-  if (tid < 64) {  // layer 0 of u = layer 0 of the filled up (u = up)
-    const int f = tid / 16, m = 1 + tid % 16;
-    int i, j;
-    ghost_ij(f, 0, m, i, j);
-#pragma unroll
-    for (int k = 0; k < NEQ; ++k) {
-      R v;
-      if (!face_value<R>(upool, bs, b, dface[f], f, 0, m, k, v)) v = upb[k * W2D_CELLS + cidx(i, j)];
+        v = v + eta * (so[k][tj][ti + 1] + so[k][tj][ti - 1] + so[k][tj + 1][ti] + so[k][tj - 1][ti] - R(4.) * uo);
       u[k * W2D_CELLS + cidx(i, j)] = v;
     }
   }
@@ -427,166 +545,102 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
 // ---------------------------------------------------------------------------
 // Fill of layer 0 of u: the non-MPI walk of src/boundaryI.f90:34-396 as
 // per-face last writers.  With stats != 0 (ADIABATIC) it also computes,
-// from calcprim(u) of the filled block, the CFL partial of timestep
-// (src/timestep.f90:21-47) and the criteria maximum (src/criteria.f90:16-50).
+// from calcprim(u) of the filled block, the CFL partial of timestep and the
+// criteria maximum.
+template <typename R, int NEQ>
+__host__ __device__ constexpr size_t smem_fill1()
+{
+  return 128 + sizeof(R) * NEQ * W2D_CELLS + 64 * sizeof(double);
+}
+
 template <typename R, int NEQ>
 __global__ void __launch_bounds__(W2D_THREADS) k_fill1(KArgs a, PhysArgs pa, int stats)
 {
-  __shared__ R sp[NEQ][18][18];
-  __shared__ double sred[2][W2D_THREADS / 32];
-  const Phys<R> ph = make_phys<R>(pa.cv, pa.gamma, pa.tempsc, pa.cooling, pa.hllc_compat,
-                                  pa.solver, pa.limiter);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
+  R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
+  double* sred = reinterpret_cast<double*>(w2d_smem + 128 + sizeof(R) * NEQ * W2D_CELLS);
+  const Phys<R> ph = make_phys<R, -1, -1>(pa);
   const int li = blockIdx.x;
   const int b = a.leaves[li];
   const int tid = threadIdx.x;
   const size_t bs = (size_t)NEQ * W2D_CELLS;
   R* __restrict__ upool = (R*)a.u;
   R* __restrict__ u = upool + (size_t)b * bs;
-
+  if (stats) load_tile<R, NEQ>(&st[0][0][0], u, bar, a.err, b);
+  R gv[NEQ];
+  bool w = false;
+  int gi = 0, gj = 0;
   if (tid < 64) {
     const int f = tid / 16, m = 1 + tid % 16;
-    int i, j;
-    ghost_ij(f, 0, m, i, j);
+    ghost_ij(f, 0, m, gi, gj);
     const int2 d = a.fd[li * 4 + f];
-    R vals[NEQ];
-    bool w = false;
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) w = face_value<R>(upool, bs, b, d, f, 0, m, k, vals[k]);
+    for (int k = 0; k < NEQ; ++k) w = face_value<R>(upool, bs, b, d, f, 0, m, k, gv[k]);
     if (w) {
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) u[k * W2D_CELLS + cidx(i, j)] = vals[k];
-    } else {
-#pragma unroll
-      for (int k = 0; k < NEQ; ++k) vals[k] = u[k * W2D_CELLS + cidx(i, j)];
-    }
-    if (stats) {
-      R q[NEQ], T;
-      uprim<NEQ>(ph, q, vals, T);
-#pragma unroll
-      for (int k = 0; k < NEQ; ++k) sp[k][j][i] = q[k];
+      for (int k = 0; k < NEQ; ++k) u[k * W2D_CELLS + cidx(gi, gj)] = gv[k];
     }
   }
   if (!stats) return;
-  for (int c = tid; c < 256; c += W2D_THREADS) {
-    const int i = 1 + c % 16, j = 1 + c / 16;
+  if (!wait_tiles(bar, a.err, b)) return;
+  if (tid < 64 && w) {
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) st[k][gj + 1][gi + 1] = gv[k];
+  }
+  __syncthreads();
+  for (int c = tid; c < 18 * 18; c += W2D_THREADS) {   // calcprim of cells 0..17
+    const int ti = 1 + c % 18, tj = 1 + c / 18;
+    if ((ti == 1 || ti == 18) && (tj == 1 || tj == 18)) continue;
     R uu[NEQ], q[NEQ], T;
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) uu[k] = u[k * W2D_CELLS + cidx(i, j)];
+    for (int k = 0; k < NEQ; ++k) uu[k] = st[k][tj][ti];
     uprim<NEQ>(ph, q, uu, T);
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) sp[k][j][i] = q[k];
+    for (int k = 0; k < NEQ; ++k) st[k][tj][ti] = q[k];
   }
   __syncthreads();
-  const int lev = a.lev[b];
-  double dtp = 1e30, grad = 0.;
-  if (tid < 256) {
-    const int i = 1 + tid % 16, j = 1 + tid / 16;
-    const R rho = sp[0][j][i], vx = sp[1][j][i], vy = sp[2][j][i], p = sp[3][j][i];
-    const R cs = sound(ph, p, rho);
-    const R dxl = R(a.dx[lev]), dyl = R(a.dy[lev]);
-    R t1 = dxl / (absr(vx) + cs);
-    R t2 = dyl / (absr(vy) + cs);
-    dtp = (double)fminr(t1, t2);
-    const R fl = R(1e-15);
-    const R am = fmaxr(fl, absr(p)), am2 = fmaxr(fl, absr(rho));
-    R gr = R(0.);
-    gr = fmaxr(gr, absr(sp[3][j][i + 1] - p) / am);
-    gr = fmaxr(gr, absr(sp[3][j][i - 1] - p) / am);
-    gr = fmaxr(gr, absr(sp[3][j + 1][i] - p) / am);
-    gr = fmaxr(gr, absr(sp[3][j - 1][i] - p) / am);
-    gr = fmaxr(gr, absr(sp[0][j][i + 1] - rho) / am2);
-    gr = fmaxr(gr, absr(sp[0][j][i - 1] - rho) / am2);
-    gr = fmaxr(gr, absr(sp[0][j + 1][i] - rho) / am2);
-    gr = fmaxr(gr, absr(sp[0][j - 1][i] - rho) / am2);
-    grad = (double)gr;
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    dtp = fmin(dtp, __shfl_xor_sync(0xffffffffu, dtp, o));
-    grad = fmax(grad, __shfl_xor_sync(0xffffffffu, grad, o));
-  }
-  if ((tid & 31) == 0) { sred[0][tid >> 5] = dtp; sred[1][tid >> 5] = grad; }
-  __syncthreads();
-  if (tid == 0) {
-    double m0 = sred[0][0], m1 = sred[1][0];
-    for (int w = 1; w < W2D_THREADS / 32; ++w) { m0 = fmin(m0, sred[0][w]); m1 = fmax(m1, sred[1][w]); }
-    a.cfl[b] = m0;
-    a.grad[b] = m1;
-  }
+  block_stats<R, NEQ>(st, ph, a, pa, b, sred);
 }
 
 // ---------------------------------------------------------------------------
-// Per-block primitives of all 400 cells (stored when DMC), CFL partial and
-// criteria of the block as it stands: calcprim (src/calcprim.f90:5-21) plus
-// the per-block parts of timestep and criteria.  Used after the pool was
-// set from the host and after standalone fills.
+// calcprim (src/calcprim.f90:5-21) of whole blocks (stored when DMC) and
+// their per-block statistics, for the blocks of `list`.  Used after the pool
+// was set from the host, after refine/coarse and after standalone fills.
+template <typename R, int NEQ>
+__host__ __device__ constexpr size_t smem_calcprim()
+{
+  return 128 + sizeof(R) * NEQ * W2D_CELLS + 64 * sizeof(double);
+}
+
 template <typename R, int NEQ>
 __global__ void __launch_bounds__(W2D_THREADS) k_calcprim(KArgs a, PhysArgs pa, const int* __restrict__ list, int n)
 {
-  __shared__ R sp[NEQ][18][18];
-  __shared__ double sred[3][W2D_THREADS / 32];
-  const Phys<R> ph = make_phys<R>(pa.cv, pa.gamma, pa.tempsc, pa.cooling, pa.hllc_compat,
-                                  pa.solver, pa.limiter);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
+  R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
+  double* sred = reinterpret_cast<double*>(w2d_smem + 128 + sizeof(R) * NEQ * W2D_CELLS);
+  const Phys<R> ph = make_phys<R, -1, -1>(pa);
   const int b = list[blockIdx.x];
   const int tid = threadIdx.x;
   const size_t bs = (size_t)NEQ * W2D_CELLS;
   const R* __restrict__ u = (const R*)a.u + (size_t)b * bs;
   R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;
+  load_tile<R, NEQ>(&st[0][0][0], u, bar, a.err, b);
+  if (!wait_tiles(bar, a.err, b)) return;
   for (int c = tid; c < W2D_CELLS; c += W2D_THREADS) {
     const int ti = c % W2D_W, tj = c / W2D_W;
     R uu[NEQ], q[NEQ], T;
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) uu[k] = u[k * W2D_CELLS + c];
+    for (int k = 0; k < NEQ; ++k) uu[k] = st[k][tj][ti];
     uprim<NEQ>(ph, q, uu, T);
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) st[k][tj][ti] = q[k];
     if (pb) {
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) pb[k * W2D_CELLS + c] = q[k];
     }
-    if (ti >= 1 && ti <= 18 && tj >= 1 && tj <= 18) {
-#pragma unroll
-      for (int k = 0; k < NEQ; ++k) sp[k][tj - 1][ti - 1] = q[k];
-    }
   }
   __syncthreads();
-  const int lev = a.lev[b];
-  double dtp = 1e30, grad = 0., dtc = 1e30;
-  if (tid < 256) {
-    const int i = 1 + tid % 16, j = 1 + tid / 16;
-    const R rho = sp[0][j][i], vx = sp[1][j][i], vy = sp[2][j][i], p = sp[3][j][i];
-    const R cs = sound(ph, p, rho);
-    R t1 = R(a.dx[lev]) / (absr(vx) + cs);
-    R t2 = R(a.dy[lev]) / (absr(vy) + cs);
-    dtp = (double)fminr(t1, t2);
-    const R fl = R(1e-15);
-    const R am = fmaxr(fl, absr(p)), am2 = fmaxr(fl, absr(rho));
-    R gr = R(0.);
-    gr = fmaxr(gr, absr(sp[3][j][i + 1] - p) / am);
-    gr = fmaxr(gr, absr(sp[3][j][i - 1] - p) / am);
-    gr = fmaxr(gr, absr(sp[3][j + 1][i] - p) / am);
-    gr = fmaxr(gr, absr(sp[3][j - 1][i] - p) / am);
-    gr = fmaxr(gr, absr(sp[0][j][i + 1] - rho) / am2);
-    gr = fmaxr(gr, absr(sp[0][j][i - 1] - rho) / am2);
-    gr = fmaxr(gr, absr(sp[0][j + 1][i] - rho) / am2);
-    gr = fmaxr(gr, absr(sp[0][j - 1][i] - rho) / am2);
-    grad = (double)gr;
-    if (pa.cooling == COOL_DMC) dtc = 1e30;  // filled by the cooling kernel
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    dtp = fmin(dtp, __shfl_xor_sync(0xffffffffu, dtp, o));
-    grad = fmax(grad, __shfl_xor_sync(0xffffffffu, grad, o));
-    dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
-  }
-  if ((tid & 31) == 0) { sred[0][tid >> 5] = dtp; sred[1][tid >> 5] = grad; sred[2][tid >> 5] = dtc; }
-  __syncthreads();
-  if (tid == 0) {
-    double m0 = sred[0][0], m1 = sred[1][0], m2 = sred[2][0];
-    for (int w = 1; w < W2D_THREADS / 32; ++w) {
-      m0 = fmin(m0, sred[0][w]); m1 = fmax(m1, sred[1][w]); m2 = fmin(m2, sred[2][w]);
-    }
-    a.cfl[b] = m0;
-    a.grad[b] = m1;
-  }
+  block_stats<R, NEQ>(st, ph, a, pa, b, sred);
 }
 
 // ---------------------------------------------------------------------------
@@ -649,25 +703,19 @@ __global__ void __launch_bounds__(256) k_coarse(R* __restrict__ u, const int* __
     const int i = r % W2D_W - 1, j = r / W2D_W - 1;
     const bool gx = (i < 1 || i > NX), gy = (j < 1 || j > NX);
     int son, i1, j1;
+    const int sx = (i > H), sy = (j > H);
+    son = 1 + sx + 2 * sy;
     if (!gx && !gy) {                       // interior, :32-51
-      const int sx = (i > H), sy = (j > H);
-      son = 1 + sx + 2 * sy;
       i1 = 2 * (i - sx * H) - 1;
       j1 = 2 * (j - sy * H) - 1;
-    } else if (gx && gy) {                  // corners, :108-159
+    } else if (gx && gy) {                  // inner corners only, :108-159
       if (!((i == 0 || i == NX + 1) && (j == 0 || j == NX + 1))) continue;
-      const int sx = (i > H), sy = (j > H);
-      son = 1 + sx + 2 * sy;
       i1 = sx ? NX + 1 : -1;
       j1 = sy ? NX + 1 : -1;
     } else if (gx) {                        // left/right ghosts, :112-138
-      const int sx = (i > H), sy = (j > H);
-      son = 1 + sx + 2 * sy;
       i1 = sx ? NX + 1 : -1;
       j1 = 2 * (j - sy * H) - 1;
     } else {                                // bottom/top ghosts, :144-170
-      const int sx = (i > H), sy = (j > H);
-      son = 1 + sx + 2 * sy;
       i1 = 2 * (i - sx * H) - 1;
       j1 = sy ? NX + 1 : -1;
     }
@@ -680,15 +728,6 @@ __global__ void __launch_bounds__(256) k_coarse(R* __restrict__ u, const int* __
     du[c] = R(0.25) * t;
   }
 }
-
-// ---------------------------------------------------------------------------
-// timestep reduction over the leaves: dt = min(cfl*dtp, 0.4*dtcool*Psc/tsc),
-// src/timestep.f90:48
-__global__ void __launch_bounds__(1024) k_dt(const int* __restrict__ leaves, int n,
-                                             const double* __restrict__ cfl,
-                                             const double* __restrict__ dtcool, int use_cool,
-                                             double courant, double psc, double tsc,
-                                             double* __restrict__ dt_out);
 
 // pool <-> staging (block-major) copies
 template <typename R>

@@ -1,6 +1,10 @@
 // w2d_kinst.cuh -- launcher table for one arithmetic type R.  Included once
 // by w2d_k64.cu (R = double, built with --fmad=false) and once by
 // w2d_k32.cu (R = float).
+//
+// The flux kernels exist in specialized forms for the solver/limiter pairs
+// of the reference's setups (HLLC with minmod, HLLC with van Leer) and in a
+// generic form that switches at run time.
 #pragma once
 
 #include "w2d_cool.cuh"
@@ -11,33 +15,85 @@ namespace W2D_INST_NS {
 
 using R = W2D_INST_REAL;
 
-#define W2D_NEQ_SWITCH(neq, CALL)             \
-  switch (neq) {                              \
+#define W2D_NEQ_SWITCH(neq, CALL)                   \
+  switch (neq) {                                    \
     case 4: { constexpr int NEQ = 4; CALL; } break; \
     case 5: { constexpr int NEQ = 5; CALL; } break; \
     case 6: { constexpr int NEQ = 6; CALL; } break; \
-    default: return cudaErrorInvalidValue;    \
+    default: return cudaErrorInvalidValue;          \
   }
+
+// Opts a kernel into more than 48 KB of dynamic shared memory (once).
+template <typename K>
+static cudaError_t smem_opt_in(K kernel, size_t bytes, bool& done)
+{
+  if (done || bytes <= 48 * 1024) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) done = true;
+  return e;
+}
+
+template <int NEQ, int S>
+static cudaError_t half_t(const KArgs& a, const PhysArgs& pa, double dt, cudaStream_t st)
+{
+  static bool done = false;
+  constexpr size_t sm = smem_half<R, NEQ>();
+  cudaError_t e = smem_opt_in(k_half<R, NEQ, S>, sm, done);
+  if (e != cudaSuccess) return e;
+  k_half<R, NEQ, S><<<a.nleaf, W2D_THREADS, sm, st>>>(a, pa, dt);
+  return cudaGetLastError();
+}
 
 static cudaError_t half(int neq, const KArgs& a, const PhysArgs& pa, double dt, cudaStream_t st)
 {
   if (a.nleaf == 0) return cudaSuccess;
-  W2D_NEQ_SWITCH(neq, (k_half<R, NEQ><<<a.nleaf, W2D_THREADS, 0, st>>>(a, pa, dt)));
+  if (pa.solver == SOLVER_HLLC) {
+    W2D_NEQ_SWITCH(neq, return (half_t<NEQ, SOLVER_HLLC>(a, pa, dt, st)));
+  }
+  W2D_NEQ_SWITCH(neq, return (half_t<NEQ, -1>(a, pa, dt, st)));
+  return cudaSuccess;
+}
+
+template <int NEQ, int S, int L>
+static cudaError_t full_t(const KArgs& a, const PhysArgs& pa, double dt, cudaStream_t st)
+{
+  static bool done = false;
+  constexpr size_t sm = smem_full<R, NEQ>();
+  cudaError_t e = smem_opt_in(k_full<R, NEQ, S, L>, sm, done);
+  if (e != cudaSuccess) return e;
+  k_full<R, NEQ, S, L><<<a.nleaf, W2D_THREADS, sm, st>>>(a, pa, dt);
   return cudaGetLastError();
 }
 
 static cudaError_t full(int neq, const KArgs& a, const PhysArgs& pa, double dt, cudaStream_t st)
 {
   if (a.nleaf == 0) return cudaSuccess;
-  W2D_NEQ_SWITCH(neq, (k_full<R, NEQ><<<a.nleaf, W2D_THREADS, 0, st>>>(a, pa, dt)));
+  if (pa.solver == SOLVER_HLLC && pa.limiter == 1) {
+    W2D_NEQ_SWITCH(neq, return (full_t<NEQ, SOLVER_HLLC, 1>(a, pa, dt, st)));
+  }
+  if (pa.solver == SOLVER_HLLC && pa.limiter == 2) {
+    W2D_NEQ_SWITCH(neq, return (full_t<NEQ, SOLVER_HLLC, 2>(a, pa, dt, st)));
+  }
+  W2D_NEQ_SWITCH(neq, return (full_t<NEQ, -1, -99>(a, pa, dt, st)));
+  return cudaSuccess;
+}
+
+template <int NEQ>
+static cudaError_t fill1_t(const KArgs& a, const PhysArgs& pa, int stats, cudaStream_t st)
+{
+  static bool done = false;
+  constexpr size_t sm = smem_fill1<R, NEQ>();
+  cudaError_t e = smem_opt_in(k_fill1<R, NEQ>, sm, done);
+  if (e != cudaSuccess) return e;
+  k_fill1<R, NEQ><<<a.nleaf, W2D_THREADS, sm, st>>>(a, pa, stats);
   return cudaGetLastError();
 }
 
 static cudaError_t fill1(int neq, const KArgs& a, const PhysArgs& pa, int stats, cudaStream_t st)
 {
   if (a.nleaf == 0) return cudaSuccess;
-  W2D_NEQ_SWITCH(neq, (k_fill1<R, NEQ><<<a.nleaf, W2D_THREADS, 0, st>>>(a, pa, stats)));
-  return cudaGetLastError();
+  W2D_NEQ_SWITCH(neq, return (fill1_t<NEQ>(a, pa, stats, st)));
+  return cudaSuccess;
 }
 
 static cudaError_t fill_only(int neq, const KArgs& a, void* pool, int layers, cudaStream_t st)
@@ -47,12 +103,23 @@ static cudaError_t fill_only(int neq, const KArgs& a, void* pool, int layers, cu
   return cudaGetLastError();
 }
 
+template <int NEQ>
+static cudaError_t calcprim_t(const KArgs& a, const PhysArgs& pa, const int* list, int n, cudaStream_t st)
+{
+  static bool done = false;
+  constexpr size_t sm = smem_calcprim<R, NEQ>();
+  cudaError_t e = smem_opt_in(k_calcprim<R, NEQ>, sm, done);
+  if (e != cudaSuccess) return e;
+  k_calcprim<R, NEQ><<<n, W2D_THREADS, sm, st>>>(a, pa, list, n);
+  return cudaGetLastError();
+}
+
 static cudaError_t calcprim(int neq, const KArgs& a, const PhysArgs& pa, const int* list, int n,
                             cudaStream_t st)
 {
   if (n == 0) return cudaSuccess;
-  W2D_NEQ_SWITCH(neq, (k_calcprim<R, NEQ><<<n, W2D_THREADS, 0, st>>>(a, pa, list, n)));
-  return cudaGetLastError();
+  W2D_NEQ_SWITCH(neq, return (calcprim_t<NEQ>(a, pa, list, n, st)));
+  return cudaSuccess;
 }
 
 static cudaError_t refine(int neq, void* u, const int* quads, int n, cudaStream_t st)
@@ -69,12 +136,23 @@ static cudaError_t coarse(int neq, void* u, const int* quads, int n, cudaStream_
   return cudaGetLastError();
 }
 
+template <int NEQ>
+static cudaError_t cool_t(const KArgs& a, const PhysArgs& pa, double dt_s, cudaStream_t st)
+{
+  static bool done = false;
+  constexpr size_t sm = smem_cool<R, NEQ>();
+  cudaError_t e = smem_opt_in(k_cool<R, NEQ>, sm, done);
+  if (e != cudaSuccess) return e;
+  k_cool<R, NEQ><<<a.nleaf, W2D_THREADS, sm, st>>>(a, pa, dt_s);
+  return cudaGetLastError();
+}
+
 static cudaError_t cool(int neq, const KArgs& a, const PhysArgs& pa, double dt_s, cudaStream_t st)
 {
   if (a.nleaf == 0) return cudaSuccess;
   if (neq < 5 && pa.cooling == COOL_H) return cudaErrorInvalidValue;
-  W2D_NEQ_SWITCH(neq, (k_cool<R, NEQ><<<a.nleaf, W2D_THREADS, 0, st>>>(a, pa, dt_s)));
-  return cudaGetLastError();
+  W2D_NEQ_SWITCH(neq, return (cool_t<NEQ>(a, pa, dt_s, st)));
+  return cudaSuccess;
 }
 
 static cudaError_t scatter(void* pool, const void* stage, const int* ids, int n, size_t bs, cudaStream_t st)

@@ -26,7 +26,13 @@ struct Launchers {
 const Launchers& launchers64();
 const Launchers& launchers32();
 
+// lev[slot], icoord[2*slot..] from n tuples (slot, level, ix, iy)
+cudaError_t launch_set_slots(const int* tuples, int n, int* lev, int* icoord, cudaStream_t st);
+
+// work: two 64-bit words holding the bit pattern of 1e30; count: zero.
+// Both are restored by the kernel for the next call.
 cudaError_t launch_dt(const int* leaves, int n, const double* cfl, const double* dtcool, int use_cool,
-                      double courant, double psc, double tsc, double* dt_out, cudaStream_t st);
+                      double courant, double psc, double tsc, unsigned long long* work, unsigned int* count,
+                      double* dt_out, cudaStream_t st);
 
 }  // namespace w2d
