@@ -249,6 +249,7 @@ def run_ours(args, ws, rank, local):
     ctx.profile(True)
     step_ms = []
     clk.mark_start()
+    sim.phase_ms(reset=True)
     for _ in range(args.steps):
         ctx.flush_l2()
         ctx.event_record(0)
@@ -256,6 +257,7 @@ def run_ours(args, ws, rank, local):
         ctx.event_record(1)
         step_ms.append(ctx.event_elapsed(0, 1))
     ctx.sync()
+    phases = {k: v / args.steps for k, v in sim.phase_ms().items()}
     time.sleep(0.06)                       # one more clock sample after the region
     clk.__exit__()
     prof = ctx.profile_read()
@@ -336,6 +338,7 @@ def run_ours(args, ws, rank, local):
             "e2e": e2e,
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
+            "host_phase_ms_per_step": phases,
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -246,6 +246,12 @@ int w2d_sim_set_amr(W2dSim* sim, int on);
 /* DMC table for the driver's context (as w2d_set_cooltab), then the
  * primitives and per-block partials of every leaf are recomputed with it. */
 int w2d_sim_set_cooltab(W2dSim* sim, const double* log_t, const double* neg_log_l, int n);
+/* Host wall-clock milliseconds spent per phase of w2d_sim_run since the
+ * last reset: [0] topology + locatebounds + plan, [1] timestep (waits for
+ * the device), [2] tstep launches, [3] criteria (waits for the device),
+ * [4] admesh integer logic, [5] refine/coarse calls, [6] whole steps.
+ * ms must hold 8 doubles; reset != 0 zeroes the counters after reading. */
+int w2d_sim_phase_ms(W2dSim* sim, double* ms, int reset);
 
 #ifdef __cplusplus
 }

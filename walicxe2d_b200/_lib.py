@@ -59,6 +59,7 @@ SIGNATURES = {
     "w2d_sim_tree": (_I, [_vp, _PI32, _PI32, _PI32, _PI32, _PI32]),
     "w2d_sim_set_amr": (_I, [_vp, _I]),
     "w2d_sim_set_cooltab": (_I, [_vp, _PD, _PD, _I]),
+    "w2d_sim_phase_ms": (_I, [_vp, _PD, _I]),
 }
 
 _LIB = None

@@ -214,6 +214,15 @@ class Simulation:
     def set_amr(self, on: bool):
         self.L.w2d_sim_set_amr(self.h, 1 if on else 0)
 
+    PHASES = ("plan", "timestep_wait", "tstep_launch", "criteria_wait", "admesh_host",
+              "amr_calls", "step_total")
+
+    def phase_ms(self, reset: bool = False) -> dict:
+        """Host wall-clock ms per phase of run() (w2d_sim_phase_ms)."""
+        ms = np.zeros(8)
+        self.L.w2d_sim_phase_ms(self.h, _pd(ms), 1 if reset else 0)
+        return {k: float(ms[i]) for i, k in enumerate(self.PHASES)}
+
     def set_cooltab(self, log_t, neg_log_l):
         """DMC table (src/DMClib/coolingDMC.tab rows); recomputes the leaves'
         primitives and time-step partials with it."""

@@ -121,7 +121,29 @@ KArgs kargs(W2dCtx* c, const int2* fd)
     a.dx[l] = c->dx[l];
     a.dy[l] = c->dy[l];
   }
+  a.jet = c->p.otherb == W2D_USERBC_JET;
+  a.jetblk = c->d_jetblk;
   return a;
+}
+
+// The jet state of impose_jet (src/jet.f90:55-75) at `time`, evaluated on
+// the host in the reference's operation order.
+void set_jet_state(W2dCtx* c, KArgs& a, double time)
+{
+  if (!a.jet) return;
+  const W2dParams& p = c->p;
+  const double pi = acos(-1.);
+  const double vjet = p.jet_v0 + p.jet_dv * sin(2. * pi * time / p.jet_tau);
+  a.jet_posx = p.jet_posx;
+  a.jet_posy = p.jet_posy;
+  a.jet_lj = p.jet_lj;
+  a.jet_rj = p.jet_rj;
+  a.jet_u[0] = p.jet_den;
+  a.jet_u[1] = p.jet_den * vjet;
+  a.jet_u[2] = 0.;
+  a.jet_u[3] = 0.5 * p.jet_den * (vjet * vjet) + p.cv * p.jet_den * 1.0001 * p.jet_temp;
+  a.jet_u[4] = p.jet_den * 0.9999;
+  a.jet_u[5] = p.jet_den;
 }
 
 PhysArgs pargs(W2dCtx* c)
@@ -202,7 +224,7 @@ int stats_for(W2dCtx* c, const int* d_list, int n)
   if (!c->have_topology || n == 0) return W2D_OK;
   KArgs a = kargs(c, c->d_fd1);
   PhysArgs pa = pargs(c);
-  return launch(c, "calcprim", [&] { return c->L->calcprim(c->neq, a, pa, d_list, n, c->st); });
+  return launch(c, "calcprim", [&] { return c->L->calcprim(c->neq, a, pa, d_list, n, 0, c->st); });
 }
 
 }  // namespace
@@ -220,7 +242,7 @@ int w2d_create(const W2dParams* p, W2dCtx** out)
       p->nlevs < 1 || p->nlevs > W2D_MAXLEV || p->nblocks < 1 || p->solver < 0 || p->solver > 2 ||
       p->limiter < -1 || p->limiter > 6 || p->cooling < 0 || p->cooling > 2 ||
       (p->cooling == W2D_COOLINGH && p->neq < 5) || (p->precision != 64 && p->precision != 32) ||
-      p->otherb != W2D_USERBC_NONE)
+      (p->otherb != W2D_USERBC_NONE && p->otherb != W2D_USERBC_JET))
     return W2D_ERR_ARG;
   W2dCtx* c = new W2dCtx();
   c->p = *p;
@@ -313,11 +335,12 @@ int w2d_destroy(W2dCtx* c)
     if (e) cudaEventDestroy(e);
   void* dev[] = {c->d_u, c->d_up, c->d_prim, c->d_lev, c->d_icoord, c->d_cfl, c->d_dtcool, c->d_grad,
                  c->d_err, c->d_dt, c->d_cooltab, c->d_leaves, c->d_fd1, c->d_fd2, c->d_stage, c->d_ids,
-                 c->d_flush, c->d_dtwork, c->d_dtcount};
+                 c->d_flush, c->d_dtwork, c->d_dtcount, c->d_jetblk};
   for (void* d : dev)
     if (d) cudaFree(d);
   void* host[] = {c->h_stage, c->h_small, c->h_grad, c->h_err, c->h_fd1[0], c->h_fd2[0], c->h_leaves[0],
-                  c->h_fd1[1], c->h_fd2[1], c->h_leaves[1], c->h_ops, c->lev, c->icoord};
+                  c->h_fd1[1], c->h_fd2[1], c->h_leaves[1], c->h_ops, c->lev, c->icoord,
+                  c->h_jetblk[0], c->h_jetblk[1]};
   for (void* h : host)
     if (h) cudaFreeHost(h);
   if (c->st) cudaStreamDestroy(c->st);
@@ -396,23 +419,27 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
       if (c->h_fd1[q]) cudaFreeHost(c->h_fd1[q]);
       if (c->h_fd2[q]) cudaFreeHost(c->h_fd2[q]);
       if (c->h_leaves[q]) cudaFreeHost(c->h_leaves[q]);
+      if (c->h_jetblk[q]) cudaFreeHost(c->h_jetblk[q]);
       c->h_fd1[q] = c->h_fd2[q] = nullptr;
-      c->h_leaves[q] = nullptr;
+      c->h_leaves[q] = c->h_jetblk[q] = nullptr;
     }
     if (c->d_fd1) cudaFree(c->d_fd1);
     if (c->d_fd2) cudaFree(c->d_fd2);
     if (c->d_leaves) cudaFree(c->d_leaves);
+    if (c->d_jetblk) cudaFree(c->d_jetblk);
     c->d_fd1 = c->d_fd2 = nullptr;
-    c->d_leaves = nullptr;
+    c->d_leaves = c->d_jetblk = nullptr;
     int cap = std::max(nl + nl / 2, 256);
     for (int q = 0; q < 2; ++q) {
       CK(cudaMallocHost(&c->h_fd1[q], sizeof(int2) * 4 * (size_t)cap));
       CK(cudaMallocHost(&c->h_fd2[q], sizeof(int2) * 4 * (size_t)cap));
       CK(cudaMallocHost(&c->h_leaves[q], sizeof(int) * (size_t)cap));
+      CK(cudaMallocHost(&c->h_jetblk[q], sizeof(int) * (size_t)cap));
     }
     CK(cudaMalloc(&c->d_fd1, sizeof(int2) * 4 * (size_t)cap));
     CK(cudaMalloc(&c->d_fd2, sizeof(int2) * 4 * (size_t)cap));
     CK(cudaMalloc(&c->d_leaves, sizeof(int) * (size_t)cap));
+    CK(cudaMalloc(&c->d_jetblk, sizeof(int) * (size_t)cap));
     c->h_plan_cap = cap;
   }
   // alternate pinned buffers; wait only for the upload that last used this one
@@ -422,22 +449,47 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
   int2* hf1 = c->h_fd1[q];
   int2* hf2 = c->h_fd2[q];
   int* hl = c->h_leaves[q];
+  int* hj = c->h_jetblk[q];
   for (int k = 0; k < 4 * nl; ++k) hf1[k] = hf2[k] = make_int2(0, FK_KEEP);
   for (int k = 0; k < nl; ++k) hl[k] = c->leaves[k];
-  auto put = [&](int2* fd, int blk, int face, int nbr, int kind, int off) {
+  // impose_jet runs after every entry on its nbs (src/boundaryI.f90:386-393,
+  // src/boundaryII.f90:505-512): first and last position of each block as nbs
+  const bool jet = c->p.otherb == W2D_USERBC_JET;
+  if (jet) {
+    if ((int)c->qfirst.size() != c->cap + 1) {
+      c->qfirst.assign((size_t)c->cap + 1, 0);
+      c->qlast.assign((size_t)c->cap + 1, 0);
+    }
+    for (int e = 1; e <= n; ++e) {
+      const int nbs = ib[e - 1];
+      if (nbs < 1 || nbs > c->nbmax) continue;
+      if (!c->qfirst[nbs]) c->qfirst[nbs] = e;
+      c->qlast[nbs] = e;
+    }
+  }
+  auto jetted_before = [&](int blk, int e) { return blk >= 1 && blk <= c->nbmax && c->qfirst[blk] && c->qfirst[blk] < e; };
+  auto put = [&](int2* fd, int blk, int face, int nbr, int kind, int off, int e) {
     if (blk < 1 || blk > c->nbmax) return;
     const int li = c->leaf_index[blk];
     if (li < 0) return;  // non-leaf targets are never read before being rewritten
-    fd[li * 4 + face] = make_int2(nbr, kind | (off << 8));
+    int y = kind | (off << 8);
+    if (jet) {
+      const int s1 = (kind == FK_MIRROR || kind == FK_REFLECT) ? blk : nbr;
+      if (jetted_before(s1, e)) y |= FD_SRC1_JET;
+      if (kind == FK_RESTRICT && jetted_before(nbr + (face < 2 ? 2 : 1), e)) y |= FD_SRC2_JET;
+      if (c->qlast[blk] >= e) y |= FD_DST_JET;
+    }
+    fd[li * 4 + face] = make_int2(nbr, y);
   };
+  int e = 0;
   auto both = [&](int blk, int face, int nbr, int kind, int off) {
-    put(hf1, blk, face, nbr, kind, off);
-    put(hf2, blk, face, nbr, kind, off);
+    put(hf1, blk, face, nbr, kind, off, e);
+    put(hf2, blk, face, nbr, kind, off, e);
   };
   const int H = W2D_NX / 2;
   const int bc[4] = {c->p.bc_left, c->p.bc_right, c->p.bc_bottom, c->p.bc_top};
   const bool f6b = (c->p.compat & W2D_COMPAT_OUTFYB) != 0;
-  for (int e = 1; e <= n; ++e) {
+  for (e = 1; e <= n; ++e) {
     const int nbs = ib[e - 1], n1 = ib[(size_t)ld + e - 1], t = ib[2 * (size_t)ld + e - 1];
     if (nbs < 1 || nbs > c->nbmax || (t > 0 && (n1 < 1 || n1 > c->nbmax)))
       return set_error(c, W2D_ERR_TOPOLOGY, nbs, e, t, "innerbounds entry %d (%d,%d,%d) out of range", e, nbs, n1, t);
@@ -451,10 +503,10 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
         if (bc[2] == W2D_BC_REFLECTIVE) {
           both(nbs, 2, nbs, FK_REFLECT, 0);
         } else {
-          put(hf2, nbs, 2, nbs, FK_MIRROR, 0);
+          put(hf2, nbs, 2, nbs, FK_MIRROR, 0, e);
           // src/boundaryI.f90:87 fills block "nb" (the list index e)
           const int tb = f6b ? e : nbs;
-          put(hf1, tb, 2, tb, FK_MIRROR, 0);
+          put(hf1, tb, 2, tb, FK_MIRROR, 0, e);
         }
         break;
       case 1:  both(nbs, 0, n1, FK_SAME, 0);  both(n1, 1, nbs, FK_SAME, 0); break;
@@ -485,10 +537,27 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
         return set_error(c, W2D_ERR_TOPOLOGY, nbs, e, t, "innerbounds type %d not in the serial list", t);
     }
   }
+  if (jet) {
+    // faces no entry writes still get the jet if their block is ever nbs;
+    // the interior of such a block always does
+    for (int li = 0; li < nl; ++li) {
+      const int b = c->leaves[li];
+      hj[li] = c->qfirst[b] > 0;
+      for (int f = 0; f < 4; ++f) {
+        if (hj[li] && (hf1[li * 4 + f].y & 0xff) == FK_KEEP) hf1[li * 4 + f].y |= FD_DST_JET;
+        if (hj[li] && (hf2[li * 4 + f].y & 0xff) == FK_KEEP) hf2[li * 4 + f].y |= FD_DST_JET;
+      }
+    }
+    for (int k = 1; k <= n; ++k) {   // clear for the next list
+      const int nbs = ib[k - 1];
+      if (nbs >= 1 && nbs <= c->nbmax) c->qfirst[nbs] = c->qlast[nbs] = 0;
+    }
+  }
   if (nl > 0) {
     CK(cudaMemcpyAsync(c->d_fd1, hf1, sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->d_fd2, hf2, sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->d_leaves, hl, sizeof(int) * (size_t)nl, cudaMemcpyHostToDevice, c->st));
+    if (jet) CK(cudaMemcpyAsync(c->d_jetblk, hj, sizeof(int) * (size_t)nl, cudaMemcpyHostToDevice, c->st));
   }
   CK(cudaEventRecord(c->ev_plan[q], c->st));
   c->have_bounds = true;
@@ -612,7 +681,6 @@ int w2d_timestep(W2dCtx* c, double* dt)
 
 int w2d_tstep(W2dCtx* c, double time, double dt)
 {
-  (void)time;
   if (!c) return W2D_ERR_ARG;
   if (!c->have_topology || !c->have_bounds)
     return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology and w2d_set_bounds first");
@@ -621,11 +689,21 @@ int w2d_tstep(W2dCtx* c, double time, double dt)
   PhysArgs pa = pargs(c);
   KArgs a2 = kargs(c, c->d_fd2);
   KArgs a1 = kargs(c, c->d_fd1);
+  set_jet_state(c, a2, time);   // both fills impose the jet at tstep's time
+  set_jet_state(c, a1, time);
+  const bool jet = a1.jet != 0;
   int rc;
   if ((rc = launch(c, "half_step", [&] { return c->L->half(c->neq, a2, pa, dt, c->st); }))) return rc;
   if ((rc = launch(c, "full_step", [&] { return c->L->full(c->neq, a2, pa, dt, c->st); }))) return rc;
-  const int stats = c->p.cooling == W2D_ADIABATIC;
+  // boundaryI; with the jet its interior writes and the statistics follow in
+  // a second pass, after every fill read of the interiors
+  const int stats = c->p.cooling == W2D_ADIABATIC && !jet;
   if ((rc = launch(c, "fill_I", [&] { return c->L->fill1(c->neq, a1, pa, stats, c->st); }))) return rc;
+  if (jet && c->p.cooling == W2D_ADIABATIC) {
+    const int nl = (int)c->leaves.size();
+    if ((rc = launch(c, "jet_calcprim", [&] { return c->L->calcprim(c->neq, a1, pa, c->d_leaves, nl, 1, c->st); })))
+      return rc;
+  }
   if (c->p.cooling != W2D_ADIABATIC) {
     const double dts = dt * c->p.tsc;
     if ((rc = launch(c, "cooling", [&] { return c->L->cool(c->neq, a1, pa, dts, c->st); }))) return rc;
@@ -718,20 +796,24 @@ int w2d_coarse(W2dCtx* c, const int32_t* quads, int n) { return amr_ops(c, quads
 
 int w2d_boundaryI(W2dCtx* c, double time)
 {
-  (void)time;
   if (!c) return W2D_ERR_ARG;
   if (!c->have_bounds) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_bounds first");
   KArgs a = kargs(c, c->d_fd1);
-  return launch(c, "fill_I_only", [&] { return c->L->fill_only(c->neq, a, c->d_u, 1, c->st); });
+  set_jet_state(c, a, time);
+  int rc = launch(c, "fill_I_only", [&] { return c->L->fill_only(c->neq, a, c->d_u, 1, c->st); });
+  if (rc || !a.jet) return rc;
+  return launch(c, "jet_only", [&] { return c->L->jet_only(c->neq, a, c->d_u, c->st); });
 }
 
 int w2d_boundaryII(W2dCtx* c, double time)
 {
-  (void)time;
   if (!c) return W2D_ERR_ARG;
   if (!c->have_bounds) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_bounds first");
   KArgs a = kargs(c, c->d_fd2);
-  return launch(c, "fill_II_only", [&] { return c->L->fill_only(c->neq, a, c->d_up, 2, c->st); });
+  set_jet_state(c, a, time);
+  int rc = launch(c, "fill_II_only", [&] { return c->L->fill_only(c->neq, a, c->d_up, 2, c->st); });
+  if (rc || !a.jet) return rc;
+  return launch(c, "jet_only", [&] { return c->L->jet_only(c->neq, a, c->d_up, c->st); });
 }
 
 int w2d_calcprim(W2dCtx* c)

@@ -120,6 +120,10 @@ __global__ void __launch_bounds__(W2D_THREADS) k_cool(KArgs a, PhysArgs pa, doub
   R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;
   load_tile<R, NEQ>(&st[0][0][0], u, bar, a.err, b);
   if (!wait_tiles(bar, a.err, b)) return;
+  if (a.jet && a.jetblk[blockIdx.x]) {   // impose_jet of boundaryI, before cooling
+    jet_interior_fn<R, NEQ>(st, a, b, u);
+    __syncthreads();
+  }
   for (int c = tid; c < 18 * 18; c += W2D_THREADS) {
     const int i = c % 18, j = c / 18;
     if ((i == 0 || i == 17) && (j == 0 || j == 17)) continue;

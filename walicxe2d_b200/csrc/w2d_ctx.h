@@ -54,6 +54,9 @@ struct W2dCtx {
   int2* h_fd1[2] = {nullptr, nullptr};
   int2* h_fd2[2] = {nullptr, nullptr};
   int* h_leaves[2] = {nullptr, nullptr};
+  int* h_jetblk[2] = {nullptr, nullptr};
+  int* d_jetblk = nullptr;                 // per leaf: named as nbs in the list
+  std::vector<int> qfirst, qlast;          // per slot: first/last list position as nbs
   cudaEvent_t ev_plan[2] = {nullptr, nullptr};
   int plan_buf = 0;
   int h_plan_cap = 0;

@@ -22,6 +22,7 @@
 // the refine/coarsen flags (markref sets them on leaves, critneighup on the
 // coarser leaves its pointers reach), so the same blocks are visited in the
 // same order and the decisions are identical.
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -50,6 +51,7 @@ struct W2dSim {
   std::vector<double> grad;
   std::vector<int32_t> rops, cops;
   std::vector<int32_t> ib1, ib2, ib3;
+  double phase_ms[8] = {0};               // see w2d_sim_phase_ms
 
   int32_t& LP(int nb, int k) { return lp[(size_t)nb * 8 + (k - 1)]; }
   int32_t& LEAF(int nb) { return leaf[(size_t)nb - 1]; }
@@ -229,14 +231,21 @@ void locatebounds(W2dSim* s)
   std::copy(s->ib3.begin(), s->ib3.end(), s->ib.begin() + 2 * (size_t)s->nib);
 }
 
+double now_ms()
+{
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 int refresh_plan(W2dSim* s)
 {
+  const double t0 = now_ms();
   int rc = push_topology(s);
   if (rc) return rc;
   locatebounds(s);
   rc = w2d_set_bounds(s->ctx, s->ib.data(), s->nib, s->nib);
   if (rc) return rc;
   s->dirty = false;
+  s->phase_ms[0] += now_ms() - t0;
   return W2D_OK;
 }
 
@@ -250,8 +259,11 @@ int admesh(W2dSim* s)
   int rc;
   if (s->dirty && (rc = refresh_plan(s))) return rc;
   // markref + criteria flags (criteria.f90:36-50 on the device maximum)
+  double t0 = now_ms();
   rc = w2d_criteria(s->ctx, s->grad.data());
   if (rc) return rc;
+  double t1 = now_ms();
+  s->phase_ms[3] += t1 - t0;
   std::fill(s->irefup.begin(), s->irefup.end(), 0);
   std::fill(s->irefdown.begin(), s->irefdown.end(), 0);
   // leaves per level in ascending ID (the only blocks that get flags)
@@ -315,9 +327,12 @@ int admesh(W2dSim* s)
       }
     }
   const int nr = (int)s->rops.size() / 5, nc = (int)s->cops.size() / 5;
+  t0 = now_ms();
+  s->phase_ms[4] += t0 - t1;
   if (nr && (rc = w2d_refine(s->ctx, s->rops.data(), nr))) return rc;
   if (nc && (rc = w2d_coarse(s->ctx, s->cops.data(), nc))) return rc;
   if (nr || nc) s->dirty = true;
+  s->phase_ms[5] += now_ms() - t0;
   return W2D_OK;
 }
 
@@ -418,16 +433,31 @@ int w2d_sim_run(W2dSim* s, int nsteps)
   if (!s || nsteps < 0) return W2D_ERR_ARG;
   int rc;
   for (int n = 0; n < nsteps; ++n) {
+    const double t0 = now_ms();
     if (s->dirty && (rc = refresh_plan(s))) return rc;
     double dt = 0.0;
+    const double t1 = now_ms();
     if ((rc = w2d_timestep(s->ctx, &dt))) return rc;       // src/main.f90:87
+    const double t2 = now_ms();
     s->dt = dt;
     s->time = s->time + dt;                                 // src/main.f90:88
     if ((rc = w2d_tstep(s->ctx, s->time, dt))) return rc;   // src/main.f90:95
+    s->phase_ms[1] += t2 - t1;
+    s->phase_ms[2] += now_ms() - t2;
     s->zone_updates += (int64_t)s->nbleafs * s->p.nx * s->p.ny;
     if (s->amr && (rc = admesh(s))) return rc;              // src/main.f90:98
     s->steps++;
+    s->phase_ms[6] += now_ms() - t0;
   }
+  return W2D_OK;
+}
+
+int w2d_sim_phase_ms(W2dSim* s, double* ms, int reset)
+{
+  if (!s || !ms) return W2D_ERR_ARG;
+  for (int k = 0; k < 8; ++k) ms[k] = s->phase_ms[k];
+  if (reset)
+    for (double& v : s->phase_ms) v = 0.0;
   return W2D_OK;
 }
 

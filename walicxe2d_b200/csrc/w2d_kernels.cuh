@@ -53,10 +53,20 @@ struct KArgs {
   int* err;           // device error word {code, block, i, j}
   const double* cooltab;  // [2][41] DMC table (T, Lambda)
   int nlevs;
-  int pad_;
+  int jet;                // impose_jet is active (OTHERB)
   double eta, psc, tempsc_d;
   double dx[W2D_MAXLEV + 1], dy[W2D_MAXLEV + 1];
+  // impose_jet (src/jet.f90:41-78): region |x-posx| <= lj, |y-posy| <= rj
+  // and the top-hat state (u1..u6) at the fill's time
+  double jet_posx, jet_posy, jet_lj, jet_rj;
+  double jet_u[6];
+  const int* jetblk;      // per leaf position: block appears as nbs in the list
 };
+
+// flags of a face descriptor (bits 16..18 of .y) for impose_jet ordering:
+// the source block(s) had the jet imposed before the face's final writer,
+// and the destination block gets it imposed at or after that writer.
+enum { FD_SRC1_JET = 1 << 16, FD_SRC2_JET = 1 << 17, FD_DST_JET = 1 << 18 };
 
 struct PhysArgs {
   double cv, gamma, tempsc;
@@ -168,6 +178,120 @@ __device__ __forceinline__ bool face_value(const R* __restrict__ arr, size_t bst
     }
     default:
       return false;
+  }
+}
+
+// Cell (i,j) of block b inside the jet source region, src/jet.f90:62-67:
+//   x = (i + icoord(b,1) - 0.5) dx(lev),  |x - posx| <= LJ  and  |y - posy| <= RJ
+__device__ __forceinline__ bool in_jet(const KArgs& a, int b, int i, int j)
+{
+  const int lev = a.lev[b];
+  const double x = ((double)(i + a.icoord[2 * b]) - 0.5) * a.dx[lev];
+  const double y = ((double)(j + a.icoord[2 * b + 1]) - 0.5) * a.dy[lev];
+  return (fabs(x - a.jet_posx) <= a.jet_lj) && (fabs(y - a.jet_posy) <= a.jet_rj);
+}
+
+// Value of equation k of cell (i,j) of block blk as a fill entry reads it:
+// the jet state if the jet was imposed on blk before that entry and the
+// cell is in the region, else the pool value.
+template <typename R>
+__device__ __forceinline__ R src_cell(const R* __restrict__ arr, size_t bs, const KArgs& a, int blk, int k,
+                                      int i, int j, bool jetted)
+{
+  if (jetted && k < 6 && in_jet(a, blk, i, j)) return R(a.jet_u[k]);
+  return arr[(size_t)blk * bs + (size_t)k * W2D_CELLS + cidx(i, j)];
+}
+
+// Final value of equation k of ghost cell (f,g,m) of block b after a list
+// walk, under descriptor d (kind, source, impose_jet order flags).  Without
+// the jet this is face_value.  With it: sources read the jet state where it
+// was imposed on them earlier in the walk, and the ghost takes the jet state
+// if the jet is imposed on b at or after the face's final writer.  Returns
+// false when the old value stays.
+template <typename R>
+__device__ __forceinline__ bool ghost_value(const R* __restrict__ arr, size_t bs, const KArgs& a, int b,
+                                            int2 d, int f, int g, int m, int k, R& out)
+{
+  if (!a.jet) return face_value<R>(arr, bs, b, d, f, g, m, k, out);
+  int gi, gj;
+  ghost_ij(f, g, m, gi, gj);
+  if ((d.y & FD_DST_JET) && k < 6 && in_jet(a, b, gi, gj)) {
+    out = R(a.jet_u[k]);
+    return true;
+  }
+  const int kind = d.y & 0xff;
+  const bool j1 = (d.y & FD_SRC1_JET) != 0, j2 = (d.y & FD_SRC2_JET) != 0;
+  const int NX = W2D_NX;
+  switch (kind) {
+    case FK_MIRROR:
+    case FK_REFLECT: {
+      int si, sj;
+      mirror_ij(f, g, m, si, sj);
+      R v = src_cell<R>(arr, bs, a, b, k, si, sj, j1);
+      if (kind == FK_REFLECT && k == ((f < 2) ? 1 : 2)) v = -v;
+      out = v;
+      return true;
+    }
+    case FK_SAME: {
+      int si, sj;
+      switch (f) {
+        case 0: si = NX - g; sj = m; break;
+        case 1: si = 1 + g; sj = m; break;
+        case 2: si = m; sj = NX - g; break;
+        default: si = m; sj = 1 + g; break;
+      }
+      out = src_cell<R>(arr, bs, a, d.x, k, si, sj, j1);
+      return true;
+    }
+    case FK_RESTRICT: {
+      int nn = d.x, mm = m;
+      bool jj = j1;
+      if (m > NX / 2) { nn = d.x + ((f < 2) ? 2 : 1); mm = m - NX / 2; jj = j2; }
+      int i1, jr;
+      switch (f) {
+        case 0: i1 = NX - 1 - 2 * g; jr = 2 * mm - 1; break;
+        case 1: i1 = 1 + 2 * g; jr = 2 * mm - 1; break;
+        case 2: i1 = 2 * mm - 1; jr = NX - 1 - 2 * g; break;
+        default: i1 = 2 * mm - 1; jr = 1 + 2 * g; break;
+      }
+      R t = R(0.);
+      t += src_cell<R>(arr, bs, a, nn, k, i1, jr, jj);
+      t += src_cell<R>(arr, bs, a, nn, k, i1 + 1, jr, jj);
+      t += src_cell<R>(arr, bs, a, nn, k, i1, jr + 1, jj);
+      t += src_cell<R>(arr, bs, a, nn, k, i1 + 1, jr + 1, jj);
+      out = R(0.25) * t;
+      return true;
+    }
+    case FK_INJECT: {
+      const int off = (d.y >> 8) & 0xff;
+      int si, sj;
+      switch (f) {
+        case 0: si = NX; sj = (m + 1) / 2 + off; break;
+        case 1: si = 1; sj = (m + 1) / 2 + off; break;
+        case 2: si = (m + 1) / 2 + off; sj = NX; break;
+        default: si = (m + 1) / 2 + off; sj = 1; break;
+      }
+      out = src_cell<R>(arr, bs, a, d.x, k, si, sj, j1);
+      return true;
+    }
+    default:
+      return false;
+  }
+}
+
+// impose_jet on the interior of block b, in a shared tile [NEQ][20][20]:
+// the reference imposes it on every block that is nbs of some list entry.
+template <typename R, int NEQ>
+__device__ __forceinline__ void jet_interior_fn(R (*st)[W2D_W][W2D_W], const KArgs& a, int b, R* gdst)
+{
+  for (int c = threadIdx.x; c < 256; c += blockDim.x) {
+    const int i = 1 + c % 16, j = 1 + c / 16;
+    if (!in_jet(a, b, i, j)) continue;
+#pragma unroll
+    for (int k = 0; k < (NEQ < 6 ? NEQ : 6); ++k) {
+      st[k][j + 1][i + 1] = R(a.jet_u[k]);
+      if (gdst) gdst[k * W2D_CELLS + cidx(i, j)] = R(a.jet_u[k]);
+    }
   }
 }
 
@@ -430,39 +554,24 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
   const bool visc = lev >= (a.nlevs - 1);
   const R eta = R(a.eta);
 
-  // ghosts gathered from the neighbours while the tiles land
-  int2 dface[4];
-#pragma unroll
-  for (int f = 0; f < 4; ++f) dface[f] = a.fd[li * 4 + f];
+  // ghosts of the filled up gathered from the pool while the tiles land
+  // (box faces read the block's own interior there too)
   R gv[NEQ];
+  bool gw = false;
   const int gf = tid / 32, gg = (tid / 16) % 2, gm = 1 + tid % 16;
-  int gkind = FK_KEEP;
   if (tid < 128) {
-    gkind = dface[gf].y & 0xff;
-    if (gkind >= FK_SAME) {
+    const int2 d = a.fd[li * 4 + gf];
 #pragma unroll
-      for (int k = 0; k < NEQ; ++k) face_value<R>(upool, bs, b, dface[gf], gf, gg, gm, k, gv[k]);
-    }
+    for (int k = 0; k < NEQ; ++k) gw = ghost_value<R>(upool, bs, a, b, d, gf, gg, gm, k, gv[k]);
   }
   if (!wait_tiles(bar, a.err, b)) return;
-  if (tid < 128 && gkind >= FK_SAME) {
+  if (tid < 128 && gw) {
     int i, j;
     ghost_ij(gf, gg, gm, i, j);
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) st[k][j + 1][i + 1] = gv[k];
   }
-  __syncthreads();
-  if (tid < 128 && (gkind == FK_MIRROR || gkind == FK_REFLECT)) {  // box faces: own interior
-    int i, j, si, sj;
-    ghost_ij(gf, gg, gm, i, j);
-    mirror_ij(gf, gg, gm, si, sj);
-#pragma unroll
-    for (int k = 0; k < NEQ; ++k) {
-      R v = st[k][sj + 1][si + 1];
-      if (gkind == FK_REFLECT && k == ((gf < 2) ? 1 : 2)) v = -v;
-      st[k][j + 1][i + 1] = v;
-    }
-  }
+  if (a.jet && a.jetblk[li]) jet_interior_fn<R, NEQ>(st, a, b, nullptr);
   __syncthreads();
 
   // u ghosts = up ghosts (u = up, src/tstep.f90:85; the old u stays in so),
@@ -575,7 +684,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_fill1(KArgs a, PhysArgs pa, int
     ghost_ij(f, 0, m, gi, gj);
     const int2 d = a.fd[li * 4 + f];
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) w = face_value<R>(upool, bs, b, d, f, 0, m, k, gv[k]);
+    for (int k = 0; k < NEQ; ++k) w = ghost_value<R>(upool, bs, a, b, d, f, 0, m, k, gv[k]);
     if (w) {
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) u[k * W2D_CELLS + cidx(gi, gj)] = gv[k];
@@ -612,8 +721,12 @@ __host__ __device__ constexpr size_t smem_calcprim()
   return 128 + sizeof(R) * NEQ * W2D_CELLS + 64 * sizeof(double);
 }
 
+// With jet_interior != 0 (list = the leaves, after the fill of layer 0) it
+// first imposes the jet on the interior of the blocks the list walk named,
+// which the reference does inside boundaryI (src/boundaryI.f90:386-393).
 template <typename R, int NEQ>
-__global__ void __launch_bounds__(W2D_THREADS) k_calcprim(KArgs a, PhysArgs pa, const int* __restrict__ list, int n)
+__global__ void __launch_bounds__(W2D_THREADS) k_calcprim(KArgs a, PhysArgs pa, const int* __restrict__ list, int n,
+                                                          int jet_interior)
 {
   uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
   R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
@@ -622,10 +735,14 @@ __global__ void __launch_bounds__(W2D_THREADS) k_calcprim(KArgs a, PhysArgs pa, 
   const int b = list[blockIdx.x];
   const int tid = threadIdx.x;
   const size_t bs = (size_t)NEQ * W2D_CELLS;
-  const R* __restrict__ u = (const R*)a.u + (size_t)b * bs;
+  R* __restrict__ u = (R*)a.u + (size_t)b * bs;
   R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;
   load_tile<R, NEQ>(&st[0][0][0], u, bar, a.err, b);
   if (!wait_tiles(bar, a.err, b)) return;
+  if (jet_interior && a.jet && a.jetblk[blockIdx.x]) {
+    jet_interior_fn<R, NEQ>(st, a, b, u);
+    __syncthreads();
+  }
   for (int c = tid; c < W2D_CELLS; c += W2D_THREADS) {
     const int ti = c % W2D_W, tj = c / W2D_W;
     R uu[NEQ], q[NEQ], T;
@@ -661,11 +778,26 @@ __global__ void __launch_bounds__(128) k_fill_only(KArgs a, R* pool, int layers)
   R vals[NEQ];
   bool w = false;
 #pragma unroll
-  for (int k = 0; k < NEQ; ++k) w = face_value<R>(pool, bs, b, d, f, g, m, k, vals[k]);
+  for (int k = 0; k < NEQ; ++k) w = ghost_value<R>(pool, bs, a, b, d, f, g, m, k, vals[k]);
   if (w) {
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) pool[(size_t)b * bs + k * W2D_CELLS + cidx(i, j)] = vals[k];
   }
+}
+
+// impose_jet on the interior of the leaves the list walk named (standalone
+// fills; runs after k_fill_only so that no fill read sees it early).
+template <typename R, int NEQ>
+__global__ void __launch_bounds__(256) k_jet_only(KArgs a, R* pool)
+{
+  const int li = blockIdx.x;
+  if (!a.jetblk[li]) return;
+  const int b = a.leaves[li];
+  const int i = 1 + threadIdx.x % 16, j = 1 + threadIdx.x / 16;
+  if (!in_jet(a, b, i, j)) return;
+  R* pb = pool + (size_t)b * NEQ * W2D_CELLS;
+#pragma unroll
+  for (int k = 0; k < (NEQ < 6 ? NEQ : 6); ++k) pb[k * W2D_CELLS + cidx(i, j)] = R(a.jet_u[k]);
 }
 
 // ---------------------------------------------------------------------------

@@ -104,22 +104,30 @@ static cudaError_t fill_only(int neq, const KArgs& a, void* pool, int layers, cu
 }
 
 template <int NEQ>
-static cudaError_t calcprim_t(const KArgs& a, const PhysArgs& pa, const int* list, int n, cudaStream_t st)
+static cudaError_t calcprim_t(const KArgs& a, const PhysArgs& pa, const int* list, int n, int jet_interior,
+                              cudaStream_t st)
 {
   static bool done = false;
   constexpr size_t sm = smem_calcprim<R, NEQ>();
   cudaError_t e = smem_opt_in(k_calcprim<R, NEQ>, sm, done);
   if (e != cudaSuccess) return e;
-  k_calcprim<R, NEQ><<<n, W2D_THREADS, sm, st>>>(a, pa, list, n);
+  k_calcprim<R, NEQ><<<n, W2D_THREADS, sm, st>>>(a, pa, list, n, jet_interior);
   return cudaGetLastError();
 }
 
 static cudaError_t calcprim(int neq, const KArgs& a, const PhysArgs& pa, const int* list, int n,
-                            cudaStream_t st)
+                            int jet_interior, cudaStream_t st)
 {
   if (n == 0) return cudaSuccess;
-  W2D_NEQ_SWITCH(neq, return (calcprim_t<NEQ>(a, pa, list, n, st)));
+  W2D_NEQ_SWITCH(neq, return (calcprim_t<NEQ>(a, pa, list, n, jet_interior, st)));
   return cudaSuccess;
+}
+
+static cudaError_t jet_only(int neq, const KArgs& a, void* pool, cudaStream_t st)
+{
+  if (a.nleaf == 0 || !a.jet) return cudaSuccess;
+  W2D_NEQ_SWITCH(neq, (k_jet_only<R, NEQ><<<a.nleaf, 256, 0, st>>>(a, (R*)pool)));
+  return cudaGetLastError();
 }
 
 static cudaError_t refine(int neq, void* u, const int* quads, int n, cudaStream_t st)
@@ -177,8 +185,8 @@ static cudaError_t to_prim(int neq, const PhysArgs& pa, const void* u, void* out
   return cudaGetLastError();
 }
 
-static const Launchers table = {half, full, fill1, fill_only, calcprim, refine,
-                                coarse, cool, scatter, gather, to_prim, sizeof(R)};
+static const Launchers table = {half,   full,    fill1,  fill_only, calcprim, jet_only,
+                                refine, coarse,  cool,   scatter,   gather,   to_prim, sizeof(R)};
 
 }  // namespace W2D_INST_NS
 }  // namespace w2d

@@ -13,7 +13,9 @@ struct Launchers {
   cudaError_t (*full)(int neq, const KArgs&, const PhysArgs&, double dt, cudaStream_t);
   cudaError_t (*fill1)(int neq, const KArgs&, const PhysArgs&, int stats, cudaStream_t);
   cudaError_t (*fill_only)(int neq, const KArgs&, void* pool, int layers, cudaStream_t);
-  cudaError_t (*calcprim)(int neq, const KArgs&, const PhysArgs&, const int* list, int n, cudaStream_t);
+  cudaError_t (*calcprim)(int neq, const KArgs&, const PhysArgs&, const int* list, int n, int jet_interior,
+                          cudaStream_t);
+  cudaError_t (*jet_only)(int neq, const KArgs&, void* pool, cudaStream_t);
   cudaError_t (*refine)(int neq, void* u, const int* quads, int n, cudaStream_t);
   cudaError_t (*coarse)(int neq, void* u, const int* quads, int n, cudaStream_t);
   cudaError_t (*cool)(int neq, const KArgs&, const PhysArgs&, double dt_s, cudaStream_t);

@@ -140,6 +140,39 @@ def sedov(nbroot: int = 4, nlevs: int = 1, tol: float = 0.1, nblocks: int | None
     return p, ic
 
 
+def jet(nbroot_x: int = 32, nbroot_y: int = 8, nlevs: int = 7, cooling: int = COOLINGDMC,
+        nblocks: int | None = None, tol: float = 0.1, rj_cm: float = 1.0e15, **kw):
+    """Planar variable-velocity jet (the reference's OTHERB set-up with
+    impose_jet, src/jet.f90): box 4e17 x 1e17 cm (xmax 1, ymax 0.25), ambient
+    1 cm^-3 at 1e3 K, jet 100 cm^-3 at 1e3 K of radius rj_cm entering at
+    x = 0, mid-height, with v = 200 (1 + 0.25 sin(2 pi t / 20 yr)) km/s;
+    reflective left wall, outflow elsewhere; neq = 6 (neutral density and a
+    tracer, as the jet state writes both)."""
+    if nblocks is None:
+        nblocks = 200000 if nlevs >= 6 else 20000
+    p = base_params(neq=6, npas=2, nlevs=nlevs, nbroot_x=nbroot_x, nbroot_y=nbroot_y,
+                    nblocks=nblocks, cooling=cooling, otherb=USERBC_JET, tol=tol, **kw)
+    p.xmax, p.ymax = 1.0, 0.25
+    p.bc_left = BC_REFLECTIVE
+    sc = scalings(4.0e17, p.xmax, p.cv)
+    p.tempsc, p.psc, p.tsc, p.rsc = sc["tempsc"], sc["psc"], sc["tsc"], sc["rsc"]
+    vsc = math.sqrt(sc["vsc2"])
+    p.jet_rj = rj_cm / sc["rsc"]
+    p.jet_lj = rj_cm / sc["rsc"]
+    p.jet_posx, p.jet_posy = 0.0, 0.5 * p.ymax
+    p.jet_den = 100.0
+    p.jet_temp = 1.0e3 / sc["tempsc"]
+    p.jet_v0 = 200.0e5 / vsc
+    p.jet_dv = 50.0e5 / vsc
+    p.jet_tau = 20.0 * YR / sc["tsc"]
+    ic = W2dInit()
+    ic.kind = IC_JET
+    ic.init_levels = 1
+    ic.startup_admesh = min(nlevs - 1, 6) if nlevs > 1 else 0
+    ic.rho0, ic.p0 = 1.0, 1.0e3      # ambient n and T (initial_conditions)
+    return p, ic
+
+
 def config(name: str):
     """Named workloads: 'sedov64' (4x4 roots, no AMR), 'sedov_amr' (8x8
     roots, 5 levels, tol 0.1) and small test variants."""
@@ -149,4 +182,10 @@ def config(name: str):
         return sedov(nbroot=8, nlevs=5, tol=0.1)
     if name == "sedov_amr_small":
         return sedov(nbroot=4, nlevs=3, tol=0.1, nblocks=4000)
+    if name == "jet_small":
+        return jet(nbroot_x=8, nbroot_y=2, nlevs=3, cooling=ADIABATIC, nblocks=4000, rj_cm=8.0e15)
+    if name == "jet_small_dmc":
+        return jet(nbroot_x=8, nbroot_y=2, nlevs=3, cooling=COOLINGDMC, nblocks=4000, rj_cm=8.0e15)
+    if name == "jet_dmc":
+        return jet()
     raise KeyError(name)
