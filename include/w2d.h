@@ -247,10 +247,13 @@ int w2d_sim_set_amr(W2dSim* sim, int on);
  * primitives and per-block partials of every leaf are recomputed with it. */
 int w2d_sim_set_cooltab(W2dSim* sim, const double* log_t, const double* neg_log_l, int n);
 /* Host wall-clock milliseconds spent per phase of w2d_sim_run since the
- * last reset: [0] topology + locatebounds + plan, [1] timestep (waits for
- * the device), [2] tstep launches, [3] criteria (waits for the device),
- * [4] admesh integer logic, [5] refine/coarse calls, [6] whole steps.
- * ms must hold 8 doubles; reset != 0 zeroes the counters after reading. */
+ * last reset: [0] topology and leaf-list upload, [1] timestep and half-step
+ * launches, [2] locatebounds + fill plans (the device meanwhile runs the
+ * reduction and the half step), [3] wait for dt, [4] launches of the rest
+ * of tstep, [5] criteria (waits for the device), [6] admesh integer logic,
+ * [7] refine/coarse calls, [8] whole steps.  ms must hold W2D_SIM_NPHASES
+ * doubles; reset != 0 zeroes the counters after reading. */
+#define W2D_SIM_NPHASES 9
 int w2d_sim_phase_ms(W2dSim* sim, double* ms, int reset);
 
 #ifdef __cplusplus

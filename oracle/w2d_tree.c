@@ -124,6 +124,26 @@ static void initial_conditions(OrcSim* s, int nb)
       }
       double x = ((double)(i + IC(s, nb, 1)) - 0.5) * s->dx[lev];
       double y = ((double)(j + IC(s, nb, 2)) - 0.5) * s->dy[lev];
+      if (ic->kind == W2D_IC_SNR) {              /* ambient + src/sn.f90:19-62 */
+        U(s, nb, 0, i, j) = ic->rho0;
+        U(s, nb, 3, i, j) = p->cv * ic->p0;
+        if (p->neq > 4) U(s, nb, 4, i, j) = ic->rho0 * ic->xh0;
+        if (p->neq > 5) U(s, nb, 5, i, j) = -ic->rho0;
+        double rsc = ic->extra[3];
+        double xs = x * rsc, ys = y * rsc;
+        double R = sqrt((xs - ic->xc) * (xs - ic->xc) + (ys - ic->yc) * (ys - ic->yc) + ic->extra[4]);
+        if (R <= ic->rb) {
+          double dens = ic->extra[0];
+          double vr = (R / ic->rb) * ic->extra[1] / ic->extra[2];
+          U(s, nb, 0, i, j) = dens;
+          U(s, nb, 1, i, j) = dens * vr * (xs - ic->xc) / (R);
+          U(s, nb, 2, i, j) = dens * vr * (ys - ic->yc) / (R);
+          U(s, nb, 3, i, j) = 0.5 * dens * (vr * vr) + ic->e_dep;
+          if (p->neq > 4) U(s, nb, 4, i, j) = dens * 0.0;
+          if (p->neq > 5) U(s, nb, 5, i, j) = dens;
+        }
+        continue;
+      }
       double r2 = (x - ic->xc) * (x - ic->xc) + (y - ic->yc) * (y - ic->yc);
       U(s, nb, 0, i, j) = ic->rho0;
       U(s, nb, 3, i, j) = p->cv * ic->p0;

@@ -214,12 +214,12 @@ class Simulation:
     def set_amr(self, on: bool):
         self.L.w2d_sim_set_amr(self.h, 1 if on else 0)
 
-    PHASES = ("plan", "timestep_wait", "tstep_launch", "criteria_wait", "admesh_host",
-              "amr_calls", "step_total")
+    PHASES = ("topology", "dt_half_launch", "plan", "dt_wait", "tstep_launch", "criteria_wait",
+              "admesh_host", "amr_calls", "step_total")
 
     def phase_ms(self, reset: bool = False) -> dict:
         """Host wall-clock ms per phase of run() (w2d_sim_phase_ms)."""
-        ms = np.zeros(8)
+        ms = np.zeros(len(self.PHASES))
         self.L.w2d_sim_phase_ms(self.h, _pd(ms), 1 if reset else 0)
         return {k: float(ms[i]) for i, k in enumerate(self.PHASES)}
 

@@ -227,7 +227,91 @@ int stats_for(W2dCtx* c, const int* d_list, int n)
   return launch(c, "calcprim", [&] { return c->L->calcprim(c->neq, a, pa, d_list, n, 0, c->st); });
 }
 
+int tstep_ready(W2dCtx* c, bool need_bounds = true)
+{
+  if (!c->have_topology || (need_bounds && !c->have_bounds))
+    return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology and w2d_set_bounds first");
+  if (c->p.cooling == W2D_COOLINGDMC && !c->have_cooltab)
+    return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_cooltab first (COOLINGDMC)");
+  return W2D_OK;
+}
+
+// src/tstep.f90:27-47: hllcfluxes(nb,1) and step(nb,dt/2) of every leaf
+int half_step(W2dCtx* c, double dt, const double* dt_dev)
+{
+  PhysArgs pa = pargs(c);
+  KArgs a2 = kargs(c, c->d_fd2);
+  a2.dt_dev = dt_dev;
+  return launch(c, "half_step", [&] { return c->L->half(c->neq, a2, pa, dt, c->st); });
+}
+
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// the split timestep/tstep of w2d_internal.h
+
+// src/timestep.f90:7-61 as one reduction kernel; dt stays in device memory
+// and is copied, with the error word, to pinned memory behind it
+int ctx_dt_launch(W2dCtx* c)
+{
+  if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
+  const int nl = (int)c->leaves.size();
+  int rc = launch(c, "timestep", [&] {
+    return launch_dt(c->d_leaves, nl, c->d_cfl, c->d_dtcool, c->p.cooling == W2D_COOLINGDMC, c->p.cfl,
+                     c->p.psc, c->p.tsc, c->d_dtwork, c->d_dtcount, c->d_dt, c->st);
+  });
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(c->h_small, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(c->h_err, c->d_err, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaEventRecord(c->ev_dt, c->st));
+  return W2D_OK;
+}
+
+int ctx_half_step(W2dCtx* c)
+{
+  int rc = tstep_ready(c, false);   // the half step reads no fill plan
+  if (rc) return rc;
+  return half_step(c, 0.0, c->d_dt);
+}
+
+int ctx_dt_wait(W2dCtx* c, double* dt)
+{
+  CK(cudaEventSynchronize(c->ev_dt));
+  int rc = check_device(c);
+  if (rc) return rc;
+  *dt = c->h_small[0];
+  return W2D_OK;
+}
+
+// src/tstep.f90:49-126 after the half step: boundaryII (inside the full
+// step's gather), the full step with viscosity and u = up, boundaryI, then
+// calcprim or cooling
+int ctx_tstep_rest(W2dCtx* c, double time, double dt)
+{
+  int rc = tstep_ready(c);
+  if (rc) return rc;
+  PhysArgs pa = pargs(c);
+  KArgs a2 = kargs(c, c->d_fd2);
+  KArgs a1 = kargs(c, c->d_fd1);
+  set_jet_state(c, a2, time);   // both fills impose the jet at tstep's time
+  set_jet_state(c, a1, time);
+  const bool jet = a1.jet != 0;
+  if ((rc = launch(c, "full_step", [&] { return c->L->full(c->neq, a2, pa, dt, c->st); }))) return rc;
+  // boundaryI; with the jet its interior writes and the statistics follow in
+  // a second pass, after every fill read of the interiors
+  const int stats = c->p.cooling == W2D_ADIABATIC && !jet;
+  if ((rc = launch(c, "fill_I", [&] { return c->L->fill1(c->neq, a1, pa, stats, c->st); }))) return rc;
+  if (jet && c->p.cooling == W2D_ADIABATIC) {
+    const int nl = (int)c->leaves.size();
+    if ((rc = launch(c, "jet_calcprim", [&] { return c->L->calcprim(c->neq, a1, pa, c->d_leaves, nl, 1, c->st); })))
+      return rc;
+  }
+  if (c->p.cooling != W2D_ADIABATIC) {
+    const double dts = dt * c->p.tsc;
+    if ((rc = launch(c, "cooling", [&] { return c->L->cool(c->neq, a1, pa, dts, c->st); }))) return rc;
+  }
+  return W2D_OK;
+}
 
 // ===========================================================================
 extern "C" {
@@ -278,6 +362,7 @@ int w2d_create(const W2dParams* p, W2dCtx** out)
   CKC(cudaMalloc(&c->d_err, sizeof(int) * 4));
   CKC(cudaMalloc(&c->d_dt, sizeof(double) * 4));
   CKC(cudaMalloc(&c->d_cooltab, sizeof(double) * 82));
+  CKC(cudaMalloc(&c->d_leaves, sizeof(int) * slots));
   CKC(cudaMemsetAsync(c->d_lev, 0, sizeof(int) * slots, c->st));
   CKC(cudaMemsetAsync(c->d_icoord, 0, sizeof(int) * 2 * slots, c->st));
   CKC(cudaMemsetAsync(c->d_err, 0, sizeof(int) * 4, c->st));
@@ -304,8 +389,18 @@ int w2d_create(const W2dParams* p, W2dCtx** out)
   CKC(cudaMallocHost(&c->h_grad, sizeof(double) * slots));
   CKC(cudaMallocHost(&c->lev, sizeof(int) * slots));
   CKC(cudaMallocHost(&c->icoord, sizeof(int) * 2 * slots));
+  CKC(cudaMallocHost(&c->h_leaflist, sizeof(int) * slots));
   CKC(cudaEventCreateWithFlags(&c->ev_topo, cudaEventDisableTiming));
   CKC(cudaEventCreateWithFlags(&c->ev_ops, cudaEventDisableTiming));
+  CKC(cudaEventCreateWithFlags(&c->ev_dt, cudaEventDisableTiming));
+  for (int q = 0; q < 2; ++q) {   // fill plans: 4 faces per leaf, at most every slot a leaf
+    CKC(cudaMallocHost(&c->h_fd1[q], sizeof(int2) * 4 * slots));
+    CKC(cudaMallocHost(&c->h_fd2[q], sizeof(int2) * 4 * slots));
+    CKC(cudaMallocHost(&c->h_jetblk[q], sizeof(int) * slots));
+  }
+  CKC(cudaMalloc(&c->d_fd1, sizeof(int2) * 4 * slots));
+  CKC(cudaMalloc(&c->d_fd2, sizeof(int2) * 4 * slots));
+  CKC(cudaMalloc(&c->d_jetblk, sizeof(int) * slots));
   CKC(cudaEventCreateWithFlags(&c->ev_plan[0], cudaEventDisableTiming));
   CKC(cudaEventCreateWithFlags(&c->ev_plan[1], cudaEventDisableTiming));
   memset(c->h_err, 0, sizeof(int) * 4);
@@ -330,7 +425,7 @@ int w2d_destroy(W2dCtx* c)
   for (auto e : c->evpool) cudaEventDestroy(e);
   for (auto e : c->ev)
     if (e) cudaEventDestroy(e);
-  cudaEvent_t evs[] = {c->ev_topo, c->ev_ops, c->ev_plan[0], c->ev_plan[1]};
+  cudaEvent_t evs[] = {c->ev_topo, c->ev_ops, c->ev_plan[0], c->ev_plan[1], c->ev_dt};
   for (auto e : evs)
     if (e) cudaEventDestroy(e);
   void* dev[] = {c->d_u, c->d_up, c->d_prim, c->d_lev, c->d_icoord, c->d_cfl, c->d_dtcool, c->d_grad,
@@ -338,9 +433,8 @@ int w2d_destroy(W2dCtx* c)
                  c->d_flush, c->d_dtwork, c->d_dtcount, c->d_jetblk};
   for (void* d : dev)
     if (d) cudaFree(d);
-  void* host[] = {c->h_stage, c->h_small, c->h_grad, c->h_err, c->h_fd1[0], c->h_fd2[0], c->h_leaves[0],
-                  c->h_fd1[1], c->h_fd2[1], c->h_leaves[1], c->h_ops, c->lev, c->icoord,
-                  c->h_jetblk[0], c->h_jetblk[1]};
+  void* host[] = {c->h_stage, c->h_small, c->h_grad, c->h_err, c->h_fd1[0], c->h_fd2[0], c->h_leaflist,
+                  c->h_fd1[1], c->h_fd2[1], c->h_ops, c->lev, c->icoord, c->h_jetblk[0], c->h_jetblk[1]};
   for (void* h : host)
     if (h) cudaFreeHost(h);
   if (c->st) cudaStreamDestroy(c->st);
@@ -399,6 +493,11 @@ int w2d_set_topology(W2dCtx* c, const int32_t* lp, int ld_lp, const int32_t* lea
   CK(cudaMemcpyAsync(c->d_lev, c->lev, sizeof(int) * (size_t)(nbmax + 1), cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(c->d_icoord, c->icoord, sizeof(int) * 2 * (size_t)(nbmax + 1),
                      cudaMemcpyHostToDevice, c->st));
+  const size_t nl = c->leaves.size();
+  if (nl > 0) {
+    memcpy(c->h_leaflist, c->leaves.data(), sizeof(int) * nl);
+    CK(cudaMemcpyAsync(c->d_leaves, c->h_leaflist, sizeof(int) * nl, cudaMemcpyHostToDevice, c->st));
+  }
   CK(cudaEventRecord(c->ev_topo, c->st));
   c->have_topology = true;
   c->have_bounds = false;
@@ -413,45 +512,14 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
   if (!c || (!ib && n > 0) || n < 0 || ld < n) return W2D_ERR_ARG;
   if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
   const int nl = (int)c->leaves.size();
-  if (nl > c->h_plan_cap) {
-    CK(cudaStreamSynchronize(c->st));
-    for (int q = 0; q < 2; ++q) {
-      if (c->h_fd1[q]) cudaFreeHost(c->h_fd1[q]);
-      if (c->h_fd2[q]) cudaFreeHost(c->h_fd2[q]);
-      if (c->h_leaves[q]) cudaFreeHost(c->h_leaves[q]);
-      if (c->h_jetblk[q]) cudaFreeHost(c->h_jetblk[q]);
-      c->h_fd1[q] = c->h_fd2[q] = nullptr;
-      c->h_leaves[q] = c->h_jetblk[q] = nullptr;
-    }
-    if (c->d_fd1) cudaFree(c->d_fd1);
-    if (c->d_fd2) cudaFree(c->d_fd2);
-    if (c->d_leaves) cudaFree(c->d_leaves);
-    if (c->d_jetblk) cudaFree(c->d_jetblk);
-    c->d_fd1 = c->d_fd2 = nullptr;
-    c->d_leaves = c->d_jetblk = nullptr;
-    int cap = std::max(nl + nl / 2, 256);
-    for (int q = 0; q < 2; ++q) {
-      CK(cudaMallocHost(&c->h_fd1[q], sizeof(int2) * 4 * (size_t)cap));
-      CK(cudaMallocHost(&c->h_fd2[q], sizeof(int2) * 4 * (size_t)cap));
-      CK(cudaMallocHost(&c->h_leaves[q], sizeof(int) * (size_t)cap));
-      CK(cudaMallocHost(&c->h_jetblk[q], sizeof(int) * (size_t)cap));
-    }
-    CK(cudaMalloc(&c->d_fd1, sizeof(int2) * 4 * (size_t)cap));
-    CK(cudaMalloc(&c->d_fd2, sizeof(int2) * 4 * (size_t)cap));
-    CK(cudaMalloc(&c->d_leaves, sizeof(int) * (size_t)cap));
-    CK(cudaMalloc(&c->d_jetblk, sizeof(int) * (size_t)cap));
-    c->h_plan_cap = cap;
-  }
   // alternate pinned buffers; wait only for the upload that last used this one
   const int q = c->plan_buf;
   c->plan_buf ^= 1;
   CK(cudaEventSynchronize(c->ev_plan[q]));
   int2* hf1 = c->h_fd1[q];
   int2* hf2 = c->h_fd2[q];
-  int* hl = c->h_leaves[q];
   int* hj = c->h_jetblk[q];
   for (int k = 0; k < 4 * nl; ++k) hf1[k] = hf2[k] = make_int2(0, FK_KEEP);
-  for (int k = 0; k < nl; ++k) hl[k] = c->leaves[k];
   // impose_jet runs after every entry on its nbs (src/boundaryI.f90:386-393,
   // src/boundaryII.f90:505-512): first and last position of each block as nbs
   const bool jet = c->p.otherb == W2D_USERBC_JET;
@@ -556,7 +624,6 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
   if (nl > 0) {
     CK(cudaMemcpyAsync(c->d_fd1, hf1, sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->d_fd2, hf2, sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->d_leaves, hl, sizeof(int) * (size_t)nl, cudaMemcpyHostToDevice, c->st));
     if (jet) CK(cudaMemcpyAsync(c->d_jetblk, hj, sizeof(int) * (size_t)nl, cudaMemcpyHostToDevice, c->st));
   }
   CK(cudaEventRecord(c->ev_plan[q], c->st));
@@ -661,19 +728,8 @@ int w2d_get_u_fortran(W2dCtx* c, double* u, int ld, int nbmin, const int32_t* id
 int w2d_timestep(W2dCtx* c, double* dt)
 {
   if (!c || !dt) return W2D_ERR_ARG;
-  if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
-  const int nl = (int)c->leaves.size();
-  if (!c->have_bounds) {  // the leaf list lives with the plan
-    int rc = w2d_set_bounds(c, nullptr, 0, 0);
-    if (rc) return rc;
-    c->have_bounds = false;
-  }
-  int rc = launch(c, "timestep", [&] {
-    return launch_dt(c->d_leaves, nl, c->d_cfl, c->d_dtcool, c->p.cooling == W2D_COOLINGDMC, c->p.cfl,
-                     c->p.psc, c->p.tsc, c->d_dtwork, c->d_dtcount, c->d_dt, c->st);
-  });
+  int rc = ctx_dt_launch(c);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(c->h_small, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   if ((rc = sync_and_check(c))) return rc;
   *dt = c->h_small[0];
   return W2D_OK;
@@ -682,33 +738,10 @@ int w2d_timestep(W2dCtx* c, double* dt)
 int w2d_tstep(W2dCtx* c, double time, double dt)
 {
   if (!c) return W2D_ERR_ARG;
-  if (!c->have_topology || !c->have_bounds)
-    return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology and w2d_set_bounds first");
-  if (c->p.cooling == W2D_COOLINGDMC && !c->have_cooltab)
-    return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_cooltab first (COOLINGDMC)");
-  PhysArgs pa = pargs(c);
-  KArgs a2 = kargs(c, c->d_fd2);
-  KArgs a1 = kargs(c, c->d_fd1);
-  set_jet_state(c, a2, time);   // both fills impose the jet at tstep's time
-  set_jet_state(c, a1, time);
-  const bool jet = a1.jet != 0;
-  int rc;
-  if ((rc = launch(c, "half_step", [&] { return c->L->half(c->neq, a2, pa, dt, c->st); }))) return rc;
-  if ((rc = launch(c, "full_step", [&] { return c->L->full(c->neq, a2, pa, dt, c->st); }))) return rc;
-  // boundaryI; with the jet its interior writes and the statistics follow in
-  // a second pass, after every fill read of the interiors
-  const int stats = c->p.cooling == W2D_ADIABATIC && !jet;
-  if ((rc = launch(c, "fill_I", [&] { return c->L->fill1(c->neq, a1, pa, stats, c->st); }))) return rc;
-  if (jet && c->p.cooling == W2D_ADIABATIC) {
-    const int nl = (int)c->leaves.size();
-    if ((rc = launch(c, "jet_calcprim", [&] { return c->L->calcprim(c->neq, a1, pa, c->d_leaves, nl, 1, c->st); })))
-      return rc;
-  }
-  if (c->p.cooling != W2D_ADIABATIC) {
-    const double dts = dt * c->p.tsc;
-    if ((rc = launch(c, "cooling", [&] { return c->L->cool(c->neq, a1, pa, dts, c->st); }))) return rc;
-  }
-  return W2D_OK;
+  int rc = tstep_ready(c);
+  if (rc) return rc;
+  if ((rc = half_step(c, dt, nullptr))) return rc;
+  return ctx_tstep_rest(c, time, dt);
 }
 
 int w2d_criteria(W2dCtx* c, double* grad)
@@ -722,77 +755,66 @@ int w2d_criteria(W2dCtx* c, double* grad)
   return W2D_OK;
 }
 
-static int amr_ops(W2dCtx* c, const int32_t* quads, int n, bool refine)
+// One admesh pass worth of refines and coarsenings: host levels/icoord of
+// the new leaves, one pinned upload, one k_amr launch.
+static int amr_pass(W2dCtx* c, const int32_t* rq, int nr, const int32_t* cq, int nc)
 {
-  if (!c || n < 0 || (n > 0 && !quads)) return W2D_ERR_ARG;
-  if (n == 0) return W2D_OK;
+  if (!c || nr < 0 || nc < 0 || (nr > 0 && !rq) || (nc > 0 && !cq)) return W2D_ERR_ARG;
+  if (nr + nc == 0) return W2D_OK;
   if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
-  int rc = valid_ids(c, quads, 5 * n);
+  int rc = valid_ids(c, rq, 5 * nr);
   if (rc) return rc;
-  // staging layout: quads (5n), new leaves (<= 4n), (slot, level, ix, iy)
-  // of the new leaves (<= 16n); pinned, sent asynchronously, reused only
+  if ((rc = valid_ids(c, cq, 5 * nc))) return rc;
+  // staging layout: quads (5 per op, refines first), then (slot, level, ix,
+  // iy) per new leaf in CTA order; pinned, sent asynchronously, reused only
   // once the previous send has completed
-  if ((rc = ensure_ids(c, 25 * n))) return rc;
-  if (25 * n > c->h_ops_cap) {
+  const int nn = 4 * nr + nc;
+  const int words = 5 * (nr + nc) + 4 * nn;
+  if ((rc = ensure_ids(c, words))) return rc;
+  if (words > c->h_ops_cap) {
     CK(cudaEventSynchronize(c->ev_ops));
     if (c->h_ops) cudaFreeHost(c->h_ops);
     c->h_ops = nullptr;
-    c->h_ops_cap = std::max(25 * n, 8192);
+    c->h_ops_cap = std::max(words, 8192);
     CK(cudaMallocHost(&c->h_ops, sizeof(int) * (size_t)c->h_ops_cap));
   }
   CK(cudaEventSynchronize(c->ev_ops));
   CK(cudaEventSynchronize(c->ev_topo));   // host lev/icoord are not being uploaded
-  // the new leaves: levels and icoord as refine/coarse set them
-  std::vector<int> newl;
-  newl.reserve(4 * n);
+  int* h = c->h_ops;
+  if (nr) memcpy(h, rq, sizeof(int) * 5 * (size_t)nr);
+  if (nc) memcpy(h + 5 * nr, cq, sizeof(int) * 5 * (size_t)nc);
+  int* tup = h + 5 * (nr + nc);
   const int NX = W2D_NX;
-  for (int q = 0; q < n; ++q) {
-    const int* o = quads + 5 * q;
-    if (refine) {
-      const int l2 = c->lev[o[0]] + 1;
-      const int nx0 = c->icoord[2 * o[0]] * 2, ny0 = c->icoord[2 * o[0] + 1] * 2;  // refine.f90:42-43
-      for (int s = 0; s < 4; ++s) {
-        const int son = o[1 + s];
-        c->lev[son] = l2;
-        c->icoord[2 * son] = nx0 + ((s & 1) ? NX : 0);
-        c->icoord[2 * son + 1] = ny0 + ((s & 2) ? NX : 0);
-        newl.push_back(son);
-      }
-    } else {
-      newl.push_back(o[0]);
+  for (int q = 0; q < nr; ++q) {
+    const int* o = rq + 5 * q;
+    const int l2 = c->lev[o[0]] + 1;
+    const int nx0 = c->icoord[2 * o[0]] * 2, ny0 = c->icoord[2 * o[0] + 1] * 2;  // refine.f90:42-43
+    for (int s = 0; s < 4; ++s) {
+      const int son = o[1 + s];
+      c->lev[son] = l2;
+      c->icoord[2 * son] = nx0 + ((s & 1) ? NX : 0);
+      c->icoord[2 * son + 1] = ny0 + ((s & 2) ? NX : 0);
+      int* t = tup + 4 * (4 * q + s);
+      t[0] = son; t[1] = l2; t[2] = c->icoord[2 * son]; t[3] = c->icoord[2 * son + 1];
     }
   }
-  const int nn = (int)newl.size();
-  int* h = c->h_ops;
-  memcpy(h, quads, sizeof(int) * 5 * (size_t)n);
-  memcpy(h + 5 * n, newl.data(), sizeof(int) * (size_t)nn);
-  int* tup = h + 5 * n + nn;
-  for (int k = 0; k < nn; ++k) {
-    const int b = newl[k];
-    tup[4 * k] = b;
-    tup[4 * k + 1] = c->lev[b];
-    tup[4 * k + 2] = c->icoord[2 * b];
-    tup[4 * k + 3] = c->icoord[2 * b + 1];
+  for (int q = 0; q < nc; ++q) {
+    const int dad = cq[5 * q];
+    int* t = tup + 4 * (4 * nr + q);
+    t[0] = dad; t[1] = c->lev[dad]; t[2] = c->icoord[2 * dad]; t[3] = c->icoord[2 * dad + 1];
   }
-  const size_t nops = 5 * (size_t)n + 5 * (size_t)nn;
-  CK(cudaMemcpyAsync(c->d_ids, h, sizeof(int) * nops, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_ids, h, sizeof(int) * (size_t)words, cudaMemcpyHostToDevice, c->st));
   CK(cudaEventRecord(c->ev_ops, c->st));
-  if ((rc = launch(c, "set_slots", [&] {
-         return launch_set_slots(c->d_ids + 5 * n + nn, nn, c->d_lev, c->d_icoord, c->st);
-       })))
-    return rc;
-  if (refine)
-    rc = launch(c, "refine", [&] { return c->L->refine(c->neq, c->d_u, c->d_ids, n, c->st); });
-  else
-    rc = launch(c, "coarse", [&] { return c->L->coarse(c->neq, c->d_u, c->d_ids, n, c->st); });
-  if (rc) return rc;
-  // d_ids is reused by the next call only after this call's kernels (stream order)
-  if ((rc = stats_for(c, c->d_ids + 5 * n, (int)newl.size()))) return rc;
-  return W2D_OK;
+  KArgs a = kargs(c, c->d_fd1);
+  PhysArgs pa = pargs(c);
+  // d_ids is reused by the next call only after this call's kernel (stream order)
+  return launch(c, "refine_coarse", [&] {
+    return c->L->amr(c->neq, a, pa, c->d_ids, nr, nc, c->d_ids + 5 * (nr + nc), c->st);
+  });
 }
 
-int w2d_refine(W2dCtx* c, const int32_t* quads, int n) { return amr_ops(c, quads, n, true); }
-int w2d_coarse(W2dCtx* c, const int32_t* quads, int n) { return amr_ops(c, quads, n, false); }
+int w2d_refine(W2dCtx* c, const int32_t* quads, int n) { return amr_pass(c, quads, n, nullptr, 0); }
+int w2d_coarse(W2dCtx* c, const int32_t* quads, int n) { return amr_pass(c, nullptr, 0, quads, n); }
 
 int w2d_boundaryI(W2dCtx* c, double time)
 {
@@ -914,3 +936,5 @@ int w2d_flush_l2(W2dCtx* c)
 }
 
 }  // extern "C"
+
+int ctx_amr(W2dCtx* c, const int32_t* rq, int nr, const int32_t* cq, int nc) { return amr_pass(c, rq, nr, cq, nc); }

@@ -34,11 +34,12 @@ struct W2dCtx {
   unsigned long long* d_dtwork = nullptr;  // k_dt minima (bit patterns)
   unsigned int* d_dtcount = nullptr;       // k_dt CTA counter
   double* d_cooltab = nullptr;
-  // per-step plan
-  int* d_leaves = nullptr;
+  // leaf list (uploaded with the topology) and per-step plan
+  int* d_leaves = nullptr;  // one per slot
+  int* h_leaflist = nullptr; // pinned staging of d_leaves (guarded by ev_topo)
   int2* d_fd1 = nullptr;   // boundaryI (layer 0 of u)
   int2* d_fd2 = nullptr;   // boundaryII (two layers of up)
-  int plan_cap = 0;
+  cudaEvent_t ev_dt = nullptr;  // dt and the error word have reached h_small/h_err
   // scratch for host transfers
   void* d_stage = nullptr;
   size_t stage_bytes = 0;
@@ -53,13 +54,11 @@ struct W2dCtx {
   // from each buffer has been consumed
   int2* h_fd1[2] = {nullptr, nullptr};
   int2* h_fd2[2] = {nullptr, nullptr};
-  int* h_leaves[2] = {nullptr, nullptr};
   int* h_jetblk[2] = {nullptr, nullptr};
   int* d_jetblk = nullptr;                 // per leaf: named as nbs in the list
   std::vector<int> qfirst, qlast;          // per slot: first/last list position as nbs
   cudaEvent_t ev_plan[2] = {nullptr, nullptr};
   int plan_buf = 0;
-  int h_plan_cap = 0;
   // pinned staging of refine/coarse lists
   int* h_ops = nullptr;
   int h_ops_cap = 0;
@@ -94,3 +93,5 @@ struct W2dCtx {
 
   W2dError err{};
 };
+
+#include "w2d_internal.h"

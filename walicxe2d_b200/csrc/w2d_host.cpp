@@ -28,37 +28,42 @@
 #include <vector>
 
 #include "../../include/w2d.h"
+#include "w2d_internal.h"
 
-struct W2dSim {
-  W2dParams p{};
-  W2dInit ic{};
-  W2dCtx* ctx = nullptr;
-  int cap = 0, nbmax = 0, nbleafs = 0;
-  std::vector<int32_t> lp;                // row-major [(cap+1)][8]
-  std::vector<int32_t> leaf, icoord;      // column-major, ld = cap
-  std::vector<int32_t> levbuf;            // lp(:,1) as one column, for w2d_set_topology
-  std::vector<double> dx, dy;             // nlevs entries
-  std::vector<int32_t> ib;                // innerbounds, column-major, ld = nib
-  int nib = 0;
-  double time = 0.0, dt = 0.0;
-  int64_t steps = 0, zone_updates = 0;
-  bool amr = true;
-  bool dirty = true;
-  std::vector<unsigned char> irefup, irefdown;
-  std::vector<uint32_t> bounds;           // locatebounds flags, valid when == gen
-  uint32_t gen = 0;
-  std::vector<std::vector<int32_t>> bucket;  // leaves per level, ascending ID
-  std::vector<double> grad;
-  std::vector<int32_t> rops, cops;
-  std::vector<int32_t> ib1, ib2, ib3;
-  double phase_ms[8] = {0};               // see w2d_sim_phase_ms
+#include "w2d_tree.h"
 
-  int32_t& LP(int nb, int k) { return lp[(size_t)nb * 8 + (k - 1)]; }
-  int32_t& LEAF(int nb) { return leaf[(size_t)nb - 1]; }
-  int32_t& IC(int nb, int k) { return icoord[(size_t)(k - 1) * cap + (nb - 1)]; }
-};
+namespace w2dh {
 
-namespace {
+// Remnant set-up of one cell at code position (x, y): ambient gas with
+// neutral fraction xh0, then impose_sn (src/sn.f90:19-62) in the
+// reference's operation order, in cm:
+//   R = sqrt((x-xc)^2 + (y-yc)^2 + 0.1 dx(nlevs) rsc);  inside R <= Rsn:
+//   u = (dens, dens vr (x-xc)/R, dens vr (y-yc)/R, dens vr^2/2 + Eth, 0, dens)
+//   with vr = (R/Rsn) S1 / S2.
+// ic: xc, yc, rb = centre and Rsn in cm; e_dep = Eth (code);
+// extra = {dens, S1, S2, rsc, 0.1 dx(nlevs) rsc}.  u: cell (0,0) of
+// equation 0, equations `stride` apart.
+void snr_cell(const W2dParams& p, const W2dInit& ic, double x, double y, double* u, size_t stride)
+{
+  const int neq = p.neq;
+  u[0] = ic.rho0;
+  u[3 * stride] = p.cv * ic.p0;
+  if (neq > 4) u[4 * stride] = ic.rho0 * ic.xh0;
+  if (neq > 5) u[5 * stride] = -ic.rho0;
+  const double rsc = ic.extra[3];
+  const double xs = x * rsc, ys = y * rsc;
+  const double R = std::sqrt((xs - ic.xc) * (xs - ic.xc) + (ys - ic.yc) * (ys - ic.yc) + ic.extra[4]);
+  if (R <= ic.rb) {
+    const double dens = ic.extra[0];
+    const double vr = (R / ic.rb) * ic.extra[1] / ic.extra[2];
+    u[0] = dens;
+    u[stride] = dens * vr * (xs - ic.xc) / (R);
+    u[2 * stride] = dens * vr * (ys - ic.yc) / (R);
+    u[3 * stride] = 0.5 * dens * (vr * vr) + ic.e_dep;
+    if (neq > 4) u[4 * stride] = dens * 0.0;
+    if (neq > 5) u[5 * stride] = dens;
+  }
+}
 
 // Initial conditions of one block at its own resolution (the Sedov set-up,
 // or src/user_mod.f90:39-62 with impose_jet, src/jet.f90:41-78, at t = 0).
@@ -90,6 +95,10 @@ void initial_block(W2dSim* s, int nb, double* ub)
           if (neq > 4) at(4, i, j) = p.jet_den * 0.9999;
           if (neq > 5) at(5, i, j) = p.jet_den;
         }
+        continue;
+      }
+      if (ic.kind == W2D_IC_SNR) {
+        snr_cell(p, ic, x, y, &at(0, i, j), (size_t)W * W);
         continue;
       }
       const double r2 = (x - ic.xc) * (x - ic.xc) + (y - ic.yc) * (y - ic.yc);
@@ -236,34 +245,32 @@ double now_ms()
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+int push_bounds(W2dSim* s)
+{
+  locatebounds(s);
+  int rc = w2d_set_bounds(s->ctx, s->ib.data(), s->nib, s->nib);
+  if (rc) return rc;
+  s->dirty = false;
+  return W2D_OK;
+}
+
 int refresh_plan(W2dSim* s)
 {
   const double t0 = now_ms();
   int rc = push_topology(s);
   if (rc) return rc;
-  locatebounds(s);
-  rc = w2d_set_bounds(s->ctx, s->ib.data(), s->nib, s->nib);
-  if (rc) return rc;
-  s->dirty = false;
-  s->phase_ms[0] += now_ms() - t0;
+  if ((rc = push_bounds(s))) return rc;
+  s->phase_ms[2] += now_ms() - t0;
   return W2D_OK;
 }
 
-// src/admesh.f90:4-111 (np = 1).  The u motion of every refine and coarse
-// of the pass is batched into one device call each: within a pass no refine
-// or coarse reads a block that another one writes.
-int admesh(W2dSim* s)
+// src/admesh.f90:4-111 (np = 1), integer part: from the criteria maxima in
+// s->grad, the flags, the tree updates and the lists of refines (s->rops)
+// and coarsenings (s->cops) of the pass.
+int admesh_decide(W2dSim* s)
 {
   auto& L = *s;
   const int nlevs = s->p.nlevs;
-  int rc;
-  if (s->dirty && (rc = refresh_plan(s))) return rc;
-  // markref + criteria flags (criteria.f90:36-50 on the device maximum)
-  double t0 = now_ms();
-  rc = w2d_criteria(s->ctx, s->grad.data());
-  if (rc) return rc;
-  double t1 = now_ms();
-  s->phase_ms[3] += t1 - t0;
   std::fill(s->irefup.begin(), s->irefup.end(), 0);
   std::fill(s->irefdown.begin(), s->irefdown.end(), 0);
   // leaves per level in ascending ID (the only blocks that get flags)
@@ -326,19 +333,36 @@ int admesh(W2dSim* s)
         updatelpdown(s, dad, s1, s2, s3, s4);
       }
     }
-  const int nr = (int)s->rops.size() / 5, nc = (int)s->cops.size() / 5;
-  t0 = now_ms();
-  s->phase_ms[4] += t0 - t1;
-  if (nr && (rc = w2d_refine(s->ctx, s->rops.data(), nr))) return rc;
-  if (nc && (rc = w2d_coarse(s->ctx, s->cops.data(), nc))) return rc;
-  if (nr || nc) s->dirty = true;
-  s->phase_ms[5] += now_ms() - t0;
+  if (!s->rops.empty() || !s->cops.empty()) s->dirty = true;
   return W2D_OK;
 }
 
-// basegrid, generalized (see w2d.h); the initial conditions of every leaf
-// are uploaded in one w2d_put_blocks.
-int basegrid(W2dSim* s)
+// admesh of the single-run driver: criteria from the device, the integer
+// part, then the u motion of every refine and coarse of the pass in one
+// device call (within a pass no refine or coarse reads a block that another
+// one writes)
+int admesh(W2dSim* s)
+{
+  int rc;
+  if (s->dirty && (rc = refresh_plan(s))) return rc;
+  // markref + criteria flags (criteria.f90:36-50 on the device maximum)
+  double t0 = now_ms();
+  rc = w2d_criteria(s->ctx, s->grad.data());
+  if (rc) return rc;
+  double t1 = now_ms();
+  s->phase_ms[5] += t1 - t0;
+  if ((rc = admesh_decide(s))) return rc;
+  const int nr = (int)s->rops.size() / 5, nc = (int)s->cops.size() / 5;
+  t0 = now_ms();
+  s->phase_ms[6] += t0 - t1;
+  if ((nr || nc) && (rc = ctx_amr(s->ctx, s->rops.data(), nr, s->cops.data(), nc))) return rc;
+  s->phase_ms[7] += now_ms() - t0;
+  return W2D_OK;
+}
+
+// basegrid, generalized (see w2d.h): the tree, then the leaf IDs and their
+// initial conditions (block-major, neq x 20 x 20 each) in ids/blocks.
+int basegrid_tree(W2dSim* s, std::vector<int32_t>& ids, std::vector<double>& blocks)
 {
   auto& L = *s;
   const int nbx = s->p.nbroot_x, nby = s->p.nbroot_y;
@@ -369,34 +393,34 @@ int basegrid(W2dSim* s)
       s->nbmax += 4;
     }
   }
-  int rc = push_topology(s);
-  if (rc) return rc;
-  std::vector<int32_t> ids;
+  ids.clear();
   for (int nb = 1; nb <= s->nbmax; ++nb)
     if (L.LEAF(nb)) ids.push_back(nb);
   const size_t bs = (size_t)s->p.neq * (s->p.nx + 4) * (s->p.nx + 4);
-  std::vector<double> blocks(bs * ids.size());
+  blocks.assign(bs * ids.size(), 0.0);
   for (size_t q = 0; q < ids.size(); ++q) initial_block(s, ids[q], blocks.data() + q * bs);
-  rc = w2d_put_blocks(s->ctx, ids.data(), (int)ids.size(), blocks.data());
-  if (rc) return rc;
   s->dirty = true;
   return W2D_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-int w2d_sim_create(const W2dParams* p, const W2dInit* ic, W2dSim** out)
+// the single-run basegrid: tree, topology, initial conditions uploaded in
+// one w2d_put_blocks
+int basegrid(W2dSim* s)
 {
-  if (!p || !ic || !out) return W2D_ERR_ARG;
-  *out = nullptr;
-  W2dSim* s = new W2dSim();
+  std::vector<int32_t> ids;
+  std::vector<double> blocks;
+  int rc = basegrid_tree(s, ids, blocks);
+  if (rc) return rc;
+  if ((rc = push_topology(s))) return rc;
+  return w2d_put_blocks(s->ctx, ids.data(), (int)ids.size(), blocks.data());
+}
+
+// the host arrays of a run of capacity p->nblocks and its spacings
+void init_tree(W2dSim* s, const W2dParams* p, const W2dInit* ic)
+{
   s->p = *p;
   s->ic = *ic;
   s->cap = p->nblocks;
-  int rc = w2d_create(p, &s->ctx);
-  if (rc) { delete s; return rc; }
   s->lp.assign((size_t)8 * (s->cap + 1), 0);
   s->levbuf.assign((size_t)s->cap, 0);
   s->bucket.assign((size_t)p->nlevs + 1, std::vector<int32_t>());
@@ -413,6 +437,22 @@ int w2d_sim_create(const W2dParams* p, const W2dInit* ic, W2dSim** out)
     s->dy[l - 1] = p->ymax / p->ny / (std::pow(2., (double)(l - 1))) / (double)(p->nbroot_y);
   }
   s->amr = p->nlevs > 1;
+}
+
+}  // namespace w2dh
+
+using namespace w2dh;
+
+extern "C" {
+
+int w2d_sim_create(const W2dParams* p, const W2dInit* ic, W2dSim** out)
+{
+  if (!p || !ic || !out) return W2D_ERR_ARG;
+  *out = nullptr;
+  W2dSim* s = new W2dSim();
+  init_tree(s, p, ic);
+  int rc = w2d_create(p, &s->ctx);
+  if (rc) { delete s; return rc; }
   if ((rc = basegrid(s))) { w2d_sim_destroy(s); return rc; }
   for (int k = 0; k < ic->startup_admesh && p->nlevs > 1; ++k)   // src/main.f90:60-63
     if ((rc = admesh(s))) { w2d_sim_destroy(s); return rc; }
@@ -432,30 +472,48 @@ int w2d_sim_run(W2dSim* s, int nsteps)
 {
   if (!s || nsteps < 0) return W2D_ERR_ARG;
   int rc;
+  // timestep + tstep as the split sequence of w2d_internal.h: after a mesh
+  // change the new leaf list goes up first, the device runs the time-step
+  // reduction and the half step while the host walks the new block list
+  // (locatebounds) and builds the fill plans, and the host reads dt back
+  // before the full step
   for (int n = 0; n < nsteps; ++n) {
     const double t0 = now_ms();
-    if (s->dirty && (rc = refresh_plan(s))) return rc;
-    double dt = 0.0;
+    const bool replan = s->dirty;
+    if (replan && (rc = push_topology(s))) return rc;
     const double t1 = now_ms();
-    if ((rc = w2d_timestep(s->ctx, &dt))) return rc;       // src/main.f90:87
+    if ((rc = ctx_dt_launch(s->ctx))) return rc;            // src/main.f90:87
+    if ((rc = ctx_half_step(s->ctx))) return rc;            // src/main.f90:95 (first pass)
     const double t2 = now_ms();
+    if (replan && (rc = push_bounds(s))) return rc;
+    const double t3 = now_ms();
+    double dt = 0.0;
+    if ((rc = ctx_dt_wait(s->ctx, &dt))) return rc;
+    const double t4 = now_ms();
     s->dt = dt;
     s->time = s->time + dt;                                 // src/main.f90:88
-    if ((rc = w2d_tstep(s->ctx, s->time, dt))) return rc;   // src/main.f90:95
+    if ((rc = ctx_tstep_rest(s->ctx, s->time, dt))) return rc;
+    const double t5 = now_ms();
+    s->phase_ms[0] += t1 - t0;
     s->phase_ms[1] += t2 - t1;
-    s->phase_ms[2] += now_ms() - t2;
+    s->phase_ms[2] += t3 - t2;
+    s->phase_ms[3] += t4 - t3;
+    s->phase_ms[4] += t5 - t4;
     s->zone_updates += (int64_t)s->nbleafs * s->p.nx * s->p.ny;
     if (s->amr && (rc = admesh(s))) return rc;              // src/main.f90:98
     s->steps++;
-    s->phase_ms[6] += now_ms() - t0;
+    s->phase_ms[8] += now_ms() - t0;
   }
+  // without AMR nothing has waited for the last step's kernels: check their
+  // error word now (with AMR the criteria wait has done so)
+  if (!s->amr && nsteps > 0) return w2d_sync(s->ctx);
   return W2D_OK;
 }
 
 int w2d_sim_phase_ms(W2dSim* s, double* ms, int reset)
 {
   if (!s || !ms) return W2D_ERR_ARG;
-  for (int k = 0; k < 8; ++k) ms[k] = s->phase_ms[k];
+  for (int k = 0; k < W2D_SIM_NPHASES; ++k) ms[k] = s->phase_ms[k];
   if (reset)
     for (double& v : s->phase_ms) v = 0.0;
   return W2D_OK;

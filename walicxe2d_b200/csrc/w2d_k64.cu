@@ -58,25 +58,6 @@ __global__ void __launch_bounds__(256) k_dt(const int* __restrict__ leaves, int 
   }
 }
 
-// level and icoord of new leaves from (slot, level, ix, iy) tuples
-__global__ void k_set_slots(const int* __restrict__ t, int n, int* __restrict__ lev, int* __restrict__ icoord)
-{
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) {
-    const int b = t[4 * k];
-    lev[b] = t[4 * k + 1];
-    icoord[2 * b] = t[4 * k + 2];
-    icoord[2 * b + 1] = t[4 * k + 3];
-  }
-}
-
-cudaError_t launch_set_slots(const int* tuples, int n, int* lev, int* icoord, cudaStream_t st)
-{
-  if (n == 0) return cudaSuccess;
-  k_set_slots<<<(n + 127) / 128, 128, 0, st>>>(tuples, n, lev, icoord);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_dt(const int* leaves, int n, const double* cfl, const double* dtcool, int use_cool,
                       double courant, double psc, double tsc, unsigned long long* work, unsigned int* count,
                       double* dt_out, cudaStream_t st)

@@ -61,6 +61,7 @@ struct KArgs {
   double jet_posx, jet_posy, jet_lj, jet_rj;
   double jet_u[6];
   const int* jetblk;      // per leaf position: block appears as nbs in the list
+  const double* dt_dev;   // k_half: dt read from here when not null
 };
 
 // flags of a face descriptor (bits 16..18 of .y) for impose_jet ordering:
@@ -462,7 +463,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_half(KArgs a, PhysArgs pa, doub
   const bool dmc = pa.cooling == COOL_DMC;
   load_tile<R, NEQ>(&st[0][0][0], dmc ? (const R*)a.prim + (size_t)b * bs : u, bar, a.err, b);
   const int lev = a.lev[b];
-  const double dtm = dt / 2.;
+  const double dtm = (a.dt_dev ? *a.dt_dev : dt) / 2.;
   const R dtdx = R(dtm / a.dx[lev]);
   const R dtdy = R(dtm / a.dy[lev]);
   if (!wait_tiles(bar, a.err, b)) return;
@@ -801,64 +802,106 @@ __global__ void __launch_bounds__(256) k_jet_only(KArgs a, R* pool)
 }
 
 // ---------------------------------------------------------------------------
-// refine data motion, src/refine.f90:30-38: son s (1..4) of parent p takes
-// u(p, (i+1)/2 [+8], (j+1)/2 [+8]) for all 20x20 cells.  One CTA per son.
+// The data motion of one admesh pass in one launch, each CTA then doing
+// calcprim and the block statistics of the new leaf it wrote:
+//   CTA k < 4*nr   son k%4 of refine k/4 (src/refine.f90:30-38): son u(i,j) =
+//                  parent u((i+1)/2 [+8], (j+1)/2 [+8]) for all 20x20 cells
+//   CTA k >= 4*nr  the parent of coarsening k-4*nr (src/coarse.f90:29-176,
+//                  serial build, nghost = 2): 2x2 means of the sons' interior
+//                  and ghost strips; the 12 outer corner cells the reference
+//                  leaves untouched keep their values
+// ops: nr + nc quads (parent or dad, s1..s4); tup: per CTA (slot, level, ix,
+// iy) of the new leaf, written to lev/icoord first.  Within a pass no block
+// that one op writes is read by another (refines read leaves and write new
+// or inactive slots, coarsenings read leaves and write non-leaves).
 template <typename R, int NEQ>
-__global__ void __launch_bounds__(256) k_refine(R* __restrict__ u, const int* __restrict__ quads)
+__host__ __device__ constexpr size_t smem_amr()
 {
-  const int op = blockIdx.x >> 2, s = blockIdx.x & 3;
-  const int parent = quads[op * 5], son = quads[op * 5 + 1 + s];
-  const int ox = (s & 1) ? W2D_NX / 2 : 0, oy = (s & 2) ? W2D_NX / 2 : 0;
-  const size_t bs = (size_t)NEQ * W2D_CELLS;
-  const R* __restrict__ pu = u + (size_t)parent * bs;
-  R* __restrict__ su = u + (size_t)son * bs;
-  for (int c = threadIdx.x; c < NEQ * W2D_CELLS; c += blockDim.x) {
-    const int k = c / W2D_CELLS, r = c % W2D_CELLS;
-    const int i = r % W2D_W - 1, j = r / W2D_W - 1;
-    su[c] = pu[k * W2D_CELLS + cidx((i + 1) / 2 + ox, (j + 1) / 2 + oy)];
-  }
+  return smem_calcprim<R, NEQ>();
 }
 
-// coarse data motion, src/coarse.f90:29-176 (serial build, nghost = 2).
-// One thread per (equation, destination cell); the 12 outer corner cells
-// the reference leaves untouched are left untouched.
 template <typename R, int NEQ>
-__global__ void __launch_bounds__(256) k_coarse(R* __restrict__ u, const int* __restrict__ quads)
+__global__ void __launch_bounds__(W2D_THREADS) k_amr(KArgs a, PhysArgs pa, const int* __restrict__ ops, int nr,
+                                                     const int* __restrict__ tup)
 {
-  const int op = blockIdx.x;
-  const int dad = quads[op * 5];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
+  R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
+  R* stf = &st[0][0][0];
+  double* sred = reinterpret_cast<double*>(w2d_smem + 128 + sizeof(R) * NEQ * W2D_CELLS);
+  const Phys<R> ph = make_phys<R, -1, -1>(pa);
+  const int k = blockIdx.x, tid = threadIdx.x;
+  const int b = tup[4 * k];
   const size_t bs = (size_t)NEQ * W2D_CELLS;
-  R* __restrict__ du = u + (size_t)dad * bs;
-  const int NX = W2D_NX, H = W2D_NX / 2;
-  for (int c = threadIdx.x; c < NEQ * W2D_CELLS; c += blockDim.x) {
-    const int k = c / W2D_CELLS, r = c % W2D_CELLS;
-    const int i = r % W2D_W - 1, j = r / W2D_W - 1;
-    const bool gx = (i < 1 || i > NX), gy = (j < 1 || j > NX);
-    int son, i1, j1;
-    const int sx = (i > H), sy = (j > H);
-    son = 1 + sx + 2 * sy;
-    if (!gx && !gy) {                       // interior, :32-51
-      i1 = 2 * (i - sx * H) - 1;
-      j1 = 2 * (j - sy * H) - 1;
-    } else if (gx && gy) {                  // inner corners only, :108-159
-      if (!((i == 0 || i == NX + 1) && (j == 0 || j == NX + 1))) continue;
-      i1 = sx ? NX + 1 : -1;
-      j1 = sy ? NX + 1 : -1;
-    } else if (gx) {                        // left/right ghosts, :112-138
-      i1 = sx ? NX + 1 : -1;
-      j1 = 2 * (j - sy * H) - 1;
-    } else {                                // bottom/top ghosts, :144-170
-      i1 = 2 * (i - sx * H) - 1;
-      j1 = sy ? NX + 1 : -1;
-    }
-    const R* s = u + (size_t)quads[op * 5 + son] * bs + k * W2D_CELLS;
-    R t = R(0.);
-    t += s[cidx(i1, j1)];
-    t += s[cidx(i1 + 1, j1)];
-    t += s[cidx(i1, j1 + 1)];
-    t += s[cidx(i1 + 1, j1 + 1)];
-    du[c] = R(0.25) * t;
+  R* __restrict__ u = (R*)a.u + (size_t)b * bs;
+  if (tid == 0) {
+    const_cast<int*>(a.lev)[b] = tup[4 * k + 1];
+    const_cast<int*>(a.icoord)[2 * b] = tup[4 * k + 2];
+    const_cast<int*>(a.icoord)[2 * b + 1] = tup[4 * k + 3];
   }
+  const int NX = W2D_NX, H = W2D_NX / 2;
+  if (k < 4 * nr) {
+    const int op = k >> 2, s = k & 3;
+    const R* __restrict__ pu = (const R*)a.u + (size_t)ops[op * 5] * bs;
+    const int ox = (s & 1) ? H : 0, oy = (s & 2) ? H : 0;
+    for (int c = tid; c < NEQ * W2D_CELLS; c += W2D_THREADS) {
+      const int q = c / W2D_CELLS, r = c % W2D_CELLS;
+      const int i = r % W2D_W - 1, j = r / W2D_W - 1;
+      stf[c] = pu[q * W2D_CELLS + cidx((i + 1) / 2 + ox, (j + 1) / 2 + oy)];
+    }
+  } else {
+    const int op = nr + (k - 4 * nr);
+    load_tile<R, NEQ>(stf, u, bar, a.err, b);
+    if (!wait_tiles(bar, a.err, b)) return;
+    for (int c = tid; c < NEQ * W2D_CELLS; c += W2D_THREADS) {
+      const int q = c / W2D_CELLS, r = c % W2D_CELLS;
+      const int i = r % W2D_W - 1, j = r / W2D_W - 1;
+      const bool gx = (i < 1 || i > NX), gy = (j < 1 || j > NX);
+      const int sx = (i > H), sy = (j > H);
+      const int son = 1 + sx + 2 * sy;
+      int i1, j1;
+      if (!gx && !gy) {                       // interior, :32-51
+        i1 = 2 * (i - sx * H) - 1;
+        j1 = 2 * (j - sy * H) - 1;
+      } else if (gx && gy) {                  // inner corners only, :108-159
+        if (!((i == 0 || i == NX + 1) && (j == 0 || j == NX + 1))) continue;
+        i1 = sx ? NX + 1 : -1;
+        j1 = sy ? NX + 1 : -1;
+      } else if (gx) {                        // left/right ghosts, :112-138
+        i1 = sx ? NX + 1 : -1;
+        j1 = 2 * (j - sy * H) - 1;
+      } else {                                // bottom/top ghosts, :144-170
+        i1 = 2 * (i - sx * H) - 1;
+        j1 = sy ? NX + 1 : -1;
+      }
+      const R* sp = (const R*)a.u + (size_t)ops[op * 5 + son] * bs + q * W2D_CELLS;
+      R t = R(0.);
+      t += sp[cidx(i1, j1)];
+      t += sp[cidx(i1 + 1, j1)];
+      t += sp[cidx(i1, j1 + 1)];
+      t += sp[cidx(i1 + 1, j1 + 1)];
+      stf[c] = R(0.25) * t;
+    }
+  }
+  __syncthreads();
+  // the new u, then calcprim (src/calcprim.f90:5-21) and the statistics
+  R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;
+  for (int c = tid; c < NEQ * W2D_CELLS; c += W2D_THREADS) u[c] = stf[c];
+  __syncthreads();
+  for (int c = tid; c < W2D_CELLS; c += W2D_THREADS) {
+    const int ti = c % W2D_W, tj = c / W2D_W;
+    R uu[NEQ], q[NEQ], T;
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) uu[e] = st[e][tj][ti];
+    uprim<NEQ>(ph, q, uu, T);
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) st[e][tj][ti] = q[e];
+    if (pb) {
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e) pb[e * W2D_CELLS + c] = q[e];
+    }
+  }
+  __syncthreads();
+  block_stats<R, NEQ>(st, ph, a, pa, b, sred);
 }
 
 // pool <-> staging (block-major) copies

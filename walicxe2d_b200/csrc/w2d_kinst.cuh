@@ -130,18 +130,24 @@ static cudaError_t jet_only(int neq, const KArgs& a, void* pool, cudaStream_t st
   return cudaGetLastError();
 }
 
-static cudaError_t refine(int neq, void* u, const int* quads, int n, cudaStream_t st)
+template <int NEQ>
+static cudaError_t amr_t(const KArgs& a, const PhysArgs& pa, const int* ops, int nr, int nc, const int* tup,
+                         cudaStream_t st)
 {
-  if (n == 0) return cudaSuccess;
-  W2D_NEQ_SWITCH(neq, (k_refine<R, NEQ><<<4 * n, 256, 0, st>>>((R*)u, quads)));
+  static bool done = false;
+  constexpr size_t sm = smem_amr<R, NEQ>();
+  cudaError_t e = smem_opt_in(k_amr<R, NEQ>, sm, done);
+  if (e != cudaSuccess) return e;
+  k_amr<R, NEQ><<<4 * nr + nc, W2D_THREADS, sm, st>>>(a, pa, ops, nr, tup);
   return cudaGetLastError();
 }
 
-static cudaError_t coarse(int neq, void* u, const int* quads, int n, cudaStream_t st)
+static cudaError_t amr(int neq, const KArgs& a, const PhysArgs& pa, const int* ops, int nr, int nc,
+                       const int* tup, cudaStream_t st)
 {
-  if (n == 0) return cudaSuccess;
-  W2D_NEQ_SWITCH(neq, (k_coarse<R, NEQ><<<n, 256, 0, st>>>((R*)u, quads)));
-  return cudaGetLastError();
+  if (nr + nc == 0) return cudaSuccess;
+  W2D_NEQ_SWITCH(neq, return (amr_t<NEQ>(a, pa, ops, nr, nc, tup, st)));
+  return cudaSuccess;
 }
 
 template <int NEQ>
@@ -185,8 +191,8 @@ static cudaError_t to_prim(int neq, const PhysArgs& pa, const void* u, void* out
   return cudaGetLastError();
 }
 
-static const Launchers table = {half,   full,    fill1,  fill_only, calcprim, jet_only,
-                                refine, coarse,  cool,   scatter,   gather,   to_prim, sizeof(R)};
+static const Launchers table = {half, full,    fill1,  fill_only, calcprim, jet_only,
+                                amr,  cool,    scatter, gather,   to_prim,  sizeof(R)};
 
 }  // namespace W2D_INST_NS
 }  // namespace w2d

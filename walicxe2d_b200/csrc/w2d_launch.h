@@ -16,8 +16,9 @@ struct Launchers {
   cudaError_t (*calcprim)(int neq, const KArgs&, const PhysArgs&, const int* list, int n, int jet_interior,
                           cudaStream_t);
   cudaError_t (*jet_only)(int neq, const KArgs&, void* pool, cudaStream_t);
-  cudaError_t (*refine)(int neq, void* u, const int* quads, int n, cudaStream_t);
-  cudaError_t (*coarse)(int neq, void* u, const int* quads, int n, cudaStream_t);
+  // nr refines then nc coarsenings (ops: quads), tup: (slot, level, ix, iy) per new leaf
+  cudaError_t (*amr)(int neq, const KArgs&, const PhysArgs&, const int* ops, int nr, int nc, const int* tup,
+                     cudaStream_t);
   cudaError_t (*cool)(int neq, const KArgs&, const PhysArgs&, double dt_s, cudaStream_t);
   cudaError_t (*scatter)(void* pool, const void* stage, const int* ids, int n, size_t bs, cudaStream_t);
   cudaError_t (*gather)(const void* pool, void* stage, const int* ids, int n, size_t bs, cudaStream_t);
@@ -27,9 +28,6 @@ struct Launchers {
 
 const Launchers& launchers64();
 const Launchers& launchers32();
-
-// lev[slot], icoord[2*slot..] from n tuples (slot, level, ix, iy)
-cudaError_t launch_set_slots(const int* tuples, int n, int* lev, int* icoord, cudaStream_t st);
 
 // work: two 64-bit words holding the bit pattern of 1e30; count: zero.
 // Both are restored by the kernel for the next call.

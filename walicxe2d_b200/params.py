@@ -173,6 +173,66 @@ def jet(nbroot_x: int = 32, nbroot_y: int = 8, nlevs: int = 7, cooling: int = CO
     return p, ic
 
 
+def snr(nbroot: int = 10, nlevs: int = 6, n_amb: float = 1.0, t_amb: float = 1.0e4, xh: float = 0.9,
+        e_sn: float = 1.0e51, m_sn: float = 4.0 * MSUN, r_sn: float = 1.0 * PC, chi: float = 0.5,
+        size_pc: float = 40.0, nblocks: int | None = None, tol: float = 0.1, precision: int = 64, **kw):
+    """Supernova remnant with coolingh (src/sn.f90 parameterized): a
+    size_pc x size_pc box of nbroot x nbroot roots, ambient n_amb cm^-3 at
+    t_amb K with neutral fraction xh, and impose_sn at the centre: ejecta of
+    mass m_sn (g) spread over radius r_sn (cm) with density (3/4pi) M/R^3 *
+    1.3/2.1, linear velocity profile holding a fraction chi of e_sn (erg) as
+    kinetic energy and the rest as uniform thermal energy.  m_sn = 0 (with
+    chi = 0) leaves the ambient density and deposits e_sn as heat only: a
+    Sedov blast in physical units.  neq = 6 (neutral density, tracer)."""
+    if nblocks is None:
+        nblocks = 60000
+    p = base_params(neq=6, npas=2, nlevs=nlevs, nbroot_x=nbroot, nbroot_y=nbroot, nblocks=nblocks,
+                    cooling=COOLINGH, tol=tol, precision=precision, **kw)
+    sc = scalings(size_pc * PC, p.xmax, p.cv)
+    p.tempsc, p.psc, p.tsc, p.rsc = sc["tempsc"], sc["psc"], sc["tsc"], sc["rsc"]
+    ic = W2dInit()
+    ic.kind = IC_SNR
+    ic.init_levels = 1
+    ic.startup_admesh = nlevs - 1 if nlevs > 1 else 0
+    ic.rho0 = n_amb
+    ic.p0 = (2.0 - xh) * n_amb * t_amb / sc["tempsc"]
+    ic.xh0 = xh
+    ic.xc = 0.5 * p.xmax * sc["rsc"]
+    ic.yc = 0.5 * p.ymax * sc["rsc"]
+    ic.rb = r_sn
+    pi = math.pi
+    r3 = r_sn * r_sn * r_sn
+    if m_sn > 0.0:
+        dens = 3.0 / 4.0 / pi * m_sn / r3 * 1.3 / 2.1 / sc["rhosc"]
+        s1 = math.sqrt(10.0 * chi * e_sn / (3.0 * m_sn))
+    else:
+        dens, s1 = n_amb, 0.0
+    ic.e_dep = 3.0 / 4.0 / pi * e_sn * (1.0 - chi) / r3 / sc["psc"]
+    dxn = p.xmax / p.nx / (2.0 ** (nlevs - 1)) / nbroot
+    for k, v in enumerate([dens, s1, math.sqrt(sc["vsc2"]), sc["rsc"], 0.1 * dxn * sc["rsc"]]):
+        ic.extra[k] = v
+    return p, ic
+
+
+def ensemble_members(count: int = 256, seed: int = 20261203, precision: int = 32, size_pc: float = 40.0):
+    """Independent Sedov-with-coolingh runs of uneven size, run r drawn with
+    seed + r: roots k x k with k uniform in 2..16, levels uniform in 3..6,
+    ambient n log-uniform in [0.1, 10] cm^-3, E log-uniform in [1e50, 1e51]
+    erg deposited as heat within 1 pc; T = 1e4 K, neutral fraction 0.9."""
+    import numpy as np
+    out = []
+    for r in range(count):
+        g = np.random.default_rng(seed + r)
+        k = int(g.integers(2, 17))
+        nl = int(g.integers(3, 7))
+        n = float(10.0 ** g.uniform(-1.0, 1.0))
+        e = float(10.0 ** g.uniform(50.0, 51.0))
+        cap = max(4 * k * k * (1 << (2 * (nl - 1))) // 6, 4 * k * k + 64)
+        out.append(snr(nbroot=k, nlevs=nl, n_amb=n, e_sn=e, m_sn=0.0, chi=0.0, size_pc=size_pc,
+                       nblocks=min(cap, 40000), precision=precision))
+    return out
+
+
 def config(name: str):
     """Named workloads: 'sedov64' (4x4 roots, no AMR), 'sedov_amr' (8x8
     roots, 5 levels, tol 0.1) and small test variants."""
@@ -188,4 +248,8 @@ def config(name: str):
         return jet(nbroot_x=8, nbroot_y=2, nlevs=3, cooling=COOLINGDMC, nblocks=4000, rj_cm=8.0e15)
     if name == "jet_dmc":
         return jet()
+    if name == "snr":
+        return snr()
+    if name == "snr_small":
+        return snr(nbroot=4, nlevs=3, nblocks=4000, size_pc=10.0)
     raise KeyError(name)
