@@ -256,6 +256,36 @@ int w2d_sim_set_cooltab(W2dSim* sim, const double* log_t, const double* neg_log_
 #define W2D_SIM_NPHASES 9
 int w2d_sim_phase_ms(W2dSim* sim, double* ms, int reset);
 
+/* ---- Ensembles (no counterpart in the reference) ---------------------------
+ * nruns independent runs of the driver above advanced together on one
+ * device: p[r], ic[r] as for w2d_sim_create (physics, precision and method
+ * fields equal across runs; root grid, levels, capacity and initial
+ * conditions free; no user boundary).  Run r owns the pool slots
+ * base+1 .. base+cap (w2d_ens_run_slots) and numbers its blocks 1..cap.
+ * One w2d_ens_run step advances every run by one step of its own dt; each
+ * run's results equal those of the run alone.  threads: host threads for
+ * the per-run integer work (0: one per core). */
+typedef struct W2dEns W2dEns;
+int w2d_ens_create(const W2dParams* p, const W2dInit* ic, int nruns, int threads, W2dEns** out);
+int w2d_ens_destroy(W2dEns* ens);
+int w2d_ens_run(W2dEns* ens, int nsteps);
+/* as w2d_sim_status for run `run`; run = -1 sums nbmax, leaves and
+ * zone-updates over the runs (time and dt 0, steps = ensemble steps) */
+int w2d_ens_status(W2dEns* ens, int run, double* time, double* dt, int64_t* steps,
+                   int32_t* nbmax, int32_t* nleaf, int64_t* zone_updates);
+W2dCtx* w2d_ens_ctx(W2dEns* ens);
+int w2d_ens_run_slots(W2dEns* ens, int run, int32_t* base, int32_t* cap);
+/* leaf block IDs of a run (ascending, run numbering); ids may be NULL */
+int w2d_ens_leaves(W2dEns* ens, int run, int32_t* ids, int32_t* n);
+int w2d_ens_set_amr(W2dEns* ens, int on);
+/* Host wall-clock ms per phase of w2d_ens_run: [0] leaf lists, [1] dt and
+ * half-step launches with locatebounds + fill plans of the changed runs,
+ * [2] launches of the rest of tstep, [3] unused, [4] criteria (waits for
+ * the device), [5] admesh integer logic, [6] refine/coarse call, [7] whole
+ * steps. */
+#define W2D_ENS_NPHASES 8
+int w2d_ens_phase_ms(W2dEns* ens, double* ms, int reset);
+
 #ifdef __cplusplus
 }
 #endif

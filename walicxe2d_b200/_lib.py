@@ -60,6 +60,15 @@ SIGNATURES = {
     "w2d_sim_set_amr": (_I, [_vp, _I]),
     "w2d_sim_set_cooltab": (_I, [_vp, _PD, _PD, _I]),
     "w2d_sim_phase_ms": (_I, [_vp, _PD, _I]),
+    "w2d_ens_create": (_I, [C.POINTER(W2dParams), C.POINTER(W2dInit), _I, _I, C.POINTER(_vp)]),
+    "w2d_ens_destroy": (_I, [_vp]),
+    "w2d_ens_run": (_I, [_vp, _I]),
+    "w2d_ens_status": (_I, [_vp, _I, _PD, _PD, C.POINTER(C.c_int64), _PI32, _PI32, C.POINTER(C.c_int64)]),
+    "w2d_ens_ctx": (_vp, [_vp]),
+    "w2d_ens_run_slots": (_I, [_vp, _I, _PI32, _PI32]),
+    "w2d_ens_leaves": (_I, [_vp, _I, _PI32, _PI32]),
+    "w2d_ens_set_amr": (_I, [_vp, _I]),
+    "w2d_ens_phase_ms": (_I, [_vp, _PD, _I]),
 }
 
 _LIB = None

@@ -268,3 +268,83 @@ class Simulation:
             _, lf, _, _ = self.tree()
             ids = np.nonzero(lf)[0].astype(np.int32)
         return np.asarray(ids, np.int32), self.ctx.get_blocks(ids)
+
+
+class Ensemble:
+    """Independent runs advanced together on one device (w2d_ens_*).
+
+    members: (W2dParams, W2dInit) per run; physics, method and precision
+    fields must agree, root grid, levels, capacity and initial conditions
+    may differ.  Run r's blocks live in pool slots base_r + ID.
+    """
+
+    PHASES = ("leaves", "dt_half_plans", "tstep_launch", "unused", "criteria_wait", "admesh_host",
+              "amr_calls", "step_total")
+
+    def __init__(self, members, threads: int = 0):
+        self.L = _lib.load()
+        n = len(members)
+        self.members = [(p.copy(), ic) for p, ic in members]
+        P = (W2dParams * n)(*[m[0] for m in self.members])
+        I = (W2dInit * n)(*[m[1] for m in self.members])
+        h = C.c_void_p()
+        rc = self.L.w2d_ens_create(P, I, n, threads, C.byref(h))
+        if rc:
+            raise _lib.W2dException(rc, None, "w2d_ens_create")
+        self.h = h
+        self.n = n
+        self.ctx = Context(self.members[0][0], handle=self.L.w2d_ens_ctx(self.h), owner=self)
+
+    def close(self):
+        if self.h:
+            self.L.w2d_ens_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, nsteps: int):
+        rc = self.L.w2d_ens_run(self.h, nsteps)
+        if rc:
+            self.ctx._check(rc, "w2d_ens_run")
+
+    def set_amr(self, on: bool):
+        self.L.w2d_ens_set_amr(self.h, 1 if on else 0)
+
+    def status(self, run: int = -1) -> dict:
+        t, dt = C.c_double(), C.c_double()
+        steps, zu = C.c_int64(), C.c_int64()
+        nbmax, nleaf = C.c_int32(), C.c_int32()
+        rc = self.L.w2d_ens_status(self.h, run, C.byref(t), C.byref(dt), C.byref(steps), C.byref(nbmax),
+                                   C.byref(nleaf), C.byref(zu))
+        if rc:
+            raise _lib.W2dException(rc, None, "w2d_ens_status")
+        return dict(time=t.value, dt=dt.value, steps=steps.value, nbmax=nbmax.value,
+                    nleaf=nleaf.value, zone_updates=zu.value)
+
+    def slots(self, run: int) -> tuple[int, int]:
+        b, c = C.c_int32(), C.c_int32()
+        self.L.w2d_ens_run_slots(self.h, run, C.byref(b), C.byref(c))
+        return b.value, c.value
+
+    def leaves(self, run: int) -> np.ndarray:
+        n = C.c_int32()
+        self.L.w2d_ens_leaves(self.h, run, None, C.byref(n))
+        ids = np.zeros(max(n.value, 1), np.int32)
+        self.L.w2d_ens_leaves(self.h, run, _pi32(ids), C.byref(n))
+        return ids[: n.value]
+
+    def blocks(self, run: int) -> tuple[np.ndarray, np.ndarray]:
+        """Leaf IDs (run numbering) and their u, block-major."""
+        ids = self.leaves(run)
+        base, _ = self.slots(run)
+        return ids, self.ctx.get_blocks(ids + base)
+
+    def phase_ms(self, reset: bool = False) -> dict:
+        ms = np.zeros(len(self.PHASES))
+        self.L.w2d_ens_phase_ms(self.h, _pd(ms), 1 if reset else 0)
+        return {k: float(ms[i]) for i, k in enumerate(self.PHASES)}
+

@@ -104,7 +104,7 @@ KArgs kargs(W2dCtx* c, const int2* fd)
   a.up = c->d_up;
   a.prim = c->d_prim;
   a.leaves = c->d_leaves;
-  a.nleaf = (int)c->leaves.size();
+  a.nleaf = c->nleaf;
   a.lev = c->d_lev;
   a.icoord = c->d_icoord;
   a.fd = fd;
@@ -123,6 +123,12 @@ KArgs kargs(W2dCtx* c, const int2* fd)
   }
   a.jet = c->p.otherb == W2D_USERBC_JET;
   a.jetblk = c->d_jetblk;
+  a.tsc = c->p.tsc;
+  if (c->nruns > 0) {
+    a.run_of = c->d_run_of;
+    a.runs = c->d_runs;
+    a.dt_run = c->d_dt_run;
+  }
   return a;
 }
 
@@ -227,6 +233,98 @@ int stats_for(W2dCtx* c, const int* d_list, int n)
   return launch(c, "calcprim", [&] { return c->L->calcprim(c->neq, a, pa, d_list, n, 0, c->st); });
 }
 
+// Face descriptors of the listed leaf slots back to "keep" (no writer).
+void plan_reset(int2* hf1, int2* hf2, const int* leaves, int nl)
+{
+  for (int k = 0; k < nl; ++k) {
+    const size_t b = (size_t)leaves[k] * 4;
+    for (int f = 0; f < 4; ++f) hf1[b + f] = hf2[b + f] = make_int2(0, FK_KEEP);
+  }
+}
+
+// The entries of one innerbounds list (columns nbs, neighbour, type; ld
+// apart; block IDs 1..nbmax_local of a run whose slots start after `base`)
+// into the per-slot descriptors hf1 (boundaryI) and hf2 (boundaryII), in
+// list order so that the last writer of every leaf face wins.  Leaves of
+// different runs occupy different slots, so runs can be planned at once.
+int plan_entries(W2dCtx* c, int2* hf1, int2* hf2, const int32_t* ib, int ld, int n, int base, int nbmax_local,
+                 bool jet)
+{
+  auto jetted_before = [&](int blk, int e) {
+    return blk >= 1 && blk <= nbmax_local && c->qfirst[blk] && c->qfirst[blk] < e;
+  };
+  auto put = [&](int2* fd, int blk, int face, int nbr, int kind, int off, int e) {
+    if (blk < 1 || blk > nbmax_local) return;
+    const int g = base + blk;
+    if (!c->leaf[g]) return;  // non-leaf targets are never read before being rewritten
+    int y = kind | (off << 8);
+    if (jet) {
+      const int s1 = (kind == FK_MIRROR || kind == FK_REFLECT) ? blk : nbr;
+      if (jetted_before(s1, e)) y |= FD_SRC1_JET;
+      if (kind == FK_RESTRICT && jetted_before(nbr + (face < 2 ? 2 : 1), e)) y |= FD_SRC2_JET;
+      if (c->qlast[blk] >= e) y |= FD_DST_JET;
+    }
+    fd[(size_t)g * 4 + face] = make_int2(base + nbr, y);
+  };
+  int e = 0;
+  auto both = [&](int blk, int face, int nbr, int kind, int off) {
+    put(hf1, blk, face, nbr, kind, off, e);
+    put(hf2, blk, face, nbr, kind, off, e);
+  };
+  const int H = W2D_NX / 2;
+  const int bc[4] = {c->p.bc_left, c->p.bc_right, c->p.bc_bottom, c->p.bc_top};
+  const bool f6b = (c->p.compat & W2D_COMPAT_OUTFYB) != 0;
+  for (e = 1; e <= n; ++e) {
+    const int nbs = ib[e - 1], n1 = ib[(size_t)ld + e - 1], t = ib[2 * (size_t)ld + e - 1];
+    if (nbs < 1 || nbs > nbmax_local || (t > 0 && (n1 < 1 || n1 > nbmax_local)))
+      return set_error(c, W2D_ERR_TOPOLOGY, nbs, e, t, "innerbounds entry %d (%d,%d,%d) out of range", e, nbs, n1, t);
+    switch (t) {
+      case -1: case -2: case -4: {
+        const int f = (t == -1) ? 0 : (t == -2) ? 1 : 3;
+        both(nbs, f, nbs, bc[f] == W2D_BC_REFLECTIVE ? FK_REFLECT : FK_MIRROR, 0);
+        break;
+      }
+      case -3:
+        if (bc[2] == W2D_BC_REFLECTIVE) {
+          both(nbs, 2, nbs, FK_REFLECT, 0);
+        } else {
+          put(hf2, nbs, 2, nbs, FK_MIRROR, 0, e);
+          // src/boundaryI.f90:87 fills block "nb" (the list index e)
+          const int tb = f6b ? e : nbs;
+          put(hf1, tb, 2, tb, FK_MIRROR, 0, e);
+        }
+        break;
+      case 1:  both(nbs, 0, n1, FK_SAME, 0);  both(n1, 1, nbs, FK_SAME, 0); break;
+      case 4:  both(nbs, 1, n1, FK_SAME, 0);  both(n1, 0, nbs, FK_SAME, 0); break;
+      case 7:  both(nbs, 2, n1, FK_SAME, 0);  both(n1, 3, nbs, FK_SAME, 0); break;
+      case 10: both(nbs, 3, n1, FK_SAME, 0);  both(n1, 2, nbs, FK_SAME, 0); break;
+      case 2:
+        both(nbs, 0, n1, FK_RESTRICT, 0);
+        both(n1, 1, nbs, FK_INJECT, 0);
+        both(n1 + 2, 1, nbs, FK_INJECT, H);
+        break;
+      case 5:
+        both(nbs, 1, n1, FK_RESTRICT, 0);
+        both(n1, 0, nbs, FK_INJECT, 0);
+        both(n1 + 2, 0, nbs, FK_INJECT, H);
+        break;
+      case 8:
+        both(nbs, 2, n1, FK_RESTRICT, 0);
+        both(n1, 3, nbs, FK_INJECT, 0);
+        both(n1 + 1, 3, nbs, FK_INJECT, H);
+        break;
+      case 11:
+        both(nbs, 3, n1, FK_RESTRICT, 0);
+        both(n1, 2, nbs, FK_INJECT, 0);
+        both(n1 + 1, 2, nbs, FK_INJECT, H);
+        break;
+      default:
+        return set_error(c, W2D_ERR_TOPOLOGY, nbs, e, t, "innerbounds type %d not in the serial list", t);
+    }
+  }
+  return W2D_OK;
+}
+
 int tstep_ready(W2dCtx* c, bool need_bounds = true)
 {
   if (!c->have_topology || (need_bounds && !c->have_bounds))
@@ -255,7 +353,7 @@ int half_step(W2dCtx* c, double dt, const double* dt_dev)
 int ctx_dt_launch(W2dCtx* c)
 {
   if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
-  const int nl = (int)c->leaves.size();
+  const int nl = c->nleaf;
   int rc = launch(c, "timestep", [&] {
     return launch_dt(c->d_leaves, nl, c->d_cfl, c->d_dtcool, c->p.cooling == W2D_COOLINGDMC, c->p.cfl,
                      c->p.psc, c->p.tsc, c->d_dtwork, c->d_dtcount, c->d_dt, c->st);
@@ -302,7 +400,7 @@ int ctx_tstep_rest(W2dCtx* c, double time, double dt)
   const int stats = c->p.cooling == W2D_ADIABATIC && !jet;
   if ((rc = launch(c, "fill_I", [&] { return c->L->fill1(c->neq, a1, pa, stats, c->st); }))) return rc;
   if (jet && c->p.cooling == W2D_ADIABATIC) {
-    const int nl = (int)c->leaves.size();
+    const int nl = c->nleaf;
     if ((rc = launch(c, "jet_calcprim", [&] { return c->L->calcprim(c->neq, a1, pa, c->d_leaves, nl, 1, c->st); })))
       return rc;
   }
@@ -428,6 +526,11 @@ int w2d_destroy(W2dCtx* c)
   cudaEvent_t evs[] = {c->ev_topo, c->ev_ops, c->ev_plan[0], c->ev_plan[1], c->ev_dt};
   for (auto e : evs)
     if (e) cudaEventDestroy(e);
+  void* dev2[] = {c->d_run_of, c->d_runs, c->d_dt_run, c->d_loff};
+  for (void* d : dev2)
+    if (d) cudaFree(d);
+  if (c->h_dt_run) cudaFreeHost(c->h_dt_run);
+  if (c->h_loff) cudaFreeHost(c->h_loff);
   void* dev[] = {c->d_u, c->d_up, c->d_prim, c->d_lev, c->d_icoord, c->d_cfl, c->d_dtcool, c->d_grad,
                  c->d_err, c->d_dt, c->d_cooltab, c->d_leaves, c->d_fd1, c->d_fd2, c->d_stage, c->d_ids,
                  c->d_flush, c->d_dtwork, c->d_dtcount, c->d_jetblk};
@@ -494,6 +597,7 @@ int w2d_set_topology(W2dCtx* c, const int32_t* lp, int ld_lp, const int32_t* lea
   CK(cudaMemcpyAsync(c->d_icoord, c->icoord, sizeof(int) * 2 * (size_t)(nbmax + 1),
                      cudaMemcpyHostToDevice, c->st));
   const size_t nl = c->leaves.size();
+  c->nleaf = (int)nl;
   if (nl > 0) {
     memcpy(c->h_leaflist, c->leaves.data(), sizeof(int) * nl);
     CK(cudaMemcpyAsync(c->d_leaves, c->h_leaflist, sizeof(int) * nl, cudaMemcpyHostToDevice, c->st));
@@ -511,7 +615,6 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
 {
   if (!c || (!ib && n > 0) || n < 0 || ld < n) return W2D_ERR_ARG;
   if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
-  const int nl = (int)c->leaves.size();
   // alternate pinned buffers; wait only for the upload that last used this one
   const int q = c->plan_buf;
   c->plan_buf ^= 1;
@@ -519,11 +622,11 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
   int2* hf1 = c->h_fd1[q];
   int2* hf2 = c->h_fd2[q];
   int* hj = c->h_jetblk[q];
-  for (int k = 0; k < 4 * nl; ++k) hf1[k] = hf2[k] = make_int2(0, FK_KEEP);
-  // impose_jet runs after every entry on its nbs (src/boundaryI.f90:386-393,
-  // src/boundaryII.f90:505-512): first and last position of each block as nbs
+  plan_reset(hf1, hf2, c->leaves.data(), (int)c->leaves.size());
   const bool jet = c->p.otherb == W2D_USERBC_JET;
   if (jet) {
+    // impose_jet runs after every entry on its nbs (src/boundaryI.f90:386-393,
+    // src/boundaryII.f90:505-512): first and last position of each block as nbs
     if ((int)c->qfirst.size() != c->cap + 1) {
       c->qfirst.assign((size_t)c->cap + 1, 0);
       c->qlast.assign((size_t)c->cap + 1, 0);
@@ -535,85 +638,15 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
       c->qlast[nbs] = e;
     }
   }
-  auto jetted_before = [&](int blk, int e) { return blk >= 1 && blk <= c->nbmax && c->qfirst[blk] && c->qfirst[blk] < e; };
-  auto put = [&](int2* fd, int blk, int face, int nbr, int kind, int off, int e) {
-    if (blk < 1 || blk > c->nbmax) return;
-    const int li = c->leaf_index[blk];
-    if (li < 0) return;  // non-leaf targets are never read before being rewritten
-    int y = kind | (off << 8);
-    if (jet) {
-      const int s1 = (kind == FK_MIRROR || kind == FK_REFLECT) ? blk : nbr;
-      if (jetted_before(s1, e)) y |= FD_SRC1_JET;
-      if (kind == FK_RESTRICT && jetted_before(nbr + (face < 2 ? 2 : 1), e)) y |= FD_SRC2_JET;
-      if (c->qlast[blk] >= e) y |= FD_DST_JET;
-    }
-    fd[li * 4 + face] = make_int2(nbr, y);
-  };
-  int e = 0;
-  auto both = [&](int blk, int face, int nbr, int kind, int off) {
-    put(hf1, blk, face, nbr, kind, off, e);
-    put(hf2, blk, face, nbr, kind, off, e);
-  };
-  const int H = W2D_NX / 2;
-  const int bc[4] = {c->p.bc_left, c->p.bc_right, c->p.bc_bottom, c->p.bc_top};
-  const bool f6b = (c->p.compat & W2D_COMPAT_OUTFYB) != 0;
-  for (e = 1; e <= n; ++e) {
-    const int nbs = ib[e - 1], n1 = ib[(size_t)ld + e - 1], t = ib[2 * (size_t)ld + e - 1];
-    if (nbs < 1 || nbs > c->nbmax || (t > 0 && (n1 < 1 || n1 > c->nbmax)))
-      return set_error(c, W2D_ERR_TOPOLOGY, nbs, e, t, "innerbounds entry %d (%d,%d,%d) out of range", e, nbs, n1, t);
-    switch (t) {
-      case -1: case -2: case -4: {
-        const int f = (t == -1) ? 0 : (t == -2) ? 1 : 3;
-        both(nbs, f, nbs, bc[f] == W2D_BC_REFLECTIVE ? FK_REFLECT : FK_MIRROR, 0);
-        break;
-      }
-      case -3:
-        if (bc[2] == W2D_BC_REFLECTIVE) {
-          both(nbs, 2, nbs, FK_REFLECT, 0);
-        } else {
-          put(hf2, nbs, 2, nbs, FK_MIRROR, 0, e);
-          // src/boundaryI.f90:87 fills block "nb" (the list index e)
-          const int tb = f6b ? e : nbs;
-          put(hf1, tb, 2, tb, FK_MIRROR, 0, e);
-        }
-        break;
-      case 1:  both(nbs, 0, n1, FK_SAME, 0);  both(n1, 1, nbs, FK_SAME, 0); break;
-      case 4:  both(nbs, 1, n1, FK_SAME, 0);  both(n1, 0, nbs, FK_SAME, 0); break;
-      case 7:  both(nbs, 2, n1, FK_SAME, 0);  both(n1, 3, nbs, FK_SAME, 0); break;
-      case 10: both(nbs, 3, n1, FK_SAME, 0);  both(n1, 2, nbs, FK_SAME, 0); break;
-      case 2:
-        both(nbs, 0, n1, FK_RESTRICT, 0);
-        both(n1, 1, nbs, FK_INJECT, 0);
-        both(n1 + 2, 1, nbs, FK_INJECT, H);
-        break;
-      case 5:
-        both(nbs, 1, n1, FK_RESTRICT, 0);
-        both(n1, 0, nbs, FK_INJECT, 0);
-        both(n1 + 2, 0, nbs, FK_INJECT, H);
-        break;
-      case 8:
-        both(nbs, 2, n1, FK_RESTRICT, 0);
-        both(n1, 3, nbs, FK_INJECT, 0);
-        both(n1 + 1, 3, nbs, FK_INJECT, H);
-        break;
-      case 11:
-        both(nbs, 3, n1, FK_RESTRICT, 0);
-        both(n1, 2, nbs, FK_INJECT, 0);
-        both(n1 + 1, 2, nbs, FK_INJECT, H);
-        break;
-      default:
-        return set_error(c, W2D_ERR_TOPOLOGY, nbs, e, t, "innerbounds type %d not in the serial list", t);
-    }
-  }
+  int rc = plan_entries(c, hf1, hf2, ib, ld, n, 0, c->nbmax, jet);
   if (jet) {
     // faces no entry writes still get the jet if their block is ever nbs;
     // the interior of such a block always does
-    for (int li = 0; li < nl; ++li) {
-      const int b = c->leaves[li];
-      hj[li] = c->qfirst[b] > 0;
+    for (int b : c->leaves) {
+      hj[b] = c->qfirst[b] > 0;
       for (int f = 0; f < 4; ++f) {
-        if (hj[li] && (hf1[li * 4 + f].y & 0xff) == FK_KEEP) hf1[li * 4 + f].y |= FD_DST_JET;
-        if (hj[li] && (hf2[li * 4 + f].y & 0xff) == FK_KEEP) hf2[li * 4 + f].y |= FD_DST_JET;
+        if (hj[b] && (hf1[b * 4 + f].y & 0xff) == FK_KEEP) hf1[b * 4 + f].y |= FD_DST_JET;
+        if (hj[b] && (hf2[b * 4 + f].y & 0xff) == FK_KEEP) hf2[b * 4 + f].y |= FD_DST_JET;
       }
     }
     for (int k = 1; k <= n; ++k) {   // clear for the next list
@@ -621,11 +654,11 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
       if (nbs >= 1 && nbs <= c->nbmax) c->qfirst[nbs] = c->qlast[nbs] = 0;
     }
   }
-  if (nl > 0) {
-    CK(cudaMemcpyAsync(c->d_fd1, hf1, sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->d_fd2, hf2, sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
-    if (jet) CK(cudaMemcpyAsync(c->d_jetblk, hj, sizeof(int) * (size_t)nl, cudaMemcpyHostToDevice, c->st));
-  }
+  if (rc) return rc;
+  const size_t ns = (size_t)c->nbmax + 1;
+  CK(cudaMemcpyAsync(c->d_fd1, hf1, sizeof(int2) * 4 * ns, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_fd2, hf2, sizeof(int2) * 4 * ns, cudaMemcpyHostToDevice, c->st));
+  if (jet) CK(cudaMemcpyAsync(c->d_jetblk, hj, sizeof(int) * ns, cudaMemcpyHostToDevice, c->st));
   CK(cudaEventRecord(c->ev_plan[q], c->st));
   c->have_bounds = true;
   return W2D_OK;
@@ -842,7 +875,7 @@ int w2d_calcprim(W2dCtx* c)
 {
   if (!c) return W2D_ERR_ARG;
   if (!c->have_bounds) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_bounds first");
-  return stats_for(c, c->d_leaves, (int)c->leaves.size());
+  return stats_for(c, c->d_leaves, c->nleaf);
 }
 
 static int cooling_only(W2dCtx* c, double dt_s, int mode)
@@ -938,3 +971,137 @@ int w2d_flush_l2(W2dCtx* c)
 }  // extern "C"
 
 int ctx_amr(W2dCtx* c, const int32_t* rq, int nr, const int32_t* cq, int nc) { return amr_pass(c, rq, nr, cq, nc); }
+
+// ---------------------------------------------------------------------------
+// ensembles (w2d_internal.h)
+
+int ctx_set_runs(W2dCtx* c, int nruns, const int* base, const int* cap, const double* dx, const double* dy,
+                 const int* nlevs)
+{
+  if (!c || nruns < 1 || c->nruns) return W2D_ERR_ARG;
+  if (c->p.otherb != W2D_USERBC_NONE)
+    return set_error(c, W2D_ERR_ARG, 0, 0, 0, "ensembles take no user boundary (impose_jet)");
+  const size_t slots = (size_t)c->cap + 1;
+  std::vector<int> run_of(slots, 0);
+  std::vector<RunGeo> geo((size_t)nruns);
+  for (int r = 0; r < nruns; ++r) {
+    if (base[r] < 0 || cap[r] < 1 || (size_t)base[r] + cap[r] >= slots + 0u || nlevs[r] < 1 ||
+        nlevs[r] > W2D_MAXLEV)
+      return set_error(c, W2D_ERR_ARG, r, 0, 0, "run %d: slots %d+1..%d outside the pool", r, base[r],
+                       base[r] + cap[r]);
+    for (int k = 1; k <= cap[r]; ++k) run_of[(size_t)base[r] + k] = r;
+    memset(&geo[r], 0, sizeof(RunGeo));
+    for (int l = 0; l <= W2D_MAXLEV; ++l) {
+      geo[r].dx[l] = dx[(size_t)r * (W2D_MAXLEV + 1) + l];
+      geo[r].dy[l] = dy[(size_t)r * (W2D_MAXLEV + 1) + l];
+    }
+    geo[r].nlevs = nlevs[r];
+  }
+  CK(cudaMalloc(&c->d_run_of, sizeof(int) * slots));
+  CK(cudaMalloc(&c->d_runs, sizeof(RunGeo) * (size_t)nruns));
+  CK(cudaMalloc(&c->d_dt_run, sizeof(double) * (size_t)nruns));
+  CK(cudaMalloc(&c->d_loff, sizeof(int) * (size_t)(nruns + 1)));
+  CK(cudaMallocHost(&c->h_dt_run, sizeof(double) * (size_t)nruns));
+  CK(cudaMallocHost(&c->h_loff, sizeof(int) * (size_t)(nruns + 1)));
+  CK(cudaMemcpy(c->d_run_of, run_of.data(), sizeof(int) * slots, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_runs, geo.data(), sizeof(RunGeo) * (size_t)nruns, cudaMemcpyHostToDevice));
+  CK(cudaMemset(c->d_dt_run, 0, sizeof(double) * (size_t)nruns));
+  c->nruns = nruns;
+  c->nbmax = c->cap;
+  return W2D_OK;
+}
+
+int ctx_run_topology(W2dCtx* c, int base, int nbmax, const int32_t* lev, const int32_t* leaf,
+                     const int32_t* icoord, int ld_icoord)
+{
+  for (int nb = 1; nb <= nbmax; ++nb) {
+    const int g = base + nb;
+    c->lev[g] = lev[nb - 1];
+    c->leaf[g] = leaf[nb - 1] != 0;
+    c->icoord[2 * g] = icoord[nb - 1];
+    c->icoord[2 * g + 1] = icoord[(size_t)ld_icoord + nb - 1];
+  }
+  return W2D_OK;
+}
+
+void ctx_run_leaf_flags(W2dCtx* c, int base, int nbmax, const int32_t* leaf)
+{
+  for (int nb = 1; nb <= nbmax; ++nb) c->leaf[base + nb] = leaf[nb - 1] != 0;
+}
+
+int ctx_upload_topology(W2dCtx* c)
+{
+  CK(cudaEventSynchronize(c->ev_topo));
+  const size_t slots = (size_t)c->cap + 1;
+  CK(cudaMemcpyAsync(c->d_lev, c->lev, sizeof(int) * slots, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_icoord, c->icoord, sizeof(int) * 2 * slots, cudaMemcpyHostToDevice, c->st));
+  CK(cudaEventRecord(c->ev_topo, c->st));
+  c->have_topology = true;
+  return W2D_OK;
+}
+
+int* ctx_leaf_staging(W2dCtx* c)
+{
+  if (cudaEventSynchronize(c->ev_topo) != cudaSuccess) return nullptr;
+  return c->h_leaflist;
+}
+
+int ctx_commit_leaves(W2dCtx* c, int nl, const int* loff)
+{
+  memcpy(c->h_loff, loff, sizeof(int) * (size_t)(c->nruns + 1));
+  if (nl > 0) CK(cudaMemcpyAsync(c->d_leaves, c->h_leaflist, sizeof(int) * (size_t)nl, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_loff, c->h_loff, sizeof(int) * (size_t)(c->nruns + 1), cudaMemcpyHostToDevice, c->st));
+  CK(cudaEventRecord(c->ev_topo, c->st));
+  c->nleaf = nl;
+  c->have_topology = true;
+  return W2D_OK;
+}
+
+int ctx_ens_dt_launch(W2dCtx* c)
+{
+  int rc = launch(c, "timestep", [&] {
+    return launch_dt_runs(c->d_leaves, c->d_loff, c->nruns, c->d_cfl, c->d_dtcool,
+                          c->p.cooling == W2D_COOLINGDMC, c->p.cfl, c->p.psc, c->p.tsc, c->d_dt_run, c->st);
+  });
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(c->h_dt_run, c->d_dt_run, sizeof(double) * (size_t)c->nruns, cudaMemcpyDeviceToHost, c->st));
+  return W2D_OK;
+}
+
+const double* ctx_ens_dt(W2dCtx* c) { return c->h_dt_run; }
+
+void* ctx_plan_begin(W2dCtx* c)
+{
+  if (cudaEventSynchronize(c->ev_plan[0]) != cudaSuccess) return nullptr;
+  return c->h_fd1[0];
+}
+
+int ctx_plan_run(W2dCtx* c, const int32_t* ib, int ld, int n, int base, int nbmax_local, const int* leaves, int nl)
+{
+  int2* hf1 = c->h_fd1[0];
+  int2* hf2 = c->h_fd2[0];
+  plan_reset(hf1, hf2, leaves, nl);
+  return plan_entries(c, hf1, hf2, ib, ld, n, base, nbmax_local, false);
+}
+
+int ctx_plan_upload(W2dCtx* c, int lo, int hi)
+{
+  if (hi >= lo) {
+    const size_t off = (size_t)lo * 4, cnt = (size_t)(hi - lo + 1) * 4;
+    CK(cudaMemcpyAsync(c->d_fd1 + off, c->h_fd1[0] + off, sizeof(int2) * cnt, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_fd2 + off, c->h_fd2[0] + off, sizeof(int2) * cnt, cudaMemcpyHostToDevice, c->st));
+  }
+  CK(cudaEventRecord(c->ev_plan[0], c->st));
+  c->have_bounds = true;
+  return W2D_OK;
+}
+
+int ctx_ens_criteria(W2dCtx* c, int hi, const double** grad)
+{
+  if (hi > 0)
+    CK(cudaMemcpyAsync(c->h_grad, c->d_grad + 1, sizeof(double) * (size_t)hi, cudaMemcpyDeviceToHost, c->st));
+  int rc = sync_and_check(c);
+  if (rc) return rc;
+  *grad = c->h_grad;   // grad of slot g at [g - 1]
+  return W2D_OK;
+}

@@ -119,8 +119,9 @@ __global__ void __launch_bounds__(W2D_THREADS) k_cool(KArgs a, PhysArgs pa, doub
   R* __restrict__ u = (R*)a.u + (size_t)b * bs;
   R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;
   load_tile<R, NEQ>(&st[0][0][0], u, bar, a.err, b);
+  if (a.run_of) dt_s = a.dt_run[a.run_of[b]] * a.tsc;   // dt*tsc of the block's run
   if (!wait_tiles(bar, a.err, b)) return;
-  if (a.jet && a.jetblk[blockIdx.x]) {   // impose_jet of boundaryI, before cooling
+  if (a.jet && a.jetblk[b]) {   // impose_jet of boundaryI, before cooling
     jet_interior_fn<R, NEQ>(st, a, b, u);
     __syncthreads();
   }

@@ -40,6 +40,15 @@ struct W2dCtx {
   int2* d_fd1 = nullptr;   // boundaryI (layer 0 of u)
   int2* d_fd2 = nullptr;   // boundaryII (two layers of up)
   cudaEvent_t ev_dt = nullptr;  // dt and the error word have reached h_small/h_err
+  // ensembles (nruns > 0): run of every slot, per-run geometry and dt, and
+  // the offsets of each run's leaves in d_leaves
+  int nruns = 0;
+  int* d_run_of = nullptr;
+  w2d::RunGeo* d_runs = nullptr;
+  double* d_dt_run = nullptr;
+  double* h_dt_run = nullptr;   // pinned
+  int* d_loff = nullptr;
+  int* h_loff = nullptr;        // pinned, nruns + 1
   // scratch for host transfers
   void* d_stage = nullptr;
   size_t stage_bytes = 0;
@@ -70,7 +79,8 @@ struct W2dCtx {
   int* icoord = nullptr;               // 2 per slot
   cudaEvent_t ev_topo = nullptr;
   std::vector<int> leaf;               // per slot
-  std::vector<int> leaves;             // leaf slots, ascending
+  std::vector<int> leaves;             // leaf slots, ascending (one run)
+  int nleaf = 0;                       // entries of d_leaves
   std::vector<int> leaf_index;         // slot -> position in leaves, -1
   int nbmax = 0;
   double dx[W2D_MAXLEV + 1] = {0}, dy[W2D_MAXLEV + 1] = {0};

@@ -4,6 +4,10 @@
 
 #include "../../include/w2d.h"
 
+#ifndef W2D_MAXLEV
+#define W2D_MAXLEV 16   // levels a context supports
+#endif
+
 // Split of timestep + tstep used by the whole-run driver so that the host
 // builds the fill plan while the device runs the time-step reduction and
 // the half step.  The sequence
@@ -19,3 +23,33 @@ int ctx_tstep_rest(W2dCtx* c, double time, double dt);  // full step, boundaryI,
 // The refines (rq, nr quads) and coarsenings (cq, nc quads) of one admesh
 // pass in one launch; equal to w2d_refine(rq) followed by w2d_coarse(cq).
 int ctx_amr(W2dCtx* c, const int32_t* rq, int nr, const int32_t* cq, int nc);
+
+// ---- ensembles: runs share one context; run r owns slots base[r]+1 ..
+// base[r]+cap[r] and numbers its blocks 1..cap[r] as a single run does.
+// dx/dy: per run W2D_MAXLEV+1 spacings indexed by level.
+int ctx_set_runs(W2dCtx* c, int nruns, const int* base, const int* cap, const double* dx, const double* dy,
+                 const int* nlevs);
+// host levels, leaf flags and icoord of a run's slots (no upload)
+int ctx_run_topology(W2dCtx* c, int base, int nbmax, const int32_t* lev, const int32_t* leaf,
+                     const int32_t* icoord, int ld_icoord);
+// leaf flags of a run's slots (runs touch disjoint slots: callable at once)
+void ctx_run_leaf_flags(W2dCtx* c, int base, int nbmax, const int32_t* leaf);
+int ctx_upload_topology(W2dCtx* c);
+// pinned staging of the combined leaf list (waits for its previous upload);
+// runs write their leaves at their offsets, then ctx_commit_leaves uploads
+int* ctx_leaf_staging(W2dCtx* c);
+int ctx_commit_leaves(W2dCtx* c, int nl, const int* loff);
+// dt of every run (device), copied behind to pinned memory read by
+// ctx_ens_dt after the next synchronizing call
+int ctx_ens_dt_launch(W2dCtx* c);
+const double* ctx_ens_dt(W2dCtx* c);
+// fill plans: begin waits for the previous upload; ctx_plan_run writes the
+// descriptors of one run's leaves from its innerbounds list (runs at once);
+// upload sends slots lo..hi
+void* ctx_plan_begin(W2dCtx* c);
+int ctx_plan_run(W2dCtx* c, const int32_t* ib, int ld, int n, int base, int nbmax_local, const int* leaves, int nl);
+int ctx_plan_upload(W2dCtx* c, int lo, int hi);
+// criteria maxima of slots 1..hi at (*grad)[g-1]; synchronizes and checks
+// the error word
+int ctx_ens_criteria(W2dCtx* c, int hi, const double** grad);
+

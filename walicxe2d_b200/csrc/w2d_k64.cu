@@ -58,6 +58,49 @@ __global__ void __launch_bounds__(256) k_dt(const int* __restrict__ leaves, int 
   }
 }
 
+// timestep of every run of an ensemble: one CTA per run reduces the
+// partials of the run's leaves (leaves[loff[r] .. loff[r+1]-1]); the minima
+// and the final formula are those of k_dt, so a run's dt equals the dt the
+// run would have alone.
+__global__ void __launch_bounds__(256) k_dt_runs(const int* __restrict__ leaves, const int* __restrict__ loff,
+                                                 const double* __restrict__ cfl,
+                                                 const double* __restrict__ dtcool, int use_cool,
+                                                 double courant, double psc, double tsc,
+                                                 double* __restrict__ dt_run)
+{
+  __shared__ double s0[8], s1[8];
+  const int r = blockIdx.x;
+  double m0 = 1.e30, m1 = 1e30;
+  for (int k = loff[r] + threadIdx.x; k < loff[r + 1]; k += blockDim.x) {
+    const int b = leaves[k];
+    m0 = fmin(m0, cfl[b]);
+    if (use_cool) m1 = fmin(m1, dtcool[b]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    m0 = fmin(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+    m1 = fmin(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+  }
+  if ((threadIdx.x & 31) == 0) { s0[threadIdx.x >> 5] = m0; s1[threadIdx.x >> 5] = m1; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    m0 = s0[0];
+    m1 = s1[0];
+    for (int w = 1; w < 8; ++w) { m0 = fmin(m0, s0[w]); m1 = fmin(m1, s1[w]); }
+    const double a = courant * m0;
+    const double c = 0.4 * m1 * psc / tsc;
+    dt_run[r] = (a < c) ? a : c;
+  }
+}
+
+cudaError_t launch_dt_runs(const int* leaves, const int* loff, int nruns, const double* cfl, const double* dtcool,
+                           int use_cool, double courant, double psc, double tsc, double* dt_run, cudaStream_t st)
+{
+  if (nruns == 0) return cudaSuccess;
+  k_dt_runs<<<nruns, 256, 0, st>>>(leaves, loff, cfl, dtcool, use_cool, courant, psc, tsc, dt_run);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_dt(const int* leaves, int n, const double* cfl, const double* dtcool, int use_cool,
                       double courant, double psc, double tsc, unsigned long long* work, unsigned int* count,
                       double* dt_out, cudaStream_t st)

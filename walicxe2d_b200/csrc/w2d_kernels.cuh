@@ -21,7 +21,9 @@
 
 namespace w2d {
 
-#define W2D_MAXLEV 16
+#ifndef W2D_MAXLEV
+#define W2D_MAXLEV 16   // levels a context supports
+#endif
 #define W2D_THREADS 288   // 9 warps: 272 interfaces per direction
 
 extern __shared__ __align__(128) unsigned char w2d_smem[];
@@ -38,6 +40,12 @@ enum FaceKind {
 
 enum { ERR_HLLC = 3, ERR_TIMEOUT = 6 };
 
+// Geometry of one run of an ensemble (spacings of levels 1..nlevs).
+struct RunGeo {
+  double dx[W2D_MAXLEV + 1], dy[W2D_MAXLEV + 1];
+  int nlevs, pad;
+};
+
 struct KArgs {
   void* u;            // R*, pool of conserved variables
   void* up;           // R*, half-step pool
@@ -46,7 +54,7 @@ struct KArgs {
   int nleaf;
   const int* lev;     // level per slot
   const int* icoord;  // icoord per slot (2 ints)
-  const int2* fd;     // face descriptors [nleaf][4] for the fill in use
+  const int2* fd;     // face descriptors [slot][4] for the fill in use (leaf slots valid)
   double* cfl;        // per slot: min over interior of min(dx/(|u|+cs), dy/(|v|+cs))
   double* dtcool;     // per slot: DMC cooling-time limit
   double* grad;       // per slot: criteria maximum jump
@@ -60,9 +68,31 @@ struct KArgs {
   // and the top-hat state (u1..u6) at the fill's time
   double jet_posx, jet_posy, jet_lj, jet_rj;
   double jet_u[6];
-  const int* jetblk;      // per leaf position: block appears as nbs in the list
+  const int* jetblk;      // per slot (leaf slots valid): block appears as nbs in the list
   const double* dt_dev;   // k_half: dt read from here when not null
+  // ensembles (all null for one run): run of every slot, per-run geometry
+  // and per-run dt in device memory; tsc converts dt to seconds for cooling
+  const int* run_of;
+  const RunGeo* runs;
+  const double* dt_run;
+  double tsc;
 };
+
+__device__ __forceinline__ double geo_dx(const KArgs& a, int b, int lev)
+{
+  return a.run_of ? a.runs[a.run_of[b]].dx[lev] : a.dx[lev];
+}
+__device__ __forceinline__ double geo_dy(const KArgs& a, int b, int lev)
+{
+  return a.run_of ? a.runs[a.run_of[b]].dy[lev] : a.dy[lev];
+}
+__device__ __forceinline__ int geo_nlevs(const KArgs& a, int b) { return a.run_of ? a.runs[a.run_of[b]].nlevs : a.nlevs; }
+// dt of block b's run: the per-run value, the device value, or the argument
+__device__ __forceinline__ double step_dt(const KArgs& a, int b, double dt)
+{
+  if (a.run_of) return a.dt_run[a.run_of[b]];
+  return a.dt_dev ? *a.dt_dev : dt;
+}
 
 // flags of a face descriptor (bits 16..18 of .y) for impose_jet ordering:
 // the source block(s) had the jet imposed before the face's final writer,
@@ -187,8 +217,8 @@ __device__ __forceinline__ bool face_value(const R* __restrict__ arr, size_t bst
 __device__ __forceinline__ bool in_jet(const KArgs& a, int b, int i, int j)
 {
   const int lev = a.lev[b];
-  const double x = ((double)(i + a.icoord[2 * b]) - 0.5) * a.dx[lev];
-  const double y = ((double)(j + a.icoord[2 * b + 1]) - 0.5) * a.dy[lev];
+  const double x = ((double)(i + a.icoord[2 * b]) - 0.5) * geo_dx(a, b, lev);
+  const double y = ((double)(j + a.icoord[2 * b + 1]) - 0.5) * geo_dy(a, b, lev);
   return (fabs(x - a.jet_posx) <= a.jet_lj) && (fabs(y - a.jet_posy) <= a.jet_rj);
 }
 
@@ -427,8 +457,8 @@ __device__ __forceinline__ void block_stats(const R (*sp)[W2D_W][W2D_W], const P
       m3 = fmin(m3, sred[48 + w]);
     }
     const int lev = a.lev[b];
-    const R t1 = R(a.dx[lev]) / R(m0);
-    const R t2 = R(a.dy[lev]) / R(m1);
+    const R t1 = R(geo_dx(a, b, lev)) / R(m0);
+    const R t2 = R(geo_dy(a, b, lev)) / R(m1);
     a.cfl[b] = (double)fminr(t1, t2);
     a.grad[b] = m2;
     if (pa.cooling == COOL_DMC) a.dtcool[b] = m3;
@@ -463,9 +493,9 @@ __global__ void __launch_bounds__(W2D_THREADS) k_half(KArgs a, PhysArgs pa, doub
   const bool dmc = pa.cooling == COOL_DMC;
   load_tile<R, NEQ>(&st[0][0][0], dmc ? (const R*)a.prim + (size_t)b * bs : u, bar, a.err, b);
   const int lev = a.lev[b];
-  const double dtm = (a.dt_dev ? *a.dt_dev : dt) / 2.;
-  const R dtdx = R(dtm / a.dx[lev]);
-  const R dtdy = R(dtm / a.dy[lev]);
+  const double dtm = step_dt(a, b, dt) / 2.;
+  const R dtdx = R(dtm / geo_dx(a, b, lev));
+  const R dtdy = R(dtm / geo_dy(a, b, lev));
   if (!wait_tiles(bar, a.err, b)) return;
 
   // primitives (in place) and sound speed of cells 0..17 (corners skipped)
@@ -550,9 +580,10 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
   R* __restrict__ u = (R*)a.u + (size_t)b * bs;
   load_two_tiles<R, NEQ>(&st[0][0][0], upool + (size_t)b * bs, &so[0][0][0], u, bar);
   const int lev = a.lev[b];
-  const R dtdx = R(dt / a.dx[lev]);
-  const R dtdy = R(dt / a.dy[lev]);
-  const bool visc = lev >= (a.nlevs - 1);
+  const double dtb = step_dt(a, b, dt);
+  const R dtdx = R(dtb / geo_dx(a, b, lev));
+  const R dtdy = R(dtb / geo_dy(a, b, lev));
+  const bool visc = lev >= (geo_nlevs(a, b) - 1);
   const R eta = R(a.eta);
 
   // ghosts of the filled up gathered from the pool while the tiles land
@@ -561,7 +592,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
   bool gw = false;
   const int gf = tid / 32, gg = (tid / 16) % 2, gm = 1 + tid % 16;
   if (tid < 128) {
-    const int2 d = a.fd[li * 4 + gf];
+    const int2 d = a.fd[(size_t)b * 4 + gf];
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) gw = ghost_value<R>(upool, bs, a, b, d, gf, gg, gm, k, gv[k]);
   }
@@ -572,7 +603,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) st[k][j + 1][i + 1] = gv[k];
   }
-  if (a.jet && a.jetblk[li]) jet_interior_fn<R, NEQ>(st, a, b, nullptr);
+  if (a.jet && a.jetblk[b]) jet_interior_fn<R, NEQ>(st, a, b, nullptr);
   __syncthreads();
 
   // u ghosts = up ghosts (u = up, src/tstep.f90:85; the old u stays in so),
@@ -683,7 +714,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_fill1(KArgs a, PhysArgs pa, int
   if (tid < 64) {
     const int f = tid / 16, m = 1 + tid % 16;
     ghost_ij(f, 0, m, gi, gj);
-    const int2 d = a.fd[li * 4 + f];
+    const int2 d = a.fd[(size_t)b * 4 + f];
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) w = ghost_value<R>(upool, bs, a, b, d, f, 0, m, k, gv[k]);
     if (w) {
@@ -740,7 +771,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_calcprim(KArgs a, PhysArgs pa, 
   R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;
   load_tile<R, NEQ>(&st[0][0][0], u, bar, a.err, b);
   if (!wait_tiles(bar, a.err, b)) return;
-  if (jet_interior && a.jet && a.jetblk[blockIdx.x]) {
+  if (jet_interior && a.jet && a.jetblk[b]) {
     jet_interior_fn<R, NEQ>(st, a, b, u);
     __syncthreads();
   }
@@ -775,7 +806,7 @@ __global__ void __launch_bounds__(128) k_fill_only(KArgs a, R* pool, int layers)
   if (g >= layers) return;
   int i, j;
   ghost_ij(f, g, m, i, j);
-  const int2 d = a.fd[li * 4 + f];
+  const int2 d = a.fd[(size_t)b * 4 + f];
   R vals[NEQ];
   bool w = false;
 #pragma unroll
@@ -791,9 +822,8 @@ __global__ void __launch_bounds__(128) k_fill_only(KArgs a, R* pool, int layers)
 template <typename R, int NEQ>
 __global__ void __launch_bounds__(256) k_jet_only(KArgs a, R* pool)
 {
-  const int li = blockIdx.x;
-  if (!a.jetblk[li]) return;
-  const int b = a.leaves[li];
+  const int b = a.leaves[blockIdx.x];
+  if (!a.jetblk[b]) return;
   const int i = 1 + threadIdx.x % 16, j = 1 + threadIdx.x / 16;
   if (!in_jet(a, b, i, j)) return;
   R* pb = pool + (size_t)b * NEQ * W2D_CELLS;

@@ -35,4 +35,8 @@ cudaError_t launch_dt(const int* leaves, int n, const double* cfl, const double*
                       double courant, double psc, double tsc, unsigned long long* work, unsigned int* count,
                       double* dt_out, cudaStream_t st);
 
+// dt_run[r] for every run of an ensemble; leaves of run r at loff[r]..loff[r+1]-1
+cudaError_t launch_dt_runs(const int* leaves, const int* loff, int nruns, const double* cfl, const double* dtcool,
+                           int use_cool, double courant, double psc, double tsc, double* dt_run, cudaStream_t st);
+
 }  // namespace w2d
