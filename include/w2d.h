@@ -286,6 +286,38 @@ int w2d_ens_set_amr(W2dEns* ens, int on);
 #define W2D_ENS_NPHASES 8
 int w2d_ens_phase_ms(W2dEns* ens, double* ms, int reset);
 
+/* ---- Learned coolingh surrogate (no counterpart in the reference) ---------
+ * A 4 -> 64 -> 64 -> 2 tanh MLP with BF16 weights on the tensor cores
+ * (FP32 accumulation) mapping (log n, log T, neutral fraction, log dt) to
+ * the updated (T, neutral fraction) of atomic (src/coolingh.f90:171-259),
+ * trained on samples that the exact routine labels on the device.
+ * Parameters: a flat FP32 vector of W2D_NN_NPARAM values, W1 [64][4], b1
+ * [64], W2 [64][64], b2 [64], W3 [2][64], b3 [2] (row = output unit).
+ * Features are columns f[q*n + i] (q = 0..3), targets t[q*n + i] (q = 0, 1);
+ * their maps are given in w2d_nn.cuh. */
+#define W2D_NN_NPARAM 4610
+typedef struct W2dNN W2dNN;
+int w2d_nn_create(uint64_t seed, W2dNN** out);   /* Glorot weights from seed */
+int w2d_nn_destroy(W2dNN* nn);
+/* n training samples drawn with `seed` (n, T, dt log-uniform over [1e-2,
+ * 1e4] cm^-3, [1e2, 1e8] K, [1e-2, 1e2] yr; neutral fraction uniform over
+ * [1e-4, 1]) and labelled by the exact routine, kept on the device */
+int w2d_nn_samples(W2dNN* nn, int64_t n, uint64_t seed);
+/* Adam over the samples in batches of `batch` (multiple of 128), learning
+ * rate cosine-decayed from lr to lr_end; *last_loss: mean squared error of
+ * the last batch */
+int w2d_nn_train(W2dNN* nn, int epochs, int batch, float lr, float lr_end, float* last_loss);
+int w2d_nn_params(W2dNN* nn, float* params, int set);   /* get (0) / set (1) */
+/* loss and gradient of the mean squared error over n host samples */
+int w2d_nn_grad(W2dNN* nn, const float* feat, const float* targ, int n, float* grad, float* loss);
+int w2d_nn_forward(W2dNN* nn, const float* feat, int n, float* out);   /* out [2][n] */
+/* The exact routine judges the surrogate on n fresh samples: [0] share
+ * the surrogate serves (inputs in range, predicted |dT/T| <= 10%), [1]
+ * median, [2] 99th percentile and [3] maximum relative error of T and [4]
+ * mean and [5] maximum error of the neutral fraction over those, [6] share
+ * whose exact |dT/T| <= 10%.  stats holds 8 doubles. */
+int w2d_nn_judge(W2dNN* nn, int64_t n, uint64_t seed, double* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -69,6 +69,15 @@ SIGNATURES = {
     "w2d_ens_leaves": (_I, [_vp, _I, _PI32, _PI32]),
     "w2d_ens_set_amr": (_I, [_vp, _I]),
     "w2d_ens_phase_ms": (_I, [_vp, _PD, _I]),
+    "w2d_nn_create": (_I, [C.c_uint64, C.POINTER(_vp)]),
+    "w2d_nn_destroy": (_I, [_vp]),
+    "w2d_nn_samples": (_I, [_vp, C.c_int64, C.c_uint64]),
+    "w2d_nn_train": (_I, [_vp, _I, _I, C.c_float, C.c_float, C.POINTER(C.c_float)]),
+    "w2d_nn_params": (_I, [_vp, C.POINTER(C.c_float), _I]),
+    "w2d_nn_grad": (_I, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float), _I, C.POINTER(C.c_float),
+                         C.POINTER(C.c_float)]),
+    "w2d_nn_forward": (_I, [_vp, C.POINTER(C.c_float), _I, C.POINTER(C.c_float)]),
+    "w2d_nn_judge": (_I, [_vp, C.c_int64, C.c_uint64, _PD]),
 }
 
 _LIB = None

@@ -348,3 +348,76 @@ class Ensemble:
         self.L.w2d_ens_phase_ms(self.h, _pd(ms), 1 if reset else 0)
         return {k: float(ms[i]) for i, k in enumerate(self.PHASES)}
 
+
+class Surrogate:
+    """The learned coolingh surrogate (w2d_nn_*): a 4 -> 64 -> 64 -> 2 MLP
+    trained and evaluated on the tensor cores."""
+
+    NPARAM = 4610
+    JUDGE = ("served", "t_err_median", "t_err_p99", "t_err_max", "y_err_mean", "y_err_max", "exact_small")
+
+    def __init__(self, seed: int = 20261203):
+        self.L = _lib.load()
+        h = C.c_void_p()
+        rc = self.L.w2d_nn_create(seed, C.byref(h))
+        if rc:
+            raise _lib.W2dException(rc, None, "w2d_nn_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.L.w2d_nn_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc:
+            raise _lib.W2dException(rc, None, what)
+
+    def samples(self, n: int, seed: int = 20261203):
+        self._check(self.L.w2d_nn_samples(self.h, n, seed), "w2d_nn_samples")
+
+    def train(self, epochs: int, batch: int = 8192, lr: float = 2e-3, lr_end: float = 2e-5) -> float:
+        loss = C.c_float()
+        self._check(self.L.w2d_nn_train(self.h, epochs, batch, lr, lr_end, C.byref(loss)), "w2d_nn_train")
+        return loss.value
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.NPARAM, np.float32)
+        self._check(self.L.w2d_nn_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float)), 0), "w2d_nn_params")
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.NPARAM
+        self._check(self.L.w2d_nn_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float)), 1), "w2d_nn_params")
+
+    def grad(self, feat: np.ndarray, targ: np.ndarray) -> tuple[float, np.ndarray]:
+        """feat (n, 4), targ (n, 2) -> (loss, gradient)."""
+        f = np.ascontiguousarray(np.asarray(feat, np.float32).T)
+        t = np.ascontiguousarray(np.asarray(targ, np.float32).T)
+        g = np.zeros(self.NPARAM, np.float32)
+        loss = C.c_float()
+        fp = C.POINTER(C.c_float)
+        self._check(self.L.w2d_nn_grad(self.h, f.ctypes.data_as(fp), t.ctypes.data_as(fp), f.shape[1],
+                                       g.ctypes.data_as(fp), C.byref(loss)), "w2d_nn_grad")
+        return loss.value, g
+
+    def forward(self, feat: np.ndarray) -> np.ndarray:
+        f = np.ascontiguousarray(np.asarray(feat, np.float32).T)
+        out = np.zeros((2, f.shape[1]), np.float32)
+        fp = C.POINTER(C.c_float)
+        self._check(self.L.w2d_nn_forward(self.h, f.ctypes.data_as(fp), f.shape[1], out.ctypes.data_as(fp)),
+                    "w2d_nn_forward")
+        return out.T.copy()
+
+    def judge(self, n: int = 1 << 20, seed: int = 7) -> dict:
+        st = np.zeros(8)
+        self._check(self.L.w2d_nn_judge(self.h, n, seed, _pd(st)), "w2d_nn_judge")
+        return {k: float(st[i]) for i, k in enumerate(self.JUDGE)}
+

@@ -233,7 +233,8 @@ int stats_for(W2dCtx* c, const int* d_list, int n)
   return launch(c, "calcprim", [&] { return c->L->calcprim(c->neq, a, pa, d_list, n, 0, c->st); });
 }
 
-// Face descriptors of the listed leaf slots back to "keep" (no writer).
+// Face descriptors of the listed leaf slots back to "keep" (no writer);
+// hf1/hf2 are the per-slot host plans.
 void plan_reset(int2* hf1, int2* hf2, const int* leaves, int nl)
 {
   for (int k = 0; k < nl; ++k) {
@@ -244,9 +245,10 @@ void plan_reset(int2* hf1, int2* hf2, const int* leaves, int nl)
 
 // The entries of one innerbounds list (columns nbs, neighbour, type; ld
 // apart; block IDs 1..nbmax_local of a run whose slots start after `base`)
-// into the per-slot descriptors hf1 (boundaryI) and hf2 (boundaryII), in
-// list order so that the last writer of every leaf face wins.  Leaves of
-// different runs occupy different slots, so runs can be planned at once.
+// into the per-slot host descriptors hf1 (boundaryI) and hf2 (boundaryII),
+// in list order so that the last writer of every leaf face wins.  Leaves of
+// different runs occupy different slots, so runs can be planned at once;
+// plan_pack then lays the descriptors out by leaf position for the device.
 int plan_entries(W2dCtx* c, int2* hf1, int2* hf2, const int32_t* ib, int ld, int n, int base, int nbmax_local,
                  bool jet)
 {
@@ -323,6 +325,21 @@ int plan_entries(W2dCtx* c, int2* hf1, int2* hf2, const int32_t* ib, int ld, int
     }
   }
   return W2D_OK;
+}
+
+// Per-leaf-position device layout of the per-slot plans of `leaves`
+// (positions pos0 ..), into the pinned staging pair.
+void plan_pack(const W2dCtx* c, int2* pf1, int2* pf2, const int* leaves, int nl, int pos0)
+{
+  const int2* s1 = c->sfd1.data();
+  const int2* s2 = c->sfd2.data();
+  for (int k = 0; k < nl; ++k) {
+    const size_t src = (size_t)leaves[k] * 4, dst = (size_t)(pos0 + k) * 4;
+    for (int f = 0; f < 4; ++f) {
+      pf1[dst + f] = s1[src + f];
+      pf2[dst + f] = s2[src + f];
+    }
+  }
 }
 
 int tstep_ready(W2dCtx* c, bool need_bounds = true)
@@ -496,6 +513,9 @@ int w2d_create(const W2dParams* p, W2dCtx** out)
     CKC(cudaMallocHost(&c->h_fd2[q], sizeof(int2) * 4 * slots));
     CKC(cudaMallocHost(&c->h_jetblk[q], sizeof(int) * slots));
   }
+  c->sfd1.assign(4 * slots, make_int2(0, FK_KEEP));
+  c->sfd2.assign(4 * slots, make_int2(0, FK_KEEP));
+  CKC(cudaMalloc(&c->d_gradleaf, sizeof(double) * slots));
   CKC(cudaMalloc(&c->d_fd1, sizeof(int2) * 4 * slots));
   CKC(cudaMalloc(&c->d_fd2, sizeof(int2) * 4 * slots));
   CKC(cudaMalloc(&c->d_jetblk, sizeof(int) * slots));
@@ -506,7 +526,6 @@ int w2d_create(const W2dParams* p, W2dCtx** out)
   memset(c->icoord, 0, sizeof(int) * 2 * slots);
 #undef CKC
   c->leaf.assign(slots, 0);
-  c->leaf_index.assign(slots, -1);
   if (cudaStreamSynchronize(c->st) != cudaSuccess) {
     w2d_destroy(c);
     return W2D_ERR_CUDA;
@@ -526,7 +545,7 @@ int w2d_destroy(W2dCtx* c)
   cudaEvent_t evs[] = {c->ev_topo, c->ev_ops, c->ev_plan[0], c->ev_plan[1], c->ev_dt};
   for (auto e : evs)
     if (e) cudaEventDestroy(e);
-  void* dev2[] = {c->d_run_of, c->d_runs, c->d_dt_run, c->d_loff};
+  void* dev2[] = {c->d_run_of, c->d_runs, c->d_dt_run, c->d_loff, c->d_gradleaf};
   for (void* d : dev2)
     if (d) cudaFree(d);
   if (c->h_dt_run) cudaFreeHost(c->h_dt_run);
@@ -574,7 +593,6 @@ int w2d_set_topology(W2dCtx* c, const int32_t* lp, int ld_lp, const int32_t* lea
   if (nbmax < 0 || nbmax > c->cap || ld_lp < nbmax || ld_icoord < nbmax)
     return set_error(c, W2D_ERR_ARG, 0, 0, 0, "nbmax %d outside the pool (capacity %d)", nbmax, c->cap);
   CK(cudaEventSynchronize(c->ev_topo));  // the previous upload has left the pinned arrays
-  for (int b : c->leaves) c->leaf_index[b] = -1;  // only the old leaves are set
   c->nbmax = nbmax;
   c->leaves.clear();
   for (int nb = 1; nb <= nbmax; ++nb) {
@@ -585,7 +603,6 @@ int w2d_set_topology(W2dCtx* c, const int32_t* lp, int ld_lp, const int32_t* lea
     if (c->leaf[nb]) {
       if (c->lev[nb] < 1 || c->lev[nb] > c->p.nlevs)
         return set_error(c, W2D_ERR_TOPOLOGY, nb, 0, 0, "leaf %d has level %d", nb, c->lev[nb]);
-      c->leaf_index[nb] = (int)c->leaves.size();
       c->leaves.push_back(nb);
     }
   }
@@ -619,8 +636,8 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
   const int q = c->plan_buf;
   c->plan_buf ^= 1;
   CK(cudaEventSynchronize(c->ev_plan[q]));
-  int2* hf1 = c->h_fd1[q];
-  int2* hf2 = c->h_fd2[q];
+  int2* hf1 = c->sfd1.data();
+  int2* hf2 = c->sfd2.data();
   int* hj = c->h_jetblk[q];
   plan_reset(hf1, hf2, c->leaves.data(), (int)c->leaves.size());
   const bool jet = c->p.otherb == W2D_USERBC_JET;
@@ -642,11 +659,13 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
   if (jet) {
     // faces no entry writes still get the jet if their block is ever nbs;
     // the interior of such a block always does
-    for (int b : c->leaves) {
-      hj[b] = c->qfirst[b] > 0;
+    for (size_t li = 0; li < c->leaves.size(); ++li) {
+      const int b = c->leaves[li];
+      const bool named = c->qfirst[b] > 0;
+      hj[li] = named;
       for (int f = 0; f < 4; ++f) {
-        if (hj[b] && (hf1[b * 4 + f].y & 0xff) == FK_KEEP) hf1[b * 4 + f].y |= FD_DST_JET;
-        if (hj[b] && (hf2[b * 4 + f].y & 0xff) == FK_KEEP) hf2[b * 4 + f].y |= FD_DST_JET;
+        if (named && (hf1[b * 4 + f].y & 0xff) == FK_KEEP) hf1[b * 4 + f].y |= FD_DST_JET;
+        if (named && (hf2[b * 4 + f].y & 0xff) == FK_KEEP) hf2[b * 4 + f].y |= FD_DST_JET;
       }
     }
     for (int k = 1; k <= n; ++k) {   // clear for the next list
@@ -655,10 +674,13 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
     }
   }
   if (rc) return rc;
-  const size_t ns = (size_t)c->nbmax + 1;
-  CK(cudaMemcpyAsync(c->d_fd1, hf1, sizeof(int2) * 4 * ns, cudaMemcpyHostToDevice, c->st));
-  CK(cudaMemcpyAsync(c->d_fd2, hf2, sizeof(int2) * 4 * ns, cudaMemcpyHostToDevice, c->st));
-  if (jet) CK(cudaMemcpyAsync(c->d_jetblk, hj, sizeof(int) * ns, cudaMemcpyHostToDevice, c->st));
+  const int nl = (int)c->leaves.size();
+  plan_pack(c, c->h_fd1[q], c->h_fd2[q], c->leaves.data(), nl, 0);
+  if (nl > 0) {
+    CK(cudaMemcpyAsync(c->d_fd1, c->h_fd1[q], sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_fd2, c->h_fd2[q], sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
+    if (jet) CK(cudaMemcpyAsync(c->d_jetblk, hj, sizeof(int) * (size_t)nl, cudaMemcpyHostToDevice, c->st));
+  }
   CK(cudaEventRecord(c->ev_plan[q], c->st));
   c->have_bounds = true;
   return W2D_OK;
@@ -1070,38 +1092,42 @@ int ctx_ens_dt_launch(W2dCtx* c)
 
 const double* ctx_ens_dt(W2dCtx* c) { return c->h_dt_run; }
 
-void* ctx_plan_begin(W2dCtx* c)
+int ctx_plan_begin(W2dCtx* c)
 {
-  if (cudaEventSynchronize(c->ev_plan[0]) != cudaSuccess) return nullptr;
-  return c->h_fd1[0];
+  return cudaEventSynchronize(c->ev_plan[0]) == cudaSuccess ? W2D_OK : W2D_ERR_CUDA;
 }
 
 int ctx_plan_run(W2dCtx* c, const int32_t* ib, int ld, int n, int base, int nbmax_local, const int* leaves, int nl)
 {
-  int2* hf1 = c->h_fd1[0];
-  int2* hf2 = c->h_fd2[0];
-  plan_reset(hf1, hf2, leaves, nl);
-  return plan_entries(c, hf1, hf2, ib, ld, n, base, nbmax_local, false);
+  plan_reset(c->sfd1.data(), c->sfd2.data(), leaves, nl);
+  return plan_entries(c, c->sfd1.data(), c->sfd2.data(), ib, ld, n, base, nbmax_local, false);
 }
 
-int ctx_plan_upload(W2dCtx* c, int lo, int hi)
+void ctx_plan_pack(W2dCtx* c, const int* leaves, int nl, int pos0)
 {
-  if (hi >= lo) {
-    const size_t off = (size_t)lo * 4, cnt = (size_t)(hi - lo + 1) * 4;
-    CK(cudaMemcpyAsync(c->d_fd1 + off, c->h_fd1[0] + off, sizeof(int2) * cnt, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->d_fd2 + off, c->h_fd2[0] + off, sizeof(int2) * cnt, cudaMemcpyHostToDevice, c->st));
+  plan_pack(c, c->h_fd1[0], c->h_fd2[0], leaves, nl, pos0);
+}
+
+int ctx_plan_upload(W2dCtx* c, int nl)
+{
+  if (nl > 0) {
+    CK(cudaMemcpyAsync(c->d_fd1, c->h_fd1[0], sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_fd2, c->h_fd2[0], sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
   }
   CK(cudaEventRecord(c->ev_plan[0], c->st));
   c->have_bounds = true;
   return W2D_OK;
 }
 
-int ctx_ens_criteria(W2dCtx* c, int hi, const double** grad)
+int ctx_ens_criteria(W2dCtx* c, const double** grad)
 {
-  if (hi > 0)
-    CK(cudaMemcpyAsync(c->h_grad, c->d_grad + 1, sizeof(double) * (size_t)hi, cudaMemcpyDeviceToHost, c->st));
+  const int nl = c->nleaf;
+  if (nl > 0) {
+    CK(launch_gather_leaf(c->d_leaves, nl, c->d_grad, c->d_gradleaf, c->st));
+    CK(cudaMemcpyAsync(c->h_grad, c->d_gradleaf, sizeof(double) * (size_t)nl, cudaMemcpyDeviceToHost, c->st));
+  }
   int rc = sync_and_check(c);
   if (rc) return rc;
-  *grad = c->h_grad;   // grad of slot g at [g - 1]
+  *grad = c->h_grad;   // grad of the leaf at position k of d_leaves at [k]
   return W2D_OK;
 }

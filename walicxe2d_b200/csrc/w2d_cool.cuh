@@ -64,35 +64,44 @@ __device__ __forceinline__ double d_aloss(double x1, double den, double dh0, dou
   return ecoll + eion + (erec + 7.033 * (eoi + eoii)) * (1. - fr) + equil * fr;
 }
 
-// src/coolingh.f90:171-259 (atomic) in FP64 on one cell's u
-template <int NEQ>
-__device__ __forceinline__ void d_atomic(const Phys<double>& ph, double dt, double* uu)
+// src/coolingh.f90:171-254 (atomic) in FP64 on one cell: from the
+// temperature T, neutral fraction y0, density dh and dt (s), the new
+// neutral fraction y1, the cooling rate ce of the temperature relaxation
+// t1 = 10 + (T - 10) exp(-ce dt) and the clamped new temperature t1.
+__device__ __forceinline__ void d_atomic_core(double T, double y0, double dh, double dt, double& y1, double& ce,
+                                              double& t1)
 {
   const double xi = 1.e-4, boltzm = 1.3807e-16;
-  double prim[NEQ], T;
-  uprim<NEQ>(ph, prim, uu, T);
   double col = d_colf(T);
   double rec = d_alpha(T);
-  double y0 = uu[4] / uu[0];
-  double dh = uu[0];
   double a = rec + col;
   double b = -((2. + xi) * rec + (1. + xi) * col);
   double c = (1. + xi) * rec;
   double d = sqrt(b * b - 4. * a * c);
   double g0 = (2. * a * y0 + b + d) / (2. * a * y0 + b - d);
   double e = exp(-d * dh * dt);
-  double y1 = (-b - d * (1. + g0 * e) / (1. - g0 * e)) / (2. * a);
+  y1 = (-b - d * (1. + g0 * e) / (1. - g0 * e)) / (2. * a);
   y1 = fminr(y1, 1.);
   y1 = fmaxr(y1, 0.0001);
-  uu[4] = y1 * uu[0];
-  double dh0 = uu[4];
+  double dh0 = y1 * dh;
   double al = d_aloss(y0, dh, dh0, T) / (dh * dh);
   double tprime = 10.;
-  double ce = (2. * dh * al) / (3. * boltzm * T);
-  double t1 = tprime + (T - tprime) * exp(-ce * dt);
+  ce = (2. * dh * al) / (3. * boltzm * T);
+  t1 = tprime + (T - tprime) * exp(-ce * dt);
   t1 = fmaxr(t1, 0.1 * T);
   t1 = fminr(t1, 10. * T);
   t1 = fmaxr(t1, tprime);
+}
+
+// src/coolingh.f90:171-259 (atomic) in FP64 on one cell's u
+template <int NEQ>
+__device__ __forceinline__ void d_atomic(const Phys<double>& ph, double dt, double* uu)
+{
+  double prim[NEQ], T;
+  uprim<NEQ>(ph, prim, uu, T);
+  double y1, ce, t1;
+  d_atomic_core(T, uu[4] / uu[0], uu[0], dt, y1, ce, t1);
+  uu[4] = y1 * uu[0];
   uu[3] = ph.cv * (2. * uu[0] - uu[4]) * t1 / ph.tempsc + 0.5 * prim[0] * (prim[1] * prim[1] + prim[2] * prim[2]);
 }
 
@@ -121,7 +130,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_cool(KArgs a, PhysArgs pa, doub
   load_tile<R, NEQ>(&st[0][0][0], u, bar, a.err, b);
   if (a.run_of) dt_s = a.dt_run[a.run_of[b]] * a.tsc;   // dt*tsc of the block's run
   if (!wait_tiles(bar, a.err, b)) return;
-  if (a.jet && a.jetblk[b]) {   // impose_jet of boundaryI, before cooling
+  if (a.jet && a.jetblk[blockIdx.x]) {   // impose_jet of boundaryI, before cooling
     jet_interior_fn<R, NEQ>(st, a, b, u);
     __syncthreads();
   }

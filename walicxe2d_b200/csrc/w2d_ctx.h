@@ -39,6 +39,8 @@ struct W2dCtx {
   int* h_leaflist = nullptr; // pinned staging of d_leaves (guarded by ev_topo)
   int2* d_fd1 = nullptr;   // boundaryI (layer 0 of u)
   int2* d_fd2 = nullptr;   // boundaryII (two layers of up)
+  std::vector<int2> sfd1, sfd2;  // host plans per slot (4 faces), packed by leaf position for upload
+  double* d_gradleaf = nullptr;  // criteria maxima gathered by leaf position
   cudaEvent_t ev_dt = nullptr;  // dt and the error word have reached h_small/h_err
   // ensembles (nruns > 0): run of every slot, per-run geometry and dt, and
   // the offsets of each run's leaves in d_leaves
@@ -81,7 +83,6 @@ struct W2dCtx {
   std::vector<int> leaf;               // per slot
   std::vector<int> leaves;             // leaf slots, ascending (one run)
   int nleaf = 0;                       // entries of d_leaves
-  std::vector<int> leaf_index;         // slot -> position in leaves, -1
   int nbmax = 0;
   double dx[W2D_MAXLEV + 1] = {0}, dy[W2D_MAXLEV + 1] = {0};
   bool have_topology = false;

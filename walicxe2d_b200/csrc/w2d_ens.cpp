@@ -148,29 +148,26 @@ int push_leaves(W2dEns* e)
   return ctx_commit_leaves(e->ctx, e->loff[nr], e->loff.data());
 }
 
-// locatebounds and fill plans of the changed runs, one upload
+// locatebounds and fill plans of the changed runs; every run's descriptors
+// at its leaf positions; one upload
 int push_plans(W2dEns* e)
 {
   const int nr = (int)e->runs.size();
-  if (!ctx_plan_begin(e->ctx)) return W2D_ERR_CUDA;
+  int rc = ctx_plan_begin(e->ctx);
+  if (rc) return rc;
   e->pool->run(nr, [&](int r) {
     e->rc[r] = W2D_OK;
-    if (!e->dirty[r]) return;
-    W2dSim& s = e->runs[r];
-    locatebounds(&s);
-    e->rc[r] = ctx_plan_run(e->ctx, s.ib.data(), s.nib, s.nib, e->base[r], s.nbmax, e->rleaves[r].data(),
-                            (int)e->rleaves[r].size());
+    if (e->dirty[r]) {
+      W2dSim& s = e->runs[r];
+      locatebounds(&s);
+      e->rc[r] = ctx_plan_run(e->ctx, s.ib.data(), s.nib, s.nib, e->base[r], s.nbmax, e->rleaves[r].data(),
+                              (int)e->rleaves[r].size());
+    }
+    ctx_plan_pack(e->ctx, e->rleaves[r].data(), (int)e->rleaves[r].size(), e->loff[r]);
   });
-  int rc = first_error(e->rc);
-  if (rc) return rc;
-  int lo = -1, hi = -2;
-  for (int r = 0; r < nr; ++r) {
-    if (!e->dirty[r]) continue;
-    if (lo < 0) lo = e->base[r] + 1;
-    hi = e->base[r] + e->runs[r].nbmax;
-    e->dirty[r] = 0;
-  }
-  return ctx_plan_upload(e->ctx, lo < 0 ? 0 : lo, hi);
+  if ((rc = first_error(e->rc))) return rc;
+  for (int r = 0; r < nr; ++r) e->dirty[r] = 0;
+  return ctx_plan_upload(e->ctx, e->loff[nr]);
 }
 
 // admesh of every run (passes below `limit` only; limit < 0: all): criteria
@@ -179,11 +176,9 @@ int push_plans(W2dEns* e)
 int admesh_all(W2dEns* e, int pass, const std::vector<int>* limit, bool timed)
 {
   const int nr = (int)e->runs.size();
-  int hi = 0;
-  for (int r = 0; r < nr; ++r) hi = std::max(hi, e->base[r] + e->runs[r].nbmax);
   double t0 = now_ms();
   const double* grad = nullptr;
-  int rc = ctx_ens_criteria(e->ctx, hi, &grad);
+  int rc = ctx_ens_criteria(e->ctx, &grad);
   if (rc) return rc;
   double t1 = now_ms();
   e->pool->run(nr, [&](int r) {
@@ -193,8 +188,10 @@ int admesh_all(W2dEns* e, int pass, const std::vector<int>* limit, bool timed)
     s.cops.clear();
     if (limit && pass >= (*limit)[r]) return;
     if (s.p.nlevs < 2) return;
-    const double* g = grad + e->base[r];
-    for (int nb = 1; nb <= s.nbmax; ++nb) s.grad[nb - 1] = s.LEAF(nb) ? g[nb - 1] : -1.0;
+    std::fill(s.grad.begin(), s.grad.begin() + s.nbmax, -1.0);
+    const double* g = grad + e->loff[r];
+    const auto& lv = e->rleaves[r];
+    for (size_t k = 0; k < lv.size(); ++k) s.grad[lv[k] - e->base[r] - 1] = g[k];
     e->rc[r] = admesh_decide(&s);
     if (!s.rops.empty() || !s.cops.empty()) e->dirty[r] = 1;
   });
@@ -342,9 +339,7 @@ int w2d_ens_run(W2dEns* e, int nsteps)
       if ((rc = admesh_all(e, 0, nullptr, true))) return rc;   // src/main.f90:98
     } else {
       const double* grad = nullptr;
-      int hi = 0;
-      for (int r = 0; r < nr; ++r) hi = std::max(hi, e->base[r] + e->runs[r].nbmax);
-      if ((rc = ctx_ens_criteria(e->ctx, hi, &grad))) return rc;
+      if ((rc = ctx_ens_criteria(e->ctx, &grad))) return rc;
     }
     const double* dt = ctx_ens_dt(e->ctx);   // valid after the criteria synchronization
     for (int r = 0; r < nr; ++r) {

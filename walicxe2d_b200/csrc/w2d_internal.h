@@ -44,12 +44,14 @@ int ctx_commit_leaves(W2dCtx* c, int nl, const int* loff);
 int ctx_ens_dt_launch(W2dCtx* c);
 const double* ctx_ens_dt(W2dCtx* c);
 // fill plans: begin waits for the previous upload; ctx_plan_run writes the
-// descriptors of one run's leaves from its innerbounds list (runs at once);
-// upload sends slots lo..hi
-void* ctx_plan_begin(W2dCtx* c);
+// per-slot descriptors of one run's leaves from its innerbounds list (runs
+// at once); ctx_plan_pack lays a run's leaves out at leaf positions pos0..
+// (runs at once); upload sends the nl positions
+int ctx_plan_begin(W2dCtx* c);
 int ctx_plan_run(W2dCtx* c, const int32_t* ib, int ld, int n, int base, int nbmax_local, const int* leaves, int nl);
-int ctx_plan_upload(W2dCtx* c, int lo, int hi);
-// criteria maxima of slots 1..hi at (*grad)[g-1]; synchronizes and checks
-// the error word
-int ctx_ens_criteria(W2dCtx* c, int hi, const double** grad);
+void ctx_plan_pack(W2dCtx* c, const int* leaves, int nl, int pos0);
+int ctx_plan_upload(W2dCtx* c, int nl);
+// criteria maxima of the leaves by position in the combined leaf list at
+// (*grad)[k]; synchronizes and checks the error word
+int ctx_ens_criteria(W2dCtx* c, const double** grad);
 

@@ -101,6 +101,20 @@ cudaError_t launch_dt_runs(const int* leaves, const int* loff, int nruns, const 
   return cudaGetLastError();
 }
 
+__global__ void k_gather_leaf(const int* __restrict__ leaves, int n, const double* __restrict__ v,
+                              double* __restrict__ out)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = v[leaves[k]];
+}
+
+cudaError_t launch_gather_leaf(const int* leaves, int n, const double* v, double* out, cudaStream_t st)
+{
+  if (n == 0) return cudaSuccess;
+  k_gather_leaf<<<(n + 255) / 256, 256, 0, st>>>(leaves, n, v, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_dt(const int* leaves, int n, const double* cfl, const double* dtcool, int use_cool,
                       double courant, double psc, double tsc, unsigned long long* work, unsigned int* count,
                       double* dt_out, cudaStream_t st)

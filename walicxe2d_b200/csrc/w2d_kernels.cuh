@@ -54,7 +54,7 @@ struct KArgs {
   int nleaf;
   const int* lev;     // level per slot
   const int* icoord;  // icoord per slot (2 ints)
-  const int2* fd;     // face descriptors [slot][4] for the fill in use (leaf slots valid)
+  const int2* fd;     // face descriptors [leaf position][4] for the fill in use
   double* cfl;        // per slot: min over interior of min(dx/(|u|+cs), dy/(|v|+cs))
   double* dtcool;     // per slot: DMC cooling-time limit
   double* grad;       // per slot: criteria maximum jump
@@ -68,7 +68,7 @@ struct KArgs {
   // and the top-hat state (u1..u6) at the fill's time
   double jet_posx, jet_posy, jet_lj, jet_rj;
   double jet_u[6];
-  const int* jetblk;      // per slot (leaf slots valid): block appears as nbs in the list
+  const int* jetblk;      // per leaf position: block appears as nbs in the list
   const double* dt_dev;   // k_half: dt read from here when not null
   // ensembles (all null for one run): run of every slot, per-run geometry
   // and per-run dt in device memory; tsc converts dt to seconds for cooling
@@ -592,7 +592,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
   bool gw = false;
   const int gf = tid / 32, gg = (tid / 16) % 2, gm = 1 + tid % 16;
   if (tid < 128) {
-    const int2 d = a.fd[(size_t)b * 4 + gf];
+    const int2 d = a.fd[li * 4 + gf];
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) gw = ghost_value<R>(upool, bs, a, b, d, gf, gg, gm, k, gv[k]);
   }
@@ -603,7 +603,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) st[k][j + 1][i + 1] = gv[k];
   }
-  if (a.jet && a.jetblk[b]) jet_interior_fn<R, NEQ>(st, a, b, nullptr);
+  if (a.jet && a.jetblk[li]) jet_interior_fn<R, NEQ>(st, a, b, nullptr);
   __syncthreads();
 
   // u ghosts = up ghosts (u = up, src/tstep.f90:85; the old u stays in so),
@@ -714,7 +714,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_fill1(KArgs a, PhysArgs pa, int
   if (tid < 64) {
     const int f = tid / 16, m = 1 + tid % 16;
     ghost_ij(f, 0, m, gi, gj);
-    const int2 d = a.fd[(size_t)b * 4 + f];
+    const int2 d = a.fd[li * 4 + f];
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) w = ghost_value<R>(upool, bs, a, b, d, f, 0, m, k, gv[k]);
     if (w) {
@@ -771,7 +771,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_calcprim(KArgs a, PhysArgs pa, 
   R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;
   load_tile<R, NEQ>(&st[0][0][0], u, bar, a.err, b);
   if (!wait_tiles(bar, a.err, b)) return;
-  if (jet_interior && a.jet && a.jetblk[b]) {
+  if (jet_interior && a.jet && a.jetblk[blockIdx.x]) {
     jet_interior_fn<R, NEQ>(st, a, b, u);
     __syncthreads();
   }
@@ -806,7 +806,7 @@ __global__ void __launch_bounds__(128) k_fill_only(KArgs a, R* pool, int layers)
   if (g >= layers) return;
   int i, j;
   ghost_ij(f, g, m, i, j);
-  const int2 d = a.fd[(size_t)b * 4 + f];
+  const int2 d = a.fd[li * 4 + f];
   R vals[NEQ];
   bool w = false;
 #pragma unroll
@@ -822,8 +822,9 @@ __global__ void __launch_bounds__(128) k_fill_only(KArgs a, R* pool, int layers)
 template <typename R, int NEQ>
 __global__ void __launch_bounds__(256) k_jet_only(KArgs a, R* pool)
 {
-  const int b = a.leaves[blockIdx.x];
-  if (!a.jetblk[b]) return;
+  const int li = blockIdx.x;
+  if (!a.jetblk[li]) return;
+  const int b = a.leaves[li];
   const int i = 1 + threadIdx.x % 16, j = 1 + threadIdx.x / 16;
   if (!in_jet(a, b, i, j)) return;
   R* pb = pool + (size_t)b * NEQ * W2D_CELLS;
