@@ -175,6 +175,94 @@ def cpu_baseline(threads: int, target_s: float = 12.0, max_steps: int = 400):
                       f"{el:.1f} s"}
 
 
+ENS_RUNS = 256
+ENS_CAP = 6000           # pool slots per run (the runs use a few hundred to a few thousand)
+NN_SAMPLES = 10_000_000
+NN_EPOCHS = 60
+
+
+def batched_measure(args, plain_value: float):
+    """The batched FP32 + learned-cooling path: the 256-run ensemble of
+    Sedov-with-coolingh runs of uneven size, its surrogate trained on the
+    device first; per-run density L1 against the same runs in FP64 with
+    the exact routine (the plain path, itself equal to the CPU oracle to
+    1e-10 with coolingh)."""
+    import numpy as np
+
+    from walicxe2d_b200.api import Ensemble, Surrogate
+    from walicxe2d_b200.params import ensemble_members
+    t0 = time.perf_counter()
+    nn = Surrogate(20261203)
+    nn.samples(NN_SAMPLES, seed=20261203)
+    t1 = time.perf_counter()
+    loss = nn.train(NN_EPOCHS, batch=8192, lr=2e-3, lr_end=2e-5)
+    t2 = time.perf_counter()
+    judge = nn.judge(1 << 22, seed=20261204)
+    pre, warm, steps = 10, max(args.warmup, 3), min(args.steps, 40)
+    nruns = args.batched_runs
+    out, states = {}, {}
+    for name, prec, use_nn in (("fp32nn", 32, True), ("fp64", 64, False)):
+        mem = ensemble_members(count=nruns, precision=prec)
+        for p, ic in mem:
+            p.nblocks = min(p.nblocks, ENS_CAP)
+        ens = Ensemble(mem, threads=0)
+        ctx = ens.ctx
+        if use_nn:
+            ctx.set_surrogate(nn)
+        ens.run(pre + warm)
+        ctx.sync()
+        st0 = ens.status(-1)
+        c0 = ctx.surrogate_counts() if use_nn else (0, 0)
+        n0 = ctx.launch_count()
+        ctx.profile(True)
+        ms = []
+        for _ in range(steps):
+            ctx.flush_l2()
+            ctx.event_record(0)
+            ens.run(1)
+            ctx.event_record(1)
+            ms.append(ctx.event_elapsed(0, 1))
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        st1 = ens.status(-1)
+        zu = st1["zone_updates"] - st0["zone_updates"]
+        rec = {"value": zu / (sum(ms) / 1000.0), "ms_per_step": sum(ms) / steps, "leaves": st1["nleaf"],
+               "gpu_launches": int(ctx.launch_count() - n0),
+               "kernels_ms_per_step": {k: round(v[1] / steps, 4) for k, v in prof.items()}}
+        if use_nn:
+            c1 = ctx.surrogate_counts()
+            sv, ex = c1[0] - c0[0], c1[1] - c0[1]
+            rec["cells_served_by_network"] = sv / max(sv + ex, 1)
+        out[name] = rec
+        states[name] = {r: (ens.leaves(r), ens.blocks(r)[1][:, 0, 2:18, 2:18]) for r in range(nruns)}
+        rec["nbmax_max_run"] = max(ens.status(r)["nbmax"] for r in range(nruns))
+        ens.close()
+    l1, same = [], 0
+    for r in range(nruns):
+        ia, ra = states["fp64"][r]
+        ib, rb = states["fp32nn"][r]
+        common, xa, xb = np.intersect1d(ia, ib, return_indices=True)
+        same += int(len(common) == len(ia) == len(ib))
+        a, b = ra[xa], rb[xb]
+        l1.append(float(np.abs(b - a).sum() / max(np.abs(a).sum(), 1e-300)))
+    l1 = np.array(l1)
+    v = out["fp32nn"]["value"]
+    return {
+        "metric": UNIT, "value": v, "unit": UNIT, "dtype": "f32+bf16-mlp",
+        "ms_per_step": out["fp32nn"]["ms_per_step"], "steps": steps,
+        "workload": f"{nruns} independent Sedov-with-coolingh runs (roots k x k, k in 2..16; 3..6 levels; "
+                    "n log-U[0.1,10] cm^-3, E log-U[1e50,1e51] erg; 40 pc box), one device context, "
+                    f"{pre}+{warm} untimed steps, L2 flushed before every timed step",
+        "leaves": out["fp32nn"]["leaves"], "ratio_to_plain_fp64_value": v / plain_value,
+        "fp32nn": out["fp32nn"], "fp64_exact_same_runs": out["fp64"],
+        "density_l1_vs_fp64": {"max": float(l1.max()), "median": float(np.median(l1)),
+                               "runs_over_1e-3": int((l1 > 1e-3).sum()), "runs_same_tree": same,
+                               "note": "interior cells of the leaves both runs share, after the same step count"},
+        "surrogate": {"samples": NN_SAMPLES, "epochs": NN_EPOCHS, "samples_s": t1 - t0, "train_s": t2 - t1,
+                      "final_batch_mse": loss, "judged_by_exact_routine": judge},
+    }
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return 0
@@ -321,6 +409,9 @@ def run_ours(args, ws, rank, local):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(os.cpu_count() or 1)
+    batched = None
+    if rank == 0 and ws == 1 and not args.no_batched and args.precision == 64:
+        batched = batched_measure(args, value)
 
     if rank == 0:
         line = {
@@ -339,6 +430,7 @@ def run_ours(args, ws, rank, local):
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
             "host_phase_ms_per_step": phases,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -355,6 +447,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", type=int, default=64, choices=[64, 32])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched FP32 + learned-cooling ensemble measurement")
+    ap.add_argument("--batched-runs", type=int, default=ENS_RUNS,
+                    help="runs in the batched ensemble (fewer for profiling)")
     ap.add_argument("--pre-steps", type=int, default=PRE_STEPS,
                     help="untimed steps before warm-up (smaller cases for profiling)")
     args = ap.parse_args()

@@ -317,6 +317,13 @@ int w2d_nn_forward(W2dNN* nn, const float* feat, int n, float* out);   /* out [2
  * mean and [5] maximum error of the neutral fraction over those, [6] share
  * whose exact |dT/T| <= 10%.  stats holds 8 doubles. */
 int w2d_nn_judge(W2dNN* nn, int64_t n, uint64_t seed, double* stats);
+/* coolingh of an FP32 context (or ensemble context) through the network:
+ * cells whose inputs lie outside the training ranges or whose predicted
+ * |dT/T| exceeds 10% take the exact routine.  The network must outlive its
+ * use by the context; nn = NULL detaches it. */
+int w2d_set_surrogate(W2dCtx* ctx, W2dNN* nn);
+/* cells served by the network and by the exact routine since creation */
+int w2d_surrogate_counts(W2dCtx* ctx, int64_t* served, int64_t* exact);
 
 #ifdef __cplusplus
 }

@@ -17,6 +17,7 @@ from __future__ import annotations
 import numpy as np
 
 H, NIN, NOUT = 64, 4, 2
+LOSS_W1 = 4.0     # weight of output 1 (temperature rate) in the loss
 P_W1 = 0
 P_B1 = P_W1 + H * NIN
 P_W2 = P_B1 + H
@@ -59,14 +60,16 @@ def forward(p, X, bf: bool = True):
 
 
 def loss_grad(p, X, Y, bf: bool = True):
-    """Mean over samples of the summed squared output error, and its gradient."""
+    """Mean over samples of the weighted summed squared output error (output
+    1 weighted LOSS_W1), and its gradient."""
     r = bf16 if bf else (lambda a: np.asarray(a, np.float64))
-    W1, b1, W2, b2, W3, b3 = unpack(p)
+    _, b1, W2, b2, W3, b3 = unpack(p)
     n = X.shape[0]
     O, (Xb, H1, H1b, H2, H2b) = forward(p, X, bf)
     E = O - Y
-    loss = float((E * E).sum() / n)
-    dO = 2.0 * E / n
+    wt = np.array([1.0, LOSS_W1])
+    loss = float((E * E * wt).sum() / n)
+    dO = 2.0 * E * wt / n
     dOb = r(dO)
     dZ2 = (dOb @ r(W3)) * (1.0 - H2 * H2)
     dZ2b = r(dZ2)

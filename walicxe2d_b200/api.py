@@ -175,6 +175,16 @@ class Context:
     def flush_l2(self):
         self._check(self.L.w2d_flush_l2(self.h), "w2d_flush_l2")
 
+    def set_surrogate(self, nn):
+        """coolingh through a trained Surrogate (None detaches it)."""
+        self._check(self.L.w2d_set_surrogate(self.h, nn.h if nn is not None else None), "w2d_set_surrogate")
+        self._nn = nn
+
+    def surrogate_counts(self) -> tuple[int, int]:
+        a, b = C.c_int64(), C.c_int64()
+        self._check(self.L.w2d_surrogate_counts(self.h, C.byref(a), C.byref(b)), "w2d_surrogate_counts")
+        return a.value, b.value
+
     def launch_count(self) -> int:
         n = C.c_int64()
         self._check(self.L.w2d_launch_count(self.h, C.byref(n)), "w2d_launch_count")

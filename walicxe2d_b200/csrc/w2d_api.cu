@@ -342,6 +342,28 @@ void plan_pack(const W2dCtx* c, int2* pf1, int2* pf2, const int* leaves, int nl,
   }
 }
 
+// coolingh through the surrogate, the exact routine on the cells it does
+// not serve, then the primitives and statistics of every leaf
+int cool_surrogate(W2dCtx* c, const KArgs& a1, const PhysArgs& pa, double dts)
+{
+  const int64_t need = (int64_t)c->nleaf * 320;
+  if (need > c->fb_cap) {
+    CK(cudaStreamSynchronize(c->st));
+    if (c->d_fb) cudaFree(c->d_fb);
+    c->d_fb = nullptr;
+    c->fb_cap = 0;
+    const int64_t cap = need + need / 4 + 4096;
+    CK(cudaMalloc(&c->d_fb, sizeof(int) * (size_t)cap));
+    c->fb_cap = cap;
+  }
+  CK(cudaMemsetAsync(c->d_fb_count, 0, sizeof(int), c->st));
+  int rc = launch(c, "cooling_nn", [&] {
+    return launch_cool_nn(c->neq, a1, pa, dts, c->nn_img, c->d_fb, c->d_fb_count, c->d_nn_counts, c->nsm, c->st);
+  });
+  if (rc) return rc;
+  return launch(c, "calcprim", [&] { return c->L->calcprim(c->neq, a1, pa, c->d_leaves, c->nleaf, 0, c->st); });
+}
+
 int tstep_ready(W2dCtx* c, bool need_bounds = true)
 {
   if (!c->have_topology || (need_bounds && !c->have_bounds))
@@ -423,6 +445,7 @@ int ctx_tstep_rest(W2dCtx* c, double time, double dt)
   }
   if (c->p.cooling != W2D_ADIABATIC) {
     const double dts = dt * c->p.tsc;
+    if (c->nn_img && c->p.cooling == W2D_COOLINGH) return cool_surrogate(c, a1, pa, dts);
     if ((rc = launch(c, "cooling", [&] { return c->L->cool(c->neq, a1, pa, dts, c->st); }))) return rc;
   }
   return W2D_OK;
@@ -478,6 +501,10 @@ int w2d_create(const W2dParams* p, W2dCtx** out)
   CKC(cudaMalloc(&c->d_dt, sizeof(double) * 4));
   CKC(cudaMalloc(&c->d_cooltab, sizeof(double) * 82));
   CKC(cudaMalloc(&c->d_leaves, sizeof(int) * slots));
+  CKC(cudaMalloc(&c->d_fb_count, sizeof(int)));
+  CKC(cudaMalloc(&c->d_nn_counts, 2 * sizeof(unsigned long long)));
+  CKC(cudaMemsetAsync(c->d_nn_counts, 0, 2 * sizeof(unsigned long long), c->st));
+  cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device);
   CKC(cudaMemsetAsync(c->d_lev, 0, sizeof(int) * slots, c->st));
   CKC(cudaMemsetAsync(c->d_icoord, 0, sizeof(int) * 2 * slots, c->st));
   CKC(cudaMemsetAsync(c->d_err, 0, sizeof(int) * 4, c->st));
@@ -545,7 +572,8 @@ int w2d_destroy(W2dCtx* c)
   cudaEvent_t evs[] = {c->ev_topo, c->ev_ops, c->ev_plan[0], c->ev_plan[1], c->ev_dt};
   for (auto e : evs)
     if (e) cudaEventDestroy(e);
-  void* dev2[] = {c->d_run_of, c->d_runs, c->d_dt_run, c->d_loff, c->d_gradleaf};
+  void* dev2[] = {c->d_run_of, c->d_runs, c->d_dt_run, c->d_loff, c->d_gradleaf, c->d_fb, c->d_fb_count,
+                  c->d_nn_counts};
   for (void* d : dev2)
     if (d) cudaFree(d);
   if (c->h_dt_run) cudaFreeHost(c->h_dt_run);
@@ -1131,3 +1159,31 @@ int ctx_ens_criteria(W2dCtx* c, const double** grad)
   *grad = c->h_grad;   // grad of the leaf at position k of d_leaves at [k]
   return W2D_OK;
 }
+
+extern "C" {
+
+int w2d_set_surrogate(W2dCtx* c, W2dNN* nn)
+{
+  if (!c) return W2D_ERR_ARG;
+  if (!nn) {
+    c->nn_img = nullptr;
+    return W2D_OK;
+  }
+  if (c->p.precision != 32 || c->p.cooling != W2D_COOLINGH)
+    return set_error(c, W2D_ERR_ARG, 0, 0, 0, "the surrogate serves coolingh of the FP32 path");
+  c->nn_img = nn_image_of(nn);
+  return W2D_OK;
+}
+
+int w2d_surrogate_counts(W2dCtx* c, int64_t* served, int64_t* exact)
+{
+  if (!c) return W2D_ERR_ARG;
+  unsigned long long h[2] = {0, 0};
+  CK(cudaMemcpyAsync(h, c->d_nn_counts, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (served) *served = (int64_t)h[0];
+  if (exact) *exact = (int64_t)h[1];
+  return W2D_OK;
+}
+
+}  // extern "C"

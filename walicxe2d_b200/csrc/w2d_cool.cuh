@@ -122,15 +122,19 @@ __global__ void __launch_bounds__(W2D_THREADS) k_cool(KArgs a, PhysArgs pa, doub
   double* sred = reinterpret_cast<double*>(w2d_smem + 128 + sizeof(R) * NEQ * W2D_CELLS);
   const Phys<R> ph = make_phys<R, -1, -1>(pa);
   const Phys<double> phd = make_phys<double, -1, -1>(pa);
-  const int b = a.leaves[blockIdx.x];
   const int tid = threadIdx.x;
   const size_t bs = (size_t)NEQ * W2D_CELLS;
+  bar_init_once(bar);
+  uint32_t par = 0;
+  const double dt_arg = dt_s;
+  for (LeafRange lr = leaf_range(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
+  const int b = a.leaves[lr.li];
   R* __restrict__ u = (R*)a.u + (size_t)b * bs;
   R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;
-  load_tile<R, NEQ>(&st[0][0][0], u, bar, a.err, b);
-  if (a.run_of) dt_s = a.dt_run[a.run_of[b]] * a.tsc;   // dt*tsc of the block's run
-  if (!wait_tiles(bar, a.err, b)) return;
-  if (a.jet && a.jetblk[blockIdx.x]) {   // impose_jet of boundaryI, before cooling
+  if (tid == 0) tile_issue<R, NEQ>(&st[0][0][0], u, bar);
+  dt_s = a.run_of ? a.dt_run[a.run_of[b]] * a.tsc : dt_arg;   // dt*tsc of the block's run
+  if (!wait_tiles_p(bar, a.err, b, par)) return;
+  if (a.jet && a.jetblk[lr.li]) {   // impose_jet of boundaryI, before cooling
     jet_interior_fn<R, NEQ>(st, a, b, u);
     __syncthreads();
   }
@@ -170,6 +174,8 @@ __global__ void __launch_bounds__(W2D_THREADS) k_cool(KArgs a, PhysArgs pa, doub
   }
   __syncthreads();
   block_stats<R, NEQ>(st, ph, a, pa, b, sred);
+  leaf_end();
+  }
 }
 
 // primitives of whole blocks into a staging buffer (w2d_get_primit when

@@ -44,6 +44,14 @@ struct W2dCtx {
   cudaEvent_t ev_dt = nullptr;  // dt and the error word have reached h_small/h_err
   // ensembles (nruns > 0): run of every slot, per-run geometry and dt, and
   // the offsets of each run's leaves in d_leaves
+  // learned coolingh surrogate (FP32 path): weights of the attached
+  // network, the list of cells it leaves to the exact routine, counters
+  const w2d::NNImage* nn_img = nullptr;
+  int* d_fb = nullptr;
+  int64_t fb_cap = 0;
+  int* d_fb_count = nullptr;
+  unsigned long long* d_nn_counts = nullptr;   // served, exact
+  int nsm = 148;
   int nruns = 0;
   int* d_run_of = nullptr;
   w2d::RunGeo* d_runs = nullptr;

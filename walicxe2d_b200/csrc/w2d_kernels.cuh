@@ -76,7 +76,27 @@ struct KArgs {
   const RunGeo* runs;
   const double* dt_run;
   double tsc;
+  // launch shape of the per-leaf kernels: grid = 0 gives one CTA per leaf;
+  // otherwise a persistent grid walks the leaves strided (sched 0) or in
+  // contiguous chunks (sched 1).  nleaf_dev: leaf count in device memory
+  // (a launch captured in a CUDA graph reads the current count from it).
+  int grid, sched;
+  const int* nleaf_dev;
 };
+
+struct LeafRange {
+  int li, end, step;
+};
+__device__ __forceinline__ LeafRange leaf_range(const KArgs& a)
+{
+  const int n = a.nleaf_dev ? *a.nleaf_dev : a.nleaf;
+  if (a.sched == 1) {
+    const int chunk = (n + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int lo = (int)blockIdx.x * chunk;
+    return {lo, lo + chunk < n ? lo + chunk : n, 1};
+  }
+  return {(int)blockIdx.x, n, (int)gridDim.x};
+}
 
 __device__ __forceinline__ double geo_dx(const KArgs& a, int b, int lev)
 {
@@ -381,6 +401,43 @@ __device__ __forceinline__ bool wait_tiles(uint64_t* bar, int* err, int b)
   return false;
 }
 
+// Tile copies of the persistent kernels: the barrier is initialised once per
+// CTA and completes once per leaf (phase parity alternates); thread 0 issues.
+template <typename R, int NEQ>
+__device__ __forceinline__ void tile_issue(R* dst, const R* src, uint64_t* bar)
+{
+  constexpr uint32_t bytes = (uint32_t)(NEQ * W2D_CELLS * sizeof(R));
+  mbar_arrive_expect(bar, bytes);
+  bulk_g2s(dst, src, bytes, bar);
+}
+template <typename R, int NEQ>
+__device__ __forceinline__ void tiles_issue2(R* d1, const R* s1, R* d2, const R* s2, uint64_t* bar)
+{
+  constexpr uint32_t bytes = (uint32_t)(NEQ * W2D_CELLS * sizeof(R));
+  mbar_arrive_expect(bar, 2 * bytes);
+  bulk_g2s(d1, s1, bytes, bar);
+  bulk_g2s(d2, s2, bytes, bar);
+}
+__device__ __forceinline__ bool wait_tiles_p(uint64_t* bar, int* err, int b, uint32_t parity)
+{
+  if (mbar_wait(bar, parity)) return true;
+  if (threadIdx.x == 0) set_err(err, ERR_TIMEOUT, b, -1, -1);
+  mbar_wait(bar, parity);
+  return false;
+}
+// end of one leaf: the shared tiles this thread wrote are ordered before the
+// next leaf's tile copies into them
+__device__ __forceinline__ void leaf_end()
+{
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+}
+__device__ __forceinline__ void bar_init_once(uint64_t* bar)
+{
+  if (threadIdx.x == 0) mbar_init(bar, 1);
+  __syncthreads();
+}
+
 // src/dmc_module.f90:14-32 on the table cooltab(1:2,1:41) (T row then
 // Lambda row); the index is clamped to the table (the reference reads row 42
 // at T == 1e8 exactly).
@@ -485,18 +542,21 @@ __global__ void __launch_bounds__(W2D_THREADS) k_half(KArgs a, PhysArgs pa, doub
   R(*sf)[16][17] = reinterpret_cast<R(*)[16][17]>(w2d_smem + 128 + sizeof(R) * (NEQ + 1) * W2D_CELLS);
   R(*sg)[17][16] = reinterpret_cast<R(*)[17][16]>(w2d_smem + 128 + sizeof(R) * ((NEQ + 1) * W2D_CELLS + NEQ * 272));
   const Phys<R> ph = make_phys<R, SOLVER, -1>(pa);
-  const int b = a.leaves[blockIdx.x];
   const int tid = threadIdx.x;
   const size_t bs = (size_t)NEQ * W2D_CELLS;
+  const bool dmc = pa.cooling == COOL_DMC;
+  bar_init_once(bar);
+  uint32_t par = 0;
+  for (LeafRange lr = leaf_range(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
+  const int b = a.leaves[lr.li];
   const R* __restrict__ u = (const R*)a.u + (size_t)b * bs;
   R* __restrict__ up = (R*)a.up + (size_t)b * bs;
-  const bool dmc = pa.cooling == COOL_DMC;
-  load_tile<R, NEQ>(&st[0][0][0], dmc ? (const R*)a.prim + (size_t)b * bs : u, bar, a.err, b);
+  if (tid == 0) tile_issue<R, NEQ>(&st[0][0][0], dmc ? (const R*)a.prim + (size_t)b * bs : u, bar);
   const int lev = a.lev[b];
   const double dtm = step_dt(a, b, dt) / 2.;
   const R dtdx = R(dtm / geo_dx(a, b, lev));
   const R dtdy = R(dtm / geo_dy(a, b, lev));
-  if (!wait_tiles(bar, a.err, b)) return;
+  if (!wait_tiles_p(bar, a.err, b, par)) return;
 
   // primitives (in place) and sound speed of cells 0..17 (corners skipped)
   for (int c = tid; c < 18 * 18; c += W2D_THREADS) {
@@ -550,6 +610,8 @@ __global__ void __launch_bounds__(W2D_THREADS) k_half(KArgs a, PhysArgs pa, doub
           uo - dtdx * (sf[k][j - 1][i] - sf[k][j - 1][i - 1]) - dtdy * (sg[k][j][i - 1] - sg[k][j - 1][i - 1]);
     }
   }
+  leaf_end();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -572,13 +634,16 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
   R(*sf)[16][17] = reinterpret_cast<R(*)[16][17]>(w2d_smem + 128 + sizeof(R) * 2 * NEQ * W2D_CELLS);
   R(*sg)[17][16] = reinterpret_cast<R(*)[17][16]>(w2d_smem + 128 + sizeof(R) * (2 * NEQ * W2D_CELLS + NEQ * 272));
   const Phys<R> ph = make_phys<R, SOLVER, LIMITER>(pa);
-  const int li = blockIdx.x;
-  const int b = a.leaves[li];
   const int tid = threadIdx.x;
   const size_t bs = (size_t)NEQ * W2D_CELLS;
   const R* __restrict__ upool = (const R*)a.up;
+  bar_init_once(bar);
+  uint32_t par = 0;
+  for (LeafRange lr = leaf_range(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
+  const int li = lr.li;
+  const int b = a.leaves[li];
   R* __restrict__ u = (R*)a.u + (size_t)b * bs;
-  load_two_tiles<R, NEQ>(&st[0][0][0], upool + (size_t)b * bs, &so[0][0][0], u, bar);
+  if (tid == 0) tiles_issue2<R, NEQ>(&st[0][0][0], upool + (size_t)b * bs, &so[0][0][0], u, bar);
   const int lev = a.lev[b];
   const double dtb = step_dt(a, b, dt);
   const R dtdx = R(dtb / geo_dx(a, b, lev));
@@ -596,7 +661,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) gw = ghost_value<R>(upool, bs, a, b, d, gf, gg, gm, k, gv[k]);
   }
-  if (!wait_tiles(bar, a.err, b)) return;
+  if (!wait_tiles_p(bar, a.err, b, par)) return;
   if (tid < 128 && gw) {
     int i, j;
     ghost_ij(gf, gg, gm, i, j);
@@ -681,6 +746,8 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
       u[k * W2D_CELLS + cidx(i, j)] = v;
     }
   }
+  leaf_end();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -701,13 +768,16 @@ __global__ void __launch_bounds__(W2D_THREADS) k_fill1(KArgs a, PhysArgs pa, int
   R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
   double* sred = reinterpret_cast<double*>(w2d_smem + 128 + sizeof(R) * NEQ * W2D_CELLS);
   const Phys<R> ph = make_phys<R, -1, -1>(pa);
-  const int li = blockIdx.x;
-  const int b = a.leaves[li];
   const int tid = threadIdx.x;
   const size_t bs = (size_t)NEQ * W2D_CELLS;
   R* __restrict__ upool = (R*)a.u;
+  bar_init_once(bar);
+  uint32_t par = 0;
+  for (LeafRange lr = leaf_range(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
+  const int li = lr.li;
+  const int b = a.leaves[li];
   R* __restrict__ u = upool + (size_t)b * bs;
-  if (stats) load_tile<R, NEQ>(&st[0][0][0], u, bar, a.err, b);
+  if (stats && tid == 0) tile_issue<R, NEQ>(&st[0][0][0], u, bar);
   R gv[NEQ];
   bool w = false;
   int gi = 0, gj = 0;
@@ -722,8 +792,8 @@ __global__ void __launch_bounds__(W2D_THREADS) k_fill1(KArgs a, PhysArgs pa, int
       for (int k = 0; k < NEQ; ++k) u[k * W2D_CELLS + cidx(gi, gj)] = gv[k];
     }
   }
-  if (!stats) return;
-  if (!wait_tiles(bar, a.err, b)) return;
+  if (!stats) continue;
+  if (!wait_tiles_p(bar, a.err, b, par)) return;
   if (tid < 64 && w) {
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) st[k][gj + 1][gi + 1] = gv[k];
@@ -741,6 +811,8 @@ __global__ void __launch_bounds__(W2D_THREADS) k_fill1(KArgs a, PhysArgs pa, int
   }
   __syncthreads();
   block_stats<R, NEQ>(st, ph, a, pa, b, sred);
+  leaf_end();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -764,14 +836,19 @@ __global__ void __launch_bounds__(W2D_THREADS) k_calcprim(KArgs a, PhysArgs pa, 
   R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
   double* sred = reinterpret_cast<double*>(w2d_smem + 128 + sizeof(R) * NEQ * W2D_CELLS);
   const Phys<R> ph = make_phys<R, -1, -1>(pa);
-  const int b = list[blockIdx.x];
   const int tid = threadIdx.x;
   const size_t bs = (size_t)NEQ * W2D_CELLS;
+  bar_init_once(bar);
+  uint32_t par = 0;
+  LeafRange lr = leaf_range(a);
+  if (list != a.leaves) lr = LeafRange{(int)blockIdx.x, n, (int)gridDim.x};
+  for (; lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
+  const int b = list[lr.li];
   R* __restrict__ u = (R*)a.u + (size_t)b * bs;
   R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;
-  load_tile<R, NEQ>(&st[0][0][0], u, bar, a.err, b);
-  if (!wait_tiles(bar, a.err, b)) return;
-  if (jet_interior && a.jet && a.jetblk[blockIdx.x]) {
+  if (tid == 0) tile_issue<R, NEQ>(&st[0][0][0], u, bar);
+  if (!wait_tiles_p(bar, a.err, b, par)) return;
+  if (jet_interior && a.jet && a.jetblk[lr.li]) {
     jet_interior_fn<R, NEQ>(st, a, b, u);
     __syncthreads();
   }
@@ -790,6 +867,8 @@ __global__ void __launch_bounds__(W2D_THREADS) k_calcprim(KArgs a, PhysArgs pa, 
   }
   __syncthreads();
   block_stats<R, NEQ>(st, ph, a, pa, b, sred);
+  leaf_end();
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -23,6 +23,9 @@ using R = W2D_INST_REAL;
     default: return cudaErrorInvalidValue;          \
   }
 
+// Grid of a per-leaf kernel: one CTA per leaf, or the persistent grid.
+static inline int launch_grid(const KArgs& a) { return a.grid > 0 ? a.grid : a.nleaf; }
+
 // Opts a kernel into more than 48 KB of dynamic shared memory (once).
 template <typename K>
 static cudaError_t smem_opt_in(K kernel, size_t bytes, bool& done)
@@ -40,7 +43,7 @@ static cudaError_t half_t(const KArgs& a, const PhysArgs& pa, double dt, cudaStr
   constexpr size_t sm = smem_half<R, NEQ>();
   cudaError_t e = smem_opt_in(k_half<R, NEQ, S>, sm, done);
   if (e != cudaSuccess) return e;
-  k_half<R, NEQ, S><<<a.nleaf, W2D_THREADS, sm, st>>>(a, pa, dt);
+  k_half<R, NEQ, S><<<launch_grid(a), W2D_THREADS, sm, st>>>(a, pa, dt);
   return cudaGetLastError();
 }
 
@@ -61,7 +64,7 @@ static cudaError_t full_t(const KArgs& a, const PhysArgs& pa, double dt, cudaStr
   constexpr size_t sm = smem_full<R, NEQ>();
   cudaError_t e = smem_opt_in(k_full<R, NEQ, S, L>, sm, done);
   if (e != cudaSuccess) return e;
-  k_full<R, NEQ, S, L><<<a.nleaf, W2D_THREADS, sm, st>>>(a, pa, dt);
+  k_full<R, NEQ, S, L><<<launch_grid(a), W2D_THREADS, sm, st>>>(a, pa, dt);
   return cudaGetLastError();
 }
 
@@ -85,7 +88,7 @@ static cudaError_t fill1_t(const KArgs& a, const PhysArgs& pa, int stats, cudaSt
   constexpr size_t sm = smem_fill1<R, NEQ>();
   cudaError_t e = smem_opt_in(k_fill1<R, NEQ>, sm, done);
   if (e != cudaSuccess) return e;
-  k_fill1<R, NEQ><<<a.nleaf, W2D_THREADS, sm, st>>>(a, pa, stats);
+  k_fill1<R, NEQ><<<launch_grid(a), W2D_THREADS, sm, st>>>(a, pa, stats);
   return cudaGetLastError();
 }
 
@@ -111,7 +114,8 @@ static cudaError_t calcprim_t(const KArgs& a, const PhysArgs& pa, const int* lis
   constexpr size_t sm = smem_calcprim<R, NEQ>();
   cudaError_t e = smem_opt_in(k_calcprim<R, NEQ>, sm, done);
   if (e != cudaSuccess) return e;
-  k_calcprim<R, NEQ><<<n, W2D_THREADS, sm, st>>>(a, pa, list, n, jet_interior);
+  const int grid = (list == a.leaves && a.grid > 0) ? a.grid : n;
+  k_calcprim<R, NEQ><<<grid, W2D_THREADS, sm, st>>>(a, pa, list, n, jet_interior);
   return cudaGetLastError();
 }
 
@@ -157,7 +161,7 @@ static cudaError_t cool_t(const KArgs& a, const PhysArgs& pa, double dt_s, cudaS
   constexpr size_t sm = smem_cool<R, NEQ>();
   cudaError_t e = smem_opt_in(k_cool<R, NEQ>, sm, done);
   if (e != cudaSuccess) return e;
-  k_cool<R, NEQ><<<a.nleaf, W2D_THREADS, sm, st>>>(a, pa, dt_s);
+  k_cool<R, NEQ><<<launch_grid(a), W2D_THREADS, sm, st>>>(a, pa, dt_s);
   return cudaGetLastError();
 }
 

@@ -42,4 +42,15 @@ cudaError_t launch_dt_runs(const int* leaves, const int* loff, int nruns, const 
 // out[k] = v[leaves[k]]
 cudaError_t launch_gather_leaf(const int* leaves, int n, const double* v, double* out, cudaStream_t st);
 
+struct NNImage;
+// coolingh (FP32 path) through the learned surrogate with the exact routine
+// on the cells it does not serve; counts[0] += served, counts[1] += exact
+cudaError_t launch_cool_nn(int neq, const KArgs& a, const PhysArgs& pa, double dt_s, const NNImage* img,
+                           int* fb_list, int* fb_count, unsigned long long* counts, int nsm, cudaStream_t st);
+
+}  // namespace w2d
+
+struct W2dNN;
+namespace w2d {
+const NNImage* nn_image_of(const W2dNN* nn);
 }  // namespace w2d

@@ -221,11 +221,11 @@ __global__ void __launch_bounds__(128, 1) k_nn_train(const float* __restrict__ f
     nn_ld64(tm, C_Z1, v);
 #pragma unroll
     for (int k = 0; k < NN_H; ++k) {
-      h1[k] = tanhf(v[k] + s.f.b1[k]);
-      const uint16_t hb = f2bf(h1[k]);
-      s.f.h1[tc_off(tid, k, NN_H) >> 1] = hb;
-      s.h1t[tc_off(k, tid, 128) >> 1] = hb;
+      h1[k] = nn_tanh(v[k] + s.f.b1[k]);
+      s.h1t[tc_off(k, tid, 128) >> 1] = f2bf(h1[k]);
     }
+#pragma unroll
+    for (int k = 0; k < NN_H; k += 8) nn_put8(s.f.h1, tid, k, NN_H, h1 + k);
     nn_sync();
     if (tid == 0) {
       nn_layer_mma(tm + C_Z2, 0, s.f.h1, s.f.w2, NN_H, NN_H);
@@ -235,11 +235,11 @@ __global__ void __launch_bounds__(128, 1) k_nn_train(const float* __restrict__ f
     nn_ld64(tm, C_Z2, v);
 #pragma unroll
     for (int k = 0; k < NN_H; ++k) {
-      h2[k] = tanhf(v[k] + s.f.b2[k]);
-      const uint16_t hb = f2bf(h2[k]);
-      s.f.h2[tc_off(tid, k, NN_H) >> 1] = hb;
-      s.h2t[tc_off(k, tid, 128) >> 1] = hb;
+      h2[k] = nn_tanh(v[k] + s.f.b2[k]);
+      s.h2t[tc_off(k, tid, 128) >> 1] = f2bf(h2[k]);
     }
+#pragma unroll
+    for (int k = 0; k < NN_H; k += 8) nn_put8(s.f.h2, tid, k, NN_H, h2 + k);
     nn_sync();
     if (tid == 0) {
       nn_layer_mma(tm + C_O, 0, s.f.h2, s.f.w3, NN_H, NN_NOUT);
@@ -249,8 +249,8 @@ __global__ void __launch_bounds__(128, 1) k_nn_train(const float* __restrict__ f
     tc_ld16(tc_addr(tm, 32 * warp, C_O), v);
     const float o0 = v[0] + s.f.b3[0], o1 = v[1] + s.f.b3[1];
     const float e0 = valid ? o0 - y[0] : 0.f, e1 = valid ? o1 - y[1] : 0.f;
-    lsum += e0 * e0 + e1 * e1;
-    const float d0 = 2.f * e0 * inv_batch, d1 = 2.f * e1 * inv_batch;
+    lsum += e0 * e0 + NN_W1 * e1 * e1;
+    const float d0 = 2.f * e0 * inv_batch, d1 = 2.f * NN_W1 * e1 * inv_batch;
     gb3a += d0;
     gb3b += d1;
     s.dout[tc_off(tid, 0, NN_NOUT) >> 1] = f2bf(d0);
@@ -268,11 +268,11 @@ __global__ void __launch_bounds__(128, 1) k_nn_train(const float* __restrict__ f
 #pragma unroll
     for (int k = 0; k < NN_H; ++k) {
       const float dz = v[k] * (1.f - h2[k] * h2[k]);
-      const uint16_t db = f2bf(dz);
-      s.dz2[tc_off(tid, k, NN_H) >> 1] = db;
-      s.dz2t[tc_off(k, tid, 128) >> 1] = db;
+      s.dz2t[tc_off(k, tid, 128) >> 1] = f2bf(dz);
       v[k] = dz;
     }
+#pragma unroll
+    for (int k = 0; k < NN_H; k += 8) nn_put8(s.dz2, tid, k, NN_H, v + k);
     // bias gradient of layer 2: column sums over the tile
 #pragma unroll
     for (int k = 0; k < NN_H; ++k) {
@@ -425,7 +425,9 @@ __global__ void __launch_bounds__(128, 1) k_nn_forward(const float* __restrict__
     float v[NN_H];
     nn_ld64(tm, 0, v);
 #pragma unroll
-    for (int k = 0; k < NN_H; ++k) s.h1[tc_off(tid, k, NN_H) >> 1] = f2bf(tanhf(v[k] + s.b1[k]));
+    for (int k = 0; k < NN_H; ++k) v[k] = nn_tanh(v[k] + s.b1[k]);
+#pragma unroll
+    for (int k = 0; k < NN_H; k += 8) nn_put8(s.h1, tid, k, NN_H, v + k);
     nn_sync();
     if (tid == 0) {
       nn_layer_mma(tm, 64, s.h1, s.w2, NN_H, NN_H);
@@ -434,7 +436,9 @@ __global__ void __launch_bounds__(128, 1) k_nn_forward(const float* __restrict__
     if (!nn_wait(&bar, phase, err)) break;
     nn_ld64(tm, 64, v);
 #pragma unroll
-    for (int k = 0; k < NN_H; ++k) s.h2[tc_off(tid, k, NN_H) >> 1] = f2bf(tanhf(v[k] + s.b2[k]));
+    for (int k = 0; k < NN_H; ++k) v[k] = nn_tanh(v[k] + s.b2[k]);
+#pragma unroll
+    for (int k = 0; k < NN_H; k += 8) nn_put8(s.h2, tid, k, NN_H, v + k);
     nn_sync();
     if (tid == 0) {
       nn_layer_mma(tm, 128, s.h2, s.w3, NN_H, NN_NOUT);
@@ -479,6 +483,224 @@ __global__ void k_nn_judge(int64_t n, uint64_t seed, const float* __restrict__ o
   res[n + k] = (float)fabs(t1p / t1 - 1.);
   res[2 * n + k] = (float)fabs(y1p - y1);
   res[3 * n + k] = (float)fabs(t1 / T - 1.);
+}
+
+// Cells 0..17 x 0..17 of a block without the four corners, q = 0..319 ->
+// position in the 20 x 20 tile
+__device__ __forceinline__ int cool_cell(int q)
+{
+  const int c = q < 16 ? q + 1 : (q < 304 ? q + 2 : q + 3);
+  return cidx(c % 18, c / 18);
+}
+
+// Shared memory of the cooling kernel: the weights once, and per warpgroup
+// stream the features and one hidden-activation buffer (layer 2's output
+// overwrites layer 1's once the MMA that reads it has completed).
+struct NNCoolSmem {
+  uint16_t w1[NN_H * NN_KIN];
+  uint16_t w2[NN_H * NN_H];
+  uint16_t w3[NN_NOUT * NN_H];
+  float b1[NN_H], b2[NN_H], b3[NN_NOUT];
+  struct Stream {
+    uint16_t x[128 * NN_KIN];
+    uint16_t h[128 * NN_H];
+  } st[2];
+  uint64_t bar[2];
+  uint32_t tmem;
+};
+
+// synchronization of one warpgroup (named barrier 1 + wg, 128 threads)
+__device__ __forceinline__ void wg_sync(int wg)
+{
+  tc_fence_smem();
+  tc_fence_before();
+  asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory");
+  tc_fence_after();
+}
+
+// bounded wait of one warpgroup for its MMAs; uniform over the warpgroup
+__device__ __forceinline__ bool wg_wait(uint64_t* bar, uint32_t& phase, int wg, int* err)
+{
+  const uint32_t mine = mbar_wait(bar, phase) ? 1u : 0u;
+  uint32_t all;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 q, %1, 0;\n\t"
+      "bar.red.and.pred p, %2, 128, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(all)
+      : "r"(mine), "r"(1 + wg)
+      : "memory");
+  if (!all) {
+    if ((threadIdx.x & 127) == 0) atomicExch(err, W2D_ERR_TIMEOUT);
+    mbar_wait(bar, phase);
+    return false;
+  }
+  phase ^= 1u;
+  tc_fence_after();
+  return true;
+}
+
+// coolingh of the FP32 path with the surrogate.  The leaves' cells (cell =
+// leaf position * 320 + q) form 128-cell tiles; each of the CTA's two
+// warpgroups runs its own stream of tiles (its TMEM columns, buffers and
+// barrier), so that one stream's MMAs overlap the other's epilogues.
+// Thread r of a warpgroup owns row r (TMEM lane r).  Served cells get
+// (T, neutral fraction) from the network; cells outside the training range
+// or with a predicted change above 10% are listed for the exact routine.
+template <int NEQ>
+__global__ void __launch_bounds__(256, 4) k_cool_nn(KArgs a, PhysArgs pa, double dt_s, const NNImage* __restrict__ img,
+                                                 int* __restrict__ fb_list, int* __restrict__ fb_count,
+                                                 unsigned long long* __restrict__ counts)
+{
+  extern __shared__ __align__(1024) uint8_t nn_smem[];
+  NNCoolSmem& s = *reinterpret_cast<NNCoolSmem*>(nn_smem);
+  const int tid = threadIdx.x, warp = tid >> 5, wg = tid >> 7, row = tid & 127;
+  const int lane0 = 32 * (warp & 3);
+  for (int k = tid; k < (int)(sizeof(s.w1) / 16); k += 256)
+    reinterpret_cast<uint4*>(s.w1)[k] = reinterpret_cast<const uint4*>(img->w1)[k];
+  for (int k = tid; k < (int)(sizeof(s.w2) / 16); k += 256)
+    reinterpret_cast<uint4*>(s.w2)[k] = reinterpret_cast<const uint4*>(img->w2)[k];
+  for (int k = tid; k < (int)(sizeof(s.w3) / 16); k += 256)
+    reinterpret_cast<uint4*>(s.w3)[k] = reinterpret_cast<const uint4*>(img->w3)[k];
+  if (tid < NN_H) {
+    s.b1[tid] = img->b1[tid];
+    s.b2[tid] = img->b2[tid];
+  }
+  if (tid < NN_NOUT) s.b3[tid] = img->b3[tid];
+  if (tid == 0) {
+    mbar_init(&s.bar[0], 1);
+    mbar_init(&s.bar[1], 1);
+  }
+  if (warp == 0) tc_alloc(&s.tmem, 128);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tm = s.tmem + 64u * (uint32_t)wg;   // this stream's 64 columns
+  NNCoolSmem::Stream& ss = s.st[wg];
+  uint64_t* bar = &s.bar[wg];
+  const Phys<float> ph = make_phys<float, -1, -1>(pa);
+  uint32_t phase = 0;
+  unsigned served = 0;
+  const int64_t ncells = (int64_t)a.nleaf * 320, ntiles = (ncells + 127) / 128;
+  for (int64_t t = 2 * (int64_t)blockIdx.x + wg; t < ntiles; t += 2 * (int64_t)gridDim.x) {
+    const int64_t c = t * 128 + row;
+    const bool valid = c < ncells;
+    float uu[NEQ], q[NEQ], T = 1.f, dts = (float)dt_s, f[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float* ub = nullptr;
+    int pc = 0;
+    bool inr = false;
+    if (valid) {
+      const int b = a.leaves[c / 320];
+      pc = cool_cell((int)(c % 320));
+      ub = (float*)a.u + (size_t)b * NEQ * W2D_CELLS;
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) uu[k] = ub[k * W2D_CELLS + pc];
+      uprim<NEQ>(ph, q, uu, T);
+      if (a.run_of) dts = (float)(a.dt_run[a.run_of[b]] * a.tsc);
+      nn_features_f(uu[0], T, uu[4] / uu[0], dts, f);
+      inr = nn_in_range(f);
+    }
+    {
+      const float z[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      nn_put8(ss.x, row, 0, NN_KIN, f);     // f[4..7] are zero
+      nn_put8(ss.x, row, 8, NN_KIN, z);
+    }
+    wg_sync(wg);
+    if (row == 0) {
+      nn_layer_mma(tm, 0, ss.x, s.w1, NN_KIN, NN_H);
+      tc_commit(bar);
+    }
+    if (!wg_wait(bar, phase, wg, a.err)) break;
+    float v[16];
+#pragma unroll
+    for (int c0 = 0; c0 < NN_H; c0 += 16) {   // 16 columns at a time keeps few registers live
+      tc_ld16(tc_addr(tm, lane0, c0), v);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) v[k] = nn_tanh(v[k] + s.b1[c0 + k]);
+      nn_put8(ss.h, row, c0, NN_H, v);
+      nn_put8(ss.h, row, c0 + 8, NN_H, v + 8);
+    }
+    wg_sync(wg);
+    if (row == 0) {
+      nn_layer_mma(tm, 0, ss.h, s.w2, NN_H, NN_H);
+      tc_commit(bar);
+    }
+    if (!wg_wait(bar, phase, wg, a.err)) break;
+    // the layer-2 MMA has completed: its input buffer takes its output
+#pragma unroll
+    for (int c0 = 0; c0 < NN_H; c0 += 16) {
+      tc_ld16(tc_addr(tm, lane0, c0), v);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) v[k] = nn_tanh(v[k] + s.b2[c0 + k]);
+      nn_put8(ss.h, row, c0, NN_H, v);
+      nn_put8(ss.h, row, c0 + 8, NN_H, v + 8);
+    }
+    wg_sync(wg);
+    if (row == 0) {
+      nn_layer_mma(tm, 0, ss.h, s.w3, NN_H, NN_NOUT);
+      tc_commit(bar);
+    }
+    if (!wg_wait(bar, phase, wg, a.err)) break;
+    tc_ld16(tc_addr(tm, lane0, 0), v);
+    bool use = false;
+    if (valid && inr) {
+      float y1, t1;
+      const float n = uu[0];
+      use = nn_update_f(v[0] + s.b3[0], v[1] + s.b3[1], n, T, uu[4] / n, dts, y1, t1);
+      if (use) {   // the energy and neutral density of atomic (src/coolingh.f90:227-258)
+        const float u4 = y1 * n;
+        ub[3 * W2D_CELLS + pc] = ph.cv * (2.f * n - u4) * t1 / ph.tempsc + 0.5f * q[0] * (q[1] * q[1] + q[2] * q[2]);
+        ub[4 * W2D_CELLS + pc] = u4;
+        ++served;
+      }
+    }
+    {   // the cells left to the exact routine: one atomic per warp
+      const bool fb = valid && !use;
+      const unsigned m = __ballot_sync(0xffffffffu, fb);
+      if (m) {
+        const int lane = tid & 31;
+        int base = 0;
+        if (lane == __ffs(m) - 1) base = atomicAdd(fb_count, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+        if (fb) fb_list[base + __popc(m & ((1u << lane) - 1u))] = (int)c;
+      }
+    }
+    // the next tile's features overwrite x and its layer-1 MMA the TMEM
+    // columns read just now
+    tc_fence_before();
+    asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory");
+    tc_fence_after();
+  }
+  for (int o = 16; o > 0; o >>= 1) served += __shfl_xor_sync(0xffffffffu, served, o);
+  if ((tid & 31) == 0 && served) atomicAdd(&counts[0], (unsigned long long)served);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tc_dealloc(s.tmem, 128);
+}
+
+// The exact routine (FP64 atomic) on the listed cells.
+template <int NEQ>
+__global__ void __launch_bounds__(256) k_cool_fb(KArgs a, PhysArgs pa, double dt_s, const int* __restrict__ list,
+                                                 const int* __restrict__ count, unsigned long long* __restrict__ counts)
+{
+  const int n = *count;
+  const Phys<double> phd = make_phys<double, -1, -1>(pa);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int c = list[k];
+    const int b = a.leaves[c / 320];
+    const int pc = cool_cell(c % 320);
+    float* ub = (float*)a.u + (size_t)b * NEQ * W2D_CELLS;
+    double uu[NEQ];
+#pragma unroll
+    for (int e = 0; e < NEQ; ++e) uu[e] = (double)ub[e * W2D_CELLS + pc];
+    const double dts = a.run_of ? a.dt_run[a.run_of[b]] * a.tsc : dt_s;
+    d_atomic<NEQ>(phd, dts, uu);
+    ub[3 * W2D_CELLS + pc] = (float)uu[3];
+    ub[4 * W2D_CELLS + pc] = (float)uu[4];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) atomicAdd(&counts[1], (unsigned long long)n);
 }
 
 size_t train_smem() { return sizeof(NNTrainSmem); }
@@ -537,6 +759,43 @@ int nn_forward_launch(W2dNN* nn, const float* feat, int64_t ld, int64_t count, f
 }
 
 }  // namespace
+
+namespace w2d {
+
+const NNImage* nn_image_of(const W2dNN* nn) { return nn ? nn->d_img : nullptr; }
+
+// coolingh of the FP32 path through the surrogate, then the exact routine on
+// the cells it does not serve; fb_count must be zero on entry
+cudaError_t launch_cool_nn(int neq, const KArgs& a, const PhysArgs& pa, double dt_s, const NNImage* img,
+                           int* fb_list, int* fb_count, unsigned long long* counts, int nsm, cudaStream_t st)
+{
+  if (a.nleaf == 0) return cudaSuccess;
+  const size_t sm = sizeof(NNCoolSmem);
+  static bool opted5 = false, opted6 = false;
+  cudaError_t e = cudaSuccess;
+  const int64_t tiles = ((int64_t)a.nleaf * 320 + 127) / 128;
+  const int grid = (int)std::min<int64_t>((tiles + 1) / 2, 4 * (int64_t)nsm);
+  if (neq == 5) {
+    if (!opted5) e = cudaFuncSetAttribute(k_cool_nn<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    opted5 = true;
+    k_cool_nn<5><<<grid, 256, sm, st>>>(a, pa, dt_s, img, fb_list, fb_count, counts);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_cool_fb<5><<<4 * nsm, 256, 0, st>>>(a, pa, dt_s, fb_list, fb_count, counts);
+  } else if (neq == 6) {
+    if (!opted6) e = cudaFuncSetAttribute(k_cool_nn<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    opted6 = true;
+    k_cool_nn<6><<<grid, 256, sm, st>>>(a, pa, dt_s, img, fb_list, fb_count, counts);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_cool_fb<6><<<4 * nsm, 256, 0, st>>>(a, pa, dt_s, fb_list, fb_count, counts);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace w2d
 
 extern "C" {
 

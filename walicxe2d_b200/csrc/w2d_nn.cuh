@@ -11,11 +11,14 @@
 //   f3 = log10(dt / yr)/2     dt in [1e-2, 1e2] yr
 // Outputs are rates, so that the update vanishes with dt:
 //   o0 = asinh((y1 - y0) / (n dt s_y)) / a_y        (s_y = 1e-16, a_y = 22)
-//   o1 = (log10 ce + 12.5) / 7.5
+//   o1 = (log10(ce / (n e)) + 15) / 5,   e = 1 - y0 + 1e-4
 // where ce is the temperature relaxation rate of atomic
 // (src/coolingh.f90:246-254): t1 = 10 + (T - 10) exp(-ce dt), clamped as
-// there.  The updated (T, neutral fraction) follow from (o0, o1) and the
-// inputs with atomic's own clamps.
+// there.  Every loss term of ALOSS carries the electron density
+// n (1 - y0 + 1e-4) (src/coolingh.f90:101-103), so dividing it out leaves
+// the network a function that varies over fewer decades.  The updated
+// (T, neutral fraction) follow from (o0, o1) and the inputs with atomic's
+// own clamps.
 #pragma once
 
 #include <cstdint>
@@ -29,6 +32,7 @@ constexpr int NN_KIN = 16;    // input K padded to one MMA slice
 constexpr int NN_NOUT = 16;   // output N padded to the smallest M = 128 shape
 constexpr double NN_YR = 3.156e7;
 constexpr float NN_SY = 1e-16f, NN_AY = 22.f;
+constexpr float NN_W1 = 4.f;  // weight of the temperature-rate output in the training loss
 
 // bf16 images of the weights in the tensor-core operand layout (tc_off),
 // all K-major: W1 [64 x 16], W2 [64 x 64], W3 [16 x 64] (rows >= 2 zero),
@@ -42,6 +46,16 @@ struct NNImage {
   uint16_t w3t[NN_H * NN_NOUT];
   float b1[NN_H], b2[NN_H], b3[NN_NOUT];
 };
+
+// hidden-layer activation: the hardware tanh (tanh.approx.f32, relative
+// error about 2^-11, below the BF16 rounding of the activations that
+// follows); training and inference use the same instruction
+__device__ __forceinline__ float nn_tanh(float x)
+{
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 
 __device__ __forceinline__ uint16_t f2bf(float x)
 {
@@ -67,24 +81,54 @@ __device__ __forceinline__ void nn_targets(double n, double y0, double dt_s, dou
 {
   t[0] = (float)(asinh((y1 - y0) / (n * dt_s * (double)NN_SY)) / (double)NN_AY);
   const double c = ce > 1e-40 ? ce : 1e-40;
-  t[1] = (float)((log10(c) + 12.5) / 7.5);
+  t[1] = (float)((log10(c / (n * (1.0 - y0 + 1e-4))) + 15.0) / 5.0);
 }
 
 // The update from the outputs, with atomic's clamps (src/coolingh.f90:
 // 227-228, 250-253); returns false when the predicted relative change of T
-// exceeds 10% (the cell then takes the exact routine).
+// or of the thermal pressure exceeds 10% (the cell then takes the exact
+// routine).
 __device__ __forceinline__ bool nn_update(float o0, float o1, double n, double T, double y0, double dt_s, double& y1,
                                           double& t1)
 {
   y1 = y0 + n * dt_s * (double)NN_SY * sinh((double)NN_AY * (double)o0);
   y1 = y1 < 1. ? y1 : 1.;
   y1 = y1 > 0.0001 ? y1 : 0.0001;
-  const double ce = exp10(7.5 * (double)o1 - 12.5);
+  const double ce = exp10(5.0 * (double)o1 - 15.0) * (n * (1.0 - y0 + 1e-4));
   t1 = 10. + (T - 10.) * exp(-ce * dt_s);
   t1 = t1 > 0.1 * T ? t1 : 0.1 * T;
   t1 = t1 < 10. * T ? t1 : 10. * T;
   t1 = t1 > 10. ? t1 : 10.;
-  return fabs(t1 / T - 1.) <= 0.1;
+  const double dp = ((2. - y1) * t1) / ((2. - y0) * T) - 1.;
+  return fabs(t1 / T - 1.) <= 0.1 && fabs(dp) <= 0.1;
+}
+
+// nn_features / nn_in_range / nn_update in single precision for the
+// cooling step of the FP32 path (expm1 keeps small temperature changes
+// exact to FP32 rounding)
+__device__ __forceinline__ void nn_features_f(float n, float T, float y0, float dt_s, float* f)
+{
+  f[0] = (log10f(n) - 1.f) * (1.f / 3.f);
+  f[1] = (log10f(T) - 5.f) * (1.f / 3.f);
+  f[2] = 2.f * y0 - 1.f;
+  f[3] = log10f(dt_s * (float)(1.0 / NN_YR)) * 0.5f;
+}
+
+__device__ __forceinline__ bool nn_update_f(float o0, float o1, float n, float T, float y0, float dt_s, float& y1,
+                                            float& t1)
+{
+  y1 = y0 + n * dt_s * NN_SY * sinhf(NN_AY * o0);
+  y1 = y1 < 1.f ? y1 : 1.f;
+  y1 = y1 > 0.0001f ? y1 : 0.0001f;
+  const float ce = exp10f(5.f * o1 - 15.f) * (n * (1.f - y0 + 1e-4f));
+  t1 = T + (T - 10.f) * expm1f(-ce * dt_s);
+  t1 = t1 > 0.1f * T ? t1 : 0.1f * T;
+  t1 = t1 < 10.f * T ? t1 : 10.f * T;
+  t1 = t1 > 10.f ? t1 : 10.f;
+  // served when the predicted relative changes of T and of the thermal
+  // pressure (2 - y) T both stay within 10%
+  const float dp = ((2.f - y1) * t1) / ((2.f - y0) * T) - 1.f;
+  return fabsf(t1 / T - 1.f) <= 0.1f && fabsf(dp) <= 0.1f;
 }
 
 // Shared memory of the forward pass of one tile
@@ -117,11 +161,26 @@ __device__ __forceinline__ void nn_load_weights(NNFwdSmem& s, const NNImage* img
   for (int k = threadIdx.x; k < NN_NOUT; k += blockDim.x) s.b3[k] = img->b3[k];
 }
 
+// Eight consecutive columns c0 .. c0+7 (c0 a multiple of 8) of row r of a
+// K-major operand as one 16-byte store: one core-matrix row, so the 32
+// rows of a warp land in four 128-byte lines without bank conflicts.
+__device__ __forceinline__ void nn_put8(uint16_t* base, int r, int c0, int K, const float* v)
+{
+  uint4 w;
+  w.x = (uint32_t)f2bf(v[0]) | ((uint32_t)f2bf(v[1]) << 16);
+  w.y = (uint32_t)f2bf(v[2]) | ((uint32_t)f2bf(v[3]) << 16);
+  w.z = (uint32_t)f2bf(v[4]) | ((uint32_t)f2bf(v[5]) << 16);
+  w.w = (uint32_t)f2bf(v[6]) | ((uint32_t)f2bf(v[7]) << 16);
+  *reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(base) + tc_off(r, c0, K)) = w;
+}
+
 // Row r of the tile: features into x (bf16, zero padding).
 __device__ __forceinline__ void nn_put_x(NNFwdSmem& s, int r, const float* f)
 {
-#pragma unroll
-  for (int k = 0; k < NN_KIN; ++k) s.x[tc_off(r, k, NN_KIN) >> 1] = k < NN_IN ? f2bf(f[k]) : (uint16_t)0;
+  const float v[8] = {f[0], f[1], f[2], f[3], 0.f, 0.f, 0.f, 0.f};
+  const float z[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  nn_put8(s.x, r, 0, NN_KIN, v);
+  nn_put8(s.x, r, 8, NN_KIN, z);
 }
 
 // MMAs of one layer: D (TMEM column col) = A[128 x K] B[N x K]^T.
