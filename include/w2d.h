@@ -286,6 +286,22 @@ int w2d_ens_set_amr(W2dEns* ens, int on);
 #define W2D_ENS_NPHASES 8
 int w2d_ens_phase_ms(W2dEns* ens, double* ms, int reset);
 
+/* ---- Launch shapes and step graphs (no counterpart in the reference) ------
+ * The per-leaf kernels (half step, full step, boundaryI, cooling, block
+ * statistics) run with one CTA per leaf or on a persistent grid of 2, 4 or
+ * 8 CTAs per SM walking the leaves strided or in contiguous chunks.
+ * w2d_autotune(ctx, reps) tries every shape for `reps` steps of the live
+ * run (results do not depend on the shape) and then keeps the fastest per
+ * kernel; w2d_tuning reports, per kernel (half, full, fill I, cooling,
+ * statistics), {shape index, CTAs per SM, order} in shape[3k..3k+2], the
+ * chosen shape's mean ms and the tuning steps left.  w2d_set_graphs(ctx, 1)
+ * makes an ensemble context replay each step's two launch sequences as
+ * CUDA graphs (persistent shapes only; the leaf count is read on the
+ * device). */
+int w2d_autotune(W2dCtx* ctx, int reps);
+int w2d_tuning(W2dCtx* ctx, int32_t* shape, double* ms, int* tuning_left);
+int w2d_set_graphs(W2dCtx* ctx, int on);
+
 /* ---- Learned coolingh surrogate (no counterpart in the reference) ---------
  * A 4 -> 64 -> 64 -> 2 tanh MLP with BF16 weights on the tensor cores
  * (FP32 accumulation) mapping (log n, log T, neutral fraction, log dt) to

@@ -107,3 +107,44 @@ def test_ensemble_members_build():
     for r in range(len(mem)):
         _, u = ens.blocks(r)
         assert np.isfinite(u).all()
+
+
+def test_autotuned_graphed_ensemble_equals_plain():
+    """Launch shapes (persistent grids, strided and chunked orders) chosen
+    by the autotuner and the step graphs change no bit of any run."""
+    from walicxe2d_b200.api import Ensemble
+    mem = _adiabatic_members()
+    plain = Ensemble(mem, threads=2)
+    tuned = Ensemble(mem, threads=2)
+    tuned.ctx.set_graphs(True)
+    tuned.ctx.autotune(2)
+    plain.run(30)
+    tuned.run(30)
+    t = tuned.ctx.tuning()
+    assert t["steps_left"] == 0
+    assert all(t[k]["ctas_per_sm"] > 0 for k in ("half_step", "full_step", "fill_I"))
+    for r in range(len(mem)):
+        np.testing.assert_array_equal(plain.leaves(r), tuned.leaves(r))
+        assert plain.status(r)["time"] == tuned.status(r)["time"]
+        _, a = plain.blocks(r)
+        _, b = tuned.blocks(r)
+        m = noncorner_mask()
+        assert compare_blocks(a, b, m)[2] == 0
+
+
+def test_autotuned_single_run_against_oracle(oracle_lib):
+    """Every launch shape of a single run (one CTA per leaf included) keeps
+    the plain path exact against the oracle."""
+    from walicxe2d_b200.api import Simulation
+    p, ic = config("sedov_amr_small")
+    o = oracle_lib.Oracle(p, ic, threads=8)
+    o.startup()
+    s = Simulation(p, ic)
+    s.ctx.autotune(2)
+    for _ in range(24):
+        o.run(1)
+        s.run(1)
+    assert s.ctx.tuning()["steps_left"] == 0
+    ids = o.leaves()
+    dmax, l1, n = compare_blocks(s.ctx.get_blocks(ids), o.u[ids], noncorner_mask())
+    assert n == 0, (dmax, l1)

@@ -78,6 +78,9 @@ SIGNATURES = {
                          C.POINTER(C.c_float)]),
     "w2d_nn_forward": (_I, [_vp, C.POINTER(C.c_float), _I, C.POINTER(C.c_float)]),
     "w2d_nn_judge": (_I, [_vp, C.c_int64, C.c_uint64, _PD]),
+    "w2d_autotune": (_I, [_vp, _I]),
+    "w2d_tuning": (_I, [_vp, _PI32, _PD, C.POINTER(_I)]),
+    "w2d_set_graphs": (_I, [_vp, _I]),
     "w2d_set_surrogate": (_I, [_vp, _vp]),
     "w2d_surrogate_counts": (_I, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
 }

@@ -175,6 +175,27 @@ class Context:
     def flush_l2(self):
         self._check(self.L.w2d_flush_l2(self.h), "w2d_flush_l2")
 
+    TUNED = ("half_step", "full_step", "fill_I", "cooling", "statistics")
+
+    def autotune(self, reps: int = 2):
+        """Try every launch shape of the per-leaf kernels for `reps` steps each
+        of the live run, then keep the fastest (w2d_autotune)."""
+        self._check(self.L.w2d_autotune(self.h, reps), "w2d_autotune")
+
+    def tuning(self) -> dict:
+        sh = np.zeros(15, np.int32)
+        ms = np.zeros(5)
+        left = C.c_int()
+        self._check(self.L.w2d_tuning(self.h, _pi32(sh), _pd(ms), C.byref(left)), "w2d_tuning")
+        out = {k: {"shape": int(sh[3 * i]), "ctas_per_sm": int(sh[3 * i + 1]),
+                   "order": "chunked" if sh[3 * i + 2] else "strided", "mean_ms": float(ms[i])}
+               for i, k in enumerate(self.TUNED)}
+        out["steps_left"] = left.value
+        return out
+
+    def set_graphs(self, on: bool = True):
+        self._check(self.L.w2d_set_graphs(self.h, 1 if on else 0), "w2d_set_graphs")
+
     def set_surrogate(self, nn):
         """coolingh through a trained Surrogate (None detaches it)."""
         self._check(self.L.w2d_set_surrogate(self.h, nn.h if nn is not None else None), "w2d_set_surrogate")

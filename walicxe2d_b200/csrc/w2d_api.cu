@@ -96,6 +96,80 @@ int launch(W2dCtx* c, const char* name, F fn)
   return W2D_OK;
 }
 
+// Launch shapes the autotuner tries for the per-leaf kernels: CTAs per SM
+// of a persistent grid (0: one CTA per leaf) and the order in which a CTA
+// takes its leaves (0 strided, 1 contiguous chunk).  Results do not depend
+// on the shape (every leaf is computed by one CTA, independently of the
+// others), so tuning on the live run changes no value.
+enum { TK_HALF, TK_FULL, TK_FILL1, TK_COOL, TK_STATS, TK_N };
+struct Shape {
+  int per_sm, sched;
+};
+constexpr Shape kShapes[] = {{0, 0}, {2, 0}, {4, 0}, {4, 1}, {8, 0}, {8, 1}};
+constexpr int kNShape = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
+
+void apply_shape(W2dCtx* c, KArgs& a, int tk)
+{
+  const int sh = c->tune_left > 0 ? c->tune_cur : c->tshape[tk];
+  a.grid = kShapes[sh].per_sm * c->nsm;
+  a.sched = kShapes[sh].sched;
+}
+
+template <class F>
+int launch(W2dCtx* c, const char* name, F fn);
+
+// a tunable launch: timed with its own event pair while tuning
+template <class F>
+int launch_tk(W2dCtx* c, int tk, const char* name, F fn)
+{
+  const bool t = c->tune_left > 0 && !c->capturing;
+  if (t) cudaEventRecord(c->tune_ev[tk][0], c->st);
+  int rc = launch(c, name, fn);
+  if (t) {
+    cudaEventRecord(c->tune_ev[tk][1], c->st);
+    c->tune_rec[tk] = true;
+  }
+  return rc;
+}
+
+// After a synchronization: the tuned kernels' times of the last step go to
+// the shape in use; after the last tuning step every kernel keeps its
+// fastest shape and the step graphs are captured anew.
+void tune_collect(W2dCtx* c)
+{
+  if (c->tune_left <= 0) return;
+  bool any = false;
+  for (int k = 0; k < TK_N; ++k) {
+    if (!c->tune_rec[k]) continue;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, c->tune_ev[k][0], c->tune_ev[k][1]) == cudaSuccess) {
+      c->tune_ms[k][c->tune_cur] += ms;
+      c->tune_n[k][c->tune_cur] += 1;
+    }
+    c->tune_rec[k] = false;
+    any = true;
+  }
+  if (!any) return;
+  c->tune_step++;
+  c->tune_left--;
+  const int ns = kNShape - c->tune_first;
+  c->tune_cur = c->tune_first + (c->tune_step / c->tune_reps) % ns;
+  if (c->tune_left > 0) return;
+  for (int k = 0; k < TK_N; ++k) {
+    int best = c->tshape[k];
+    double bm = 1e300;
+    for (int q = c->tune_first; q < kNShape; ++q)
+      if (c->tune_n[k][q] > 0 && c->tune_ms[k][q] / c->tune_n[k][q] < bm) {
+        bm = c->tune_ms[k][q] / c->tune_n[k][q];
+        best = q;
+      }
+    c->tshape[k] = best;
+  }
+  if (c->gx_first) cudaGraphExecDestroy(c->gx_first);
+  if (c->gx_rest) cudaGraphExecDestroy(c->gx_rest);
+  c->gx_first = c->gx_rest = nullptr;
+}
+
 KArgs kargs(W2dCtx* c, const int2* fd)
 {
   KArgs a;
@@ -128,6 +202,7 @@ KArgs kargs(W2dCtx* c, const int2* fd)
     a.run_of = c->d_run_of;
     a.runs = c->d_runs;
     a.dt_run = c->d_dt_run;
+    a.nleaf_dev = c->d_nleaf;
   }
   return a;
 }
@@ -213,6 +288,7 @@ int sync_and_check(W2dCtx* c)
 {
   CK(cudaMemcpyAsync(c->h_err, c->d_err, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  tune_collect(c);
   return check_device(c);
 }
 
@@ -342,26 +418,41 @@ void plan_pack(const W2dCtx* c, int2* pf1, int2* pf2, const int* leaves, int nl,
   }
 }
 
+// room in the list of cells left to the exact routine; false: the buffer
+// moved (a captured graph that holds it is stale)
+int ensure_fb(W2dCtx* c, bool* moved)
+{
+  const int64_t need = (int64_t)c->nleaf * 320;
+  if (moved) *moved = false;
+  if (need <= c->fb_cap) return W2D_OK;
+  CK(cudaStreamSynchronize(c->st));
+  if (c->d_fb) cudaFree(c->d_fb);
+  c->d_fb = nullptr;
+  c->fb_cap = 0;
+  const int64_t cap = need + need / 2 + 4096;
+  CK(cudaMalloc(&c->d_fb, sizeof(int) * (size_t)cap));
+  c->fb_cap = cap;
+  if (moved) *moved = true;
+  return W2D_OK;
+}
+
 // coolingh through the surrogate, the exact routine on the cells it does
 // not serve, then the primitives and statistics of every leaf
 int cool_surrogate(W2dCtx* c, const KArgs& a1, const PhysArgs& pa, double dts)
 {
-  const int64_t need = (int64_t)c->nleaf * 320;
-  if (need > c->fb_cap) {
-    CK(cudaStreamSynchronize(c->st));
-    if (c->d_fb) cudaFree(c->d_fb);
-    c->d_fb = nullptr;
-    c->fb_cap = 0;
-    const int64_t cap = need + need / 4 + 4096;
-    CK(cudaMalloc(&c->d_fb, sizeof(int) * (size_t)cap));
-    c->fb_cap = cap;
+  if (!c->capturing) {
+    int rc0 = ensure_fb(c, nullptr);
+    if (rc0) return rc0;
   }
   CK(cudaMemsetAsync(c->d_fb_count, 0, sizeof(int), c->st));
   int rc = launch(c, "cooling_nn", [&] {
     return launch_cool_nn(c->neq, a1, pa, dts, c->nn_img, c->d_fb, c->d_fb_count, c->d_nn_counts, c->nsm, c->st);
   });
   if (rc) return rc;
-  return launch(c, "calcprim", [&] { return c->L->calcprim(c->neq, a1, pa, c->d_leaves, c->nleaf, 0, c->st); });
+  KArgs as = a1;
+  apply_shape(c, as, TK_STATS);
+  return launch_tk(c, TK_STATS, "calcprim",
+                   [&] { return c->L->calcprim(c->neq, as, pa, c->d_leaves, c->nleaf, 0, c->st); });
 }
 
 int tstep_ready(W2dCtx* c, bool need_bounds = true)
@@ -379,7 +470,8 @@ int half_step(W2dCtx* c, double dt, const double* dt_dev)
   PhysArgs pa = pargs(c);
   KArgs a2 = kargs(c, c->d_fd2);
   a2.dt_dev = dt_dev;
-  return launch(c, "half_step", [&] { return c->L->half(c->neq, a2, pa, dt, c->st); });
+  apply_shape(c, a2, TK_HALF);
+  return launch_tk(c, TK_HALF, "half_step", [&] { return c->L->half(c->neq, a2, pa, dt, c->st); });
 }
 
 }  // namespace
@@ -433,11 +525,15 @@ int ctx_tstep_rest(W2dCtx* c, double time, double dt)
   set_jet_state(c, a2, time);   // both fills impose the jet at tstep's time
   set_jet_state(c, a1, time);
   const bool jet = a1.jet != 0;
-  if ((rc = launch(c, "full_step", [&] { return c->L->full(c->neq, a2, pa, dt, c->st); }))) return rc;
+  KArgs af = a2;
+  apply_shape(c, af, TK_FULL);
+  if ((rc = launch_tk(c, TK_FULL, "full_step", [&] { return c->L->full(c->neq, af, pa, dt, c->st); }))) return rc;
   // boundaryI; with the jet its interior writes and the statistics follow in
   // a second pass, after every fill read of the interiors
   const int stats = c->p.cooling == W2D_ADIABATIC && !jet;
-  if ((rc = launch(c, "fill_I", [&] { return c->L->fill1(c->neq, a1, pa, stats, c->st); }))) return rc;
+  KArgs ai = a1;
+  apply_shape(c, ai, TK_FILL1);
+  if ((rc = launch_tk(c, TK_FILL1, "fill_I", [&] { return c->L->fill1(c->neq, ai, pa, stats, c->st); }))) return rc;
   if (jet && c->p.cooling == W2D_ADIABATIC) {
     const int nl = c->nleaf;
     if ((rc = launch(c, "jet_calcprim", [&] { return c->L->calcprim(c->neq, a1, pa, c->d_leaves, nl, 1, c->st); })))
@@ -446,7 +542,9 @@ int ctx_tstep_rest(W2dCtx* c, double time, double dt)
   if (c->p.cooling != W2D_ADIABATIC) {
     const double dts = dt * c->p.tsc;
     if (c->nn_img && c->p.cooling == W2D_COOLINGH) return cool_surrogate(c, a1, pa, dts);
-    if ((rc = launch(c, "cooling", [&] { return c->L->cool(c->neq, a1, pa, dts, c->st); }))) return rc;
+    KArgs ac = a1;
+    apply_shape(c, ac, TK_COOL);
+    if ((rc = launch_tk(c, TK_COOL, "cooling", [&] { return c->L->cool(c->neq, ac, pa, dts, c->st); }))) return rc;
   }
   return W2D_OK;
 }
@@ -502,6 +600,11 @@ int w2d_create(const W2dParams* p, W2dCtx** out)
   CKC(cudaMalloc(&c->d_cooltab, sizeof(double) * 82));
   CKC(cudaMalloc(&c->d_leaves, sizeof(int) * slots));
   CKC(cudaMalloc(&c->d_fb_count, sizeof(int)));
+  CKC(cudaMalloc(&c->d_nleaf, sizeof(int)));
+  CKC(cudaMemsetAsync(c->d_nleaf, 0, sizeof(int), c->st));
+  CKC(cudaMallocHost(&c->h_nleaf, sizeof(int)));
+  for (int k = 0; k < 5; ++k)
+    for (int q = 0; q < 2; ++q) CKC(cudaEventCreate(&c->tune_ev[k][q]));
   CKC(cudaMalloc(&c->d_nn_counts, 2 * sizeof(unsigned long long)));
   CKC(cudaMemsetAsync(c->d_nn_counts, 0, 2 * sizeof(unsigned long long), c->st));
   cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device);
@@ -572,8 +675,14 @@ int w2d_destroy(W2dCtx* c)
   cudaEvent_t evs[] = {c->ev_topo, c->ev_ops, c->ev_plan[0], c->ev_plan[1], c->ev_dt};
   for (auto e : evs)
     if (e) cudaEventDestroy(e);
+  if (c->gx_first) cudaGraphExecDestroy(c->gx_first);
+  if (c->gx_rest) cudaGraphExecDestroy(c->gx_rest);
+  for (int k = 0; k < 5; ++k)
+    for (int q = 0; q < 2; ++q)
+      if (c->tune_ev[k][q]) cudaEventDestroy(c->tune_ev[k][q]);
+  if (c->h_nleaf) cudaFreeHost(c->h_nleaf);
   void* dev2[] = {c->d_run_of, c->d_runs, c->d_dt_run, c->d_loff, c->d_gradleaf, c->d_fb, c->d_fb_count,
-                  c->d_nn_counts};
+                  c->d_nn_counts, c->d_nleaf};
   for (void* d : dev2)
     if (d) cudaFree(d);
   if (c->h_dt_run) cudaFreeHost(c->h_dt_run);
@@ -1101,6 +1210,8 @@ int ctx_commit_leaves(W2dCtx* c, int nl, const int* loff)
   memcpy(c->h_loff, loff, sizeof(int) * (size_t)(c->nruns + 1));
   if (nl > 0) CK(cudaMemcpyAsync(c->d_leaves, c->h_leaflist, sizeof(int) * (size_t)nl, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(c->d_loff, c->h_loff, sizeof(int) * (size_t)(c->nruns + 1), cudaMemcpyHostToDevice, c->st));
+  c->h_nleaf[0] = nl;
+  CK(cudaMemcpyAsync(c->d_nleaf, c->h_nleaf, sizeof(int), cudaMemcpyHostToDevice, c->st));
   CK(cudaEventRecord(c->ev_topo, c->st));
   c->nleaf = nl;
   c->have_topology = true;
@@ -1151,7 +1262,7 @@ int ctx_ens_criteria(W2dCtx* c, const double** grad)
 {
   const int nl = c->nleaf;
   if (nl > 0) {
-    CK(launch_gather_leaf(c->d_leaves, nl, c->d_grad, c->d_gradleaf, c->st));
+    CK(launch_gather_leaf(c->d_leaves, nl, nullptr, c->d_grad, c->d_gradleaf, c->st));
     CK(cudaMemcpyAsync(c->h_grad, c->d_gradleaf, sizeof(double) * (size_t)nl, cudaMemcpyDeviceToHost, c->st));
   }
   int rc = sync_and_check(c);
@@ -1183,6 +1294,134 @@ int w2d_surrogate_counts(W2dCtx* c, int64_t* served, int64_t* exact)
   CK(cudaStreamSynchronize(c->st));
   if (served) *served = (int64_t)h[0];
   if (exact) *exact = (int64_t)h[1];
+  return W2D_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// autotuner and step graphs
+
+int ctx_tune_begin(W2dCtx* c, int reps)
+{
+  if (reps < 1) reps = 1;
+  c->tune_first = (c->want_graphs || c->nruns > 0) ? 1 : 0;
+  c->tune_reps = reps;
+  c->tune_step = 0;
+  c->tune_cur = c->tune_first;
+  c->tune_left = reps * (kNShape - c->tune_first);
+  memset(c->tune_ms, 0, sizeof(c->tune_ms));
+  memset(c->tune_n, 0, sizeof(c->tune_n));
+  memset(c->tune_rec, 0, sizeof(c->tune_rec));
+  return W2D_OK;
+}
+
+namespace {
+
+// captures body() on the context's stream into *gx; the launches inside
+// count once per replay
+template <class F>
+int capture(W2dCtx* c, cudaGraphExec_t* gx, int64_t* nkernels, F body)
+{
+  cudaGraph_t g = nullptr;
+  const int64_t n0 = c->nlaunch;
+  if (cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return set_error(c, W2D_ERR_CUDA, 0, 0, 0, "stream capture could not begin");
+  c->capturing = true;
+  int rc = body();
+  c->capturing = false;
+  const cudaError_t e = cudaStreamEndCapture(c->st, &g);
+  if (rc || e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return rc ? rc : set_error(c, W2D_ERR_CUDA, 0, 0, 0, "stream capture: %s", cudaGetErrorString(e));
+  }
+  const cudaError_t e2 = cudaGraphInstantiate(gx, g, 0);
+  cudaGraphDestroy(g);
+  if (e2 != cudaSuccess) return set_error(c, W2D_ERR_CUDA, 0, 0, 0, "graph: %s", cudaGetErrorString(e2));
+  *nkernels = c->nlaunch - n0;
+  c->nlaunch = n0;
+  return W2D_OK;
+}
+
+bool graphs_now(const W2dCtx* c) { return c->want_graphs && !c->prof && c->tune_left == 0 && c->nruns > 0; }
+
+}  // namespace
+
+// first part of an ensemble step: dt of every run (and its copy to the
+// host), the half step
+int ctx_ens_first(W2dCtx* c)
+{
+  auto body = [&] {
+    int rc = ctx_ens_dt_launch(c);
+    return rc ? rc : ctx_half_step(c);
+  };
+  if (!graphs_now(c)) return body();
+  if (!c->gx_first) {
+    int rc = capture(c, &c->gx_first, &c->nlaunch_graph_first, body);
+    if (rc) return rc;
+  }
+  CK(cudaGraphLaunch(c->gx_first, c->st));
+  c->nlaunch += c->nlaunch_graph_first;
+  return W2D_OK;
+}
+
+// the rest of the ensemble step: full step, boundaryI, cooling, statistics
+int ctx_ens_rest(W2dCtx* c)
+{
+  auto body = [&] { return ctx_tstep_rest(c, 0.0, 0.0); };
+  if (!graphs_now(c)) return body();
+  if (c->nn_img) {
+    bool moved = false;
+    int rc = ensure_fb(c, &moved);
+    if (rc) return rc;
+    if (moved && c->gx_rest) {
+      cudaGraphExecDestroy(c->gx_rest);
+      c->gx_rest = nullptr;
+    }
+  }
+  if (!c->gx_rest) {
+    int rc = capture(c, &c->gx_rest, &c->nlaunch_graph_rest, body);
+    if (rc) return rc;
+  }
+  CK(cudaGraphLaunch(c->gx_rest, c->st));
+  c->nlaunch += c->nlaunch_graph_rest;
+  return W2D_OK;
+}
+
+extern "C" {
+
+int w2d_autotune(W2dCtx* c, int reps)
+{
+  if (!c) return W2D_ERR_ARG;
+  return ctx_tune_begin(c, reps);
+}
+
+int w2d_tuning(W2dCtx* c, int32_t* shape, double* ms, int* tuning_left)
+{
+  if (!c) return W2D_ERR_ARG;
+  for (int k = 0; k < TK_N; ++k) {
+    const int sh = c->tshape[k];
+    if (shape) {
+      shape[3 * k] = sh;
+      shape[3 * k + 1] = kShapes[sh].per_sm;
+      shape[3 * k + 2] = kShapes[sh].sched;
+    }
+    if (ms) ms[k] = c->tune_n[k][sh] > 0 ? c->tune_ms[k][sh] / c->tune_n[k][sh] : 0.0;
+  }
+  if (tuning_left) *tuning_left = c->tune_left;
+  return W2D_OK;
+}
+
+int w2d_set_graphs(W2dCtx* c, int on)
+{
+  if (!c) return W2D_ERR_ARG;
+  c->want_graphs = on != 0;
+  if (c->want_graphs)   // a captured launch needs a grid independent of the leaf count
+    for (int k = 0; k < TK_N; ++k)
+      if (kShapes[c->tshape[k]].per_sm == 0) c->tshape[k] = 2;
+  if (c->gx_first) cudaGraphExecDestroy(c->gx_first);
+  if (c->gx_rest) cudaGraphExecDestroy(c->gx_rest);
+  c->gx_first = c->gx_rest = nullptr;
   return W2D_OK;
 }
 

@@ -114,8 +114,8 @@ __host__ __device__ constexpr size_t smem_cool()
   return 128 + sizeof(R) * NEQ * W2D_CELLS + 64 * sizeof(double);
 }
 
-template <typename R, int NEQ>
-__global__ void __launch_bounds__(W2D_THREADS) k_cool(KArgs a, PhysArgs pa, double dt_s)
+template <typename R, int NEQ, bool P>
+__global__ void __launch_bounds__(W2D_THREADS, 2) k_cool(KArgs a, PhysArgs pa, double dt_s)
 {
   uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
   R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_cool(KArgs a, PhysArgs pa, doub
   bar_init_once(bar);
   uint32_t par = 0;
   const double dt_arg = dt_s;
-  for (LeafRange lr = leaf_range(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
+  for (LeafRange lr = leaf_range<P>(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
   const int b = a.leaves[lr.li];
   R* __restrict__ u = (R*)a.u + (size_t)b * bs;
   R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;

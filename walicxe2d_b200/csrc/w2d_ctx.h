@@ -52,6 +52,20 @@ struct W2dCtx {
   int* d_fb_count = nullptr;
   unsigned long long* d_nn_counts = nullptr;   // served, exact
   int nsm = 148;
+  // launch shapes of the per-leaf kernels (online autotuner: every shape in
+  // turn for a few steps, then the fastest per kernel) and the CUDA graphs of
+  // the ensemble step
+  int tshape[5] = {0, 0, 0, 0, 0};
+  int tune_left = 0, tune_step = 0, tune_cur = 0, tune_first = 0, tune_reps = 2;
+  double tune_ms[5][8] = {};
+  int tune_n[5][8] = {};
+  cudaEvent_t tune_ev[5][2] = {};
+  bool tune_rec[5] = {};
+  int* d_nleaf = nullptr;        // leaf count in device memory (ensembles)
+  int* h_nleaf = nullptr;        // pinned
+  bool want_graphs = false, capturing = false;
+  cudaGraphExec_t gx_first = nullptr, gx_rest = nullptr;
+  int64_t nlaunch_graph_first = 0, nlaunch_graph_rest = 0;
   int nruns = 0;
   int* d_run_of = nullptr;
   w2d::RunGeo* d_runs = nullptr;

@@ -55,3 +55,8 @@ int ctx_plan_upload(W2dCtx* c, int nl);
 // (*grad)[k]; synchronizes and checks the error word
 int ctx_ens_criteria(W2dCtx* c, const double** grad);
 
+// the two halves of an ensemble step (as CUDA graphs when enabled with
+// w2d_set_graphs, captured again after tuning or when a buffer moves)
+int ctx_ens_first(W2dCtx* c);
+int ctx_ens_rest(W2dCtx* c);
+

@@ -101,17 +101,19 @@ cudaError_t launch_dt_runs(const int* leaves, const int* loff, int nruns, const 
   return cudaGetLastError();
 }
 
-__global__ void k_gather_leaf(const int* __restrict__ leaves, int n, const double* __restrict__ v,
-                              double* __restrict__ out)
+__global__ void k_gather_leaf(const int* __restrict__ leaves, int n, const int* __restrict__ n_dev,
+                              const double* __restrict__ v, double* __restrict__ out)
 {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) out[k] = v[leaves[k]];
+  const int m = n_dev ? *n_dev : n;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) out[k] = v[leaves[k]];
 }
 
-cudaError_t launch_gather_leaf(const int* leaves, int n, const double* v, double* out, cudaStream_t st)
+cudaError_t launch_gather_leaf(const int* leaves, int n, const int* n_dev, const double* v, double* out,
+                               cudaStream_t st)
 {
-  if (n == 0) return cudaSuccess;
-  k_gather_leaf<<<(n + 255) / 256, 256, 0, st>>>(leaves, n, v, out);
+  if (n == 0 && !n_dev) return cudaSuccess;
+  const int grid = n_dev ? 1184 : (n + 255) / 256;
+  k_gather_leaf<<<grid, 256, 0, st>>>(leaves, n, n_dev, v, out);
   return cudaGetLastError();
 }
 

@@ -87,8 +87,12 @@ struct KArgs {
 struct LeafRange {
   int li, end, step;
 };
+// P = false: one CTA per leaf (a single pass, compiled without loop state);
+// P = true: the persistent walk below
+template <bool P>
 __device__ __forceinline__ LeafRange leaf_range(const KArgs& a)
 {
+  if (!P) return {(int)blockIdx.x, (int)blockIdx.x + 1, 1};
   const int n = a.nleaf_dev ? *a.nleaf_dev : a.nleaf;
   if (a.sched == 1) {
     const int chunk = (n + (int)gridDim.x - 1) / (int)gridDim.x;
@@ -401,6 +405,14 @@ __device__ __forceinline__ bool wait_tiles(uint64_t* bar, int* err, int b)
   return false;
 }
 
+// CTAs per SM the per-leaf kernels are compiled for (register bound: 72
+// registers in FP64, 56 in FP32 at 288 threads)
+template <typename R>
+__host__ __device__ constexpr int w2d_minb(bool)
+{
+  return sizeof(R) == 8 ? 3 : 4;
+}
+
 // Tile copies of the persistent kernels: the barrier is initialised once per
 // CTA and completes once per leaf (phase parity alternates); thread 0 issues.
 template <typename R, int NEQ>
@@ -533,8 +545,8 @@ __host__ __device__ constexpr size_t smem_half()
   return 128 + sizeof(R) * (NEQ * W2D_CELLS + W2D_CELLS + 2 * NEQ * 272);
 }
 
-template <typename R, int NEQ, int SOLVER>
-__global__ void __launch_bounds__(W2D_THREADS) k_half(KArgs a, PhysArgs pa, double dt)
+template <typename R, int NEQ, int SOLVER, bool P>
+__global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_half(KArgs a, PhysArgs pa, double dt)
 {
   uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
   R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
@@ -547,7 +559,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_half(KArgs a, PhysArgs pa, doub
   const bool dmc = pa.cooling == COOL_DMC;
   bar_init_once(bar);
   uint32_t par = 0;
-  for (LeafRange lr = leaf_range(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
+  for (LeafRange lr = leaf_range<P>(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
   const int b = a.leaves[lr.li];
   const R* __restrict__ u = (const R*)a.u + (size_t)b * bs;
   R* __restrict__ up = (R*)a.up + (size_t)b * bs;
@@ -625,8 +637,8 @@ __host__ __device__ constexpr size_t smem_full()
   return 128 + sizeof(R) * (2 * NEQ * W2D_CELLS + 2 * NEQ * 272);
 }
 
-template <typename R, int NEQ, int SOLVER, int LIMITER>
-__global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, double dt)
+template <typename R, int NEQ, int SOLVER, int LIMITER, bool P>
+__global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_full(KArgs a, PhysArgs pa, double dt)
 {
   uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
   R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
@@ -639,7 +651,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_full(KArgs a, PhysArgs pa, doub
   const R* __restrict__ upool = (const R*)a.up;
   bar_init_once(bar);
   uint32_t par = 0;
-  for (LeafRange lr = leaf_range(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
+  for (LeafRange lr = leaf_range<P>(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
   const int li = lr.li;
   const int b = a.leaves[li];
   R* __restrict__ u = (R*)a.u + (size_t)b * bs;
@@ -761,8 +773,8 @@ __host__ __device__ constexpr size_t smem_fill1()
   return 128 + sizeof(R) * NEQ * W2D_CELLS + 64 * sizeof(double);
 }
 
-template <typename R, int NEQ>
-__global__ void __launch_bounds__(W2D_THREADS) k_fill1(KArgs a, PhysArgs pa, int stats)
+template <typename R, int NEQ, bool P>
+__global__ void __launch_bounds__(W2D_THREADS, 4) k_fill1(KArgs a, PhysArgs pa, int stats)
 {
   uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
   R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
@@ -773,7 +785,7 @@ __global__ void __launch_bounds__(W2D_THREADS) k_fill1(KArgs a, PhysArgs pa, int
   R* __restrict__ upool = (R*)a.u;
   bar_init_once(bar);
   uint32_t par = 0;
-  for (LeafRange lr = leaf_range(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
+  for (LeafRange lr = leaf_range<P>(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
   const int li = lr.li;
   const int b = a.leaves[li];
   R* __restrict__ u = upool + (size_t)b * bs;
@@ -828,9 +840,10 @@ __host__ __device__ constexpr size_t smem_calcprim()
 // With jet_interior != 0 (list = the leaves, after the fill of layer 0) it
 // first imposes the jet on the interior of the blocks the list walk named,
 // which the reference does inside boundaryI (src/boundaryI.f90:386-393).
-template <typename R, int NEQ>
-__global__ void __launch_bounds__(W2D_THREADS) k_calcprim(KArgs a, PhysArgs pa, const int* __restrict__ list, int n,
-                                                          int jet_interior)
+template <typename R, int NEQ, bool P>
+__global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_calcprim(KArgs a, PhysArgs pa,
+                                                                         const int* __restrict__ list, int n,
+                                                                         int jet_interior)
 {
   uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
   R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
@@ -840,8 +853,8 @@ __global__ void __launch_bounds__(W2D_THREADS) k_calcprim(KArgs a, PhysArgs pa, 
   const size_t bs = (size_t)NEQ * W2D_CELLS;
   bar_init_once(bar);
   uint32_t par = 0;
-  LeafRange lr = leaf_range(a);
-  if (list != a.leaves) lr = LeafRange{(int)blockIdx.x, n, (int)gridDim.x};
+  LeafRange lr = leaf_range<P>(a);
+  if (P && list != a.leaves) lr = LeafRange{(int)blockIdx.x, n, (int)gridDim.x};
   for (; lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
   const int b = list[lr.li];
   R* __restrict__ u = (R*)a.u + (size_t)b * bs;

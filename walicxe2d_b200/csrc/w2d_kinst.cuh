@@ -36,15 +36,20 @@ static cudaError_t smem_opt_in(K kernel, size_t bytes, bool& done)
   return e;
 }
 
-template <int NEQ, int S>
-static cudaError_t half_t(const KArgs& a, const PhysArgs& pa, double dt, cudaStream_t st)
+template <int NEQ, int S, bool P>
+static cudaError_t half_p(const KArgs& a, const PhysArgs& pa, double dt, cudaStream_t st)
 {
   static bool done = false;
   constexpr size_t sm = smem_half<R, NEQ>();
-  cudaError_t e = smem_opt_in(k_half<R, NEQ, S>, sm, done);
+  cudaError_t e = smem_opt_in(k_half<R, NEQ, S, P>, sm, done);
   if (e != cudaSuccess) return e;
-  k_half<R, NEQ, S><<<launch_grid(a), W2D_THREADS, sm, st>>>(a, pa, dt);
+  k_half<R, NEQ, S, P><<<launch_grid(a), W2D_THREADS, sm, st>>>(a, pa, dt);
   return cudaGetLastError();
+}
+template <int NEQ, int S>
+static cudaError_t half_t(const KArgs& a, const PhysArgs& pa, double dt, cudaStream_t st)
+{
+  return a.grid > 0 ? half_p<NEQ, S, true>(a, pa, dt, st) : half_p<NEQ, S, false>(a, pa, dt, st);
 }
 
 static cudaError_t half(int neq, const KArgs& a, const PhysArgs& pa, double dt, cudaStream_t st)
@@ -57,15 +62,20 @@ static cudaError_t half(int neq, const KArgs& a, const PhysArgs& pa, double dt, 
   return cudaSuccess;
 }
 
-template <int NEQ, int S, int L>
-static cudaError_t full_t(const KArgs& a, const PhysArgs& pa, double dt, cudaStream_t st)
+template <int NEQ, int S, int L, bool P>
+static cudaError_t full_p(const KArgs& a, const PhysArgs& pa, double dt, cudaStream_t st)
 {
   static bool done = false;
   constexpr size_t sm = smem_full<R, NEQ>();
-  cudaError_t e = smem_opt_in(k_full<R, NEQ, S, L>, sm, done);
+  cudaError_t e = smem_opt_in(k_full<R, NEQ, S, L, P>, sm, done);
   if (e != cudaSuccess) return e;
-  k_full<R, NEQ, S, L><<<launch_grid(a), W2D_THREADS, sm, st>>>(a, pa, dt);
+  k_full<R, NEQ, S, L, P><<<launch_grid(a), W2D_THREADS, sm, st>>>(a, pa, dt);
   return cudaGetLastError();
+}
+template <int NEQ, int S, int L>
+static cudaError_t full_t(const KArgs& a, const PhysArgs& pa, double dt, cudaStream_t st)
+{
+  return a.grid > 0 ? full_p<NEQ, S, L, true>(a, pa, dt, st) : full_p<NEQ, S, L, false>(a, pa, dt, st);
 }
 
 static cudaError_t full(int neq, const KArgs& a, const PhysArgs& pa, double dt, cudaStream_t st)
@@ -81,15 +91,20 @@ static cudaError_t full(int neq, const KArgs& a, const PhysArgs& pa, double dt, 
   return cudaSuccess;
 }
 
-template <int NEQ>
-static cudaError_t fill1_t(const KArgs& a, const PhysArgs& pa, int stats, cudaStream_t st)
+template <int NEQ, bool P>
+static cudaError_t fill1_p(const KArgs& a, const PhysArgs& pa, int stats, cudaStream_t st)
 {
   static bool done = false;
   constexpr size_t sm = smem_fill1<R, NEQ>();
-  cudaError_t e = smem_opt_in(k_fill1<R, NEQ>, sm, done);
+  cudaError_t e = smem_opt_in(k_fill1<R, NEQ, P>, sm, done);
   if (e != cudaSuccess) return e;
-  k_fill1<R, NEQ><<<launch_grid(a), W2D_THREADS, sm, st>>>(a, pa, stats);
+  k_fill1<R, NEQ, P><<<launch_grid(a), W2D_THREADS, sm, st>>>(a, pa, stats);
   return cudaGetLastError();
+}
+template <int NEQ>
+static cudaError_t fill1_t(const KArgs& a, const PhysArgs& pa, int stats, cudaStream_t st)
+{
+  return a.grid > 0 ? fill1_p<NEQ, true>(a, pa, stats, st) : fill1_p<NEQ, false>(a, pa, stats, st);
 }
 
 static cudaError_t fill1(int neq, const KArgs& a, const PhysArgs& pa, int stats, cudaStream_t st)
@@ -106,17 +121,23 @@ static cudaError_t fill_only(int neq, const KArgs& a, void* pool, int layers, cu
   return cudaGetLastError();
 }
 
+template <int NEQ, bool P>
+static cudaError_t calcprim_p(const KArgs& a, const PhysArgs& pa, const int* list, int n, int jet_interior,
+                              int grid, cudaStream_t st)
+{
+  static bool done = false;
+  constexpr size_t sm = smem_calcprim<R, NEQ>();
+  cudaError_t e = smem_opt_in(k_calcprim<R, NEQ, P>, sm, done);
+  if (e != cudaSuccess) return e;
+  k_calcprim<R, NEQ, P><<<grid, W2D_THREADS, sm, st>>>(a, pa, list, n, jet_interior);
+  return cudaGetLastError();
+}
 template <int NEQ>
 static cudaError_t calcprim_t(const KArgs& a, const PhysArgs& pa, const int* list, int n, int jet_interior,
                               cudaStream_t st)
 {
-  static bool done = false;
-  constexpr size_t sm = smem_calcprim<R, NEQ>();
-  cudaError_t e = smem_opt_in(k_calcprim<R, NEQ>, sm, done);
-  if (e != cudaSuccess) return e;
-  const int grid = (list == a.leaves && a.grid > 0) ? a.grid : n;
-  k_calcprim<R, NEQ><<<grid, W2D_THREADS, sm, st>>>(a, pa, list, n, jet_interior);
-  return cudaGetLastError();
+  if (list == a.leaves && a.grid > 0) return calcprim_p<NEQ, true>(a, pa, list, n, jet_interior, a.grid, st);
+  return calcprim_p<NEQ, false>(a, pa, list, n, jet_interior, n, st);
 }
 
 static cudaError_t calcprim(int neq, const KArgs& a, const PhysArgs& pa, const int* list, int n,
@@ -154,15 +175,20 @@ static cudaError_t amr(int neq, const KArgs& a, const PhysArgs& pa, const int* o
   return cudaSuccess;
 }
 
-template <int NEQ>
-static cudaError_t cool_t(const KArgs& a, const PhysArgs& pa, double dt_s, cudaStream_t st)
+template <int NEQ, bool P>
+static cudaError_t cool_p(const KArgs& a, const PhysArgs& pa, double dt_s, cudaStream_t st)
 {
   static bool done = false;
   constexpr size_t sm = smem_cool<R, NEQ>();
-  cudaError_t e = smem_opt_in(k_cool<R, NEQ>, sm, done);
+  cudaError_t e = smem_opt_in(k_cool<R, NEQ, P>, sm, done);
   if (e != cudaSuccess) return e;
-  k_cool<R, NEQ><<<launch_grid(a), W2D_THREADS, sm, st>>>(a, pa, dt_s);
+  k_cool<R, NEQ, P><<<launch_grid(a), W2D_THREADS, sm, st>>>(a, pa, dt_s);
   return cudaGetLastError();
+}
+template <int NEQ>
+static cudaError_t cool_t(const KArgs& a, const PhysArgs& pa, double dt_s, cudaStream_t st)
+{
+  return a.grid > 0 ? cool_p<NEQ, true>(a, pa, dt_s, st) : cool_p<NEQ, false>(a, pa, dt_s, st);
 }
 
 static cudaError_t cool(int neq, const KArgs& a, const PhysArgs& pa, double dt_s, cudaStream_t st)

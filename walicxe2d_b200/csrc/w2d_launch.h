@@ -39,8 +39,9 @@ cudaError_t launch_dt(const int* leaves, int n, const double* cfl, const double*
 cudaError_t launch_dt_runs(const int* leaves, const int* loff, int nruns, const double* cfl, const double* dtcool,
                            int use_cool, double courant, double psc, double tsc, double* dt_run, cudaStream_t st);
 
-// out[k] = v[leaves[k]]
-cudaError_t launch_gather_leaf(const int* leaves, int n, const double* v, double* out, cudaStream_t st);
+// out[k] = v[leaves[k]] for k < n (or < *n_dev when n_dev is set)
+cudaError_t launch_gather_leaf(const int* leaves, int n, const int* n_dev, const double* v, double* out,
+                               cudaStream_t st);
 
 struct NNImage;
 // coolingh (FP32 path) through the learned surrogate with the exact routine

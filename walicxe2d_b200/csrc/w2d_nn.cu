@@ -582,7 +582,8 @@ __global__ void __launch_bounds__(256, 4) k_cool_nn(KArgs a, PhysArgs pa, double
   const Phys<float> ph = make_phys<float, -1, -1>(pa);
   uint32_t phase = 0;
   unsigned served = 0;
-  const int64_t ncells = (int64_t)a.nleaf * 320, ntiles = (ncells + 127) / 128;
+  const int nl = a.nleaf_dev ? *a.nleaf_dev : a.nleaf;
+  const int64_t ncells = (int64_t)nl * 320, ntiles = (ncells + 127) / 128;
   for (int64_t t = 2 * (int64_t)blockIdx.x + wg; t < ntiles; t += 2 * (int64_t)gridDim.x) {
     const int64_t c = t * 128 + row;
     const bool valid = c < ncells;
@@ -769,12 +770,12 @@ const NNImage* nn_image_of(const W2dNN* nn) { return nn ? nn->d_img : nullptr; }
 cudaError_t launch_cool_nn(int neq, const KArgs& a, const PhysArgs& pa, double dt_s, const NNImage* img,
                            int* fb_list, int* fb_count, unsigned long long* counts, int nsm, cudaStream_t st)
 {
-  if (a.nleaf == 0) return cudaSuccess;
+  if (a.nleaf == 0 && !a.nleaf_dev) return cudaSuccess;
   const size_t sm = sizeof(NNCoolSmem);
   static bool opted5 = false, opted6 = false;
   cudaError_t e = cudaSuccess;
   const int64_t tiles = ((int64_t)a.nleaf * 320 + 127) / 128;
-  const int grid = (int)std::min<int64_t>((tiles + 1) / 2, 4 * (int64_t)nsm);
+  const int grid = a.nleaf_dev ? 4 * nsm : (int)std::min<int64_t>((tiles + 1) / 2, 4 * (int64_t)nsm);
   if (neq == 5) {
     if (!opted5) e = cudaFuncSetAttribute(k_cool_nn<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
