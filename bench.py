@@ -153,14 +153,15 @@ class ClockSampler:
                 "samples": len(rows), "reasons": sorted(reasons)}
 
 
-def _traffic_per_zone(kernel: str):
-    """DRAM bytes per zone of `kernel` from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    try:
-        with open(path) as f:
-            return json.load(f)[kernel]["dram_bytes_per_zone"]
-    except Exception:
-        return None
+# DRAM bytes (read + write) per zone of one launch, from one ncu capture of
+# the same workload at 3,470 leaves (profiles/traffic_sedov_amr_fp64.md:
+# 90.1 MB per full-step launch of 888,320 zones); traffic grows with the
+# zones a launch processes
+DRAM_BYTES_PER_ZONE = {("full_step", 64): 101.4, ("half_step", 64): 65.5, ("fill_I", 64): 49.2}
+
+
+def _traffic_per_zone(kernel: str, precision: int):
+    return DRAM_BYTES_PER_ZONE.get((kernel, precision))
 
 
 def cpu_baseline(threads: int, target_s: float = 12.0, max_steps: int = 400):
@@ -385,7 +386,7 @@ def run_ours(args, ws, rank, local):
     per_launch_zones = zu / max(nl, 1) if dom in ("half_step", "full_step") else zu / max(nl, 1)
     achieved = bytes_per_zone * per_launch_zones / (tot_ms / nl / 1000.0) / 1e9
     peak, peak_kind = _measured_peaks()
-    tpz = _traffic_per_zone(dom)
+    tpz = _traffic_per_zone(dom, args.precision)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
                 "traffic": (tpz * per_launch_zones) if tpz is not None else None,
