@@ -87,40 +87,79 @@ def _measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML
+    polled every 2 ms from a thread (read-only queries), so that a region of
+    tens of milliseconds still gets many samples; nvidia-smi at 50 ms when
+    NVML cannot be loaded."""
 
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int = 0):
-        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        self.proc = None
         self.gpu = gpu_index
+        self.rows = []          # (time, sm MHz, max MHz, reason bits)
+        self.start = self.stop = None
+        self.thread = None
+        self.proc = None
+        self.source = "nvml"
+
+    def _poll(self):
+        import pynvml
+        while not self._halt:
+            try:
+                sm = pynvml.nvmlDeviceGetClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+                rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.rows.append((time.time(), float(sm), self.max_mhz, int(rs)))
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def __enter__(self):
+        import threading
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "50", "-i", str(self.gpu)], stdout=self.tmp, stderr=subprocess.DEVNULL)
+            import pynvml
+            pynvml.nvmlInit()
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self._halt = False
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
         except Exception:
-            self.proc = None
-        # wait for the first sample so that the timed region is covered
+            self.thread = None
+            self.source = "nvidia-smi"
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            try:
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                     "-lms", "50", "-i", str(self.gpu)], stdout=self.tmp, stderr=subprocess.DEVNULL)
+            except Exception:
+                self.proc = None
         t0 = time.time()
-        while self.proc is not None and time.time() - t0 < 5.0:
-            self.tmp.flush()
-            if os.path.getsize(self.tmp.name) > 0:
-                break
-            time.sleep(0.05)
+        while time.time() - t0 < 2.0 and not self._have_rows():
+            time.sleep(0.01)
         self.start = time.time()
         return self
+
+    def _have_rows(self):
+        if self.thread is not None:
+            return len(self.rows) > 0
+        if self.proc is None:
+            return True
+        self.tmp.flush()
+        return os.path.getsize(self.tmp.name) > 0
 
     def mark_start(self):
         """Samples taken before this call are dropped from the summary."""
         self.start = time.time()
-        self.skip = sum(1 for _ in open(self.tmp.name)) if os.path.exists(self.tmp.name) else 0
 
     def __exit__(self, *a):
+        self.stop = time.time()
+        if self.thread is not None:
+            self._halt = True
+            self.thread.join(timeout=1.0)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -128,29 +167,37 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
-    def summary(self):
+    def _smi_rows(self):
         self.tmp.flush()
+        out = []
         try:
-            rows = [r.split(",") for r in open(self.tmp.name).read().strip().splitlines() if r.strip()]
+            for r in open(self.tmp.name).read().strip().splitlines():
+                f = r.split(",")
+                bits = 0
+                for k, (_, b) in enumerate(self.REASONS[:4]):
+                    if len(f) > 5 + k and "Active" in f[5 + k] and "Not" not in f[5 + k]:
+                        bits |= b
+                try:
+                    out.append((None, float(f[1]), float(f[2]), bits))
+                except ValueError:
+                    pass
         except Exception:
-            rows = []
+            pass
         os.unlink(self.tmp.name)
-        skip = getattr(self, "skip", 0)
-        if len(rows) > skip + 1:
-            rows = rows[max(skip - 1, 0):]   # keep the sample just before the region too
+        return out
+
+    def summary(self):
+        if self.thread is not None:
+            rows = [r for r in self.rows if self.start - 0.01 <= r[0] <= (self.stop or time.time()) + 0.01]
+        elif self.proc is not None:
+            rows = self._smi_rows()
+        else:
+            rows = []
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in rows:
-            for k, n in enumerate(names):
-                if len(r) > 5 + k and "Active" in r[5 + k] and "Not" not in r[5 + k]:
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None,
-                "samples": len(rows), "reasons": sorted(reasons)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "source": self.source}
+        reasons = sorted({n for r in rows for n, b in self.REASONS if r[3] & b})
+        return {"sm_mhz": statistics.median(r[1] for r in rows), "sm_max_mhz": max(r[2] for r in rows),
+                "samples": len(rows), "reasons": reasons, "source": self.source}
 
 
 # DRAM bytes (read + write) per zone of one launch, from one ncu capture of
@@ -192,7 +239,17 @@ def cpu_baseline(threads: int, target_s: float = 12.0, max_steps: int = 400):
 ENS_RUNS = 256
 ENS_CAP = 6000           # pool slots per run (the runs use a few hundred to a few thousand)
 NN_SAMPLES = 10_000_000
-NN_EPOCHS = 60
+NN_EPOCHS = 100
+
+
+def _finish_tuning(runner, ctx, at_least: int):
+    """Untimed steps until the autotuner has timed every launch shape (and
+    at least `at_least` steps)."""
+    n = 0
+    while n < at_least or (ctx.tuning().get("steps_left", 0) > 0 and n < 64):
+        runner.run(1)
+        n += 1
+    return n
 
 
 def batched_measure(args, plain_value: float):
@@ -224,8 +281,10 @@ def batched_measure(args, plain_value: float):
         if use_nn:
             ctx.set_surrogate(nn)
         ctx.set_graphs(True)
+        ens.run(pre)
         ctx.autotune(2)            # 2 steps per launch shape, inside the untimed steps
-        ens.run(pre + warm)
+        _finish_tuning(ens, ctx, 0)
+        ens.run(warm)
         ctx.sync()
         st0 = ens.status(-1)
         c0 = ctx.surrogate_counts() if use_nn else (0, 0)
@@ -271,15 +330,79 @@ def batched_measure(args, plain_value: float):
         "ms_per_step": out["fp32nn"]["ms_per_step"], "steps": steps,
         "workload": f"{nruns} independent Sedov-with-coolingh runs (roots k x k, k in 2..16; 3..6 levels; "
                     "n log-U[0.1,10] cm^-3, E log-U[1e50,1e51] erg; 40 pc box), one device context, "
-                    f"{pre}+{warm} untimed steps, L2 flushed before every timed step",
+                    f"{pre} untimed steps, then the autotuner's steps and {warm} more, L2 flushed before "
+                    "every timed step",
         "leaves": out["fp32nn"]["leaves"], "ratio_to_plain_fp64_value": v / plain_value,
         "fp32nn": out["fp32nn"], "fp64_exact_same_runs": out["fp64"],
         "density_l1_vs_fp64": {"max": float(l1.max()), "median": float(np.median(l1)),
                                "runs_over_1e-3": int((l1 > 1e-3).sum()), "runs_same_tree": same,
                                "note": "interior cells of the leaves both runs share, after the same step count"},
         "surrogate": {"samples": NN_SAMPLES, "epochs": NN_EPOCHS, "samples_s": t1 - t0, "train_s": t2 - t1,
-                      "final_batch_mse": loss, "judged_by_exact_routine": judge},
-    }
+                      "final_batch_mse": loss, "judged_by_exact_routine": judge,
+                      "serve_tolerance": "predicted |dT/T| and |dp/p| <= 0.2% (exact routine otherwise)"},
+    }, nn
+
+
+def _dmc_table():
+    import numpy as np
+    rows = np.loadtxt(os.path.join(ROOT, "tests", "golden", "coolingDMC.tab"))
+    return rows[:, 0], rows[:, 1]
+
+
+def variants_measure(args, nn_h):
+    """The remnant with coolingh (10x10 roots, 6 levels) and the DMC jet
+    (32x8 roots, 7 levels): the plain FP64 path against the FP32 path with
+    the learned cooling (coolingh network from the batched section; a
+    coolingdmc network trained here), same step count, density L1 on the
+    leaves both runs share."""
+    import numpy as np
+
+    from walicxe2d_b200.api import Simulation, Surrogate
+    from walicxe2d_b200.params import config
+    log_t, neg_l = _dmc_table()
+    out = {}
+    for name, cfg, steps in (("snr", "snr", 30), ("jet_dmc", "jet_dmc", 30)):
+        p, ic = config(cfg)
+        nn = nn_h
+        if cfg == "jet_dmc":
+            nn = Surrogate(5)
+            nn.samples_dmc(2_000_000, log_t, neg_l, p, seed=20261205)
+            nn.train(30, batch=8192, lr=2e-3, lr_end=2e-5)
+        res, st = {}, {}
+        for prec in (64, 32):
+            q = p.copy()
+            q.precision = prec
+            sim = Simulation(q, ic)
+            if cfg == "jet_dmc":
+                sim.set_cooltab(log_t, neg_l)
+            if prec == 32:
+                sim.ctx.set_surrogate(nn)
+            sim.run(5)
+            sim.ctx.sync()
+            s0 = sim.status()
+            sim.ctx.event_record(0)
+            sim.run(steps)
+            sim.ctx.event_record(1)
+            ms = sim.ctx.event_elapsed(0, 1)
+            s1 = sim.status()
+            r = {"value": (s1["zone_updates"] - s0["zone_updates"]) / (ms / 1000.0), "ms_per_step": ms / steps,
+                 "leaves": s1["nleaf"]}
+            if prec == 32:
+                sv, ex = sim.ctx.surrogate_counts()
+                r["cells_served_by_network"] = sv / max(sv + ex, 1)
+            res["fp64" if prec == 64 else "fp32nn"] = r
+            lp, lf, icd, ib = sim.tree()
+            ids = np.nonzero(lf)[0].astype(np.int32)
+            st[prec] = (ids, sim.ctx.get_blocks(ids)[:, 0, 2:18, 2:18])
+            sim.close()
+        common, xa, xb = np.intersect1d(st[64][0], st[32][0], return_indices=True)
+        a, b = st[64][1][xa], st[32][1][xb]
+        res["density_l1_vs_fp64"] = float(np.abs(b - a).sum() / max(np.abs(a).sum(), 1e-300))
+        res["same_tree"] = bool(len(common) == len(st[64][0]) == len(st[32][0]))
+        res["steps"] = steps
+        res["ratio"] = res["fp32nn"]["value"] / res["fp64"]["value"]
+        out[name] = res
+    return out
 
 
 def run_reference(args, ws, rank):
@@ -338,7 +461,10 @@ def run_ours(args, ws, rank, local):
     p.precision = args.precision
     sim = Simulation(p, ic)
     ctx = sim.ctx
-    sim.run(args.pre_steps)
+    ctx.set_graphs(True)        # each step as two CUDA graphs over persistent launches
+    sim.run(max(args.pre_steps - 16, 0))
+    ctx.autotune(2)             # launch shapes chosen on the developed blast, in untimed steps
+    _finish_tuning(sim, ctx, min(args.pre_steps, 16))
 
     def barrier():
         if dist:
@@ -353,7 +479,6 @@ def run_ours(args, ws, rank, local):
     ctx.sync()
     st0 = sim.status()
     n0 = ctx.launch_count()
-    ctx.profile(True)
     step_ms = []
     clk.mark_start()
     sim.phase_ms(reset=True)
@@ -367,12 +492,22 @@ def run_ours(args, ws, rank, local):
     phases = {k: v / args.steps for k, v in sim.phase_ms().items()}
     time.sleep(0.06)                       # one more clock sample after the region
     clk.__exit__()
-    prof = ctx.profile_read()
-    ctx.profile(False)
     launches = ctx.launch_count() - n0
     st1 = sim.status()
     barrier()
     zu = st1["zone_updates"] - st0["zone_updates"]
+    # per-kernel times: more steps with an event pair around every launch
+    # (the graphs are replaced by the same launches while profiling)
+    nprof = min(args.steps, 30)
+    ctx.profile(True)
+    sp0 = sim.status()
+    for _ in range(nprof):
+        ctx.flush_l2()
+        sim.run(1)
+    ctx.sync()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    zu_prof = sim.status()["zone_updates"] - sp0["zone_updates"]
     t_ms = sum(step_ms)
     t_all, zu_all = aggregate(t_ms, float(zu), dist[1] if dist else None, "cuda")
     value = zu_all / (t_all / 1000.0)
@@ -383,7 +518,7 @@ def run_ours(args, ws, rank, local):
     nl, tot_ms = prof[dom]
     elem = 8 if args.precision == 64 else 4
     bytes_per_zone = 2.5625 * p.neq * elem          # halo tile read + block write
-    per_launch_zones = zu / max(nl, 1) if dom in ("half_step", "full_step") else zu / max(nl, 1)
+    per_launch_zones = zu_prof / max(nl, 1)
     achieved = bytes_per_zone * per_launch_zones / (tot_ms / nl / 1000.0) / 1e9
     peak, peak_kind = _measured_peaks()
     tpz = _traffic_per_zone(dom, args.precision)
@@ -419,9 +554,11 @@ def run_ours(args, ws, rank, local):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(os.cpu_count() or 1)
-    batched = None
+    batched = variants = None
     if rank == 0 and ws == 1 and not args.no_batched and args.precision == 64:
-        batched = batched_measure(args, value)
+        batched, nn_h = batched_measure(args, value)
+        if not args.no_variants:
+            variants = variants_measure(args, nn_h)
 
     if rank == 0:
         line = {
@@ -433,7 +570,8 @@ def run_ours(args, ws, rank, local):
                                    "HLLC+minmod, outflow, plain path",
                        "leaves_at_start": st0["nleaf"], "leaves_at_end": st1["nleaf"],
                        "pre_steps": args.pre_steps, "l2": "flushed (256 MB write) before every timed step",
-                       "parallelism": f"replicas x{ws}"},
+                       "parallelism": f"replicas x{ws}",
+                       "cuda_graphs": True, "launch_shapes": ctx.tuning()},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -441,6 +579,7 @@ def run_ours(args, ws, rank, local):
             "gpu_launches": int(launches),
             "host_phase_ms_per_step": phases,
             "batched": batched,
+            "configs_3_4": variants,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -459,6 +598,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched FP32 + learned-cooling ensemble measurement")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the remnant and DMC-jet comparisons of FP64 and FP32 + learned cooling")
     ap.add_argument("--batched-runs", type=int, default=ENS_RUNS,
                     help="runs in the batched ensemble (fewer for profiling)")
     ap.add_argument("--pre-steps", type=int, default=PRE_STEPS,

@@ -295,9 +295,10 @@ int w2d_ens_phase_ms(W2dEns* ens, double* ms, int reset);
  * kernel; w2d_tuning reports, per kernel (half, full, fill I, cooling,
  * statistics), {shape index, CTAs per SM, order} in shape[3k..3k+2], the
  * chosen shape's mean ms and the tuning steps left.  w2d_set_graphs(ctx, 1)
- * makes an ensemble context replay each step's two launch sequences as
- * CUDA graphs (persistent shapes only; the leaf count is read on the
- * device). */
+ * makes an ensemble context, or the context of a single run without the
+ * jet (w2d_sim_ctx), replay each step's two launch sequences as CUDA
+ * graphs (persistent shapes only; leaf count and dt are read on the
+ * device, dt reaches the host with the step's synchronization). */
 int w2d_autotune(W2dCtx* ctx, int reps);
 int w2d_tuning(W2dCtx* ctx, int32_t* shape, double* ms, int* tuning_left);
 int w2d_set_graphs(W2dCtx* ctx, int on);
@@ -319,6 +320,14 @@ int w2d_nn_destroy(W2dNN* nn);
  * 1e4] cm^-3, [1e2, 1e8] K, [1e-2, 1e2] yr; neutral fraction uniform over
  * [1e-4, 1]) and labelled by the exact routine, kept on the device */
 int w2d_nn_samples(W2dNN* nn, int64_t n, uint64_t seed);
+/* the same for coolingdmc (src/coolingdmc.f90:30-40): T log-uniform over
+ * [1e4, 1e8] K, labels from the 41-row table as w2d_set_cooltab takes it
+ * and the context's cv, tempsc and psc; the network then serves coolingdmc
+ * contexts (it learns the rate per unit density, a function of T) */
+int w2d_nn_samples_dmc(W2dNN* nn, int64_t n, uint64_t seed, const double* log_t, const double* neg_log_l,
+                       int rows, double cv, double tempsc, double psc);
+/* W2D_COOLINGH or W2D_COOLINGDMC: the routine the samples came from */
+int w2d_nn_kind(W2dNN* nn);
 /* Adam over the samples in batches of `batch` (multiple of 128), learning
  * rate cosine-decayed from lr to lr_end; *last_loss: mean squared error of
  * the last batch */
@@ -331,13 +340,20 @@ int w2d_nn_forward(W2dNN* nn, const float* feat, int n, float* out);   /* out [2
  * the surrogate serves (inputs in range, predicted |dT/T| <= 10%), [1]
  * median, [2] 99th percentile and [3] maximum relative error of T and [4]
  * mean and [5] maximum error of the neutral fraction over those, [6] share
- * whose exact |dT/T| <= 10%.  stats holds 8 doubles. */
+ * whose exact |dT/T| <= 10%.  stats holds 8 doubles.  coolingh networks
+ * only: W2D_ERR_STATE for a coolingdmc network. */
 int w2d_nn_judge(W2dNN* nn, int64_t n, uint64_t seed, double* stats);
 /* coolingh of an FP32 context (or ensemble context) through the network:
  * cells whose inputs lie outside the training ranges or whose predicted
- * |dT/T| exceeds 10% take the exact routine.  The network must outlive its
+ * relative change exceeds the serve tolerance (below) take the exact
+ * routine.  The network must outlive its
  * use by the context; nn = NULL detaches it. */
 int w2d_set_surrogate(W2dCtx* ctx, W2dNN* nn);
+/* largest predicted relative change of T and of the thermal pressure that
+ * the network serves, in (0, 0.1] (default 0.002: cells that change faster
+ * are few -- on Sedov-with-coolingh runs the share served falls from 81.4%
+ * at 0.01 to 80.8% -- and the exact routine keeps their evolution exact) */
+int w2d_set_surrogate_tol(W2dCtx* ctx, double tol);
 /* cells served by the network and by the exact routine since creation */
 int w2d_surrogate_counts(W2dCtx* ctx, int64_t* served, int64_t* exact);
 

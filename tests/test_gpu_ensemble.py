@@ -148,3 +148,25 @@ def test_autotuned_single_run_against_oracle(oracle_lib):
     ids = o.leaves()
     dmax, l1, n = compare_blocks(s.ctx.get_blocks(ids), o.u[ids], noncorner_mask())
     assert n == 0, (dmax, l1)
+
+
+@pytest.mark.parametrize("name,amr", [("sedov_amr_small", True), ("sedov64", False)])
+def test_single_run_step_graphs_against_oracle(oracle_lib, name, amr):
+    """A single run stepping through its two step graphs (dt and the leaf
+    count read on the device, persistent tuned shapes) stays exact against
+    the oracle, with and without AMR."""
+    from walicxe2d_b200.api import Simulation
+    p, ic = config(name)
+    o = oracle_lib.Oracle(p, ic, threads=8)
+    o.startup()
+    s = Simulation(p, ic)
+    s.ctx.set_graphs(True)
+    s.ctx.autotune(1)
+    for _ in range(20):
+        dto = o.run(1, amr=amr)
+        s.run(1)
+        assert s.status()["dt"] == dto
+    assert s.status()["time"] == o.time
+    ids = o.leaves()
+    dmax, l1, n = compare_blocks(s.ctx.get_blocks(ids), o.u[ids], noncorner_mask())
+    assert n == 0, (dmax, l1)

@@ -98,6 +98,32 @@ def test_surrogate_in_fp32_remnant_against_fp64_oracle(oracle_lib, trained):
         assert l1 <= 1e-3, l1
 
 
+def test_surrogate_tiny_tolerance_follows_the_exact_fp32_run(trained):
+    """With a serve tolerance of 1e-6 the surrogate path leaves nearly every
+    cell to the exact routine and so follows the exact FP32 run (same tree;
+    density L1 <= 1e-6 from the few cells whose predicted change is below
+    1e-6)."""
+    from walicxe2d_b200.api import Simulation
+    from walicxe2d_b200.params import config
+    p, ic = config("snr_small")
+    p.precision = 32
+    out = {}
+    for tol in (None, 1e-6):
+        s = Simulation(p, ic)
+        if tol is not None:
+            s.ctx.set_surrogate(trained)
+            s.ctx.set_surrogate_tol(tol)
+        s.run(30)
+        ids = np.nonzero(s.tree()[1])[0]
+        out[tol] = (ids, s.ctx.get_blocks(ids)[:, 0, 2:18, 2:18])
+        s.close()
+    assert np.array_equal(out[None][0], out[1e-6][0])
+    a, b = out[None][1], out[1e-6][1]
+    l1 = float(np.abs(b - a).sum() / np.abs(a).sum())
+    print("remnant density L1, tolerance 1e-6 against the exact FP32 run:", l1)
+    assert l1 <= 1e-6, l1
+
+
 def test_surrogate_gain_over_exact_cooling(trained):
     """What the trained network gains: the same FP32 ensemble step with and
     without it (cooling kernels' device time), and the share it serves."""
@@ -125,3 +151,96 @@ def test_surrogate_gain_over_exact_cooling(trained):
           f"served {sv / (sv + ex):.2f}")
     assert sv / (sv + ex) > 0.5
     assert gain > 1.0, gain
+
+
+def test_dmc_surrogate_in_fp32_blast_against_fp64_oracle(oracle_lib):
+    """The coolingdmc mode: samples labelled with the DMC table; the FP32
+    64x64 blast with DMC cooling and the network against the FP64 oracle
+    (density L1 <= 1e-3), the exact FP32 path beside it."""
+    import os
+    from walicxe2d_b200.api import Simulation, Surrogate
+    from walicxe2d_b200.params import COOLINGDMC, config, scalings
+    rows = np.loadtxt(os.path.join(os.path.dirname(__file__), "golden", "coolingDMC.tab"))
+    p, ic = config("sedov64")
+    p.cooling = COOLINGDMC
+    sc = scalings(3.0e17, p.xmax, p.cv)
+    p.tempsc, p.psc, p.tsc, p.rsc = sc["tempsc"], sc["psc"], sc["tsc"], sc["rsc"]
+    nn = Surrogate(3)
+    nn.samples_dmc(4_000_000, rows[:, 0], rows[:, 1], p, seed=11)
+    assert nn.L.w2d_nn_kind(nn.h) == 2
+    nn.train(60, batch=8192, lr=2e-3, lr_end=2e-5)
+    o = oracle_lib.Oracle(p, ic, threads=8)
+    o.set_cooltab(rows[:, 0], rows[:, 1])
+    o.startup()
+    l1 = {}
+    for use in (False, True):
+        p32 = p.copy()
+        p32.precision = 32
+        s = Simulation(p32, ic)
+        s.set_cooltab(rows[:, 0], rows[:, 1])
+        if use:
+            s.ctx.set_surrogate(nn)
+        s.run(60)
+        if use:
+            served, exact = s.ctx.surrogate_counts()
+            assert served > 0, (served, exact)
+        ids = np.nonzero(s.tree()[1])[0]
+        l1[use] = s.ctx.get_blocks(ids)[:, 0, 2:18, 2:18]
+    o.run(60, amr=False)
+    ids = o.leaves()
+    ro = o.u[ids, 0, 2:18, 2:18]
+    e = {k: float(np.abs(v - ro).sum() / np.abs(ro).sum()) for k, v in l1.items()}
+    print("DMC blast density L1: FP32", e[False], "FP32 + network", e[True])
+    assert e[True] <= 1e-3, e
+
+
+def test_dmc_surrogate_keeps_the_jet():
+    """The jet with coolingdmc through the network: boundaryI's impose_jet
+    on the interiors still precedes cooling.  With a serve tolerance of 1e-6
+    (nearly every cooling cell takes the exact routine) the run equals the
+    exact FP32 run to rounding; with the default tolerance it runs on and
+    the network serves cells."""
+    import os
+    from walicxe2d_b200.api import Simulation, Surrogate
+    from walicxe2d_b200.params import config
+    rows = np.loadtxt(os.path.join(os.path.dirname(__file__), "golden", "coolingDMC.tab"))
+    p, ic = config("jet_small_dmc")
+    nn = Surrogate(4)
+    nn.samples_dmc(1_000_000, rows[:, 0], rows[:, 1], p, seed=13)
+    nn.train(20, batch=8192, lr=2e-3, lr_end=2e-5)
+    rho, served = {}, {}
+    for tol in (None, 1e-6, 0.01):
+        p32 = p.copy()
+        p32.precision = 32
+        s = Simulation(p32, ic)
+        s.set_cooltab(rows[:, 0], rows[:, 1])
+        if tol is not None:
+            s.ctx.set_surrogate(nn)
+            s.ctx.set_surrogate_tol(tol)
+        s.run(60)
+        if tol is not None:
+            served[tol] = s.ctx.surrogate_counts()
+        lf = s.tree()[1]
+        ids = np.nonzero(lf)[0]
+        rho[tol] = (ids, s.ctx.get_blocks(ids)[:, 0, 2:18, 2:18])
+        s.close()
+
+    def l1(a, b):
+        assert np.array_equal(a[0], b[0]), "different trees"
+        return float(np.abs(b[1] - a[1]).sum() / np.abs(a[1]).sum())
+
+    e_tight, e_def = l1(rho[None], rho[1e-6]), l1(rho[None], rho[0.01])
+    print("jet DMC density L1 against the exact FP32 run: tol 1e-6", e_tight, "tol 0.01", e_def,
+          "served/exact", served)
+    assert e_tight <= 1e-6, e_tight
+    assert served[0.01][0] > 0, served
+
+
+def test_surrogate_refuses_the_wrong_cooling(trained):
+    from walicxe2d_b200.api import Simulation
+    from walicxe2d_b200.params import config
+    p, ic = config("jet_small_dmc")
+    p.precision = 32
+    s = Simulation(p, ic)
+    with pytest.raises(Exception):
+        s.ctx.set_surrogate(trained)      # a coolingh network on a coolingdmc run

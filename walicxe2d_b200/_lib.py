@@ -72,6 +72,8 @@ SIGNATURES = {
     "w2d_nn_create": (_I, [C.c_uint64, C.POINTER(_vp)]),
     "w2d_nn_destroy": (_I, [_vp]),
     "w2d_nn_samples": (_I, [_vp, C.c_int64, C.c_uint64]),
+    "w2d_nn_samples_dmc": (_I, [_vp, C.c_int64, C.c_uint64, _PD, _PD, _I, _D, _D, _D]),
+    "w2d_nn_kind": (_I, [_vp]),
     "w2d_nn_train": (_I, [_vp, _I, _I, C.c_float, C.c_float, C.POINTER(C.c_float)]),
     "w2d_nn_params": (_I, [_vp, C.POINTER(C.c_float), _I]),
     "w2d_nn_grad": (_I, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float), _I, C.POINTER(C.c_float),
@@ -82,6 +84,7 @@ SIGNATURES = {
     "w2d_tuning": (_I, [_vp, _PI32, _PD, C.POINTER(_I)]),
     "w2d_set_graphs": (_I, [_vp, _I]),
     "w2d_set_surrogate": (_I, [_vp, _vp]),
+    "w2d_set_surrogate_tol": (_I, [_vp, _D]),
     "w2d_surrogate_counts": (_I, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
 }
 

@@ -201,6 +201,9 @@ class Context:
         self._check(self.L.w2d_set_surrogate(self.h, nn.h if nn is not None else None), "w2d_set_surrogate")
         self._nn = nn
 
+    def set_surrogate_tol(self, tol: float):
+        self._check(self.L.w2d_set_surrogate_tol(self.h, tol), "w2d_set_surrogate_tol")
+
     def surrogate_counts(self) -> tuple[int, int]:
         a, b = C.c_int64(), C.c_int64()
         self._check(self.L.w2d_surrogate_counts(self.h, C.byref(a), C.byref(b)), "w2d_surrogate_counts")
@@ -412,6 +415,14 @@ class Surrogate:
 
     def samples(self, n: int, seed: int = 20261203):
         self._check(self.L.w2d_nn_samples(self.h, n, seed), "w2d_nn_samples")
+
+    def samples_dmc(self, n: int, log_t, neg_log_l, p, seed: int = 20261203):
+        """Training samples of coolingdmc with the DMC table and the
+        scalings (cv, tempsc, psc) of the parameters p."""
+        a = np.ascontiguousarray(log_t, np.float64)
+        b = np.ascontiguousarray(neg_log_l, np.float64)
+        self._check(self.L.w2d_nn_samples_dmc(self.h, n, seed, _pd(a), _pd(b), a.size, p.cv, p.tempsc, p.psc),
+                    "w2d_nn_samples_dmc")
 
     def train(self, epochs: int, batch: int = 8192, lr: float = 2e-3, lr_end: float = 2e-5) -> float:
         loss = C.c_float()

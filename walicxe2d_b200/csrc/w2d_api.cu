@@ -203,6 +203,9 @@ KArgs kargs(W2dCtx* c, const int2* fd)
     a.runs = c->d_runs;
     a.dt_run = c->d_dt_run;
     a.nleaf_dev = c->d_nleaf;
+  } else if (c->want_graphs && !a.jet) {   // a single run's step graphs: count and dt on the device
+    a.nleaf_dev = c->d_nleaf;
+    a.dt_dev = c->d_dt;
   }
   return a;
 }
@@ -436,7 +439,8 @@ int ensure_fb(W2dCtx* c, bool* moved)
   return W2D_OK;
 }
 
-// coolingh through the surrogate, the exact routine on the cells it does
+// coolingh or coolingdmc through the surrogate (after impose_jet on the
+// interiors), the exact routine on the cells it does
 // not serve, then the primitives and statistics of every leaf
 int cool_surrogate(W2dCtx* c, const KArgs& a1, const PhysArgs& pa, double dts)
 {
@@ -444,15 +448,23 @@ int cool_surrogate(W2dCtx* c, const KArgs& a1, const PhysArgs& pa, double dts)
     int rc0 = ensure_fb(c, nullptr);
     if (rc0) return rc0;
   }
+  int rc;
+  if (a1.jet) {   // impose_jet of boundaryI on the interiors, before cooling (the exact kernel does it in its tile)
+    if ((rc = launch(c, "jet_interior", [&] { return c->L->jet_only(c->neq, a1, c->d_u, c->st); }))) return rc;
+  }
   CK(cudaMemsetAsync(c->d_fb_count, 0, sizeof(int), c->st));
-  int rc = launch(c, "cooling_nn", [&] {
-    return launch_cool_nn(c->neq, a1, pa, dts, c->nn_img, c->d_fb, c->d_fb_count, c->d_nn_counts, c->nsm, c->st);
+  rc = launch(c, "cooling_nn", [&] {
+    return launch_cool_nn(c->neq, a1, pa, dts, c->nn_img, c->d_fb, c->d_fb_count, c->d_nn_counts, c->nsm,
+                          c->nn_tol, c->st);
   });
   if (rc) return rc;
   KArgs as = a1;
   apply_shape(c, as, TK_STATS);
+  // coolingdmc: the cooling kernels stored the primitives as the exact
+  // routine does; the statistics read them
+  const int mode = c->p.cooling == W2D_COOLINGDMC ? 2 : 0;
   return launch_tk(c, TK_STATS, "calcprim",
-                   [&] { return c->L->calcprim(c->neq, as, pa, c->d_leaves, c->nleaf, 0, c->st); });
+                   [&] { return c->L->calcprim(c->neq, as, pa, c->d_leaves, c->nleaf, mode, c->st); });
 }
 
 int tstep_ready(W2dCtx* c, bool need_bounds = true)
@@ -485,14 +497,16 @@ int ctx_dt_launch(W2dCtx* c)
 {
   if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
   const int nl = c->nleaf;
+  const bool dev = c->want_graphs && c->p.otherb == W2D_USERBC_NONE;   // count on the device, fixed grid
   int rc = launch(c, "timestep", [&] {
-    return launch_dt(c->d_leaves, nl, c->d_cfl, c->d_dtcool, c->p.cooling == W2D_COOLINGDMC, c->p.cfl,
-                     c->p.psc, c->p.tsc, c->d_dtwork, c->d_dtcount, c->d_dt, c->st);
+    return launch_dt(c->d_leaves, nl, dev ? c->d_nleaf : nullptr, dev ? 2 * c->nsm : 0, c->d_cfl, c->d_dtcool,
+                     c->p.cooling == W2D_COOLINGDMC, c->p.cfl, c->p.psc, c->p.tsc, c->d_dtwork, c->d_dtcount,
+                     c->d_dt, c->st);
   });
   if (rc) return rc;
   CK(cudaMemcpyAsync(c->h_small, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CK(cudaMemcpyAsync(c->h_err, c->d_err, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
-  CK(cudaEventRecord(c->ev_dt, c->st));
+  if (!c->capturing) CK(cudaEventRecord(c->ev_dt, c->st));
   return W2D_OK;
 }
 
@@ -541,7 +555,7 @@ int ctx_tstep_rest(W2dCtx* c, double time, double dt)
   }
   if (c->p.cooling != W2D_ADIABATIC) {
     const double dts = dt * c->p.tsc;
-    if (c->nn_img && c->p.cooling == W2D_COOLINGH) return cool_surrogate(c, a1, pa, dts);
+    if (c->nn_img) return cool_surrogate(c, a1, pa, dts);
     KArgs ac = a1;
     apply_shape(c, ac, TK_COOL);
     if ((rc = launch_tk(c, TK_COOL, "cooling", [&] { return c->L->cool(c->neq, ac, pa, dts, c->st); }))) return rc;
@@ -752,6 +766,8 @@ int w2d_set_topology(W2dCtx* c, const int32_t* lp, int ld_lp, const int32_t* lea
                      cudaMemcpyHostToDevice, c->st));
   const size_t nl = c->leaves.size();
   c->nleaf = (int)nl;
+  c->h_nleaf[0] = (int)nl;   // the device copy of the count (step graphs)
+  CK(cudaMemcpyAsync(c->d_nleaf, c->h_nleaf, sizeof(int), cudaMemcpyHostToDevice, c->st));
   if (nl > 0) {
     memcpy(c->h_leaflist, c->leaves.data(), sizeof(int) * nl);
     CK(cudaMemcpyAsync(c->d_leaves, c->h_leaflist, sizeof(int) * nl, cudaMemcpyHostToDevice, c->st));
@@ -1280,9 +1296,20 @@ int w2d_set_surrogate(W2dCtx* c, W2dNN* nn)
     c->nn_img = nullptr;
     return W2D_OK;
   }
-  if (c->p.precision != 32 || c->p.cooling != W2D_COOLINGH)
-    return set_error(c, W2D_ERR_ARG, 0, 0, 0, "the surrogate serves coolingh of the FP32 path");
+  if (c->p.precision != 32 || c->p.cooling == W2D_ADIABATIC || w2d_nn_kind(nn) != c->p.cooling)
+    return set_error(c, W2D_ERR_ARG, 0, 0, 0, "the surrogate serves the cooling routine it was trained on, FP32 path");
   c->nn_img = nn_image_of(nn);
+  return W2D_OK;
+}
+
+int w2d_set_surrogate_tol(W2dCtx* c, double tol)
+{
+  if (!c || !(tol > 0.0) || tol > 0.1) return W2D_ERR_ARG;
+  c->nn_tol = (float)tol;
+  if (c->gx_rest) {   // the tolerance is an argument of a captured launch
+    cudaGraphExecDestroy(c->gx_rest);
+    c->gx_rest = nullptr;
+  }
   return W2D_OK;
 }
 
@@ -1343,16 +1370,22 @@ int capture(W2dCtx* c, cudaGraphExec_t* gx, int64_t* nkernels, F body)
   return W2D_OK;
 }
 
-bool graphs_now(const W2dCtx* c) { return c->want_graphs && !c->prof && c->tune_left == 0 && c->nruns > 0; }
+bool graphs_now(const W2dCtx* c)
+{
+  return c->want_graphs && !c->prof && c->tune_left == 0 && c->p.otherb == W2D_USERBC_NONE;
+}
 
 }  // namespace
 
-// first part of an ensemble step: dt of every run (and its copy to the
-// host), the half step
-int ctx_ens_first(W2dCtx* c)
+bool ctx_device_dt(W2dCtx* c) { return c->want_graphs && c->p.otherb == W2D_USERBC_NONE; }
+double ctx_last_dt(W2dCtx* c) { return c->h_small[0]; }
+
+// first part of a step: dt (of every run of an ensemble) and its copy to
+// the host, the half step
+int ctx_step_first(W2dCtx* c)
 {
   auto body = [&] {
-    int rc = ctx_ens_dt_launch(c);
+    int rc = c->nruns > 0 ? ctx_ens_dt_launch(c) : ctx_dt_launch(c);
     return rc ? rc : ctx_half_step(c);
   };
   if (!graphs_now(c)) return body();
@@ -1365,8 +1398,8 @@ int ctx_ens_first(W2dCtx* c)
   return W2D_OK;
 }
 
-// the rest of the ensemble step: full step, boundaryI, cooling, statistics
-int ctx_ens_rest(W2dCtx* c)
+// the rest of the step: full step, boundaryI, cooling, statistics
+int ctx_step_rest(W2dCtx* c)
 {
   auto body = [&] { return ctx_tstep_rest(c, 0.0, 0.0); };
   if (!graphs_now(c)) return body();

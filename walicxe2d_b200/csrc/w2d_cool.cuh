@@ -132,7 +132,8 @@ __global__ void __launch_bounds__(W2D_THREADS, 2) k_cool(KArgs a, PhysArgs pa, d
   R* __restrict__ u = (R*)a.u + (size_t)b * bs;
   R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;
   if (tid == 0) tile_issue<R, NEQ>(&st[0][0][0], u, bar);
-  dt_s = a.run_of ? a.dt_run[a.run_of[b]] * a.tsc : dt_arg;   // dt*tsc of the block's run
+  // dt*tsc of the block's run, of the device dt, or the argument
+  dt_s = a.run_of ? a.dt_run[a.run_of[b]] * a.tsc : (a.dt_dev ? *a.dt_dev * a.tsc : dt_arg);
   if (!wait_tiles_p(bar, a.err, b, par)) return;
   if (a.jet && a.jetblk[lr.li]) {   // impose_jet of boundaryI, before cooling
     jet_interior_fn<R, NEQ>(st, a, b, u);

@@ -47,6 +47,7 @@ struct W2dCtx {
   // learned coolingh surrogate (FP32 path): weights of the attached
   // network, the list of cells it leaves to the exact routine, counters
   const w2d::NNImage* nn_img = nullptr;
+  float nn_tol = 0.002f;   // largest predicted relative change the network serves
   int* d_fb = nullptr;
   int64_t fb_cap = 0;
   int* d_fb_count = nullptr;

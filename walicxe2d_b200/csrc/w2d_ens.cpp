@@ -325,10 +325,10 @@ int w2d_ens_run(W2dEns* e, int nsteps)
     for (int r = 0; r < nr; ++r) any = any || e->dirty[r];
     if (any && (rc = push_leaves(e))) return rc;
     const double t1 = now_ms();
-    if ((rc = ctx_ens_first(e->ctx))) return rc;    // src/main.f90:87 for every run, then tstep's first pass
+    if ((rc = ctx_step_first(e->ctx))) return rc;    // src/main.f90:87 for every run, then tstep's first pass
     if (any && (rc = push_plans(e))) return rc;
     const double t2 = now_ms();
-    if ((rc = ctx_ens_rest(e->ctx))) return rc;     // the rest of tstep, dt of each run from the device
+    if ((rc = ctx_step_rest(e->ctx))) return rc;     // the rest of tstep, dt of each run from the device
     const double t3 = now_ms();
     e->phase_ms[0] += t1 - t0;
     e->phase_ms[1] += t2 - t1;

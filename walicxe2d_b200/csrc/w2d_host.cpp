@@ -477,7 +477,36 @@ int w2d_sim_run(W2dSim* s, int nsteps)
   // reduction and the half step while the host walks the new block list
   // (locatebounds) and builds the fill plans, and the host reads dt back
   // before the full step
-  for (int n = 0; n < nsteps; ++n) {
+  const bool dev_dt = ctx_device_dt(s->ctx);
+  for (int n = 0; n < nsteps && dev_dt; ++n) {
+    // step graphs: dt stays on the device (the kernels read it there) and
+    // comes to the host with the step's synchronization
+    const double t0 = now_ms();
+    const bool replan = s->dirty;
+    if (replan && (rc = push_topology(s))) return rc;
+    const double t1 = now_ms();
+    if ((rc = ctx_step_first(s->ctx))) return rc;           // src/main.f90:87, then tstep's first pass
+    const double t2 = now_ms();
+    if (replan && (rc = push_bounds(s))) return rc;
+    const double t3 = now_ms();
+    if ((rc = ctx_step_rest(s->ctx))) return rc;            // the rest of tstep
+    const double t4 = now_ms();
+    s->phase_ms[0] += t1 - t0;
+    s->phase_ms[1] += t2 - t1;
+    s->phase_ms[2] += t3 - t2;
+    s->phase_ms[4] += t4 - t3;
+    s->zone_updates += (int64_t)s->nbleafs * s->p.nx * s->p.ny;
+    if (s->amr) {
+      if ((rc = admesh(s))) return rc;                       // src/main.f90:98 (synchronizes)
+    } else if ((rc = w2d_sync(s->ctx))) {
+      return rc;
+    }
+    s->dt = ctx_last_dt(s->ctx);
+    s->time = s->time + s->dt;                               // src/main.f90:88
+    s->steps++;
+    s->phase_ms[8] += now_ms() - t0;
+  }
+  for (int n = 0; n < nsteps && !dev_dt; ++n) {
     const double t0 = now_ms();
     const bool replan = s->dirty;
     if (replan && (rc = push_topology(s))) return rc;

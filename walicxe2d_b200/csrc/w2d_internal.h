@@ -55,8 +55,13 @@ int ctx_plan_upload(W2dCtx* c, int nl);
 // (*grad)[k]; synchronizes and checks the error word
 int ctx_ens_criteria(W2dCtx* c, const double** grad);
 
-// the two halves of an ensemble step (as CUDA graphs when enabled with
+// the two halves of a step of an ensemble, or of a single run without the
+// jet, with dt read on the device (as CUDA graphs when enabled with
 // w2d_set_graphs, captured again after tuning or when a buffer moves)
-int ctx_ens_first(W2dCtx* c);
-int ctx_ens_rest(W2dCtx* c);
+int ctx_step_first(W2dCtx* c);
+int ctx_step_rest(W2dCtx* c);
+// a single run steps through ctx_step_first/rest (w2d_set_graphs on, no jet)
+bool ctx_device_dt(W2dCtx* c);
+// the dt copied by the last ctx_dt_launch (valid after a synchronization)
+double ctx_last_dt(W2dCtx* c);
 

@@ -13,7 +13,7 @@ const Launchers& launchers64() { return k64::table; }
 // 256 leaves and folds its minima into work[0..1] with 64-bit atomicMin on
 // the bit patterns (for non-negative doubles the integer order is the
 // numeric order); the last CTA to finish forms dt and resets work/count.
-__global__ void __launch_bounds__(256) k_dt(const int* __restrict__ leaves, int n,
+__global__ void __launch_bounds__(256) k_dt(const int* __restrict__ leaves, int n, const int* __restrict__ n_dev,
                                             const double* __restrict__ cfl,
                                             const double* __restrict__ dtcool, int use_cool,
                                             double courant, double psc, double tsc,
@@ -22,12 +22,12 @@ __global__ void __launch_bounds__(256) k_dt(const int* __restrict__ leaves, int 
 {
   __shared__ double s0[8], s1[8];
   __shared__ bool last;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nn = n_dev ? *n_dev : n;
   double m0 = 1.e30, m1 = 1e30;
-  if (k < n) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
     const int b = leaves[k];
-    m0 = cfl[b];
-    if (use_cool) m1 = dtcool[b];
+    m0 = fmin(m0, cfl[b]);
+    if (use_cool) m1 = fmin(m1, dtcool[b]);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -117,12 +117,12 @@ cudaError_t launch_gather_leaf(const int* leaves, int n, const int* n_dev, const
   return cudaGetLastError();
 }
 
-cudaError_t launch_dt(const int* leaves, int n, const double* cfl, const double* dtcool, int use_cool,
-                      double courant, double psc, double tsc, unsigned long long* work, unsigned int* count,
-                      double* dt_out, cudaStream_t st)
+cudaError_t launch_dt(const int* leaves, int n, const int* n_dev, int grid, const double* cfl, const double* dtcool,
+                      int use_cool, double courant, double psc, double tsc, unsigned long long* work,
+                      unsigned int* count, double* dt_out, cudaStream_t st)
 {
-  const int grid = n > 0 ? (n + 255) / 256 : 1;
-  k_dt<<<grid, 256, 0, st>>>(leaves, n, cfl, dtcool, use_cool, courant, psc, tsc, work, count, dt_out);
+  if (grid <= 0) grid = n > 0 ? (n + 255) / 256 : 1;
+  k_dt<<<grid, 256, 0, st>>>(leaves, n, n_dev, cfl, dtcool, use_cool, courant, psc, tsc, work, count, dt_out);
   return cudaGetLastError();
 }
 

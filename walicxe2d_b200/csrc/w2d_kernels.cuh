@@ -837,13 +837,15 @@ __host__ __device__ constexpr size_t smem_calcprim()
   return 128 + sizeof(R) * NEQ * W2D_CELLS + 64 * sizeof(double);
 }
 
-// With jet_interior != 0 (list = the leaves, after the fill of layer 0) it
-// first imposes the jet on the interior of the blocks the list walk named,
-// which the reference does inside boundaryI (src/boundaryI.f90:386-393).
+// mode bit 1 (list = the leaves, after the fill of layer 0): first imposes
+// the jet on the interior of the blocks the list walk named, which the
+// reference does inside boundaryI (src/boundaryI.f90:386-393).  mode bit 2
+// (coolingdmc, after cooling): the statistics of the stored primitives of
+// cells 0..17, which the cooling step wrote, without recomputing them.
 template <typename R, int NEQ, bool P>
 __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_calcprim(KArgs a, PhysArgs pa,
                                                                          const int* __restrict__ list, int n,
-                                                                         int jet_interior)
+                                                                         int mode)
 {
   uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
   R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
@@ -859,13 +861,14 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_calcprim(KArgs 
   const int b = list[lr.li];
   R* __restrict__ u = (R*)a.u + (size_t)b * bs;
   R* __restrict__ pb = (pa.cooling == COOL_DMC) ? (R*)a.prim + (size_t)b * bs : nullptr;
-  if (tid == 0) tile_issue<R, NEQ>(&st[0][0][0], u, bar);
+  const bool from_prim = (mode & 2) && pb;
+  if (tid == 0) tile_issue<R, NEQ>(&st[0][0][0], from_prim ? pb : u, bar);
   if (!wait_tiles_p(bar, a.err, b, par)) return;
-  if (jet_interior && a.jet && a.jetblk[lr.li]) {
+  if ((mode & 1) && a.jet && a.jetblk[lr.li]) {
     jet_interior_fn<R, NEQ>(st, a, b, u);
     __syncthreads();
   }
-  for (int c = tid; c < W2D_CELLS; c += W2D_THREADS) {
+  for (int c = tid; c < W2D_CELLS && !from_prim; c += W2D_THREADS) {
     const int ti = c % W2D_W, tj = c / W2D_W;
     R uu[NEQ], q[NEQ], T;
 #pragma unroll

@@ -122,29 +122,29 @@ static cudaError_t fill_only(int neq, const KArgs& a, void* pool, int layers, cu
 }
 
 template <int NEQ, bool P>
-static cudaError_t calcprim_p(const KArgs& a, const PhysArgs& pa, const int* list, int n, int jet_interior,
+static cudaError_t calcprim_p(const KArgs& a, const PhysArgs& pa, const int* list, int n, int mode,
                               int grid, cudaStream_t st)
 {
   static bool done = false;
   constexpr size_t sm = smem_calcprim<R, NEQ>();
   cudaError_t e = smem_opt_in(k_calcprim<R, NEQ, P>, sm, done);
   if (e != cudaSuccess) return e;
-  k_calcprim<R, NEQ, P><<<grid, W2D_THREADS, sm, st>>>(a, pa, list, n, jet_interior);
+  k_calcprim<R, NEQ, P><<<grid, W2D_THREADS, sm, st>>>(a, pa, list, n, mode);
   return cudaGetLastError();
 }
 template <int NEQ>
-static cudaError_t calcprim_t(const KArgs& a, const PhysArgs& pa, const int* list, int n, int jet_interior,
+static cudaError_t calcprim_t(const KArgs& a, const PhysArgs& pa, const int* list, int n, int mode,
                               cudaStream_t st)
 {
-  if (list == a.leaves && a.grid > 0) return calcprim_p<NEQ, true>(a, pa, list, n, jet_interior, a.grid, st);
-  return calcprim_p<NEQ, false>(a, pa, list, n, jet_interior, n, st);
+  if (list == a.leaves && a.grid > 0) return calcprim_p<NEQ, true>(a, pa, list, n, mode, a.grid, st);
+  return calcprim_p<NEQ, false>(a, pa, list, n, mode, n, st);
 }
 
 static cudaError_t calcprim(int neq, const KArgs& a, const PhysArgs& pa, const int* list, int n,
-                            int jet_interior, cudaStream_t st)
+                            int mode, cudaStream_t st)
 {
   if (n == 0) return cudaSuccess;
-  W2D_NEQ_SWITCH(neq, return (calcprim_t<NEQ>(a, pa, list, n, jet_interior, st)));
+  W2D_NEQ_SWITCH(neq, return (calcprim_t<NEQ>(a, pa, list, n, mode, st)));
   return cudaSuccess;
 }
 

@@ -13,7 +13,7 @@ struct Launchers {
   cudaError_t (*full)(int neq, const KArgs&, const PhysArgs&, double dt, cudaStream_t);
   cudaError_t (*fill1)(int neq, const KArgs&, const PhysArgs&, int stats, cudaStream_t);
   cudaError_t (*fill_only)(int neq, const KArgs&, void* pool, int layers, cudaStream_t);
-  cudaError_t (*calcprim)(int neq, const KArgs&, const PhysArgs&, const int* list, int n, int jet_interior,
+  cudaError_t (*calcprim)(int neq, const KArgs&, const PhysArgs&, const int* list, int n, int mode,
                           cudaStream_t);
   cudaError_t (*jet_only)(int neq, const KArgs&, void* pool, cudaStream_t);
   // nr refines then nc coarsenings (ops: quads), tup: (slot, level, ix, iy) per new leaf
@@ -31,9 +31,11 @@ const Launchers& launchers32();
 
 // work: two 64-bit words holding the bit pattern of 1e30; count: zero.
 // Both are restored by the kernel for the next call.
-cudaError_t launch_dt(const int* leaves, int n, const double* cfl, const double* dtcool, int use_cool,
-                      double courant, double psc, double tsc, unsigned long long* work, unsigned int* count,
-                      double* dt_out, cudaStream_t st);
+// n_dev: leaf count in device memory (then grid > 0 is the CTA count); with
+// grid <= 0 one CTA per 256 leaves
+cudaError_t launch_dt(const int* leaves, int n, const int* n_dev, int grid, const double* cfl, const double* dtcool,
+                      int use_cool, double courant, double psc, double tsc, unsigned long long* work,
+                      unsigned int* count, double* dt_out, cudaStream_t st);
 
 // dt_run[r] for every run of an ensemble; leaves of run r at loff[r]..loff[r+1]-1
 cudaError_t launch_dt_runs(const int* leaves, const int* loff, int nruns, const double* cfl, const double* dtcool,
@@ -47,7 +49,8 @@ struct NNImage;
 // coolingh (FP32 path) through the learned surrogate with the exact routine
 // on the cells it does not serve; counts[0] += served, counts[1] += exact
 cudaError_t launch_cool_nn(int neq, const KArgs& a, const PhysArgs& pa, double dt_s, const NNImage* img,
-                           int* fb_list, int* fb_count, unsigned long long* counts, int nsm, cudaStream_t st);
+                           int* fb_list, int* fb_count, unsigned long long* counts, int nsm, float tol,
+                           cudaStream_t st);
 
 }  // namespace w2d
 

@@ -56,6 +56,9 @@ struct W2dNN {
   int64_t nsamp = 0;
   int64_t adam_t = 0;
   int nsm = 148;
+  int kind = W2D_COOLINGH;   // the cooling routine the network was trained on
+  double* d_tab = nullptr;   // coolingdmc: the table its samples used
+  double cv = 1.5, tempsc = 1.0, psc = 1.0;
 };
 
 namespace {
@@ -84,6 +87,31 @@ __device__ __forceinline__ void nn_draw(uint64_t seed, int64_t i, double& n, dou
   T = exp10(2.0 + 6.0 * u01(splitmix(k + 2)));
   y0 = 1e-4 + (1.0 - 1e-4) * u01(splitmix(k + 3));
   dts = exp10(-2.0 + 4.0 * u01(splitmix(k + 4))) * NN_YR;
+}
+
+// Training set of the coolingdmc mode, labelled by the exact rate of
+// src/coolingdmc.f90:30-40 (cooldmc on the table, src/dmc_module.f90:14-32):
+// T log-uniform over [1e4, 1e8] K, n as for coolingh; the neutral-fraction
+// and dt features are zero (the rate per unit density depends on T alone,
+// and dt enters only through exp(-Ce dt), so no dt range limits the use).
+__global__ void k_nn_samples_dmc(int64_t n, uint64_t seed, const double* __restrict__ tab, double cv, double tempsc,
+                                 double psc, float* __restrict__ feat, float* __restrict__ targ, int64_t ld)
+{
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double dn, T, y0, dts;
+  nn_draw(seed, k, dn, T, y0, dts);
+  T = exp10(4.0 + 4.0 * (log10(T) - 2.0) / 6.0);
+  const double p = dn * T / tempsc;
+  const double eth0 = cv * p;
+  const double ce = (d_cooldmc(tab, T) * (dn * dn)) / (eth0 * psc);
+  float f[4], t[2];
+  nn_features(dn, T, y0, dts, f);
+  f[2] = f[3] = 0.f;
+  nn_targets_dmc(dn, ce, t);
+  for (int q = 0; q < 4; ++q) feat[q * ld + k] = f[q];
+  targ[k] = t[0];
+  targ[ld + k] = t[1];
 }
 
 // Training set labelled by the exact routine (atomic, src/coolingh.f90).
@@ -547,11 +575,14 @@ __device__ __forceinline__ bool wg_wait(uint64_t* bar, uint32_t& phase, int wg, 
 // barrier), so that one stream's MMAs overlap the other's epilogues.
 // Thread r of a warpgroup owns row r (TMEM lane r).  Served cells get
 // (T, neutral fraction) from the network; cells outside the training range
-// or with a predicted change above 10% are listed for the exact routine.
-template <int NEQ>
+// or with a predicted change above the tolerance are listed for the exact
+// routine.  coolingdmc takes the primitives in FP64 as the exact routine
+// does and stores them (with the cooled pressure) for every cell it serves
+// or leaves uncooled; the exact routine stores those of the listed cells.
+template <int NEQ, int KIND>
 __global__ void __launch_bounds__(256, 4) k_cool_nn(KArgs a, PhysArgs pa, double dt_s, const NNImage* __restrict__ img,
                                                  int* __restrict__ fb_list, int* __restrict__ fb_count,
-                                                 unsigned long long* __restrict__ counts)
+                                                 unsigned long long* __restrict__ counts, float tol)
 {
   extern __shared__ __align__(1024) uint8_t nn_smem[];
   NNCoolSmem& s = *reinterpret_cast<NNCoolSmem*>(nn_smem);
@@ -580,6 +611,7 @@ __global__ void __launch_bounds__(256, 4) k_cool_nn(KArgs a, PhysArgs pa, double
   NNCoolSmem::Stream& ss = s.st[wg];
   uint64_t* bar = &s.bar[wg];
   const Phys<float> ph = make_phys<float, -1, -1>(pa);
+  const Phys<double> phd = make_phys<double, -1, -1>(pa);
   uint32_t phase = 0;
   unsigned served = 0;
   const int nl = a.nleaf_dev ? *a.nleaf_dev : a.nleaf;
@@ -588,19 +620,33 @@ __global__ void __launch_bounds__(256, 4) k_cool_nn(KArgs a, PhysArgs pa, double
     const int64_t c = t * 128 + row;
     const bool valid = c < ncells;
     float uu[NEQ], q[NEQ], T = 1.f, dts = (float)dt_s, f[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    double qd[NEQ];   // coolingdmc: primitives in FP64
     float* ub = nullptr;
+    float* pbk = nullptr;
     int pc = 0;
-    bool inr = false;
+    bool inr = false, cools = true;
     if (valid) {
       const int b = a.leaves[c / 320];
       pc = cool_cell((int)(c % 320));
       ub = (float*)a.u + (size_t)b * NEQ * W2D_CELLS;
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) uu[k] = ub[k * W2D_CELLS + pc];
-      uprim<NEQ>(ph, q, uu, T);
+      if (KIND == COOL_DMC) {
+        double ud[NEQ], Td;
+#pragma unroll
+        for (int k = 0; k < NEQ; ++k) ud[k] = (double)uu[k];
+        uprim<NEQ>(phd, qd, ud, Td);
+        T = (float)Td;
+        cools = Td > 1.e4;                      // src/coolingdmc.f90:30
+        pbk = (float*)a.prim + (size_t)b * NEQ * W2D_CELLS;
+      } else {
+        uprim<NEQ>(ph, q, uu, T);
+      }
       if (a.run_of) dts = (float)(a.dt_run[a.run_of[b]] * a.tsc);
-      nn_features_f(uu[0], T, uu[4] / uu[0], dts, f);
-      inr = nn_in_range(f);
+      else if (a.dt_dev) dts = (float)(*a.dt_dev * a.tsc);
+      nn_features_f(uu[0], T, NEQ > 4 ? uu[NEQ > 4 ? 4 : 0] / uu[0] : 0.5f, dts, f);
+      if (KIND == COOL_DMC) f[2] = f[3] = 0.f;   // as in the coolingdmc training set
+      inr = cools && nn_in_range(f);
     }
     {
       const float z[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -645,19 +691,32 @@ __global__ void __launch_bounds__(256, 4) k_cool_nn(KArgs a, PhysArgs pa, double
     if (!wg_wait(bar, phase, wg, a.err)) break;
     tc_ld16(tc_addr(tm, lane0, 0), v);
     bool use = false;
-    if (valid && inr) {
+    if (valid && inr && KIND == COOL_H) {
       float y1, t1;
       const float n = uu[0];
-      use = nn_update_f(v[0] + s.b3[0], v[1] + s.b3[1], n, T, uu[4] / n, dts, y1, t1);
+      use = nn_update_f(v[0] + s.b3[0], v[1] + s.b3[1], n, T, uu[NEQ > 4 ? 4 : 0] / n, dts, y1, t1, tol);
       if (use) {   // the energy and neutral density of atomic (src/coolingh.f90:227-258)
         const float u4 = y1 * n;
         ub[3 * W2D_CELLS + pc] = ph.cv * (2.f * n - u4) * t1 / ph.tempsc + 0.5f * q[0] * (q[1] * q[1] + q[2] * q[2]);
-        ub[4 * W2D_CELLS + pc] = u4;
+        if (NEQ > 4) ub[(NEQ > 4 ? 4 : 0) * W2D_CELLS + pc] = u4;
+        ++served;
+      }
+    } else if (valid && inr) {   // coolingdmc: p1 = p exp(-Ce dt), u4 += cv (p1 - p)
+      const float df = expm1f(-nn_dmc_rate_f(v[1] + s.b3[1], uu[0]) * dts);
+      use = fabsf(df) <= tol;
+      if (use) {
+        const double eth0 = phd.cv * qd[3];
+        qd[3] = qd[3] + qd[3] * (double)df;
+        ub[3 * W2D_CELLS + pc] = (float)((double)uu[3] - eth0 + phd.cv * qd[3]);
         ++served;
       }
     }
+    if (KIND == COOL_DMC && valid && (use || !cools)) {   // the stored primitives
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) pbk[k * W2D_CELLS + pc] = (float)qd[k];
+    }
     {   // the cells left to the exact routine: one atomic per warp
-      const bool fb = valid && !use;
+      const bool fb = valid && !use && cools;
       const unsigned m = __ballot_sync(0xffffffffu, fb);
       if (m) {
         const int lane = tid & 31;
@@ -681,8 +740,9 @@ __global__ void __launch_bounds__(256, 4) k_cool_nn(KArgs a, PhysArgs pa, double
   if (warp == 0) tc_dealloc(s.tmem, 128);
 }
 
-// The exact routine (FP64 atomic) on the listed cells.
-template <int NEQ>
+// The exact routine (FP64 atomic, or coolingdmc on the table) on the
+// listed cells.
+template <int NEQ, int KIND>
 __global__ void __launch_bounds__(256) k_cool_fb(KArgs a, PhysArgs pa, double dt_s, const int* __restrict__ list,
                                                  const int* __restrict__ count, unsigned long long* __restrict__ counts)
 {
@@ -696,10 +756,26 @@ __global__ void __launch_bounds__(256) k_cool_fb(KArgs a, PhysArgs pa, double dt
     double uu[NEQ];
 #pragma unroll
     for (int e = 0; e < NEQ; ++e) uu[e] = (double)ub[e * W2D_CELLS + pc];
-    const double dts = a.run_of ? a.dt_run[a.run_of[b]] * a.tsc : dt_s;
-    d_atomic<NEQ>(phd, dts, uu);
-    ub[3 * W2D_CELLS + pc] = (float)uu[3];
-    ub[4 * W2D_CELLS + pc] = (float)uu[4];
+    const double dts = a.run_of ? a.dt_run[a.run_of[b]] * a.tsc : (a.dt_dev ? *a.dt_dev * a.tsc : dt_s);
+    if (KIND == COOL_H) {
+      d_atomic<NEQ>(phd, dts, uu);
+      ub[3 * W2D_CELLS + pc] = (float)uu[3];
+      if (NEQ > 4) ub[(NEQ > 4 ? 4 : 0) * W2D_CELLS + pc] = (float)uu[NEQ > 4 ? 4 : 0];
+    } else {   // src/coolingdmc.f90:30-40, and the stored primitives
+      double q[NEQ], T;
+      uprim<NEQ>(phd, q, uu, T);
+      if (T > 1.e4) {
+        const double eth0 = phd.cv * q[3];
+        const double aloss = d_cooldmc(a.cooltab, T);
+        const double dens = q[0];
+        const double ce = (aloss * (dens * dens)) / (eth0 * a.psc);
+        q[3] = q[3] * exp(-ce * dts);
+        ub[3 * W2D_CELLS + pc] = (float)(uu[3] - eth0 + phd.cv * q[3]);
+      }
+      float* pb = (float*)a.prim + (size_t)b * NEQ * W2D_CELLS;
+#pragma unroll
+      for (int e = 0; e < NEQ; ++e) pb[e * W2D_CELLS + pc] = (float)q[e];
+    }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) atomicAdd(&counts[1], (unsigned long long)n);
 }
@@ -767,33 +843,48 @@ const NNImage* nn_image_of(const W2dNN* nn) { return nn ? nn->d_img : nullptr; }
 
 // coolingh of the FP32 path through the surrogate, then the exact routine on
 // the cells it does not serve; fb_count must be zero on entry
-cudaError_t launch_cool_nn(int neq, const KArgs& a, const PhysArgs& pa, double dt_s, const NNImage* img,
-                           int* fb_list, int* fb_count, unsigned long long* counts, int nsm, cudaStream_t st)
+template <int NEQ, int KIND>
+static cudaError_t cool_nn_t(const KArgs& a, const PhysArgs& pa, double dt_s, const NNImage* img, int* fb_list,
+                             int* fb_count, unsigned long long* counts, int nsm, float tol, cudaStream_t st)
 {
-  if (a.nleaf == 0 && !a.nleaf_dev) return cudaSuccess;
+  static bool opted = false;
   const size_t sm = sizeof(NNCoolSmem);
-  static bool opted5 = false, opted6 = false;
-  cudaError_t e = cudaSuccess;
+  if (!opted) {
+    cudaError_t e = cudaFuncSetAttribute(k_cool_nn<NEQ, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    opted = true;
+  }
   const int64_t tiles = ((int64_t)a.nleaf * 320 + 127) / 128;
   const int grid = a.nleaf_dev ? 4 * nsm : (int)std::min<int64_t>((tiles + 1) / 2, 4 * (int64_t)nsm);
-  if (neq == 5) {
-    if (!opted5) e = cudaFuncSetAttribute(k_cool_nn<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    opted5 = true;
-    k_cool_nn<5><<<grid, 256, sm, st>>>(a, pa, dt_s, img, fb_list, fb_count, counts);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_cool_fb<5><<<4 * nsm, 256, 0, st>>>(a, pa, dt_s, fb_list, fb_count, counts);
-  } else if (neq == 6) {
-    if (!opted6) e = cudaFuncSetAttribute(k_cool_nn<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    opted6 = true;
-    k_cool_nn<6><<<grid, 256, sm, st>>>(a, pa, dt_s, img, fb_list, fb_count, counts);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_cool_fb<6><<<4 * nsm, 256, 0, st>>>(a, pa, dt_s, fb_list, fb_count, counts);
-  } else {
-    return cudaErrorInvalidValue;
-  }
+  k_cool_nn<NEQ, KIND><<<grid, 256, sm, st>>>(a, pa, dt_s, img, fb_list, fb_count, counts, tol);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_cool_fb<NEQ, KIND><<<4 * nsm, 256, 0, st>>>(a, pa, dt_s, fb_list, fb_count, counts);
   return cudaGetLastError();
+}
+
+// coolingh or coolingdmc (FP32 path) through the learned surrogate, then the
+// exact routine on the cells it does not serve; fb_count must be zero on
+// entry
+cudaError_t launch_cool_nn(int neq, const KArgs& a, const PhysArgs& pa, double dt_s, const NNImage* img,
+                           int* fb_list, int* fb_count, unsigned long long* counts, int nsm, float tol,
+                           cudaStream_t st)
+{
+  if (a.nleaf == 0 && !a.nleaf_dev) return cudaSuccess;
+  const bool dmc = pa.cooling == COOL_DMC;
+  switch (neq) {
+    case 4:
+      if (!dmc) return cudaErrorInvalidValue;
+      return cool_nn_t<4, COOL_DMC>(a, pa, dt_s, img, fb_list, fb_count, counts, nsm, tol, st);
+    case 5:
+      return dmc ? cool_nn_t<5, COOL_DMC>(a, pa, dt_s, img, fb_list, fb_count, counts, nsm, tol, st)
+                 : cool_nn_t<5, COOL_H>(a, pa, dt_s, img, fb_list, fb_count, counts, nsm, tol, st);
+    case 6:
+      return dmc ? cool_nn_t<6, COOL_DMC>(a, pa, dt_s, img, fb_list, fb_count, counts, nsm, tol, st)
+                 : cool_nn_t<6, COOL_H>(a, pa, dt_s, img, fb_list, fb_count, counts, nsm, tol, st);
+    default:
+      return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace w2d
@@ -847,7 +938,7 @@ int w2d_nn_destroy(W2dNN* nn)
 {
   if (!nn) return W2D_ERR_ARG;
   if (nn->st) cudaStreamSynchronize(nn->st);
-  void* d[] = {nn->d_p, nn->d_g, nn->d_m, nn->d_v, nn->d_img, nn->d_err, nn->d_feat, nn->d_targ};
+  void* d[] = {nn->d_p, nn->d_g, nn->d_m, nn->d_v, nn->d_img, nn->d_err, nn->d_feat, nn->d_targ, nn->d_tab};
   for (void* x : d)
     if (x) cudaFree(x);
   if (nn->st) cudaStreamDestroy(nn->st);
@@ -867,8 +958,39 @@ int w2d_nn_samples(W2dNN* nn, int64_t n, uint64_t seed)
   NCK(cudaGetLastError());
   NCK(cudaStreamSynchronize(nn->st));
   nn->nsamp = n;
+  nn->kind = W2D_COOLINGH;
   return W2D_OK;
 }
+
+int w2d_nn_samples_dmc(W2dNN* nn, int64_t n, uint64_t seed, const double* log_t, const double* neg_log_l, int rows,
+                       double cv, double tempsc, double psc)
+{
+  if (!nn || n < 128 || !log_t || !neg_log_l || rows != 41) return W2D_ERR_ARG;
+  double tab[82];   // (T, Lambda) as w2d_set_cooltab stores it
+  for (int k = 0; k < 41; ++k) {
+    tab[k] = pow(10.e0, (log_t[k]));
+    tab[41 + k] = pow(10.e0, (-neg_log_l[k]));
+  }
+  if (!nn->d_tab) NCK(cudaMalloc(&nn->d_tab, sizeof(tab)));
+  NCK(cudaMemcpy(nn->d_tab, tab, sizeof(tab), cudaMemcpyHostToDevice));
+  if (nn->d_feat) cudaFree(nn->d_feat);
+  if (nn->d_targ) cudaFree(nn->d_targ);
+  nn->d_feat = nn->d_targ = nullptr;
+  NCK(cudaMalloc(&nn->d_feat, sizeof(float) * 4 * (size_t)n));
+  NCK(cudaMalloc(&nn->d_targ, sizeof(float) * 2 * (size_t)n));
+  k_nn_samples_dmc<<<(unsigned)((n + 255) / 256), 256, 0, nn->st>>>(n, seed, nn->d_tab, cv, tempsc, psc, nn->d_feat,
+                                                                    nn->d_targ, n);
+  NCK(cudaGetLastError());
+  NCK(cudaStreamSynchronize(nn->st));
+  nn->nsamp = n;
+  nn->kind = W2D_COOLINGDMC;
+  nn->cv = cv;
+  nn->tempsc = tempsc;
+  nn->psc = psc;
+  return W2D_OK;
+}
+
+int w2d_nn_kind(W2dNN* nn) { return nn ? nn->kind : -1; }
 
 int w2d_nn_train(W2dNN* nn, int epochs, int batch, float lr, float lr_end, float* last_loss)
 {
@@ -966,6 +1088,7 @@ int w2d_nn_forward(W2dNN* nn, const float* feat, int n, float* out)
 int w2d_nn_judge(W2dNN* nn, int64_t n, uint64_t seed, double* stats)
 {
   if (!nn || !stats || n < 128) return W2D_ERR_ARG;
+  if (nn->kind != W2D_COOLINGH) return W2D_ERR_STATE;   // the judge runs coolingh's routine
   float *df = nullptr, *dout = nullptr, *dres = nullptr;
   NCK(cudaMalloc(&df, sizeof(float) * 4 * (size_t)n));
   NCK(cudaMalloc(&dout, sizeof(float) * 2 * (size_t)n));

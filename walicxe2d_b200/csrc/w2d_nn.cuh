@@ -115,7 +115,7 @@ __device__ __forceinline__ void nn_features_f(float n, float T, float y0, float 
 }
 
 __device__ __forceinline__ bool nn_update_f(float o0, float o1, float n, float T, float y0, float dt_s, float& y1,
-                                            float& t1)
+                                            float& t1, float tol)
 {
   y1 = y0 + n * dt_s * NN_SY * sinhf(NN_AY * o0);
   y1 = y1 < 1.f ? y1 : 1.f;
@@ -126,10 +126,27 @@ __device__ __forceinline__ bool nn_update_f(float o0, float o1, float n, float T
   t1 = t1 < 10.f * T ? t1 : 10.f * T;
   t1 = t1 > 10.f ? t1 : 10.f;
   // served when the predicted relative changes of T and of the thermal
-  // pressure (2 - y) T both stay within 10%
+  // pressure (2 - y) T both stay within tol (at most 10%)
   const float dp = ((2.f - y1) * t1) / ((2.f - y0) * T) - 1.f;
-  return fabsf(t1 / T - 1.f) <= 0.1f && fabsf(dp) <= 0.1f;
+  return fabsf(t1 / T - 1.f) <= tol && fabsf(dp) <= tol;
 }
+
+// coolingdmc mode (src/coolingdmc.f90:30-40): above 1e4 K the pressure
+// relaxes as p1 = p exp(-Ce dt) with Ce = Lambda(T) n^2 / (cv p Psc); per
+// unit density Ce depends on T alone, so the network's second output is
+//   o1 = (log10(Ce / n) + 12.5) / 3.5
+// and its first output is trained to zero.  Its neutral-fraction and dt
+// inputs are held at zero (training and use), so any dt is served.  Cells
+// at or below 1e4 K do not cool (the exact routine leaves them as they are).
+__device__ __forceinline__ void nn_targets_dmc(double n, double ce, float* t)
+{
+  t[0] = 0.f;
+  const double c = ce > 1e-40 ? ce : 1e-40;
+  t[1] = (float)((log10(c / n) + 12.5) / 3.5);
+}
+
+__device__ __forceinline__ double nn_dmc_rate(float o1, double n) { return exp10(3.5 * (double)o1 - 12.5) * n; }
+__device__ __forceinline__ float nn_dmc_rate_f(float o1, float n) { return exp10f(3.5f * o1 - 12.5f) * n; }
 
 // Shared memory of the forward pass of one tile
 struct NNFwdSmem {
