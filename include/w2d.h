@@ -255,6 +255,24 @@ int w2d_sim_set_cooltab(W2dSim* sim, const double* log_t, const double* neg_log_
  * doubles; reset != 0 zeroes the counters after reading. */
 #define W2D_SIM_NPHASES 9
 int w2d_sim_phase_ms(W2dSim* sim, double* ms, int reset);
+/* output(itprint) with OUTBIN, src/output.f90:39-67 (serial build): writes
+ * the pointers file (nbmin = 1, nbmax, nbleafs, nblocks, then lp, leaf and
+ * icoord of blocks 1..nbmax, column-major 4-byte integers) and the blocks
+ * file (u of every leaf in ascending ID in the order of u(nb,:,:,:), 8-byte
+ * reals), little-endian streams, from the device pool.  true_value encodes
+ * .true. in leaf (-1 as ifort writes it and the reference's py/ reader
+ * expects, 1 as gfortran writes it).  An FP32 run writes its state as
+ * 8-byte reals. */
+int w2d_sim_write_bin(W2dSim* sim, const char* pointers_path, const char* blocks_path,
+                      int32_t true_value);
+/* Warm start, src/basegrid.f90:167-251 (serial build): replaces the run's
+ * tree and leaf blocks with those of the two files (any nonzero leaf value
+ * is .true.; the file's nbmax must fit the run's nblocks), recomputes the
+ * leaves' primitives, sets the run time to `time` (the reference uses
+ * itprint*dtprint) and makes nadmesh admesh passes (src/main.f90:59-62 makes
+ * 4).  A COOLINGDMC run needs its table (w2d_sim_set_cooltab) first. */
+int w2d_sim_read_bin(W2dSim* sim, const char* pointers_path, const char* blocks_path,
+                     double time, int nadmesh);
 
 /* ---- Ensembles (no counterpart in the reference) ---------------------------
  * nruns independent runs of the driver above advanced together on one

@@ -84,6 +84,10 @@ def lib():
         L.orc_cooldmc.argtypes = [vp, D]
         L.orc_aloss.restype = D
         L.orc_aloss.argtypes = [D, D, D, D, D, D]
+        L.orc_output_bin.restype = I
+        L.orc_output_bin.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int32]
+        L.orc_read_bin.restype = I
+        L.orc_read_bin.argtypes = [vp, C.c_char_p, C.c_char_p, D]
         _LIB = L
     return _LIB
 
@@ -243,6 +247,14 @@ class Oracle:
 
     def cooldmc(self, T: float) -> float:
         return self.L.orc_cooldmc(self.h, T)
+
+    def write_bin(self, pointers: str, blocks: str, true_value: int = -1):
+        """output(itprint) with OUTBIN (serial build) into the two files."""
+        self._check(self.L.orc_output_bin(self.h, pointers.encode(), blocks.encode(), true_value))
+
+    def read_bin(self, pointers: str, blocks: str, time: float):
+        """The serial warm start from the two files, then calcprim."""
+        self._check(self.L.orc_read_bin(self.h, pointers.encode(), blocks.encode(), time))
 
 
 # ---- point functions -------------------------------------------------------

@@ -72,6 +72,10 @@ int    orc_admesh(OrcSim* s);
 int    orc_criteria_grad(OrcSim* s, double* grad);
 int    orc_refine(OrcSim* s, int nb, int s1, int s2, int s3, int s4);
 int    orc_coarse(OrcSim* s, int dad, int s1, int s2, int s3, int s4);
+/* output (OUTBIN) and warm start of the serial build: the pointers and
+ * blocks files (src/output.f90:39-67, src/basegrid.f90:167-251) */
+int    orc_output_bin(OrcSim* s, const char* pointers, const char* blocks, int32_t true_value);
+int    orc_read_bin(OrcSim* s, const char* pointers, const char* blocks, double time);
 /* main loop: nsteps x (timestep, time+=dt, tstep, admesh if amr) */
 int    orc_run(OrcSim* s, int nsteps, int amr, double* dt_last);
 /* the sequential walks with the given list instead of locatebounds' one */

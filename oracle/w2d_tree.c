@@ -8,6 +8,7 @@
 
 #include <math.h>
 #include <stdlib.h>
+#include <stdio.h>
 #include <string.h>
 #ifdef _OPENMP
 #include <omp.h>
@@ -616,4 +617,93 @@ int orc_run(OrcSim* s, int nsteps, int amr, double* dt_last)
     s->steps++;
   }
   return 0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* src/output.f90:39-67 (OUTBIN, serial build).  Both files are unformatted
+ * little-endian streams.  pointers: nbmin, nbmax, nbleafs, nblocks, then
+ * lp(nbmin:nbmax,1:8), leaf(nbmin:nbmax) and icoord(nbmin:nbmax,1:2), each
+ * array column-major (block ID fastest) in 4-byte integers, leaf holding
+ * true_value for .true. and 0 for .false.; blocks: u(nb,:,:,:) of every
+ * leaf in ascending ID, the equation index fastest, then i, then j, 8-byte
+ * reals (DOUBLEP).  nbmin is 1 in the serial build. */
+int orc_output_bin(OrcSim* s, const char* pointers, const char* blocks, int32_t true_value)
+{
+  FILE* f = fopen(pointers, "wb");
+  if (!f) return s->err = W2D_ERR_ARG;
+  const int32_t head[4] = {1, s->nbmax, s->nbleafs, s->cap};
+  fwrite(head, sizeof(int32_t), 4, f);
+  for (int k = 1; k <= 8; ++k)
+    for (int nb = 1; nb <= s->nbmax; ++nb) fwrite(&LP(s, nb, k), sizeof(int32_t), 1, f);
+  for (int nb = 1; nb <= s->nbmax; ++nb) {
+    const int32_t v = s->leaf[nb] ? true_value : 0;
+    fwrite(&v, sizeof(int32_t), 1, f);
+  }
+  for (int k = 1; k <= 2; ++k)
+    for (int nb = 1; nb <= s->nbmax; ++nb) fwrite(&IC(s, nb, k), sizeof(int32_t), 1, f);
+  if (fclose(f)) return s->err = W2D_ERR_ARG;
+  f = fopen(blocks, "wb");
+  if (!f) return s->err = W2D_ERR_ARG;
+  const int W = s->W, neq = s->p.neq;
+  for (int nb = 1; nb <= s->nbmax; ++nb) {
+    if (!s->leaf[nb]) continue;
+    for (int j = -1; j <= W - 2; ++j)
+      for (int i = -1; i <= W - 2; ++i)
+        for (int k = 0; k < neq; ++k) fwrite(&U(s, nb, k, i, j), sizeof(double), 1, f);
+  }
+  if (fclose(f)) return s->err = W2D_ERR_ARG;
+  return 0;
+}
+
+/* src/basegrid.f90:167-251, the warm start of the serial build: the tree
+ * and the leaf blocks from the two files of orc_output_bin, then calcprim of
+ * every leaf (src/basegrid.f90:241-247); the run time is set to `time` (the
+ * reference takes itprint*dtprint, src/initmain.f90:69-73).  The pointer
+ * renumbering of basegrid.f90:188-206 applies only to files of several MPI
+ * ranks, whose pointers exceed nblocks; a serial file never does.  Any
+ * nonzero leaf value reads as .true. */
+int orc_read_bin(OrcSim* s, const char* pointers, const char* blocks, double time)
+{
+  FILE* f = fopen(pointers, "rb");
+  if (!f) return s->err = W2D_ERR_ARG;
+  int32_t head[4];
+  int ok = fread(head, sizeof(int32_t), 4, f) == 4;
+  const int nbmax = head[1];
+  if (!ok || head[0] != 1 || nbmax < 1 || nbmax > s->cap) {
+    fclose(f);
+    return s->err = ok && nbmax > s->cap ? W2D_ERR_CAPACITY : W2D_ERR_ARG;
+  }
+  memset(s->lp, 0, sizeof(int32_t) * 8 * ((size_t)s->cap + 1));
+  memset(s->leaf, 0, sizeof(int32_t) * ((size_t)s->cap + 1));
+  memset(s->icoord, 0, sizeof(int32_t) * 2 * ((size_t)s->cap + 1));
+  for (int k = 1; k <= 8 && ok; ++k)
+    for (int nb = 1; nb <= nbmax && ok; ++nb) ok = fread(&LP(s, nb, k), sizeof(int32_t), 1, f) == 1;
+  int nleaf = 0;
+  for (int nb = 1; nb <= nbmax && ok; ++nb) {
+    int32_t v;
+    ok = fread(&v, sizeof(int32_t), 1, f) == 1;
+    s->leaf[nb] = v != 0;
+    nleaf += v != 0;
+  }
+  for (int k = 1; k <= 2 && ok; ++k)
+    for (int nb = 1; nb <= nbmax && ok; ++nb) ok = fread(&IC(s, nb, k), sizeof(int32_t), 1, f) == 1;
+  fclose(f);
+  if (!ok || nleaf != head[2]) return s->err = W2D_ERR_ARG;
+  s->nbmax = nbmax;
+  s->nbleafs = head[2];
+  f = fopen(blocks, "rb");
+  if (!f) return s->err = W2D_ERR_ARG;
+  const int W = s->W, neq = s->p.neq;
+  for (int nb = 1; nb <= nbmax && ok; ++nb) {
+    if (!s->leaf[nb]) continue;
+    for (int j = -1; j <= W - 2 && ok; ++j)
+      for (int i = -1; i <= W - 2 && ok; ++i)
+        for (int k = 0; k < neq && ok; ++k) ok = fread(&U(s, nb, k, i, j), sizeof(double), 1, f) == 1;
+  }
+  char extra;
+  if (ok) ok = fread(&extra, 1, 1, f) == 0;   /* nothing may follow the last leaf */
+  fclose(f);
+  if (!ok) return s->err = W2D_ERR_ARG;
+  s->time = time;
+  return orc_calcprim_all(s);
 }

@@ -59,6 +59,8 @@ SIGNATURES = {
     "w2d_sim_tree": (_I, [_vp, _PI32, _PI32, _PI32, _PI32, _PI32]),
     "w2d_sim_set_amr": (_I, [_vp, _I]),
     "w2d_sim_set_cooltab": (_I, [_vp, _PD, _PD, _I]),
+    "w2d_sim_write_bin": (_I, [_vp, C.c_char_p, C.c_char_p, C.c_int32]),
+    "w2d_sim_read_bin": (_I, [_vp, C.c_char_p, C.c_char_p, _D, _I]),
     "w2d_sim_phase_ms": (_I, [_vp, _PD, _I]),
     "w2d_ens_create": (_I, [C.POINTER(W2dParams), C.POINTER(W2dInit), _I, _I, C.POINTER(_vp)]),
     "w2d_ens_destroy": (_I, [_vp]),

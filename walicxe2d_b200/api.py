@@ -266,6 +266,21 @@ class Simulation:
         if rc:
             self.ctx._check(rc, "w2d_sim_set_cooltab")
 
+    def write_bin(self, pointers: str, blocks: str, true_value: int = -1):
+        """output(itprint) with OUTBIN: the reference's pointers and blocks
+        files of the current state (w2d_sim_write_bin)."""
+        rc = self.L.w2d_sim_write_bin(self.h, pointers.encode(), blocks.encode(), true_value)
+        if rc:
+            self.ctx._check(rc, "w2d_sim_write_bin")
+
+    def read_bin(self, pointers: str, blocks: str, time: float, nadmesh: int = 0):
+        """Warm start from the reference's pointers and blocks files
+        (w2d_sim_read_bin); nadmesh admesh passes follow (the reference's
+        main program makes 4)."""
+        rc = self.L.w2d_sim_read_bin(self.h, pointers.encode(), blocks.encode(), time, nadmesh)
+        if rc:
+            self.ctx._check(rc, "w2d_sim_read_bin")
+
     def status(self) -> dict:
         t, dt = C.c_double(), C.c_double()
         steps, zu = C.c_int64(), C.c_int64()

@@ -23,6 +23,7 @@
 // coarser leaves its pointers reach), so the same blocks are visited in the
 // same order and the decisions are identical.
 #include <chrono>
+#include <cstdio>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -591,6 +592,121 @@ int w2d_sim_set_cooltab(W2dSim* s, const double* log_t, const double* neg_log_l,
   if (rc) return rc;
   if (s->dirty && (rc = refresh_plan(s))) return rc;
   return w2d_calcprim(s->ctx);
+}
+
+// output(itprint) with OUTBIN, src/output.f90:39-67 (serial build): the
+// pointers file (nbmin = 1, nbmax, nbleafs, nblocks; lp, leaf and icoord of
+// blocks 1..nbmax, column-major, 4-byte integers) and the blocks file
+// (u(nb,:,:,:) of every leaf in ascending ID: equation fastest, then i, then
+// j; 8-byte reals), both little-endian streams.  The leaves come from the
+// device pool in one w2d_get_blocks.
+int w2d_sim_write_bin(W2dSim* s, const char* pointers, const char* blocks, int32_t true_value)
+{
+  if (!s || !pointers || !blocks) return W2D_ERR_ARG;
+  const int W = s->p.nx + 4, neq = s->p.neq;
+  const size_t bs = (size_t)neq * W * W;
+  std::vector<int32_t> ids;
+  for (int nb = 1; nb <= s->nbmax; ++nb)
+    if (s->LEAF(nb)) ids.push_back(nb);
+  std::vector<double> u(bs * ids.size());
+  int rc;
+  if (!ids.empty() && (rc = w2d_get_blocks(s->ctx, ids.data(), (int)ids.size(), u.data()))) return rc;
+  std::vector<int32_t> ptr;
+  ptr.reserve(4 + 11 * (size_t)s->nbmax);
+  ptr.insert(ptr.end(), {1, s->nbmax, s->nbleafs, s->cap});
+  for (int k = 1; k <= 8; ++k)
+    for (int nb = 1; nb <= s->nbmax; ++nb) ptr.push_back(s->LP(nb, k));
+  for (int nb = 1; nb <= s->nbmax; ++nb) ptr.push_back(s->LEAF(nb) ? true_value : 0);
+  for (int k = 1; k <= 2; ++k)
+    for (int nb = 1; nb <= s->nbmax; ++nb) ptr.push_back(s->IC(nb, k));
+  std::vector<double> out(u.size());
+  for (size_t q = 0; q < ids.size(); ++q) {   // [eq][j][i] -> u(nb, eq, i, j) order
+    const double* src = u.data() + q * bs;
+    double* dst = out.data() + q * bs;
+    for (int j = 0; j < W; ++j)
+      for (int i = 0; i < W; ++i)
+        for (int k = 0; k < neq; ++k) *dst++ = src[((size_t)k * W + j) * W + i];
+  }
+  FILE* f = fopen(pointers, "wb");
+  if (!f) return W2D_ERR_ARG;
+  bool ok = fwrite(ptr.data(), sizeof(int32_t), ptr.size(), f) == ptr.size();
+  ok = (fclose(f) == 0) && ok;
+  if (!ok) return W2D_ERR_ARG;
+  f = fopen(blocks, "wb");
+  if (!f) return W2D_ERR_ARG;
+  ok = fwrite(out.data(), sizeof(double), out.size(), f) == out.size();
+  ok = (fclose(f) == 0) && ok;
+  return ok ? W2D_OK : W2D_ERR_ARG;
+}
+
+// The warm start of src/basegrid.f90:167-251 (serial build) from the files
+// of w2d_sim_write_bin: the tree replaces the run's, the leaves go to the
+// device pool (w2d_put_blocks, which recomputes their primitives as the
+// reference's calcprim does, basegrid.f90:241-247), the run time is set to
+// `time` (the reference takes itprint*dtprint, src/initmain.f90:69-73), and
+// nadmesh admesh passes follow (src/main.f90:59-62 makes 4).  A serial file's
+// pointers never exceed its nblocks, so the renumbering for files of several
+// MPI ranks (basegrid.f90:188-206) does not apply.  Any nonzero leaf value
+// reads as .true.
+int w2d_sim_read_bin(W2dSim* s, const char* pointers, const char* blocks, double time, int nadmesh)
+{
+  if (!s || !pointers || !blocks || nadmesh < 0) return W2D_ERR_ARG;
+  FILE* f = fopen(pointers, "rb");
+  if (!f) return W2D_ERR_ARG;
+  int32_t head[4];
+  bool ok = fread(head, sizeof(int32_t), 4, f) == 4;
+  const int nbmax = ok ? head[1] : 0;
+  if (!ok || head[0] != 1 || nbmax < 1 || nbmax > s->cap || head[2] < 1) {
+    fclose(f);
+    return ok && nbmax > s->cap ? W2D_ERR_CAPACITY : W2D_ERR_ARG;
+  }
+  std::vector<int32_t> arr((size_t)11 * nbmax);
+  ok = fread(arr.data(), sizeof(int32_t), arr.size(), f) == arr.size();
+  fclose(f);
+  if (!ok) return W2D_ERR_ARG;
+  const int32_t* lp = arr.data();
+  const int32_t* lf = lp + (size_t)8 * nbmax;
+  const int32_t* icd = lf + nbmax;
+  std::vector<int32_t> ids;
+  for (int nb = 1; nb <= nbmax; ++nb)
+    if (lf[nb - 1]) ids.push_back(nb);
+  if ((int)ids.size() != head[2]) return W2D_ERR_ARG;
+  const int W = s->p.nx + 4, neq = s->p.neq;
+  const size_t bs = (size_t)neq * W * W;
+  std::vector<double> in(bs * ids.size()), u(bs * ids.size());
+  f = fopen(blocks, "rb");
+  if (!f) return W2D_ERR_ARG;
+  ok = fread(in.data(), sizeof(double), in.size(), f) == in.size();
+  char extra;
+  ok = ok && fread(&extra, 1, 1, f) == 0;   // nothing may follow the last leaf
+  fclose(f);
+  if (!ok) return W2D_ERR_ARG;
+  for (size_t q = 0; q < ids.size(); ++q) {   // u(nb, eq, i, j) order -> [eq][j][i]
+    const double* src = in.data() + q * bs;
+    double* dst = u.data() + q * bs;
+    for (int j = 0; j < W; ++j)
+      for (int i = 0; i < W; ++i)
+        for (int k = 0; k < neq; ++k) dst[((size_t)k * W + j) * W + i] = *src++;
+  }
+  std::fill(s->lp.begin(), s->lp.end(), 0);
+  std::fill(s->leaf.begin(), s->leaf.end(), 0);
+  std::fill(s->icoord.begin(), s->icoord.end(), 0);
+  for (int k = 1; k <= 8; ++k)
+    for (int nb = 1; nb <= nbmax; ++nb) s->LP(nb, k) = lp[(size_t)(k - 1) * nbmax + (nb - 1)];
+  for (int nb = 1; nb <= nbmax; ++nb) s->LEAF(nb) = lf[nb - 1] != 0;
+  for (int k = 1; k <= 2; ++k)
+    for (int nb = 1; nb <= nbmax; ++nb) s->IC(nb, k) = icd[(size_t)(k - 1) * nbmax + (nb - 1)];
+  s->nbmax = nbmax;
+  s->nbleafs = head[2];
+  s->time = time;
+  s->dt = 0.0;
+  s->dirty = true;
+  int rc = push_topology(s);
+  if (rc) return rc;
+  if ((rc = w2d_put_blocks(s->ctx, ids.data(), (int)ids.size(), u.data()))) return rc;
+  for (int k = 0; k < nadmesh && s->p.nlevs > 1; ++k)
+    if ((rc = admesh(s))) return rc;
+  return W2D_OK;
 }
 
 }  // extern "C"

@@ -185,7 +185,7 @@ def snr(nbroot: int = 10, nlevs: int = 6, n_amb: float = 1.0, t_amb: float = 1.0
     chi = 0) leaves the ambient density and deposits e_sn as heat only: a
     Sedov blast in physical units.  neq = 6 (neutral density, tracer)."""
     if nblocks is None:
-        nblocks = 60000
+        nblocks = 200000
     p = base_params(neq=6, npas=2, nlevs=nlevs, nbroot_x=nbroot, nbroot_y=nbroot, nblocks=nblocks,
                     cooling=COOLINGH, tol=tol, precision=precision, **kw)
     sc = scalings(size_pc * PC, p.xmax, p.cv)
