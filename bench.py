@@ -349,59 +349,96 @@ def _dmc_table():
     return rows[:, 0], rows[:, 1]
 
 
+VARIANT_PRE_STEPS = {"snr": 4000, "jet_dmc": 15000}
+
+
 def variants_measure(args, nn_h):
     """The remnant with coolingh (10x10 roots, 6 levels) and the DMC jet
-    (32x8 roots, 7 levels): the plain FP64 path against the FP32 path with
+    (32x8 roots, 7 levels) at a developed state: one FP64 run is advanced
+    from the initial conditions (untimed; the jet to ~10k leaves) and saved
+    as the reference's BIN files; the plain FP64 path and the FP32 path with
     the learned cooling (coolingh network from the batched section; a
-    coolingdmc network trained here), same step count, density L1 on the
-    leaves both runs share."""
+    coolingdmc network trained here) both warm-start from those files, take
+    the autotuner's steps and 3 more, then the timed steps (CUDA events per
+    step, L2 flushed before each); density L1 on the leaves both runs
+    share."""
+    import shutil
+    import tempfile
+
     import numpy as np
 
     from walicxe2d_b200.api import Simulation, Surrogate
     from walicxe2d_b200.params import config
     log_t, neg_l = _dmc_table()
+    steps = min(args.steps, 30)
     out = {}
-    for name, cfg, steps in (("snr", "snr", 30), ("jet_dmc", "jet_dmc", 30)):
-        p, ic = config(cfg)
-        nn = nn_h
-        if cfg == "jet_dmc":
-            nn = Surrogate(5)
-            nn.samples_dmc(2_000_000, log_t, neg_l, p, seed=20261205)
-            nn.train(30, batch=8192, lr=2e-3, lr_end=2e-5)
-        res, st = {}, {}
-        for prec in (64, 32):
-            q = p.copy()
-            q.precision = prec
-            sim = Simulation(q, ic)
-            if cfg == "jet_dmc":
-                sim.set_cooltab(log_t, neg_l)
-            if prec == 32:
-                sim.ctx.set_surrogate(nn)
-            sim.run(5)
-            sim.ctx.sync()
-            s0 = sim.status()
-            sim.ctx.event_record(0)
-            sim.run(steps)
-            sim.ctx.event_record(1)
-            ms = sim.ctx.event_elapsed(0, 1)
-            s1 = sim.status()
-            r = {"value": (s1["zone_updates"] - s0["zone_updates"]) / (ms / 1000.0), "ms_per_step": ms / steps,
-                 "leaves": s1["nleaf"]}
-            if prec == 32:
-                sv, ex = sim.ctx.surrogate_counts()
-                r["cells_served_by_network"] = sv / max(sv + ex, 1)
-            res["fp64" if prec == 64 else "fp32nn"] = r
-            lp, lf, icd, ib = sim.tree()
-            ids = np.nonzero(lf)[0].astype(np.int32)
-            st[prec] = (ids, sim.ctx.get_blocks(ids)[:, 0, 2:18, 2:18])
-            sim.close()
-        common, xa, xb = np.intersect1d(st[64][0], st[32][0], return_indices=True)
-        a, b = st[64][1][xa], st[32][1][xb]
-        res["density_l1_vs_fp64"] = float(np.abs(b - a).sum() / max(np.abs(a).sum(), 1e-300))
-        res["same_tree"] = bool(len(common) == len(st[64][0]) == len(st[32][0]))
-        res["steps"] = steps
-        res["ratio"] = res["fp32nn"]["value"] / res["fp64"]["value"]
-        out[name] = res
+    tmp = tempfile.mkdtemp(prefix="w2d_bin_")
+    try:
+        for name in ("snr", "jet_dmc"):
+            p, ic = config(name)
+            nn = nn_h
+            if name == "jet_dmc":
+                nn = Surrogate(5)
+                nn.samples_dmc(2_000_000, log_t, neg_l, p, seed=20261205)
+                nn.train(30, batch=8192, lr=2e-3, lr_end=2e-5)
+            base = Simulation(p, ic)
+            if name == "jet_dmc":
+                base.set_cooltab(log_t, neg_l)
+            base.ctx.set_graphs(True)
+            t0 = time.perf_counter()
+            base.run(VARIANT_PRE_STEPS[name])
+            pre_s = time.perf_counter() - t0
+            files = (os.path.join(tmp, f"pointers_{name}.bin"), os.path.join(tmp, f"blocks_{name}.bin"))
+            base.write_bin(*files)
+            b0 = base.status()
+            base.close()
+            res, st = {}, {}
+            for prec in (64, 32):
+                q = p.copy()
+                q.precision = prec
+                sim = Simulation(q, ic)
+                if name == "jet_dmc":
+                    sim.set_cooltab(log_t, neg_l)
+                sim.read_bin(*files, time=b0["time"])
+                if prec == 32:
+                    sim.ctx.set_surrogate(nn)
+                sim.ctx.set_graphs(True)
+                sim.ctx.autotune(2)
+                _finish_tuning(sim, sim.ctx, 0)
+                sim.run(3)
+                sim.ctx.sync()
+                s0 = sim.status()
+                c0 = sim.ctx.surrogate_counts() if prec == 32 else (0, 0)
+                ms = 0.0
+                for _ in range(steps):
+                    sim.ctx.flush_l2()
+                    sim.ctx.event_record(0)
+                    sim.run(1)
+                    sim.ctx.event_record(1)
+                    ms += sim.ctx.event_elapsed(0, 1)
+                s1 = sim.status()
+                r = {"value": (s1["zone_updates"] - s0["zone_updates"]) / (ms / 1000.0),
+                     "ms_per_step": ms / steps, "leaves": s1["nleaf"], "steps_after_warm_start": s1["steps"]}
+                if prec == 32:
+                    c1 = sim.ctx.surrogate_counts()
+                    sv, ex = c1[0] - c0[0], c1[1] - c0[1]
+                    r["cells_served_by_network"] = sv / max(sv + ex, 1)
+                res["fp64" if prec == 64 else "fp32nn"] = r
+                lp, lf, icd, ib = sim.tree()
+                ids = np.nonzero(lf)[0].astype(np.int32)
+                st[prec] = (ids, sim.ctx.get_blocks(ids)[:, 0, 2:18, 2:18])
+                sim.close()
+            common, xa, xb = np.intersect1d(st[64][0], st[32][0], return_indices=True)
+            a, b = st[64][1][xa], st[32][1][xb]
+            res["density_l1_vs_fp64"] = float(np.abs(b - a).sum() / max(np.abs(a).sum(), 1e-300))
+            res["same_tree"] = bool(len(common) == len(st[64][0]) == len(st[32][0]))
+            res["timed_steps"] = steps
+            res["warm_start"] = {"fp64_steps_from_ic": VARIANT_PRE_STEPS[name], "leaves": b0["nleaf"],
+                                 "time_code_units": b0["time"], "untimed_s": pre_s}
+            res["ratio"] = res["fp32nn"]["value"] / res["fp64"]["value"]
+            out[name] = res
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
     return out
 
 

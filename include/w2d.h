@@ -57,6 +57,9 @@ extern "C" {
 #define W2D_USERBC_NONE 0
 #define W2D_USERBC_JET  1   /* -DOTHERB with impose_jet, src/jet.f90:41 */
 
+#define W2D_GEOM_CARTESIAN   0
+#define W2D_GEOM_CYLINDRICAL 1  /* -DCYLINDRICAL: x -> z, y -> r, source terms of src/step.f90:42-78 */
+
 /* Reproduce the reference's known defects (default: both on).             */
 #define W2D_COMPAT_HLLC_STAR 1  /* primr(4)/(primr(4)*srmur): hllcfluxes.f90:157 */
 #define W2D_COMPAT_OUTFYB    2  /* u(nb,...) with nb the list index: boundaryI.f90:87 */
@@ -77,7 +80,7 @@ typedef struct W2dParams {
   int32_t otherb;     /* W2D_USERBC_*                                        */
   int32_t compat;     /* W2D_COMPAT_* bit set                                */
   int32_t precision;  /* 64 (plain FP64 path) or 32 (FP32 state and fluxes)  */
-  int32_t pad_;
+  int32_t geometry;   /* W2D_GEOM_* (JET/Makefile:39 CYLINDRICAL)             */
   double cv, gamma, cfl, eta;      /* src/parameters.f90:39,61-63           */
   double xmax, ymax;               /* box size, code units                   */
   double tempsc, psc, tsc, rsc;    /* scalings, src/parameters.f90:50-54     */

@@ -356,16 +356,37 @@ static int fluxes_block(OrcSim* s, int nb, int choice, double* f, double* g,
   return 0;
 }
 
-/* src/step.f90:5-40 (no CYLINDRICAL) */
+/* src/step.f90:46-73 (prims): geometric source terms of cylindrical
+ * coordinates (y -> r, x -> z) from the global primit of cell (i,j) */
+static void prims_cell(OrcSim* s, int nb, int i, int j, double* S)
+{
+  const W2dParams* p = &s->p;
+  const int lev = LP(s, nb, 1);
+  double radius = ((double)(j + IC(s, nb, 2)) - 0.5) * s->dy[lev];
+  double rho = PR(s, nb, 0, i, j);
+  double H = 0.5 * rho * (PR(s, nb, 1, i, j) * PR(s, nb, 1, i, j)
+                          + PR(s, nb, 2, i, j) * PR(s, nb, 2, i, j))
+             + (p->cv + 1.) * PR(s, nb, 3, i, j);
+  S[0] = -(rho * PR(s, nb, 2, i, j) / radius);
+  S[1] = -(rho * PR(s, nb, 1, i, j) * PR(s, nb, 2, i, j) / radius);
+  S[2] = -(rho * PR(s, nb, 2, i, j) * PR(s, nb, 2, i, j) / radius);
+  S[3] = -(H * PR(s, nb, 2, i, j) / radius);
+  for (int k = 4; k < p->neq; ++k) S[k] = -(PR(s, nb, k, i, j) * PR(s, nb, 2, i, j) / radius);
+}
+
+/* src/step.f90:5-40 */
 static void step_block(OrcSim* s, int nb, double dt, const double* f, const double* g)
 {
   const W2dParams* p = &s->p;
   const int neq = p->neq, nx = p->nx, ny = p->ny, F = nx + 1;
   const int lev = LP(s, nb, 1);
+  const int cyl = p->geometry == W2D_GEOM_CYLINDRICAL;
   double dtdx = dt / s->dx[lev];
   double dtdy = dt / s->dy[lev];
+  double S[W2D_MAXEQ];
   for (int i = 1; i <= nx; ++i)
     for (int j = 1; j <= ny; ++j) {
+      if (cyl) prims_cell(s, nb, i, j, S);
       int im = i - 1, jm = j - 1;
       for (int k = 0; k < neq; ++k) {
         double fi = f[(k * (ny + 1) + j) * F + i];
@@ -373,6 +394,7 @@ static void step_block(OrcSim* s, int nb, double dt, const double* f, const doub
         double gj = g[(k * (ny + 1) + j) * F + i];
         double gjm = g[(k * (ny + 1) + jm) * F + i];
         UP(s, nb, k, i, j) = U(s, nb, k, i, j) - dtdx * (fi - fim) - dtdy * (gj - gjm);
+        if (cyl) UP(s, nb, k, i, j) = UP(s, nb, k, i, j) + dt * S[k];
       }
     }
 }

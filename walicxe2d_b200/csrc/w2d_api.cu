@@ -240,6 +240,7 @@ PhysArgs pargs(W2dCtx* c)
   pa.hllc_compat = (c->p.compat & W2D_COMPAT_HLLC_STAR) ? 1 : 0;
   pa.solver = c->p.solver;
   pa.limiter = c->p.limiter;
+  pa.cyl = c->p.geometry == W2D_GEOM_CYLINDRICAL;
   return pa;
 }
 
@@ -576,7 +577,8 @@ int w2d_create(const W2dParams* p, W2dCtx** out)
       p->nlevs < 1 || p->nlevs > W2D_MAXLEV || p->nblocks < 1 || p->solver < 0 || p->solver > 2 ||
       p->limiter < -1 || p->limiter > 6 || p->cooling < 0 || p->cooling > 2 ||
       (p->cooling == W2D_COOLINGH && p->neq < 5) || (p->precision != 64 && p->precision != 32) ||
-      (p->otherb != W2D_USERBC_NONE && p->otherb != W2D_USERBC_JET))
+      (p->otherb != W2D_USERBC_NONE && p->otherb != W2D_USERBC_JET) ||
+      (p->geometry != W2D_GEOM_CARTESIAN && p->geometry != W2D_GEOM_CYLINDRICAL))
     return W2D_ERR_ARG;
   W2dCtx* c = new W2dCtx();
   c->p = *p;

@@ -219,7 +219,7 @@ bool same_physics(const W2dParams& a, const W2dParams& b)
          a.limiter == b.limiter && a.cooling == b.cooling && a.bc_left == b.bc_left && a.bc_right == b.bc_right &&
          a.bc_bottom == b.bc_bottom && a.bc_top == b.bc_top && a.otherb == b.otherb && a.compat == b.compat &&
          a.precision == b.precision && a.cv == b.cv && a.gamma == b.gamma && a.cfl == b.cfl && a.eta == b.eta &&
-         a.tempsc == b.tempsc && a.psc == b.psc && a.tsc == b.tsc;
+         a.tempsc == b.tempsc && a.psc == b.psc && a.tsc == b.tsc && a.geometry == b.geometry;
 }
 
 }  // namespace

@@ -126,6 +126,7 @@ enum { FD_SRC1_JET = 1 << 16, FD_SRC2_JET = 1 << 17, FD_DST_JET = 1 << 18 };
 struct PhysArgs {
   double cv, gamma, tempsc;
   int cooling, hllc_compat, solver, limiter;
+  int cyl;   // CYLINDRICAL geometric source terms in step
 };
 
 __device__ __forceinline__ int cidx(int i, int j) { return (j + 1) * W2D_W + (i + 1); }
@@ -534,6 +535,29 @@ __device__ __forceinline__ void block_stats(const R (*sp)[W2D_W][W2D_W], const P
   }
 }
 
+// Geometric source terms of cylindrical coordinates (x -> z, y -> r) for
+// cell (ti, tj) of a primitive tile, src/step.f90:46-73 (prims): with
+// r = (j + icoord(nb,2) - 0.5) dy(lev) and H = rho (vz^2 + vr^2)/2 +
+// (cv + 1) p, S = -(rho, rho vz, rho vr, H, passives) vr / r, each product
+// formed left to right as the reference writes it.
+template <typename R, int NEQ>
+__device__ __forceinline__ void cyl_sources(const R (*st)[W2D_W][W2D_W], int ti, int tj, R radius, R cv, R* S)
+{
+  const R rho = st[0][tj][ti], vz = st[1][tj][ti], vr = st[2][tj][ti], p = st[3][tj][ti];
+  const R H = R(0.5) * rho * (vz * vz + vr * vr) + (cv + R(1.)) * p;
+  S[0] = -(rho * vr / radius);
+  S[1] = -(rho * vz * vr / radius);
+  S[2] = -(rho * vr * vr / radius);
+  S[3] = -(H * vr / radius);
+#pragma unroll
+  for (int k = 4; k < NEQ; ++k) S[k] = -(st[k][tj][ti] * vr / radius);
+}
+
+__device__ __forceinline__ double cyl_radius(const KArgs& a, int b, int lev, int j)
+{
+  return ((double)(j + a.icoord[2 * b + 1]) - 0.5) * geo_dy(a, b, lev);
+}
+
 // ---------------------------------------------------------------------------
 // Half step: src/tstep.f90:22-46 -- hllcfluxes(nb,1) from primit (cells
 // 0..17) and step(nb,dt/2) into up.  Primitives come from u (ADIABATIC,
@@ -615,11 +639,14 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_half(KArgs a, P
 
   if (tid < 256) {  // src/step.f90:20-40
     const int i = 1 + tid % 16, j = 1 + tid / 16;
+    R S[NEQ];
+    if (pa.cyl) cyl_sources<R, NEQ>(st, i + 1, j + 1, R(cyl_radius(a, b, lev, j)), ph.cv, S);
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) {
       const R uo = u[k * W2D_CELLS + cidx(i, j)];
-      up[k * W2D_CELLS + cidx(i, j)] =
-          uo - dtdx * (sf[k][j - 1][i] - sf[k][j - 1][i - 1]) - dtdy * (sg[k][j][i - 1] - sg[k][j - 1][i - 1]);
+      R v = uo - dtdx * (sf[k][j - 1][i] - sf[k][j - 1][i - 1]) - dtdy * (sg[k][j][i - 1] - sg[k][j - 1][i - 1]);
+      if (pa.cyl) v = v + R(dtm) * S[k];
+      up[k * W2D_CELLS + cidx(i, j)] = v;
     }
   }
   leaf_end();
@@ -749,10 +776,13 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_full(KArgs a, P
   if (tid < 256) {
     const int i = 1 + tid % 16, j = 1 + tid / 16;
     const int ti = i + 1, tj = j + 1;
+    R S[NEQ];
+    if (pa.cyl) cyl_sources<R, NEQ>(st, ti, tj, R(cyl_radius(a, b, lev, j)), ph.cv, S);
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) {
       const R uo = so[k][tj][ti];
       R v = uo - dtdx * (sf[k][j - 1][i] - sf[k][j - 1][i - 1]) - dtdy * (sg[k][j][i - 1] - sg[k][j - 1][i - 1]);
+      if (pa.cyl) v = v + R(dtb) * S[k];   // src/step.f90:35-36, before viscosity
       if (visc)
         v = v + eta * (so[k][tj][ti + 1] + so[k][tj][ti - 1] + so[k][tj + 1][ti] + so[k][tj - 1][ti] - R(4.) * uo);
       u[k * W2D_CELLS + cidx(i, j)] = v;

@@ -15,6 +15,7 @@ HLLC, HLL, HLL_HLLC = 0, 1, 2
 ADIABATIC, COOLINGH, COOLINGDMC = 0, 1, 2
 BC_OUTFLOW, BC_REFLECTIVE = 0, 1
 USERBC_NONE, USERBC_JET = 0, 1
+GEOM_CARTESIAN, GEOM_CYLINDRICAL = 0, 1   # JET/Makefile:39 CYLINDRICAL
 COMPAT_HLLC_STAR = 1   # src/hllcfluxes.f90:157
 COMPAT_OUTFYB = 2      # src/boundaryI.f90:87
 IC_SEDOV, IC_SNR, IC_JET = 0, 1, 2
@@ -36,7 +37,7 @@ class W2dParams(C.Structure):
         ("nblocks", C.c_int32), ("solver", C.c_int32), ("limiter", C.c_int32),
         ("cooling", C.c_int32), ("bc_left", C.c_int32), ("bc_right", C.c_int32),
         ("bc_bottom", C.c_int32), ("bc_top", C.c_int32), ("otherb", C.c_int32),
-        ("compat", C.c_int32), ("precision", C.c_int32), ("pad_", C.c_int32),
+        ("compat", C.c_int32), ("precision", C.c_int32), ("geometry", C.c_int32),
         ("cv", C.c_double), ("gamma", C.c_double), ("cfl", C.c_double), ("eta", C.c_double),
         ("xmax", C.c_double), ("ymax", C.c_double),
         ("tempsc", C.c_double), ("psc", C.c_double), ("tsc", C.c_double), ("rsc", C.c_double),
@@ -93,6 +94,7 @@ def base_params(**kw) -> W2dParams:
     p.otherb = USERBC_NONE
     p.compat = COMPAT_HLLC_STAR | COMPAT_OUTFYB
     p.precision = 64
+    p.geometry = GEOM_CARTESIAN
     p.cv = 1.5
     sc = scalings(3.0e17, 1.0, p.cv)
     p.gamma = sc["gamma"]
@@ -173,6 +175,44 @@ def jet(nbroot_x: int = 32, nbroot_y: int = 8, nlevs: int = 7, cooling: int = CO
     return p, ic
 
 
+def jet_cyl(nlevs: int = 7, nbroot_x: int = 4, nbroot_y: int = 1, cooling: int = COOLINGDMC,
+            nblocks: int | None = None, rj_cm: float = 1.0e15, **kw):
+    """The reference's shipped jet set-up in cylindrical coordinates
+    (JET/Makefile:27-62, src/parameters.f90, src/jet.f90:16-33,
+    src/user_mod.f90:39-62): x -> z, y -> r; box 3e17 x 0.75e17 cm (xmax 1,
+    ymax 0.25) of 4 x 1 roots; HLLC, limiter 2, cfl 0.7, DMC cooling,
+    passives (neutral density, tracer); reflective left wall and axis,
+    outflow right and top; ambient 15 cm^-3 at 1e3 K; the jet, 5000 cm^-3 at
+    1e3 K with radius and length rj_cm, on the axis at z = 0 with
+    v = 250 + 30 sin(2 pi t / 30 yr) km/s."""
+    p, ic = jet(nbroot_x=nbroot_x, nbroot_y=nbroot_y, nlevs=nlevs, cooling=cooling, nblocks=nblocks,
+                rj_cm=rj_cm, **kw)
+    p.geometry = GEOM_CYLINDRICAL
+    p.limiter = 2
+    p.cfl = 0.7
+    p.bc_left = p.bc_bottom = BC_REFLECTIVE
+    p.bc_right = p.bc_top = BC_OUTFLOW
+    sc = scalings(3.0e17, p.xmax, p.cv)
+    p.tempsc, p.psc, p.tsc, p.rsc = sc["tempsc"], sc["psc"], sc["tsc"], sc["rsc"]
+    vsc = math.sqrt(sc["vsc2"])
+    p.jet_rj = rj_cm / sc["rsc"]
+    p.jet_lj = rj_cm / sc["rsc"]
+    p.jet_posx, p.jet_posy = 0.0, 0.0
+    p.jet_den = 5000.0
+    p.jet_temp = 1.0e3 / sc["tempsc"]
+    p.jet_v0 = 250.0e5 / vsc
+    p.jet_dv = 30.0e5 / vsc
+    p.jet_tau = 30.0 * YR / sc["tsc"]
+    ic.rho0, ic.p0 = 15.0, 1.0e3
+    # the jet (1e15 cm) is narrower than a root cell: start from the finest
+    # level everywhere (the reference's basegrid forces refinement along the
+    # axis, src/basegrid.f90:113-160) and let the four startup admesh passes
+    # of src/main.f90:59-62 coarsen the rest
+    ic.init_levels = nlevs
+    ic.startup_admesh = 4 if nlevs > 1 else 0
+    return p, ic
+
+
 def snr(nbroot: int = 10, nlevs: int = 6, n_amb: float = 1.0, t_amb: float = 1.0e4, xh: float = 0.9,
         e_sn: float = 1.0e51, m_sn: float = 4.0 * MSUN, r_sn: float = 1.0 * PC, chi: float = 0.5,
         size_pc: float = 40.0, nblocks: int | None = None, tol: float = 0.1, precision: int = 64, **kw):
@@ -248,6 +288,15 @@ def config(name: str):
         return jet(nbroot_x=8, nbroot_y=2, nlevs=3, cooling=COOLINGDMC, nblocks=4000, rj_cm=8.0e15)
     if name == "jet_dmc":
         return jet()
+    if name == "jet_cyl":
+        return jet_cyl()
+    if name == "jet_cyl_small":
+        return jet_cyl(nlevs=5, nblocks=4000)
+    if name == "sedov_cyl_small":
+        p, ic = sedov(nbroot=4, nlevs=3, tol=0.1, nblocks=4000)
+        p.geometry = GEOM_CYLINDRICAL
+        p.bc_bottom = BC_REFLECTIVE
+        return p, ic
     if name == "snr":
         return snr()
     if name == "snr_small":
