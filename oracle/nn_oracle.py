@@ -3,7 +3,9 @@
 Used by tests/ to check the device training kernel's loss and gradients and
 the forward pass.  The library never imports this module.
 
-The network is 4 -> 64 -> 64 -> 2 with tanh hidden layers; parameters are a
+The network is 4 -> 64 -> 64 -> 2; hidden layer 1 uses the cubic saturating
+activation g(x) = y (1 - y^2/12), y = clamp(x, -2, 2), hidden layer 2
+uses tanh; parameters are a
 flat vector (W1 [64][4], b1, W2 [64][64], b2, W3 [2][64], b3).  The device
 computes its matrix products on BF16 operands with FP32 accumulation; with
 ``bf16=True`` this restatement rounds the same operands to BF16 (round to
@@ -51,12 +53,13 @@ def forward(p, X, bf: bool = True):
     r = bf16 if bf else (lambda a: np.asarray(a, np.float64))
     W1, b1, W2, b2, W3, b3 = unpack(p)
     Xb = r(X)
-    H1 = np.tanh(Xb @ r(W1).T + b1)
+    Y1 = np.clip(Xb @ r(W1).T + b1, -2.0, 2.0)
+    H1 = Y1 * (1.0 - Y1 * Y1 / 12.0)
     H1b = r(H1)
     H2 = np.tanh(H1b @ r(W2).T + b2)
     H2b = r(H2)
     O = H2b @ r(W3).T + b3
-    return O, (Xb, H1, H1b, H2, H2b)
+    return O, (Xb, Y1, H1b, H2, H2b)
 
 
 def loss_grad(p, X, Y, bf: bool = True):
@@ -65,7 +68,7 @@ def loss_grad(p, X, Y, bf: bool = True):
     r = bf16 if bf else (lambda a: np.asarray(a, np.float64))
     _, b1, W2, b2, W3, b3 = unpack(p)
     n = X.shape[0]
-    O, (Xb, H1, H1b, H2, H2b) = forward(p, X, bf)
+    O, (Xb, Y1, H1b, H2, H2b) = forward(p, X, bf)
     E = O - Y
     wt = np.array([1.0, LOSS_W1])
     loss = float((E * E * wt).sum() / n)
@@ -73,7 +76,7 @@ def loss_grad(p, X, Y, bf: bool = True):
     dOb = r(dO)
     dZ2 = (dOb @ r(W3)) * (1.0 - H2 * H2)
     dZ2b = r(dZ2)
-    dZ1 = (dZ2b @ r(W2)) * (1.0 - H1 * H1)
+    dZ1 = (dZ2b @ r(W2)) * (1.0 - Y1 * Y1 / 4.0)
     dZ1b = r(dZ1)
     g = np.zeros(NPARAM)
     g[P_W1:P_B1] = (dZ1b.T @ Xb).ravel()

@@ -247,13 +247,15 @@ __global__ void __launch_bounds__(128, 1) k_nn_train(const float* __restrict__ f
     if (!(ok = nn_wait(&s.bar, phase, err))) break;
     float h1[NN_H], h2[NN_H], v[NN_H];
     nn_ld64(tm, C_Z1, v);
+    // h1 holds the clamped pre-activation y of layer 1 (its gradient needs y)
 #pragma unroll
     for (int k = 0; k < NN_H; ++k) {
-      h1[k] = nn_tanh(v[k] + s.f.b1[k]);
-      s.h1t[tc_off(k, tid, 128) >> 1] = f2bf(h1[k]);
+      h1[k] = nn_clamp2(v[k] + s.f.b1[k]);
+      v[k] = nn_cubic(h1[k]);
+      s.h1t[tc_off(k, tid, 128) >> 1] = f2bf(v[k]);
     }
 #pragma unroll
-    for (int k = 0; k < NN_H; k += 8) nn_put8(s.f.h1, tid, k, NN_H, h1 + k);
+    for (int k = 0; k < NN_H; k += 8) nn_put8(s.f.h1, tid, k, NN_H, v + k);
     nn_sync();
     if (tid == 0) {
       nn_layer_mma(tm + C_Z2, 0, s.f.h1, s.f.w2, NN_H, NN_H);
@@ -318,7 +320,7 @@ __global__ void __launch_bounds__(128, 1) k_nn_train(const float* __restrict__ f
     nn_ld64(tm, C_Z1, v);
 #pragma unroll
     for (int k = 0; k < NN_H; ++k) {
-      const float dz = v[k] * (1.f - h1[k] * h1[k]);
+      const float dz = v[k] * nn_cubic_grad(h1[k]);
       s.dz1t[tc_off(k, tid, 128) >> 1] = f2bf(dz);
       v[k] = dz;
     }
@@ -453,7 +455,7 @@ __global__ void __launch_bounds__(128, 1) k_nn_forward(const float* __restrict__
     float v[NN_H];
     nn_ld64(tm, 0, v);
 #pragma unroll
-    for (int k = 0; k < NN_H; ++k) v[k] = nn_tanh(v[k] + s.b1[k]);
+    for (int k = 0; k < NN_H; ++k) v[k] = nn_cubic(nn_clamp2(v[k] + s.b1[k]));
 #pragma unroll
     for (int k = 0; k < NN_H; k += 8) nn_put8(s.h1, tid, k, NN_H, v + k);
     nn_sync();
@@ -664,7 +666,7 @@ __global__ void __launch_bounds__(256, 4) k_cool_nn(KArgs a, PhysArgs pa, double
     for (int c0 = 0; c0 < NN_H; c0 += 16) {   // 16 columns at a time keeps few registers live
       tc_ld16(tc_addr(tm, lane0, c0), v);
 #pragma unroll
-      for (int k = 0; k < 16; ++k) v[k] = nn_tanh(v[k] + s.b1[c0 + k]);
+      for (int k = 0; k < 16; ++k) v[k] = nn_cubic(nn_clamp2(v[k] + s.b1[c0 + k]));
       nn_put8(ss.h, row, c0, NN_H, v);
       nn_put8(ss.h, row, c0 + 8, NN_H, v + 8);
     }

@@ -2,8 +2,12 @@
 // target maps, and the forward pass of one 128-cell tile on the tensor
 // cores (shared by training, evaluation and the cooling kernel).
 //
-// Network: 4 -> 64 -> 64 -> 2, tanh hidden layers, BF16 weights and
-// activations as MMA operands, FP32 accumulation in tensor memory.
+// Network: 4 -> 64 -> 64 -> 2, BF16 weights and activations as MMA
+// operands, FP32 accumulation in tensor memory.  Hidden layer 1 uses a
+// cubic saturating activation evaluated on the FMA pipe, hidden layer 2
+// the hardware tanh on the XU pipe, so that the two pipes share the
+// activation work (the XU pipe, 16 lanes per SM and clock, bounded the
+// surrogate when both layers used tanh).
 // Inputs (log n, log T, neutral fraction, log dt) map to [-1, 1]:
 //   f0 = (log10 n - 1)/3      n  in [1e-2, 1e4] cm^-3
 //   f1 = (log10 T - 5)/3      T  in [1e2, 1e8] K
@@ -47,15 +51,22 @@ struct NNImage {
   float b1[NN_H], b2[NN_H], b3[NN_NOUT];
 };
 
-// hidden-layer activation: the hardware tanh (tanh.approx.f32, relative
-// error about 2^-11, below the BF16 rounding of the activations that
-// follows); training and inference use the same instruction
+// hidden layer 2: the hardware tanh (tanh.approx.f32, relative error about
+// 2^-11, below the BF16 rounding of the activations that follows);
+// training and inference use the same instruction
 __device__ __forceinline__ float nn_tanh(float x)
 {
   float y;
   asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
+
+// hidden layer 1: g(x) = y (1 - y^2/12) with y = clamp(x, -2, 2), a
+// smooth (C1) saturating cubic, |g| <= 4/3, g'(x) = 1 - y^2/4 (zero where
+// x is clamped).  nn_clamp2 gives y, the backward pass keeps it.
+__device__ __forceinline__ float nn_clamp2(float x) { return fminf(fmaxf(x, -2.f), 2.f); }
+__device__ __forceinline__ float nn_cubic(float y) { return y * fmaf(y * y, -1.f / 12.f, 1.f); }
+__device__ __forceinline__ float nn_cubic_grad(float y) { return fmaf(y * y, -0.25f, 1.f); }
 
 __device__ __forceinline__ uint16_t f2bf(float x)
 {
