@@ -27,6 +27,8 @@
 
 #include <cstdint>
 
+#include <cuda_bf16.h>
+
 #include "w2d_tc.cuh"
 
 namespace w2d {
@@ -189,16 +191,21 @@ __device__ __forceinline__ void nn_load_weights(NNFwdSmem& s, const NNImage* img
   for (int k = threadIdx.x; k < NN_NOUT; k += blockDim.x) s.b3[k] = img->b3[k];
 }
 
+// Two floats as a packed BF16 pair (round to nearest even, a in the low
+// half) with one conversion instruction: conversions run on the XU pipe,
+// which the surrogate's epilogues share with tanh.
+__device__ __forceinline__ uint32_t bf2(float a, float b)
+{
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
 // Eight consecutive columns c0 .. c0+7 (c0 a multiple of 8) of row r of a
 // K-major operand as one 16-byte store: one core-matrix row, so the 32
 // rows of a warp land in four 128-byte lines without bank conflicts.
 __device__ __forceinline__ void nn_put8(uint16_t* base, int r, int c0, int K, const float* v)
 {
-  uint4 w;
-  w.x = (uint32_t)f2bf(v[0]) | ((uint32_t)f2bf(v[1]) << 16);
-  w.y = (uint32_t)f2bf(v[2]) | ((uint32_t)f2bf(v[3]) << 16);
-  w.z = (uint32_t)f2bf(v[4]) | ((uint32_t)f2bf(v[5]) << 16);
-  w.w = (uint32_t)f2bf(v[6]) | ((uint32_t)f2bf(v[7]) << 16);
+  const uint4 w = make_uint4(bf2(v[0], v[1]), bf2(v[2], v[3]), bf2(v[4], v[5]), bf2(v[6], v[7]));
   *reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(base) + tc_off(r, c0, K)) = w;
 }
 
