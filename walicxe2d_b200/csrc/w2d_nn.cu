@@ -650,11 +650,7 @@ __global__ void __launch_bounds__(256, 4) k_cool_nn(KArgs a, PhysArgs pa, double
       if (KIND == COOL_DMC) f[2] = f[3] = 0.f;   // as in the coolingdmc training set
       inr = cools && nn_in_range(f);
     }
-    {
-      const float z[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      nn_put8(ss.x, row, 0, NN_KIN, f);     // f[4..7] are zero
-      nn_put8(ss.x, row, 8, NN_KIN, z);
-    }
+    nn_put_feat(ss.x, row, f);
     wg_sync(wg);
     if (row == 0) {
       nn_layer_mma(tm, 0, ss.x, s.w1, NN_KIN, NN_H);

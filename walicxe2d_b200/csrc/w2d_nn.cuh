@@ -209,14 +209,17 @@ __device__ __forceinline__ void nn_put8(uint16_t* base, int r, int c0, int K, co
   *reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(base) + tc_off(r, c0, K)) = w;
 }
 
-// Row r of the tile: features into x (bf16, zero padding).
-__device__ __forceinline__ void nn_put_x(NNFwdSmem& s, int r, const float* f)
+// Row r of a features operand (K = NN_KIN): f0..f3 in BF16, the padding
+// zero (written as zero words, no conversions).
+__device__ __forceinline__ void nn_put_feat(uint16_t* x, int r, const float* f)
 {
-  const float v[8] = {f[0], f[1], f[2], f[3], 0.f, 0.f, 0.f, 0.f};
-  const float z[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  nn_put8(s.x, r, 0, NN_KIN, v);
-  nn_put8(s.x, r, 8, NN_KIN, z);
+  uint8_t* b = reinterpret_cast<uint8_t*>(x);
+  *reinterpret_cast<uint4*>(b + tc_off(r, 0, NN_KIN)) = make_uint4(bf2(f[0], f[1]), bf2(f[2], f[3]), 0u, 0u);
+  *reinterpret_cast<uint4*>(b + tc_off(r, 8, NN_KIN)) = make_uint4(0u, 0u, 0u, 0u);
 }
+
+// Row r of the tile: features into x (bf16, zero padding).
+__device__ __forceinline__ void nn_put_x(NNFwdSmem& s, int r, const float* f) { nn_put_feat(s.x, r, f); }
 
 // MMAs of one layer: D (TMEM column col) = A[128 x K] B[N x K]^T.
 __device__ __forceinline__ void nn_layer_mma(uint32_t tmem, int col, const uint16_t* a, const uint16_t* b, int K,
