@@ -93,11 +93,17 @@ class Context:
         assert u.shape == (ids.size, self.neq, W, W)
         self._check(self.L.w2d_put_blocks(self.h, _pi32(ids), ids.size, _pd(u)), "w2d_put_blocks")
 
-    def get_blocks(self, ids) -> np.ndarray:
+    def get_blocks(self, ids, out: np.ndarray | None = None) -> np.ndarray:
+        """u of the blocks ids, block-major; into `out` (C-contiguous
+        float64 of shape (len(ids), neq, 20, 20), e.g. pinned memory) when
+        given."""
         ids = np.ascontiguousarray(ids, np.int32)
-        u = np.zeros((ids.size, self.neq, W, W))
-        self._check(self.L.w2d_get_blocks(self.h, _pi32(ids), ids.size, _pd(u)), "w2d_get_blocks")
-        return u
+        if out is None:
+            out = np.empty((ids.size, self.neq, W, W))
+        elif out.shape != (ids.size, self.neq, W, W) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("out must be C-contiguous float64 of shape (len(ids), neq, 20, 20)")
+        self._check(self.L.w2d_get_blocks(self.h, _pi32(ids), ids.size, _pd(out)), "w2d_get_blocks")
+        return out
 
     def get_primit(self, ids) -> np.ndarray:
         ids = np.ascontiguousarray(ids, np.int32)
@@ -311,12 +317,19 @@ class Simulation:
         ibr = ib[: 3 * nib].reshape(3, nib).T.copy() if nib else np.zeros((0, 3), np.int32)
         return lp2, lf2, ic2, ibr
 
-    def blocks(self, ids=None) -> tuple[np.ndarray, np.ndarray]:
-        """u of the given (default: all leaf) blocks, block-major."""
+    def leaf_ids(self) -> np.ndarray:
+        """IDs of the leaf blocks, ascending."""
+        lf = np.zeros(self.p.nblocks, np.int32)
+        self.L.w2d_sim_tree(self.h, None, _pi32(lf), None, None, None)
+        return (np.nonzero(lf)[0] + 1).astype(np.int32)
+
+    def blocks(self, ids=None, out: np.ndarray | None = None) -> tuple[np.ndarray, np.ndarray]:
+        """u of the given (default: all leaf) blocks, block-major; into
+        `out[:len(ids)]` when given (see Context.get_blocks)."""
         if ids is None:
-            _, lf, _, _ = self.tree()
-            ids = np.nonzero(lf)[0].astype(np.int32)
-        return np.asarray(ids, np.int32), self.ctx.get_blocks(ids)
+            ids = self.leaf_ids()
+        ids = np.asarray(ids, np.int32)
+        return ids, self.ctx.get_blocks(ids, None if out is None else out[: ids.size])
 
 
 class Ensemble:

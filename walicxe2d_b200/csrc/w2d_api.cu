@@ -255,21 +255,20 @@ int ensure_ids(W2dCtx* c, int n)
   return W2D_OK;
 }
 
+// Device staging of block transfers (FP64, block-major); grows by half
+// again each time so that a growing run reallocates rarely.  The host side
+// is the caller's own array: the copies run straight from and into it
+// (at full speed when the caller's memory is pinned).
 int ensure_stage(W2dCtx* c, size_t bytes)
 {
   if (bytes > c->stage_bytes) {
+    const size_t cap = std::max(bytes, c->stage_bytes + c->stage_bytes / 2);
     CK(cudaStreamSynchronize(c->st));
     if (c->d_stage) cudaFree(c->d_stage);
     c->d_stage = nullptr;
-    CK(cudaMalloc(&c->d_stage, bytes));
-    c->stage_bytes = bytes;
-  }
-  if (bytes > c->h_stage_bytes) {
-    CK(cudaStreamSynchronize(c->st));
-    if (c->h_stage) cudaFreeHost(c->h_stage);
-    c->h_stage = nullptr;
-    CK(cudaMallocHost(&c->h_stage, bytes));
-    c->h_stage_bytes = bytes;
+    c->stage_bytes = 0;
+    CK(cudaMalloc(&c->d_stage, cap));
+    c->stage_bytes = cap;
   }
   return W2D_OK;
 }
@@ -708,7 +707,7 @@ int w2d_destroy(W2dCtx* c)
                  c->d_flush, c->d_dtwork, c->d_dtcount, c->d_jetblk};
   for (void* d : dev)
     if (d) cudaFree(d);
-  void* host[] = {c->h_stage, c->h_small, c->h_grad, c->h_err, c->h_fd1[0], c->h_fd2[0], c->h_leaflist,
+  void* host[] = {c->h_small, c->h_grad, c->h_err, c->h_fd1[0], c->h_fd2[0], c->h_leaflist,
                   c->h_fd1[1], c->h_fd2[1], c->h_ops, c->lev, c->icoord, c->h_jetblk[0], c->h_jetblk[1]};
   for (void* h : host)
     if (h) cudaFreeHost(h);
@@ -847,15 +846,8 @@ int w2d_put_blocks(W2dCtx* c, const int32_t* ids, int n, const double* u)
   if (n == 0) return W2D_OK;
   int rc = valid_ids(c, ids, n);
   if (rc) return rc;
-  if ((rc = ensure_stage(c, (size_t)n * c->bs * c->elem)) || (rc = ensure_ids(c, n))) return rc;
-  CK(cudaStreamSynchronize(c->st));
-  if (c->elem == sizeof(double)) {
-    memcpy(c->h_stage, u, (size_t)n * c->bs * sizeof(double));
-  } else {
-    float* h = (float*)c->h_stage;
-    for (size_t k = 0; k < (size_t)n * c->bs; ++k) h[k] = (float)u[k];
-  }
-  CK(cudaMemcpyAsync(c->d_stage, c->h_stage, (size_t)n * c->bs * c->elem, cudaMemcpyHostToDevice, c->st));
+  if ((rc = ensure_stage(c, (size_t)n * c->bs * sizeof(double))) || (rc = ensure_ids(c, n))) return rc;
+  CK(cudaMemcpyAsync(c->d_stage, u, (size_t)n * c->bs * sizeof(double), cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(c->d_ids, ids, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st));
   if ((rc = launch(c, "scatter", [&] { return c->L->scatter(c->d_u, c->d_stage, c->d_ids, n, c->bs, c->st); })))
     return rc;
@@ -868,7 +860,7 @@ static int get_pool(W2dCtx* c, void* pool, const int32_t* ids, int n, double* u)
 {
   int rc = valid_ids(c, ids, n);
   if (rc) return rc;
-  if ((rc = ensure_stage(c, (size_t)n * c->bs * c->elem)) || (rc = ensure_ids(c, n))) return rc;
+  if ((rc = ensure_stage(c, (size_t)n * c->bs * sizeof(double))) || (rc = ensure_ids(c, n))) return rc;
   CK(cudaMemcpyAsync(c->d_ids, ids, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st));
   if (pool) {
     if ((rc = launch(c, "gather", [&] { return c->L->gather(pool, c->d_stage, c->d_ids, n, c->bs, c->st); })))
@@ -878,15 +870,8 @@ static int get_pool(W2dCtx* c, void* pool, const int32_t* ids, int n, double* u)
     if ((rc = launch(c, "to_prim", [&] { return c->L->to_prim(c->neq, pa, c->d_u, c->d_stage, c->d_ids, n, c->st); })))
       return rc;
   }
-  CK(cudaMemcpyAsync(c->h_stage, c->d_stage, (size_t)n * c->bs * c->elem, cudaMemcpyDeviceToHost, c->st));
-  if ((rc = sync_and_check(c))) return rc;
-  if (c->elem == sizeof(double)) {
-    memcpy(u, c->h_stage, (size_t)n * c->bs * sizeof(double));
-  } else {
-    const float* h = (const float*)c->h_stage;
-    for (size_t k = 0; k < (size_t)n * c->bs; ++k) u[k] = (double)h[k];
-  }
-  return W2D_OK;
+  CK(cudaMemcpyAsync(u, c->d_stage, (size_t)n * c->bs * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  return sync_and_check(c);
 }
 
 int w2d_get_blocks(W2dCtx* c, const int32_t* ids, int n, double* u)

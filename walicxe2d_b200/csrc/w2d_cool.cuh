@@ -182,13 +182,13 @@ __global__ void __launch_bounds__(W2D_THREADS, 2) k_cool(KArgs a, PhysArgs pa, d
 // primitives of whole blocks into a staging buffer (w2d_get_primit when
 // the pool does not store them)
 template <typename R, int NEQ>
-__global__ void k_to_prim(PhysArgs pa, const R* __restrict__ u, R* __restrict__ out,
+__global__ void k_to_prim(PhysArgs pa, const R* __restrict__ u, double* __restrict__ out,
                           const int* __restrict__ ids)
 {
   const Phys<R> ph = make_phys<R, -1, -1>(pa);
   const size_t bs = (size_t)NEQ * W2D_CELLS;
   const R* ub = u + (size_t)ids[blockIdx.x] * bs;
-  R* ob = out + (size_t)blockIdx.x * bs;
+  double* ob = out + (size_t)blockIdx.x * bs;
   for (int c = threadIdx.x; c < W2D_CELLS; c += blockDim.x) {
     R uu[NEQ], q[NEQ], T;
 #pragma unroll

@@ -79,8 +79,6 @@ struct W2dCtx {
   size_t stage_bytes = 0;
   int* d_ids = nullptr;
   int ids_cap = 0;
-  void* h_stage = nullptr;   // pinned
-  size_t h_stage_bytes = 0;
   double* h_small = nullptr; // pinned scalars (dt, ...)
   double* h_grad = nullptr;  // pinned, one per slot
   int* h_err = nullptr;      // pinned error word

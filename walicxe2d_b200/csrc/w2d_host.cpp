@@ -572,7 +572,7 @@ int w2d_sim_tree(W2dSim* s, int32_t* lp, int32_t* leaf, int32_t* icoord, int32_t
       for (int nb = 1; nb <= s->cap; ++nb) lp[(size_t)(k - 1) * s->cap + (nb - 1)] = s->LP(nb, k);
   if (leaf) memcpy(leaf, s->leaf.data(), sizeof(int32_t) * s->leaf.size());
   if (icoord) memcpy(icoord, s->icoord.data(), sizeof(int32_t) * s->icoord.size());
-  if (s->dirty) locatebounds(s);
+  if (s->dirty && (innerbounds || ninternal)) locatebounds(s);
   if (innerbounds) memcpy(innerbounds, s->ib.data(), sizeof(int32_t) * s->ib.size());
   if (ninternal) *ninternal = s->nib;
   return W2D_OK;

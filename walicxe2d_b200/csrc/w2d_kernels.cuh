@@ -1060,22 +1060,23 @@ __global__ void __launch_bounds__(W2D_THREADS) k_amr(KArgs a, PhysArgs pa, const
   block_stats<R, NEQ>(st, ph, a, pa, b, sred);
 }
 
-// pool <-> staging (block-major) copies
+// pool <-> staging (block-major, FP64 as the C-ABI's host arrays) copies;
+// an FP32 pool converts on the way
 template <typename R>
-__global__ void k_scatter(R* __restrict__ pool, const R* __restrict__ stage,
+__global__ void k_scatter(R* __restrict__ pool, const double* __restrict__ stage,
                           const int* __restrict__ ids, size_t bs)
 {
   const int b = ids[blockIdx.x];
   for (size_t c = threadIdx.x; c < bs; c += blockDim.x)
-    pool[(size_t)b * bs + c] = stage[(size_t)blockIdx.x * bs + c];
+    pool[(size_t)b * bs + c] = R(stage[(size_t)blockIdx.x * bs + c]);
 }
 template <typename R>
-__global__ void k_gather(const R* __restrict__ pool, R* __restrict__ stage,
+__global__ void k_gather(const R* __restrict__ pool, double* __restrict__ stage,
                          const int* __restrict__ ids, size_t bs)
 {
   const int b = ids[blockIdx.x];
   for (size_t c = threadIdx.x; c < bs; c += blockDim.x)
-    stage[(size_t)blockIdx.x * bs + c] = pool[(size_t)b * bs + c];
+    stage[(size_t)blockIdx.x * bs + c] = (double)pool[(size_t)b * bs + c];
 }
 
 }  // namespace w2d

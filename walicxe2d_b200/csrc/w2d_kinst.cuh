@@ -202,14 +202,14 @@ static cudaError_t cool(int neq, const KArgs& a, const PhysArgs& pa, double dt_s
 static cudaError_t scatter(void* pool, const void* stage, const int* ids, int n, size_t bs, cudaStream_t st)
 {
   if (n == 0) return cudaSuccess;
-  k_scatter<R><<<n, 256, 0, st>>>((R*)pool, (const R*)stage, ids, bs);
+  k_scatter<R><<<n, 256, 0, st>>>((R*)pool, (const double*)stage, ids, bs);
   return cudaGetLastError();
 }
 
 static cudaError_t gather(const void* pool, void* stage, const int* ids, int n, size_t bs, cudaStream_t st)
 {
   if (n == 0) return cudaSuccess;
-  k_gather<R><<<n, 256, 0, st>>>((const R*)pool, (R*)stage, ids, bs);
+  k_gather<R><<<n, 256, 0, st>>>((const R*)pool, (double*)stage, ids, bs);
   return cudaGetLastError();
 }
 
@@ -217,7 +217,7 @@ static cudaError_t to_prim(int neq, const PhysArgs& pa, const void* u, void* out
                            cudaStream_t st)
 {
   if (n == 0) return cudaSuccess;
-  W2D_NEQ_SWITCH(neq, (k_to_prim<R, NEQ><<<n, 256, 0, st>>>(pa, (const R*)u, (R*)out, ids)));
+  W2D_NEQ_SWITCH(neq, (k_to_prim<R, NEQ><<<n, 256, 0, st>>>(pa, (const R*)u, (double*)out, ids)));
   return cudaGetLastError();
 }
 

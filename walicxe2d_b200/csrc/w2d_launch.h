@@ -20,6 +20,7 @@ struct Launchers {
   cudaError_t (*amr)(int neq, const KArgs&, const PhysArgs&, const int* ops, int nr, int nc, const int* tup,
                      cudaStream_t);
   cudaError_t (*cool)(int neq, const KArgs&, const PhysArgs&, double dt_s, cudaStream_t);
+  // stage: FP64 block-major; a pool of the other precision converts
   cudaError_t (*scatter)(void* pool, const void* stage, const int* ids, int n, size_t bs, cudaStream_t);
   cudaError_t (*gather)(const void* pool, void* stage, const int* ids, int n, size_t bs, cudaStream_t);
   cudaError_t (*to_prim)(int neq, const PhysArgs&, const void* u, void* out, const int* ids, int n, cudaStream_t);
