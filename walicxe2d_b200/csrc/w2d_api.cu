@@ -255,23 +255,29 @@ int ensure_ids(W2dCtx* c, int n)
   return W2D_OK;
 }
 
-// Device staging of block transfers (FP64, block-major); grows by half
-// again each time so that a growing run reallocates rarely.  The host side
-// is the caller's own array: the copies run straight from and into it
-// (at full speed when the caller's memory is pinned).
+// Device staging of block transfers (FP64, block-major) of at most
+// kStageBytes: larger transfers go through it in chunks, one after another
+// on the context's stream, so the staging never grows with the run.  The
+// host side is the caller's own array: the copies run straight from and
+// into it (at full speed when the caller's memory is pinned).
+constexpr size_t kStageBytes = (size_t)64 << 20;
+
 int ensure_stage(W2dCtx* c, size_t bytes)
 {
+  bytes = std::min(bytes, kStageBytes);
   if (bytes > c->stage_bytes) {
-    const size_t cap = std::max(bytes, c->stage_bytes + c->stage_bytes / 2);
     CK(cudaStreamSynchronize(c->st));
     if (c->d_stage) cudaFree(c->d_stage);
     c->d_stage = nullptr;
     c->stage_bytes = 0;
-    CK(cudaMalloc(&c->d_stage, cap));
-    c->stage_bytes = cap;
+    CK(cudaMalloc(&c->d_stage, bytes));
+    c->stage_bytes = bytes;
   }
   return W2D_OK;
 }
+
+// blocks per chunk of a staged transfer
+int stage_chunk(const W2dCtx* c) { return (int)std::max<size_t>(1, c->stage_bytes / (c->bs * sizeof(double))); }
 
 // Checks the device error word (the queue must have drained).
 int check_device(W2dCtx* c)
@@ -847,10 +853,16 @@ int w2d_put_blocks(W2dCtx* c, const int32_t* ids, int n, const double* u)
   int rc = valid_ids(c, ids, n);
   if (rc) return rc;
   if ((rc = ensure_stage(c, (size_t)n * c->bs * sizeof(double))) || (rc = ensure_ids(c, n))) return rc;
-  CK(cudaMemcpyAsync(c->d_stage, u, (size_t)n * c->bs * sizeof(double), cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(c->d_ids, ids, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st));
-  if ((rc = launch(c, "scatter", [&] { return c->L->scatter(c->d_u, c->d_stage, c->d_ids, n, c->bs, c->st); })))
-    return rc;
+  const int chunk = stage_chunk(c);
+  for (int q0 = 0; q0 < n; q0 += chunk) {
+    const int m = std::min(chunk, n - q0);
+    CK(cudaMemcpyAsync(c->d_stage, u + (size_t)q0 * c->bs, (size_t)m * c->bs * sizeof(double),
+                       cudaMemcpyHostToDevice, c->st));
+    if ((rc = launch(c, "scatter",
+                     [&] { return c->L->scatter(c->d_u, c->d_stage, c->d_ids + q0, m, c->bs, c->st); })))
+      return rc;
+  }
   if ((rc = stats_for(c, c->d_ids, n))) return rc;
   CK(cudaStreamSynchronize(c->st));
   return W2D_OK;
@@ -862,15 +874,21 @@ static int get_pool(W2dCtx* c, void* pool, const int32_t* ids, int n, double* u)
   if (rc) return rc;
   if ((rc = ensure_stage(c, (size_t)n * c->bs * sizeof(double))) || (rc = ensure_ids(c, n))) return rc;
   CK(cudaMemcpyAsync(c->d_ids, ids, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st));
-  if (pool) {
-    if ((rc = launch(c, "gather", [&] { return c->L->gather(pool, c->d_stage, c->d_ids, n, c->bs, c->st); })))
+  const int chunk = stage_chunk(c);
+  const PhysArgs pa = pargs(c);
+  for (int q0 = 0; q0 < n; q0 += chunk) {
+    const int m = std::min(chunk, n - q0);
+    const int* d_ids = c->d_ids + q0;
+    if (pool) {
+      if ((rc = launch(c, "gather", [&] { return c->L->gather(pool, c->d_stage, d_ids, m, c->bs, c->st); })))
+        return rc;
+    } else if ((rc = launch(c, "to_prim",
+                            [&] { return c->L->to_prim(c->neq, pa, c->d_u, c->d_stage, d_ids, m, c->st); }))) {
       return rc;
-  } else {
-    PhysArgs pa = pargs(c);
-    if ((rc = launch(c, "to_prim", [&] { return c->L->to_prim(c->neq, pa, c->d_u, c->d_stage, c->d_ids, n, c->st); })))
-      return rc;
+    }
+    CK(cudaMemcpyAsync(u + (size_t)q0 * c->bs, c->d_stage, (size_t)m * c->bs * sizeof(double),
+                       cudaMemcpyDeviceToHost, c->st));
   }
-  CK(cudaMemcpyAsync(u, c->d_stage, (size_t)n * c->bs * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   return sync_and_check(c);
 }
 
