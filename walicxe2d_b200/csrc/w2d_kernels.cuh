@@ -857,6 +857,44 @@ __global__ void __launch_bounds__(W2D_THREADS, 4) k_fill1(KArgs a, PhysArgs pa, 
   }
 }
 
+// Fill of layer 0 without the statistics (cooling runs and the jet, whose
+// statistics follow in a later pass): 64 threads per leaf, four leaves per
+// 256-thread CTA.  Persistent (P): the CTA walks its leaves as leaf_range
+// gives them, four at a time (li, li + step, li + 2 step, li + 3 step);
+// otherwise CTA k takes leaves 4k .. 4k + 3.
+template <typename R, int NEQ, bool P>
+__global__ void __launch_bounds__(256) k_fill1g(KArgs a)
+{
+  const int tid = threadIdx.x, g = tid >> 6, t = tid & 63;
+  const int f = t / 16, m = 1 + t % 16;
+  const size_t bs = (size_t)NEQ * W2D_CELLS;
+  R* __restrict__ upool = (R*)a.u;
+  LeafRange lr;
+  if (P) {
+    lr = leaf_range<true>(a);
+  } else {
+    const int lo = 4 * (int)blockIdx.x;
+    lr = {lo, lo + 4 < a.nleaf ? lo + 4 : a.nleaf, 1};
+  }
+  int gi, gj;
+  ghost_ij(f, 0, m, gi, gj);
+  for (; lr.li < lr.end; lr.li += 4 * lr.step) {
+    const int li = lr.li + g * lr.step;
+    if (li >= lr.end) continue;
+    const int b = a.leaves[li];
+    const int2 d = a.fd[li * 4 + f];
+    R gv[NEQ];
+    bool w = false;
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) w = ghost_value<R>(upool, bs, a, b, d, f, 0, m, k, gv[k]);
+    if (w) {
+      R* __restrict__ u = upool + (size_t)b * bs;
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) u[k * W2D_CELLS + cidx(gi, gj)] = gv[k];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // calcprim (src/calcprim.f90:5-21) of whole blocks (stored when DMC) and
 // their per-block statistics, for the blocks of `list`.  Used after the pool

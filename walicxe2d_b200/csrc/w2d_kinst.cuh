@@ -104,6 +104,13 @@ static cudaError_t fill1_p(const KArgs& a, const PhysArgs& pa, int stats, cudaSt
 template <int NEQ>
 static cudaError_t fill1_t(const KArgs& a, const PhysArgs& pa, int stats, cudaStream_t st)
 {
+  if (!stats) {   // ghost faces only: four leaves per CTA
+    if (a.grid > 0)
+      k_fill1g<R, NEQ, true><<<a.grid, 256, 0, st>>>(a);
+    else
+      k_fill1g<R, NEQ, false><<<(a.nleaf + 3) / 4, 256, 0, st>>>(a);
+    return cudaGetLastError();
+  }
   return a.grid > 0 ? fill1_p<NEQ, true>(a, pa, stats, st) : fill1_p<NEQ, false>(a, pa, stats, st);
 }
 
