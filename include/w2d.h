@@ -107,6 +107,13 @@ int w2d_destroy(W2dCtx* ctx);
 int w2d_last_error(W2dCtx* ctx, W2dError* err);
 /* DMC table as read in src/initmain.f90:83-98: n rows of (log10 T, -log10 L). */
 int w2d_set_cooltab(W2dCtx* ctx, const double* log_t, const double* neg_log_l, int n);
+/* Failure detection check (no counterpart in the reference): one kernel
+ * waits on a barrier that nothing completes.  Every device wait of the
+ * library is bounded (about a second); this one runs out, the kernel
+ * reports W2D_ERR_TIMEOUT through the context's error word and ends, and
+ * the call returns W2D_ERR_TIMEOUT (w2d_last_error holds the message).  The
+ * context stays usable.  Takes a second or so. */
+int w2d_wait_selftest(W2dCtx* ctx);
 /* Library version string and the build's target architecture. */
 const char* w2d_version(void);
 

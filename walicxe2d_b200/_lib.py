@@ -25,6 +25,7 @@ SIGNATURES = {
     "w2d_create": (_I, [C.POINTER(W2dParams), C.POINTER(_vp)]),
     "w2d_destroy": (_I, [_vp]),
     "w2d_last_error": (_I, [_vp, C.POINTER(W2dError)]),
+    "w2d_wait_selftest": (_I, [_vp]),
     "w2d_set_cooltab": (_I, [_vp, _PD, _PD, _I]),
     "w2d_set_topology": (_I, [_vp, _PI32, _I, _PI32, _PI32, _I, _I, _PD, _PD]),
     "w2d_set_bounds": (_I, [_vp, _PI32, _I, _I]),

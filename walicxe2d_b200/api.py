@@ -105,6 +105,14 @@ class Context:
         self._check(self.L.w2d_get_blocks(self.h, _pi32(ids), ids.size, _pd(out)), "w2d_get_blocks")
         return out
 
+    def wait_selftest(self) -> tuple[int, str]:
+        """w2d_wait_selftest: a device wait that nothing completes runs out;
+        returns the status (W2D_ERR_TIMEOUT) and the error message."""
+        rc = self.L.w2d_wait_selftest(self.h)
+        e = _lib.W2dError()
+        self.L.w2d_last_error(self.h, C.byref(e))
+        return rc, e.message.decode(errors="replace")
+
     def get_primit(self, ids) -> np.ndarray:
         ids = np.ascontiguousarray(ids, np.int32)
         u = np.zeros((ids.size, self.neq, W, W))

@@ -285,7 +285,9 @@ int check_device(W2dCtx* c)
   if (c->h_err[0] != 0) {
     int code = c->h_err[0];
     int rc = set_error(c, code, c->h_err[1], c->h_err[2], c->h_err[3],
-                       code == W2D_ERR_HLLC ? "Error in hllc: NaN contact speed" : "device error");
+                       code == W2D_ERR_HLLC      ? "Error in hllc: NaN contact speed"
+                       : code == W2D_ERR_TIMEOUT ? "a bounded device wait gave up"
+                                                 : "device error");
     c->h_err[0] = 0;
     cudaMemsetAsync(c->d_err, 0, 4 * sizeof(int), c->st);
     return rc;
@@ -720,6 +722,13 @@ int w2d_destroy(W2dCtx* c)
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return W2D_OK;
+}
+
+int w2d_wait_selftest(W2dCtx* c)
+{
+  if (!c) return W2D_ERR_ARG;
+  CK(launch_wait_selftest(c->d_err, c->st));
+  return sync_and_check(c);
 }
 
 int w2d_last_error(W2dCtx* c, W2dError* e)

@@ -108,6 +108,24 @@ __global__ void k_gather_leaf(const int* __restrict__ leaves, int n, const int* 
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) out[k] = v[leaves[k]];
 }
 
+// A wait that nothing completes: an mbarrier expecting one arrival that no
+// thread makes.  The bounded wait every kernel uses gives up and the error
+// word reports W2D_ERR_TIMEOUT; no copy is in flight, so the CTA just ends.
+__global__ void k_wait_selftest(int* err)
+{
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  const bool done = mbar_wait(&bar, 0);
+  if (!__syncthreads_or(done) && threadIdx.x == 0) set_err(err, ERR_TIMEOUT, 0, -1, -1);
+}
+
+cudaError_t launch_wait_selftest(int* err, cudaStream_t st)
+{
+  k_wait_selftest<<<1, 32, 0, st>>>(err);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_gather_leaf(const int* leaves, int n, const int* n_dev, const double* v, double* out,
                                cudaStream_t st)
 {

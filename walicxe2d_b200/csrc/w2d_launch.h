@@ -42,6 +42,9 @@ cudaError_t launch_dt(const int* leaves, int n, const int* n_dev, int grid, cons
 cudaError_t launch_dt_runs(const int* leaves, const int* loff, int nruns, const double* cfl, const double* dtcool,
                            int use_cool, double courant, double psc, double tsc, double* dt_run, cudaStream_t st);
 
+// one bounded wait that runs out (see w2d_wait_selftest)
+cudaError_t launch_wait_selftest(int* err, cudaStream_t st);
+
 // out[k] = v[leaves[k]] for k < n (or < *n_dev when n_dev is set)
 cudaError_t launch_gather_leaf(const int* leaves, int n, const int* n_dev, const double* v, double* out,
                                cudaStream_t st);

@@ -4,15 +4,17 @@
 // NEQ*400 values (12.8 KB in FP64 with NEQ = 4), so it moves with a single
 // non-tensor cp.async.bulk whose completion is tracked by an mbarrier
 // transaction count.  Only the GPU's own HBM is read this way (no multicast).
-// Every wait is bounded: after kMaxSpins polls the caller gets false and
-// records W2D_ERR_TIMEOUT instead of hanging.
+// Every wait is bounded: after kMaxSpins polls (about a second: a poll
+// that finds the phase incomplete suspends for a few microseconds; 2^22
+// polls measured 16.6 s) the caller gets false and records W2D_ERR_TIMEOUT
+// instead of hanging.  The copies and MMAs waited on take microseconds.
 #pragma once
 
 #include <cstdint>
 
 namespace w2d {
 
-constexpr unsigned kMaxSpins = 1u << 22;
+constexpr unsigned kMaxSpins = 1u << 18;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
