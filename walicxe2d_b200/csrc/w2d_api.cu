@@ -337,7 +337,7 @@ void plan_reset(int2* hf1, int2* hf2, const int* leaves, int nl)
 // different runs occupy different slots, so runs can be planned at once;
 // plan_pack then lays the descriptors out by leaf position for the device.
 int plan_entries(W2dCtx* c, int2* hf1, int2* hf2, const int32_t* ib, int ld, int n, int base, int nbmax_local,
-                 bool jet)
+                 bool jet, const int* row)
 {
   auto jetted_before = [&](int blk, int e) {
     return blk >= 1 && blk <= nbmax_local && c->qfirst[blk] && c->qfirst[blk] < e;
@@ -353,7 +353,7 @@ int plan_entries(W2dCtx* c, int2* hf1, int2* hf2, const int32_t* ib, int ld, int
       if (kind == FK_RESTRICT && jetted_before(nbr + (face < 2 ? 2 : 1), e)) y |= FD_SRC2_JET;
       if (c->qlast[blk] >= e) y |= FD_DST_JET;
     }
-    fd[(size_t)g * 4 + face] = make_int2(base + nbr, y);
+    fd[(size_t)(row ? row[g] : g) * 4 + face] = make_int2(base + nbr, y);
   };
   int e = 0;
   auto both = [&](int blk, int face, int nbr, int kind, int off) {
@@ -667,6 +667,7 @@ int w2d_create(const W2dParams* p, W2dCtx** out)
     CKC(cudaMallocHost(&c->h_jetblk[q], sizeof(int) * slots));
   }
   c->sfd1.assign(4 * slots, make_int2(0, FK_KEEP));
+  c->pos_of.assign(slots, 0);
   c->sfd2.assign(4 * slots, make_int2(0, FK_KEEP));
   CKC(cudaMalloc(&c->d_gradleaf, sizeof(double) * slots));
   CKC(cudaMalloc(&c->d_fd1, sizeof(int2) * 4 * slots));
@@ -770,6 +771,7 @@ int w2d_set_topology(W2dCtx* c, const int32_t* lp, int ld_lp, const int32_t* lea
     if (c->leaf[nb]) {
       if (c->lev[nb] < 1 || c->lev[nb] > c->p.nlevs)
         return set_error(c, W2D_ERR_TOPOLOGY, nb, 0, 0, "leaf %d has level %d", nb, c->lev[nb]);
+      c->pos_of[nb] = (int)c->leaves.size();
       c->leaves.push_back(nb);
     }
   }
@@ -805,10 +807,13 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
   const int q = c->plan_buf;
   c->plan_buf ^= 1;
   CK(cudaEventSynchronize(c->ev_plan[q]));
-  int2* hf1 = c->sfd1.data();
-  int2* hf2 = c->sfd2.data();
+  // the plans go straight into the pinned upload arrays, by leaf position
+  const int nl = (int)c->leaves.size();
+  int2* hf1 = c->h_fd1[q];
+  int2* hf2 = c->h_fd2[q];
   int* hj = c->h_jetblk[q];
-  plan_reset(hf1, hf2, c->leaves.data(), (int)c->leaves.size());
+  std::fill(hf1, hf1 + 4 * (size_t)nl, make_int2(0, FK_KEEP));
+  std::fill(hf2, hf2 + 4 * (size_t)nl, make_int2(0, FK_KEEP));
   const bool jet = c->p.otherb == W2D_USERBC_JET;
   if (jet) {
     // impose_jet runs after every entry on its nbs (src/boundaryI.f90:386-393,
@@ -824,17 +829,16 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
       c->qlast[nbs] = e;
     }
   }
-  int rc = plan_entries(c, hf1, hf2, ib, ld, n, 0, c->nbmax, jet);
+  int rc = plan_entries(c, hf1, hf2, ib, ld, n, 0, c->nbmax, jet, c->pos_of.data());
   if (jet) {
     // faces no entry writes still get the jet if their block is ever nbs;
     // the interior of such a block always does
-    for (size_t li = 0; li < c->leaves.size(); ++li) {
-      const int b = c->leaves[li];
-      const bool named = c->qfirst[b] > 0;
+    for (int li = 0; li < nl; ++li) {
+      const bool named = c->qfirst[c->leaves[li]] > 0;
       hj[li] = named;
       for (int f = 0; f < 4; ++f) {
-        if (named && (hf1[b * 4 + f].y & 0xff) == FK_KEEP) hf1[b * 4 + f].y |= FD_DST_JET;
-        if (named && (hf2[b * 4 + f].y & 0xff) == FK_KEEP) hf2[b * 4 + f].y |= FD_DST_JET;
+        if (named && (hf1[li * 4 + f].y & 0xff) == FK_KEEP) hf1[li * 4 + f].y |= FD_DST_JET;
+        if (named && (hf2[li * 4 + f].y & 0xff) == FK_KEEP) hf2[li * 4 + f].y |= FD_DST_JET;
       }
     }
     for (int k = 1; k <= n; ++k) {   // clear for the next list
@@ -843,8 +847,6 @@ int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
     }
   }
   if (rc) return rc;
-  const int nl = (int)c->leaves.size();
-  plan_pack(c, c->h_fd1[q], c->h_fd2[q], c->leaves.data(), nl, 0);
   if (nl > 0) {
     CK(cudaMemcpyAsync(c->d_fd1, c->h_fd1[q], sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->d_fd2, c->h_fd2[q], sizeof(int2) * 4 * (size_t)nl, cudaMemcpyHostToDevice, c->st));
@@ -1269,7 +1271,7 @@ int ctx_plan_begin(W2dCtx* c)
 int ctx_plan_run(W2dCtx* c, const int32_t* ib, int ld, int n, int base, int nbmax_local, const int* leaves, int nl)
 {
   plan_reset(c->sfd1.data(), c->sfd2.data(), leaves, nl);
-  return plan_entries(c, c->sfd1.data(), c->sfd2.data(), ib, ld, n, base, nbmax_local, false);
+  return plan_entries(c, c->sfd1.data(), c->sfd2.data(), ib, ld, n, base, nbmax_local, false, nullptr);
 }
 
 void ctx_plan_pack(W2dCtx* c, const int* leaves, int nl, int pos0)

@@ -40,6 +40,7 @@ struct W2dCtx {
   int2* d_fd1 = nullptr;   // boundaryI (layer 0 of u)
   int2* d_fd2 = nullptr;   // boundaryII (two layers of up)
   std::vector<int2> sfd1, sfd2;  // host plans per slot (4 faces), packed by leaf position for upload
+  std::vector<int> pos_of;         // leaf position of each leaf slot (w2d_set_topology)
   double* d_gradleaf = nullptr;  // criteria maxima gathered by leaf position
   cudaEvent_t ev_dt = nullptr;  // dt and the error word have reached h_small/h_err
   // ensembles (nruns > 0): run of every slot, per-run geometry and dt, and

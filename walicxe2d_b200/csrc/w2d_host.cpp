@@ -272,8 +272,9 @@ int admesh_decide(W2dSim* s)
 {
   auto& L = *s;
   const int nlevs = s->p.nlevs;
-  std::fill(s->irefup.begin(), s->irefup.end(), 0);
-  std::fill(s->irefdown.begin(), s->irefdown.end(), 0);
+  // flags above nbmax are never set (new sons only ever get zeros)
+  std::fill(s->irefup.begin(), s->irefup.begin() + s->nbmax + 1, 0);
+  std::fill(s->irefdown.begin(), s->irefdown.begin() + s->nbmax + 1, 0);
   // leaves per level in ascending ID (the only blocks that get flags)
   for (auto& v : s->bucket) v.clear();
   for (int nb = 1; nb <= s->nbmax; ++nb)
