@@ -258,12 +258,31 @@ def _finish_tuning(runner, ctx, at_least: int):
     return n
 
 
-def batched_measure(args, plain_value: float):
+def shard_runs(n: int, ws: int, rank: int) -> list:
+    """The runs of an ensemble of n independent runs that rank `rank` of
+    `ws` advances: every ws-th one, so that each GPU gets a mix of sizes."""
+    return list(range(rank, n, ws))
+
+
+def gather_runs(l1: list, same: int, td=None):
+    """Every rank's per-run L1 figures and same-tree count, on every rank (a
+    few numbers per run, after the timed region)."""
+    if td is None or td.get_world_size() == 1:
+        return list(l1), same
+    gathered = [None] * td.get_world_size()
+    td.all_gather_object(gathered, (list(l1), same))
+    return [x for g in gathered for x in g[0]], sum(g[1] for g in gathered)
+
+
+def batched_measure(args, plain_value: float, td=None, rank: int = 0, ws: int = 1):
     """The batched FP32 + learned-cooling path: the 256-run ensemble of
     Sedov-with-coolingh runs of uneven size, its surrogate trained on the
     device first; per-run density L1 against the same runs in FP64 with
     the exact routine (the plain path, itself equal to the CPU oracle to
-    1e-10 with coolingh)."""
+    1e-10 with coolingh).  With several GPUs the runs are shared out
+    (shard_runs; no collective on the data path): the value is all ranks'
+    zone-updates over the slowest rank's time, the L1 statistics cover every
+    run."""
     import numpy as np
 
     from walicxe2d_b200.api import Ensemble, Surrogate
@@ -277,9 +296,12 @@ def batched_measure(args, plain_value: float):
     judge = nn.judge(1 << 22, seed=20261204)
     pre, warm, steps = 12, max(args.warmup, 3), min(args.steps, 40)
     nruns = args.batched_runs
+    mine = shard_runs(nruns, ws, rank)
+    nloc = len(mine)
     out, states = {}, {}
     for name, prec, use_nn in (("fp32nn", 32, True), ("fp64", 64, False)):
-        mem = ensemble_members(count=nruns, precision=prec)
+        every = ensemble_members(count=nruns, precision=prec)
+        mem = [every[r] for r in mine]
         for p, ic in mem:
             p.nblocks = min(p.nblocks, ENS_CAP)
         ens = Ensemble(mem, threads=0)
@@ -310,7 +332,8 @@ def batched_measure(args, plain_value: float):
         prof = ctx.profile_read()
         ctx.profile(False)
         zu = st1["zone_updates"] - st0["zone_updates"]
-        rec = {"value": zu / (sum(ms) / 1000.0), "ms_per_step": sum(ms) / steps, "leaves": st1["nleaf"],
+        t_all, zu_all = aggregate(sum(ms), float(zu), td, "cuda")
+        rec = {"value": zu_all / (t_all / 1000.0), "ms_per_step": t_all / steps, "leaves": st1["nleaf"],
                "gpu_launches": launches, "cuda_graphs": True, "launch_shapes": ctx.tuning(),
                "kernels_ms_per_step": {k: round(v[1] / 3, 4) for k, v in prof.items()}}
         if use_nn:
@@ -318,26 +341,29 @@ def batched_measure(args, plain_value: float):
             sv, ex = c1[0] - c0[0], c1[1] - c0[1]
             rec["cells_served_by_network"] = sv / max(sv + ex, 1)
         out[name] = rec
-        states[name] = {r: (ens.leaves(r), ens.blocks(r)[1][:, 0, 2:18, 2:18]) for r in range(nruns)}
-        rec["nbmax_max_run"] = max(ens.status(r)["nbmax"] for r in range(nruns))
+        states[name] = {r: (ens.leaves(r), ens.blocks(r)[1][:, 0, 2:18, 2:18]) for r in range(nloc)}
+        rec["nbmax_max_run"] = max(ens.status(r)["nbmax"] for r in range(nloc))
         ens.close()
     l1, same = [], 0
-    for r in range(nruns):
+    for r in range(nloc):
         ia, ra = states["fp64"][r]
         ib, rb = states["fp32nn"][r]
         common, xa, xb = np.intersect1d(ia, ib, return_indices=True)
         same += int(len(common) == len(ia) == len(ib))
         a, b = ra[xa], rb[xb]
         l1.append(float(np.abs(b - a).sum() / max(np.abs(a).sum(), 1e-300)))
+    l1, same = gather_runs(l1, same, td)
     l1 = np.array(l1)
     v = out["fp32nn"]["value"]
     return {
         "metric": UNIT, "value": v, "unit": UNIT, "dtype": "f32+bf16-mlp",
         "ms_per_step": out["fp32nn"]["ms_per_step"], "steps": steps,
         "workload": f"{nruns} independent Sedov-with-coolingh runs (roots k x k, k in 2..16; 3..6 levels; "
-                    "n log-U[0.1,10] cm^-3, E log-U[1e50,1e51] erg; 40 pc box), one device context, "
+                    "n log-U[0.1,10] cm^-3, E log-U[1e50,1e51] erg; 40 pc box), one device context per GPU "
+                    f"({ws} GPU(s), every {ws}-th run each), "
                     f"{pre} untimed steps, then the autotuner's steps and {warm} more, L2 flushed before "
                     "every timed step",
+        "scaling": "strong", "n_gpus": ws,
         "leaves": out["fp32nn"]["leaves"], "ratio_to_plain_fp64_value": v / plain_value,
         "fp32nn": out["fp32nn"], "fp64_exact_same_runs": out["fp64"],
         "density_l1_vs_fp64": {"max": float(l1.max()), "median": float(np.median(l1)),
@@ -602,9 +628,10 @@ def run_ours(args, ws, rank, local):
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(os.cpu_count() or 1)
     batched = variants = None
-    if rank == 0 and ws == 1 and not args.no_batched and args.precision == 64:
-        batched, nn_h = batched_measure(args, value)
-        if not args.no_variants:
+    if not args.no_batched and args.precision == 64:
+        # every rank takes part (its share of the runs, then the aggregation)
+        batched, nn_h = batched_measure(args, value, dist[1] if dist else None, rank, ws)
+        if rank == 0 and ws == 1 and not args.no_variants:
             variants = variants_measure(args, nn_h)
 
     if rank == 0:

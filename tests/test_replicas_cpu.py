@@ -1,6 +1,8 @@
-"""The several-GPU path of bench.py is independent replicas: its only
-exchange is the aggregation of the timed totals (slowest rank's time, sum
-of zone-updates).  Checked here with two gloo ranks on the CPU."""
+"""The several-GPU path of bench.py is independent replicas for the plain
+path and a share of the runs per rank for the ensemble: its only exchanges
+are the aggregation of the timed totals (slowest rank's time, sum of
+zone-updates) and, after the timed region, the per-run L1 figures.  Checked
+here with two gloo ranks on the CPU."""
 import os
 import socket
 
@@ -25,7 +27,8 @@ def _rank(rank, world, port, out):
     td.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     assert bench._dist_env() == (world, rank, rank)
     t, zu = bench.aggregate(10.0 + rank, 1000.0 * (rank + 1), td, "cpu")
-    out[rank] = (t, zu)
+    l1, same = bench.gather_runs([0.1 * rank, 0.2 * rank], rank + 1, td)
+    out[rank] = (t, zu, tuple(l1), same)
     td.barrier()
     td.destroy_process_group()
 
@@ -42,9 +45,19 @@ def test_two_replicas_aggregate_on_gloo():
         for p in procs:
             p.join(90)
         assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
-        assert out[0] == out[1] == (11.0, 3000.0)
+        assert out[0] == out[1] == (11.0, 3000.0, (0.0, 0.0, 0.1, 0.2), 3)
 
 
 def test_single_process_aggregate_is_identity():
     import bench
     assert bench.aggregate(5.0, 7.0) == (5.0, 7.0)
+
+
+@pytest.mark.parametrize("n,ws", [(256, 1), (256, 2), (256, 8), (7, 4), (3, 8)])
+def test_ensemble_shards_cover_every_run_once(n, ws):
+    import bench
+    shards = [bench.shard_runs(n, ws, r) for r in range(ws)]
+    allr = sorted(x for sh in shards for x in sh)
+    assert allr == list(range(n))
+    assert max(map(len, shards)) - min(map(len, shards)) <= 1
+    assert bench.gather_runs([1.0], 2) == ([1.0], 2)
