@@ -442,6 +442,7 @@ def variants_measure(args, nn_h):
                 s0 = sim.status()
                 c0 = sim.ctx.surrogate_counts() if prec == 32 else (0, 0)
                 ms = 0.0
+                sim.phase_ms(reset=True)
                 for _ in range(steps):
                     sim.ctx.flush_l2()
                     sim.ctx.event_record(0)
@@ -450,7 +451,8 @@ def variants_measure(args, nn_h):
                     ms += sim.ctx.event_elapsed(0, 1)
                 s1 = sim.status()
                 r = {"value": (s1["zone_updates"] - s0["zone_updates"]) / (ms / 1000.0),
-                     "ms_per_step": ms / steps, "leaves": s1["nleaf"], "steps_after_warm_start": s1["steps"]}
+                     "ms_per_step": ms / steps, "leaves": s1["nleaf"], "steps_after_warm_start": s1["steps"],
+                     "host_phase_ms_per_step": {k: round(v / steps, 4) for k, v in sim.phase_ms().items()}}
                 if prec == 32:
                     c1 = sim.ctx.surrogate_counts()
                     sv, ex = c1[0] - c0[0], c1[1] - c0[1]

@@ -157,6 +157,31 @@ int w2d_tstep(W2dCtx* ctx, double time, double dt);
  * flags follow on the host: grad >= tol -> refine (level < nlevs), else
  * grad <= tol2 -> coarsen. */
 int w2d_criteria(W2dCtx* ctx, double* grad);
+/* The admesh flags on the device, for hosts that keep lp on the host but
+ * want neither the per-block criteria download nor the flag loops over
+ * nbmax.  w2d_set_links mirrors lp(nb,4:8) (son position and the four
+ * neighbours) of the listed rows to the device: element (nb,k) of lp is
+ * lp[(nb-1)*row_stride + (k-1)*col_stride] (Fortran lp(nbmin:,8) with
+ * nbmin = 1: row_stride 1, col_stride = its leading dimension).  rows NULL
+ * sends blocks 1..nbmax of the last w2d_set_topology; otherwise the nrows
+ * IDs listed (duplicates allowed), e.g. those updatelpup/updatelpdown
+ * changed.  Neighbours must be -1 or block IDs within the pool. */
+int w2d_set_links(W2dCtx* ctx, const int32_t* lp, int row_stride, int col_stride,
+                  const int32_t* rows, int nrows);
+/* markref (src/markref.f90:23-44 with criteria's flags), critneighup
+ * (src/critneighup.f90:19-58) and critneighdown (src/critneighdown.f90:22-48)
+ * of one admesh pass (src/admesh.f90:23-105) on the device, from the
+ * criteria maxima of the last step and the tree of w2d_set_topology +
+ * w2d_set_links.  refine receives the blocks the pass refines in the order
+ * admesh visits them (level ascending, then ID); coarsen the first sons
+ * (lp(nb,4) = 1) of the families it coarsens, in its order (level
+ * descending, then ID).  The effect of the pass's refines on critneighdown
+ * (updatelpup runs before it) is accounted for.  The host then applies
+ * updatelpup / updatelpdown in list order and calls w2d_refine /
+ * w2d_coarse.  *nrefine / *ncoarsen receive the counts; W2D_ERR_ARG if a
+ * list is longer than its capacity (the counts are still set). */
+int w2d_admesh_flags(W2dCtx* ctx, int32_t* refine, int cap_refine, int* nrefine,
+                     int32_t* coarsen, int cap_coarsen, int* ncoarsen);
 /* The u motion of refine (src/refine.f90:30-38, 227-258): quads[k*5+0] is
  * the parent, quads[k*5+1..4] the four sons (BL, BR, TL, TR). */
 int w2d_refine(W2dCtx* ctx, const int32_t* quads, int n);
@@ -253,6 +278,10 @@ int w2d_sim_tree(W2dSim* sim, int32_t* lp, int32_t* leaf, int32_t* icoord,
                  int32_t* innerbounds, int32_t* ninternal);
 /* Enables/disables AMR (admesh after each step); on by default if nlevs>1. */
 int w2d_sim_set_amr(W2dSim* sim, int on);
+/* Where admesh takes its flags: 1 (default) on the device through
+ * w2d_admesh_flags, 0 on the host from the w2d_criteria download.  Both
+ * give the same refines and coarsenings. */
+int w2d_sim_set_device_flags(W2dSim* sim, int on);
 /* DMC table for the driver's context (as w2d_set_cooltab), then the
  * primitives and per-block partials of every leaf are recomputed with it. */
 int w2d_sim_set_cooltab(W2dSim* sim, const double* log_t, const double* neg_log_l, int n);
@@ -260,7 +289,8 @@ int w2d_sim_set_cooltab(W2dSim* sim, const double* log_t, const double* neg_log_
  * last reset: [0] topology and leaf-list upload, [1] timestep and half-step
  * launches, [2] locatebounds + fill plans (the device meanwhile runs the
  * reduction and the half step), [3] wait for dt, [4] launches of the rest
- * of tstep, [5] criteria (waits for the device), [6] admesh integer logic,
+ * of tstep, [5] the admesh flags from the device (w2d_admesh_flags, or the
+ * w2d_criteria download; waits for the device), [6] admesh integer logic,
  * [7] refine/coarse calls, [8] whole steps.  ms must hold W2D_SIM_NPHASES
  * doubles; reset != 0 zeroes the counters after reading. */
 #define W2D_SIM_NPHASES 9

@@ -1,0 +1,104 @@
+"""admesh's flag loops on the device (w2d_admesh_flags: markref,
+critneighup and critneighdown with the effect of the pass's refines, then
+the refine and coarsen lists in admesh's order) against the same loops on
+the host from the criteria download (src/admesh.f90:23-105).
+
+- the single-run driver with either source of flags takes the same refines
+  and coarsenings every step: identical lp, leaf and icoord after every
+  step, identical blocks at the end (AMR blast, jet, remnant with coolingh,
+  cylindrical jet);
+- passes that refine or coarsen thousands of blocks at once (more than one
+  download of the lists);
+- the device mirror of lp(:,4:8) rejects neighbours outside the pool.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import noncorner_mask
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(p, ic):
+    from walicxe2d_b200.api import Simulation
+    from walicxe2d_b200.params import COOLINGDMC
+    a = Simulation(p, ic)               # device flags (the default)
+    b = Simulation(p, ic)
+    b.set_device_flags(False)           # host loops over w2d_criteria
+    if p.cooling == COOLINGDMC:
+        rows = np.loadtxt(os.path.join(os.path.dirname(__file__), "golden", "coolingDMC.tab"))
+        for s in (a, b):
+            s.set_cooltab(rows[:, 0], rows[:, 1])
+    return a, b
+
+
+def _same_tree(a, b):
+    for x, y in zip(a.tree(), b.tree()):
+        assert np.array_equal(x, y)
+
+
+def _same_blocks(a, b):
+    ia, ua = a.blocks()
+    ib, ub = b.blocks()
+    assert np.array_equal(ia, ib)
+    m = noncorner_mask()
+    assert np.array_equal(ua[:, :, m], ub[:, :, m])
+
+
+@pytest.mark.parametrize("name,steps", [("sedov_amr_small", 80), ("jet_small", 80), ("snr_small", 40),
+                                        ("jet_cyl_small", 40)])
+def test_device_flags_equal_host_flags(name, steps):
+    from walicxe2d_b200.params import config
+    p, ic = config(name)
+    a, b = _pair(p, ic)
+    _same_tree(a, b)
+    leaves = set()
+    for _ in range(steps):
+        a.run(1)
+        b.run(1)
+        _same_tree(a, b)
+        assert a.status()["dt"] == b.status()["dt"]
+        leaves.add(a.status()["nleaf"])
+    assert len(leaves) >= 2, leaves         # the mesh did change
+    _same_blocks(a, b)
+
+
+@pytest.mark.parametrize("mode", ["refine_all", "coarsen_all"])
+def test_passes_with_thousands_of_changes(mode):
+    from walicxe2d_b200.params import sedov
+    p, ic = sedov(nbroot=48, nlevs=3, tol=0.1, nblocks=50000, startup_admesh=0)
+    if mode == "refine_all":
+        p.tol = -1.0                   # every leaf below nlevs refines: 2,304 then 9,216
+    else:
+        p.tol, p.tol2 = 1e30, 1e30     # every family coarsens: 9,216 then 2,304
+        ic.init_levels = 3
+    a, b = _pair(p, ic)
+    n0 = a.status()["nleaf"]
+    for _ in range(2):
+        a.run(1)
+        b.run(1)
+        _same_tree(a, b)
+    n1 = a.status()["nleaf"]
+    if mode == "refine_all":
+        assert n0 == 2304 and n1 == 2304 * 16, (n0, n1)
+    else:
+        assert n0 == 2304 * 16 and n1 == 2304, (n0, n1)
+    _same_blocks(a, b)
+
+
+def test_links_reject_blocks_outside_the_pool():
+    from walicxe2d_b200.api import Simulation
+    from walicxe2d_b200.params import config
+    p, ic = config("sedov_amr_small")
+    s = Simulation(p, ic)
+    lp, lf, icd, _ = s.tree()                # row = block ID (row 0 unused)
+    nb = int(np.nonzero(lf)[0][0])           # a leaf
+    good = np.asfortranarray(lp[1:], np.int32)
+    bad = good.copy(order="F")
+    bad[nb - 1, 5] = p.nblocks + 7           # lp(nb,6) outside the pool
+    with pytest.raises(Exception):
+        s.ctx.set_links(bad, rows=[nb])
+    s.ctx.set_links(good)                    # the real tree is accepted again
+    s.run(5)

@@ -148,6 +148,24 @@ class Context:
         self._check(self.L.w2d_criteria(self.h, _pd(g)), "w2d_criteria")
         return g[:nbmax]
 
+    def set_links(self, lp, rows=None):
+        """Device mirror of lp(:,4:8) (w2d_set_links); lp column-major
+        [nblocks, 8] as the reference holds it (block IDs from 1)."""
+        lp = np.asfortranarray(lp, np.int32)
+        r = None if rows is None else np.ascontiguousarray(rows, np.int32)
+        self._check(self.L.w2d_set_links(self.h, _pi32(lp), 1, lp.shape[0], None if r is None else _pi32(r),
+                                         0 if r is None else r.size), "w2d_set_links")
+
+    def admesh_flags(self, cap: int):
+        """(refines, first sons of the families coarsened) of one admesh
+        pass, from the device's flag loops (w2d_admesh_flags)."""
+        r = np.zeros(max(cap, 1), np.int32)
+        q = np.zeros(max(cap, 1), np.int32)
+        nr, nc = C.c_int(0), C.c_int(0)
+        self._check(self.L.w2d_admesh_flags(self.h, _pi32(r), cap, C.byref(nr), _pi32(q), cap, C.byref(nc)),
+                    "w2d_admesh_flags")
+        return r[:nr.value].copy(), q[:nc.value].copy()
+
     def refine(self, quads):
         q = np.ascontiguousarray(quads, np.int32).reshape(-1, 5)
         self._check(self.L.w2d_refine(self.h, _pi32(q), q.shape[0]), "w2d_refine")
@@ -261,6 +279,10 @@ class Simulation:
 
     def set_amr(self, on: bool):
         self.L.w2d_sim_set_amr(self.h, 1 if on else 0)
+
+    def set_device_flags(self, on: bool):
+        """admesh flags on the device (default) or on the host."""
+        self.L.w2d_sim_set_device_flags(self.h, 1 if on else 0)
 
     PHASES = ("topology", "dt_half_launch", "plan", "dt_wait", "tstep_launch", "criteria_wait",
               "admesh_host", "amr_calls", "step_total")

@@ -696,7 +696,7 @@ int w2d_destroy(W2dCtx* c)
   for (auto e : c->evpool) cudaEventDestroy(e);
   for (auto e : c->ev)
     if (e) cudaEventDestroy(e);
-  cudaEvent_t evs[] = {c->ev_topo, c->ev_ops, c->ev_plan[0], c->ev_plan[1], c->ev_dt};
+  cudaEvent_t evs[] = {c->ev_topo, c->ev_ops, c->ev_plan[0], c->ev_plan[1], c->ev_dt, c->ev_links};
   for (auto e : evs)
     if (e) cudaEventDestroy(e);
   if (c->gx_first) cudaGraphExecDestroy(c->gx_first);
@@ -706,10 +706,12 @@ int w2d_destroy(W2dCtx* c)
       if (c->tune_ev[k][q]) cudaEventDestroy(c->tune_ev[k][q]);
   if (c->h_nleaf) cudaFreeHost(c->h_nleaf);
   void* dev2[] = {c->d_run_of, c->d_runs, c->d_dt_run, c->d_loff, c->d_gradleaf, c->d_fb, c->d_fb_count,
-                  c->d_nn_counts, c->d_nleaf};
+                  c->d_nn_counts, c->d_nleaf, c->d_links, c->d_son, c->d_mflags, c->d_mlists, c->d_rows6};
   for (void* d : dev2)
     if (d) cudaFree(d);
   if (c->h_dt_run) cudaFreeHost(c->h_dt_run);
+  if (c->h_mlists) cudaFreeHost(c->h_mlists);
+  if (c->h_rows6) cudaFreeHost(c->h_rows6);
   if (c->h_loff) cudaFreeHost(c->h_loff);
   void* dev[] = {c->d_u, c->d_up, c->d_prim, c->d_lev, c->d_icoord, c->d_cfl, c->d_dtcool, c->d_grad,
                  c->d_err, c->d_dt, c->d_cooltab, c->d_leaves, c->d_fd1, c->d_fd2, c->d_stage, c->d_ids,
@@ -976,6 +978,139 @@ int w2d_criteria(W2dCtx* c, double* grad)
   int rc = sync_and_check(c);
   if (rc) return rc;
   for (int nb = 1; nb <= c->nbmax; ++nb) grad[nb - 1] = c->leaf[nb] ? c->h_grad[nb - 1] : -1.0;
+  return W2D_OK;
+}
+
+namespace {
+
+// The device side of the admesh flags, allocated on first use (contexts
+// whose host takes the flags from w2d_criteria never hold it).
+int ensure_mark(W2dCtx* c)
+{
+  if (c->d_links) return W2D_OK;
+  const size_t slots = (size_t)c->cap + 1;
+  CK(cudaMalloc(&c->d_links, sizeof(int4) * slots));
+  CK(cudaMalloc(&c->d_son, sizeof(int) * slots));
+  CK(cudaMalloc(&c->d_mflags, 4 * slots));
+  CK(cudaMalloc(&c->d_mlists, sizeof(int) * (4 + 2 * slots)));
+  CK(cudaMalloc(&c->d_rows6, sizeof(int) * 6 * slots));
+  CK(cudaMallocHost(&c->h_mlists, sizeof(int) * (4 + 2 * slots)));
+  CK(cudaMallocHost(&c->h_rows6, sizeof(int) * 6 * slots));
+  CK(cudaEventCreateWithFlags(&c->ev_links, cudaEventDisableTiming));
+  CK(cudaMemsetAsync(c->d_links, 0xff, sizeof(int4) * slots, c->st));   // -1: no neighbour
+  CK(cudaMemsetAsync(c->d_son, 0, sizeof(int) * slots, c->st));
+  return W2D_OK;
+}
+
+}  // namespace
+
+int w2d_set_links(W2dCtx* c, const int32_t* lp, int row_stride, int col_stride, const int32_t* rows, int nrows)
+{
+  if (!c || !lp || (rows && nrows < 0) || (!rows && nrows != 0)) return W2D_ERR_ARG;
+  if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
+  int rc = ensure_mark(c);
+  if (rc) return rc;
+  const int n = rows ? nrows : c->nbmax;
+  const int chunk = c->cap + 1;
+  for (int k0 = 0; k0 < n; k0 += chunk) {
+    const int m = std::min(chunk, n - k0);
+    CK(cudaEventSynchronize(c->ev_links));   // the previous chunk has left the staging
+    int* h = c->h_rows6;
+    for (int k = 0; k < m; ++k) {
+      const int nb = rows ? rows[k0 + k] : k0 + k + 1;
+      if (nb < 1 || nb > c->cap)
+        return set_error(c, W2D_ERR_ARG, nb, 0, 0, "block ID %d outside 1..%d", nb, c->cap);
+      const int32_t* r = lp + (size_t)(nb - 1) * row_stride;
+      int* o = h + 6 * (size_t)k;
+      o[0] = nb;
+      o[1] = r[(size_t)3 * col_stride];
+      for (int s = 0; s < 4; ++s) {
+        const int v = r[(size_t)(4 + s) * col_stride];
+        if (v != -1 && (v < 1 || v > c->cap))
+          return set_error(c, W2D_ERR_ARG, nb, 5 + s, 0, "lp(%d,%d) = %d is no block of the pool", nb, 5 + s, v);
+        o[2 + s] = v;
+      }
+    }
+    CK(cudaMemcpyAsync(c->d_rows6, h, sizeof(int) * 6 * (size_t)m, cudaMemcpyHostToDevice, c->st));
+    if ((rc = launch(c, "set_links", [&] { return launch_set_links(c->d_rows6, m, c->d_links, c->d_son, c->st); })))
+      return rc;
+    CK(cudaEventRecord(c->ev_links, c->st));
+  }
+  c->have_links = true;
+  return W2D_OK;
+}
+
+int w2d_admesh_flags(W2dCtx* c, int32_t* refine, int cap_refine, int* nrefine, int32_t* coarsen, int cap_coarsen,
+                     int* ncoarsen)
+{
+  if (!c || !nrefine || !ncoarsen || cap_refine < 0 || cap_coarsen < 0 || (cap_refine > 0 && !refine) ||
+      (cap_coarsen > 0 && !coarsen))
+    return W2D_ERR_ARG;
+  *nrefine = *ncoarsen = 0;
+  if (!c->have_topology || !c->have_links)
+    return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology and w2d_set_links first");
+  if (c->nruns > 0) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "one run per context");
+  const size_t slots = (size_t)c->cap + 1;
+  CK(cudaMemsetAsync(c->d_mflags, 0, 4 * slots, c->st));
+  CK(cudaMemsetAsync(c->d_mlists, 0, 4 * sizeof(int), c->st));
+  MarkArgs a{};
+  a.leaves = c->d_leaves;
+  a.nleaf = c->nleaf;
+  a.nbmax = c->nbmax;
+  a.cap = c->cap;
+  a.nlevs = c->p.nlevs;
+  a.lev = c->d_lev;
+  a.links = c->d_links;
+  a.son = c->d_son;
+  a.grad = c->d_grad;
+  a.tol = c->p.tol;
+  a.tol2 = c->p.tol2;
+  a.leafp = c->d_mflags;
+  a.up = c->d_mflags + slots;
+  a.down = c->d_mflags + 2 * slots;
+  a.down2 = c->d_mflags + 3 * slots;
+  a.counts = c->d_mlists;
+  a.rlist = c->d_mlists + 4;
+  a.clist = c->d_mlists + 4 + slots;
+  int rc = launch(c, "markref", [&] { return launch_markref(a, c->st); });
+  for (int nl = c->p.nlevs - 1; nl >= 1 && !rc; --nl)
+    rc = launch(c, "critneighup", [&] { return launch_critneighup(a, nl, c->st); });
+  if (!rc) rc = launch(c, "critneighdown", [&] { return launch_critneighdown(a, c->st); });
+  if (!rc) rc = launch(c, "coarsen_families", [&] { return launch_coarsen_families(a, c->st); });
+  if (rc) return rc;
+  // the counters and the heads of both lists in one wait; longer lists
+  // (rare: a pass that remeshes thousands of blocks) in a second one
+  const int head = (int)std::min<size_t>(slots, 2048);
+  int* h = c->h_mlists;
+  CK(cudaMemcpyAsync(h, c->d_mlists, sizeof(int) * (4 + (size_t)head), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(h + 4 + slots, c->d_mlists + 4 + slots, sizeof(int) * (size_t)head, cudaMemcpyDeviceToHost,
+                     c->st));
+  if ((rc = sync_and_check(c))) return rc;
+  const int nr = std::min(h[0], (int)slots), nc = std::min(h[1], (int)slots);
+  if (nr > head || nc > head) {
+    if (nr > head)
+      CK(cudaMemcpyAsync(h + 4 + head, c->d_mlists + 4 + head, sizeof(int) * (size_t)(nr - head),
+                         cudaMemcpyDeviceToHost, c->st));
+    if (nc > head)
+      CK(cudaMemcpyAsync(h + 4 + slots + head, c->d_mlists + 4 + slots + head, sizeof(int) * (size_t)(nc - head),
+                         cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  // admesh's visiting order: refines by level ascending, coarsenings by
+  // level descending, IDs ascending within a level (the device appended
+  // them in atomic order)
+  int* r = h + 4;
+  int* q = h + 4 + slots;
+  const int* lev = c->lev;
+  std::sort(r, r + nr, [lev](int x, int y) { return lev[x] != lev[y] ? lev[x] < lev[y] : x < y; });
+  std::sort(q, q + nc, [lev](int x, int y) { return lev[x] != lev[y] ? lev[x] > lev[y] : x < y; });
+  *nrefine = nr;
+  *ncoarsen = nc;
+  if (nr > cap_refine || nc > cap_coarsen)
+    return set_error(c, W2D_ERR_ARG, 0, 0, 0, "admesh lists of %d and %d entries exceed %d and %d", nr, nc,
+                     cap_refine, cap_coarsen);
+  if (nr) memcpy(refine, r, sizeof(int) * (size_t)nr);
+  if (nc) memcpy(coarsen, q, sizeof(int) * (size_t)nc);
   return W2D_OK;
 }
 

@@ -92,6 +92,18 @@ struct W2dCtx {
   std::vector<int> qfirst, qlast;          // per slot: first/last list position as nbs
   cudaEvent_t ev_plan[2] = {nullptr, nullptr};
   int plan_buf = 0;
+  // admesh flags on the device (allocated by the first w2d_set_links): the
+  // mirror of lp(:,4:8), four byte planes of cap+1 flags, the two lists
+  // behind two counters, and the pinned row staging of w2d_set_links
+  int4* d_links = nullptr;
+  int* d_son = nullptr;
+  unsigned char* d_mflags = nullptr;
+  int* d_mlists = nullptr;    // [4 counters][cap+1 refines][cap+1 first sons]
+  int* h_mlists = nullptr;    // pinned, same layout
+  int* d_rows6 = nullptr;     // (nb, lp(nb,4:8)) per row, cap+1 rows
+  int* h_rows6 = nullptr;     // pinned
+  cudaEvent_t ev_links = nullptr;
+  bool have_links = false;
   // pinned staging of refine/coarse lists
   int* h_ops = nullptr;
   int h_ops_cap = 0;

@@ -117,6 +117,15 @@ void updatelpup(W2dSim* s, int nb, int s1, int s2, int s3, int s4)
   const int nlev2 = L.LP(nb, 1) + 1;
   int nsr;
   s->nbleafs += 3;
+  if (s->devflags) {   // rows whose lp(:,4:8) this call may change
+    const int rows[4] = {s1, s2, s3, s4};
+    s->touched.insert(s->touched.end(), rows, rows + 4);
+    for (int k = 5; k <= 8; ++k) {
+      const int n1 = L.LP(nb, k);
+      if (n1 != -1 && !L.LEAF(n1))
+        for (int q = 0; q < 4; ++q) s->touched.push_back(L.LP(n1, 3) + q);
+    }
+  }
   L.LP(s1, 1) = nlev2; L.LP(s1, 2) = nb; L.LP(s1, 4) = 1; L.LP(s1, 6) = s2; L.LP(s1, 8) = s3;
   if (L.LP(nb, 5) == -1 || L.LEAF(L.LP(nb, 5))) L.LP(s1, 5) = L.LP(nb, 5);
   else { nsr = L.LP(L.LP(nb, 5), 3) + 1; L.LP(s1, 5) = nsr; L.LP(nsr, 6) = s1; }
@@ -161,6 +170,12 @@ void updatelpdown(W2dSim* s, int dad, int s1, int s2, int s3, int s4)
   L.LEAF(dad) = 1;
   L.LEAF(s1) = L.LEAF(s2) = L.LEAF(s3) = L.LEAF(s4) = 0;
   s->nbleafs -= 3;
+  if (s->devflags)     // the sons of dad's non-leaf neighbours get new links
+    for (int k = 5; k <= 8; ++k) {
+      const int n1 = L.LP(dad, k);
+      if (n1 != -1 && !L.LEAF(n1))
+        for (int q = 0; q < 4; ++q) s->touched.push_back(L.LP(n1, 3) + q);
+    }
   int nb1 = L.LP(dad, 5);
   if (nb1 != -1 && !L.LEAF(nb1)) { nb1 = L.LP(L.LP(nb1, 3), 6); L.LP(nb1, 6) = dad; L.LP(L.LP(nb1, 8), 6) = dad; }
   nb1 = L.LP(dad, 6);
@@ -339,16 +354,82 @@ int admesh_decide(W2dSim* s)
   return W2D_OK;
 }
 
-// admesh of the single-run driver: criteria from the device, the integer
-// part, then the u motion of every refine and coarse of the pass in one
-// device call (within a pass no refine or coarse reads a block that another
-// one writes)
+// src/admesh.f90:29-105 from the lists of the flag loops (the device's
+// w2d_admesh_flags): the refines in order, allocating sons as admesh does,
+// then the coarsenings in order.
+int admesh_apply(W2dSim* s, const int32_t* refine, int nr, const int32_t* first_sons, int nc)
+{
+  auto& L = *s;
+  int nbmaxp = s->nbmax;
+  s->rops.clear();
+  s->cops.clear();
+  for (int k = 0; k < nr; ++k) {
+    const int nb = refine[k];
+    int s1, s2, s3, s4;
+    if (L.LP(nb, 3) == 0) {
+      s1 = nbmaxp + 1; s2 = s1 + 1; s3 = s1 + 2; s4 = s1 + 3;
+      if (s4 > s->cap) return W2D_ERR_CAPACITY;   // admesh.f90:44-47
+      L.LP(nb, 3) = s1;
+      nbmaxp += 4;
+    } else {
+      s1 = L.LP(nb, 3); s2 = L.LP(s1, 6); s3 = L.LP(s1, 8); s4 = L.LP(s3, 6);
+    }
+    s->nbmax = nbmaxp;
+    const int q[5] = {nb, s1, s2, s3, s4};
+    s->rops.insert(s->rops.end(), q, q + 5);
+    updatelpup(s, nb, s1, s2, s3, s4);
+  }
+  for (int k = 0; k < nc; ++k) {
+    const int nb = first_sons[k];
+    const int dad = L.LP(nb, 2), s1 = nb, s2 = L.LP(nb, 6), s3 = L.LP(nb, 8);
+    const int s4 = L.LP(L.LP(nb, 6), 8);
+    const int q[5] = {dad, s1, s2, s3, s4};
+    s->cops.insert(s->cops.end(), q, q + 5);
+    updatelpdown(s, dad, s1, s2, s3, s4);
+  }
+  if (!s->rops.empty() || !s->cops.empty()) s->dirty = true;
+  return W2D_OK;
+}
+
+// the device mirror of lp(:,4:8): every row after a new tree, else the rows
+// the last pass changed
+int push_links(W2dSim* s)
+{
+  const int32_t* rows = s->links_all ? nullptr : s->touched.data();
+  const int n = s->links_all ? 0 : (int)s->touched.size();
+  if (!s->links_all && n == 0) return W2D_OK;
+  int rc = w2d_set_links(s->ctx, s->lp.data() + 8, 8, 1, rows, n);
+  if (rc) return rc;
+  s->links_all = false;
+  s->touched.clear();
+  return W2D_OK;
+}
+
+// admesh of the single-run driver: the flags (on the device, or on the host
+// from the criteria download), the integer part, then the u motion of every
+// refine and coarse of the pass in one device call (within a pass no refine
+// or coarse reads a block that another one writes)
 int admesh(W2dSim* s)
 {
   int rc;
   if (s->dirty && (rc = refresh_plan(s))) return rc;
-  // markref + criteria flags (criteria.f90:36-50 on the device maximum)
   double t0 = now_ms();
+  if (s->devflags) {
+    if ((rc = push_links(s))) return rc;
+    int nr = 0, nc = 0;
+    const int n = s->cap + 1;
+    if ((int)s->rlist.size() < n) { s->rlist.resize(n); s->clist.resize(n); }
+    if ((rc = w2d_admesh_flags(s->ctx, s->rlist.data(), n, &nr, s->clist.data(), n, &nc))) return rc;
+    double t1 = now_ms();
+    s->phase_ms[5] += t1 - t0;
+    if ((rc = admesh_apply(s, s->rlist.data(), nr, s->clist.data(), nc))) return rc;
+    t0 = now_ms();
+    s->phase_ms[6] += t0 - t1;
+    if ((nr || nc) && (rc = ctx_amr(s->ctx, s->rops.data(), nr, s->cops.data(), nc))) return rc;
+    s->phase_ms[7] += now_ms() - t0;
+    return W2D_OK;
+  }
+  // markref + criteria flags (criteria.f90:36-50 on the device maximum)
   rc = w2d_criteria(s->ctx, s->grad.data());
   if (rc) return rc;
   double t1 = now_ms();
@@ -402,6 +483,7 @@ int basegrid_tree(W2dSim* s, std::vector<int32_t>& ids, std::vector<double>& blo
   blocks.assign(bs * ids.size(), 0.0);
   for (size_t q = 0; q < ids.size(); ++q) initial_block(s, ids[q], blocks.data() + q * bs);
   s->dirty = true;
+  s->links_all = true;
   return W2D_OK;
 }
 
@@ -453,6 +535,7 @@ int w2d_sim_create(const W2dParams* p, const W2dInit* ic, W2dSim** out)
   *out = nullptr;
   W2dSim* s = new W2dSim();
   init_tree(s, p, ic);
+  s->devflags = true;
   int rc = w2d_create(p, &s->ctx);
   if (rc) { delete s; return rc; }
   if ((rc = basegrid(s))) { w2d_sim_destroy(s); return rc; }
@@ -586,6 +669,17 @@ int w2d_sim_set_amr(W2dSim* s, int on)
   return W2D_OK;
 }
 
+int w2d_sim_set_device_flags(W2dSim* s, int on)
+{
+  if (!s) return W2D_ERR_ARG;
+  if ((on != 0) != s->devflags) {
+    s->devflags = on != 0;
+    s->links_all = true;    // the mirror is rebuilt from the host tree
+    s->touched.clear();
+  }
+  return W2D_OK;
+}
+
 int w2d_sim_set_cooltab(W2dSim* s, const double* log_t, const double* neg_log_l, int n)
 {
   if (!s) return W2D_ERR_ARG;
@@ -702,6 +796,8 @@ int w2d_sim_read_bin(W2dSim* s, const char* pointers, const char* blocks, double
   s->time = time;
   s->dt = 0.0;
   s->dirty = true;
+  s->links_all = true;
+  s->touched.clear();
   int rc = push_topology(s);
   if (rc) return rc;
   if ((rc = w2d_put_blocks(s->ctx, ids.data(), (int)ids.size(), u.data()))) return rc;

@@ -42,6 +42,31 @@ cudaError_t launch_dt(const int* leaves, int n, const int* n_dev, int grid, cons
 cudaError_t launch_dt_runs(const int* leaves, const int* loff, int nruns, const double* cfl, const double* dtcool,
                            int use_cool, double courant, double psc, double tsc, double* dt_run, cudaStream_t st);
 
+// admesh flags on the device (w2d_mark.cu).  Per slot: lev, the mirror of
+// lp(:,4) (son) and lp(:,5:8) (links), the criteria maximum grad; byte
+// planes leafp, up, down, down2 zeroed before markref; counts[0..1] the
+// lengths of rlist (refines) and clist (first sons of coarsened families),
+// zeroed before, in atomic order.
+struct MarkArgs {
+  const int* leaves;
+  int nleaf, nbmax, cap, nlevs;
+  const int* lev;
+  const int4* links;
+  const int* son;
+  const double* grad;
+  double tol, tol2;
+  unsigned char *leafp, *up, *down, *down2;
+  int* counts;
+  int* rlist;
+  int* clist;
+};
+cudaError_t launch_markref(const MarkArgs& a, cudaStream_t st);
+cudaError_t launch_critneighup(const MarkArgs& a, int nl, cudaStream_t st);
+cudaError_t launch_critneighdown(const MarkArgs& a, cudaStream_t st);
+cudaError_t launch_coarsen_families(const MarkArgs& a, cudaStream_t st);
+// rows6: (nb, lp(nb,4), lp(nb,5..8)) per row
+cudaError_t launch_set_links(const int* rows6, int n, int4* links, int* son, cudaStream_t st);
+
 // one bounded wait that runs out (see w2d_wait_selftest)
 cudaError_t launch_wait_selftest(int* err, cudaStream_t st);
 

@@ -30,6 +30,11 @@ struct W2dSim {
   std::vector<std::vector<int32_t>> bucket;  // leaves per level, ascending ID
   std::vector<double> grad;
   std::vector<int32_t> rops, cops;
+  // admesh flags from the device (single-run driver): rows of lp(:,4:8)
+  // changed since the device mirror was last updated (all of them while
+  // links_all), and the lists w2d_admesh_flags returns
+  bool devflags = false, links_all = true;
+  std::vector<int32_t> touched, rlist, clist;
   std::vector<int32_t> ib1, ib2, ib3;
   double phase_ms[W2D_SIM_NPHASES] = {0};               // see w2d_sim_phase_ms
 
@@ -46,6 +51,10 @@ double now_ms();
 void locatebounds(W2dSim* s);
 // src/admesh.f90:4-111 integer part from s->grad: fills s->rops / s->cops
 int admesh_decide(W2dSim* s);
+// the same pass from the refine list (level ascending, then ID) and the
+// first sons of the families to coarsen (level descending, then ID) that
+// the flag loops produce: fills s->rops / s->cops
+int admesh_apply(W2dSim* s, const int32_t* refine, int nr, const int32_t* first_sons, int nc);
 // basegrid tree and initial conditions of the leaves (ids, block-major u)
 int basegrid_tree(W2dSim* s, std::vector<int32_t>& ids, std::vector<double>& blocks);
 // host arrays of a run of capacity p->nblocks, spacings of its levels
