@@ -531,6 +531,7 @@ def run_ours(args, ws, rank, local):
     p, ic = config("sedov_amr")
     p.precision = args.precision
     sim = Simulation(p, ic)
+    sim.set_tree_mode(args.tree)   # where admesh flags and fill plans are built
     ctx = sim.ctx
     ctx.set_graphs(True)        # each step as two CUDA graphs over persistent launches
     sim.run(max(args.pre_steps - 16, 0))
@@ -647,7 +648,8 @@ def run_ours(args, ws, rank, local):
                        "leaves_at_start": st0["nleaf"], "leaves_at_end": st1["nleaf"],
                        "pre_steps": args.pre_steps, "l2": "flushed (256 MB write) before every timed step",
                        "parallelism": f"replicas x{ws}",
-                       "cuda_graphs": True, "launch_shapes": ctx.tuning()},
+                       "cuda_graphs": True, "launch_shapes": ctx.tuning(),
+                       "tree_work": "%s (%s at the end)" % sim.tree_mode()},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -678,6 +680,9 @@ def main():
                     help="skip the remnant and DMC-jet comparisons of FP64 and FP32 + learned cooling")
     ap.add_argument("--batched-runs", type=int, default=ENS_RUNS,
                     help="runs in the batched ensemble (fewer for profiling)")
+    ap.add_argument("--tree", default="auto", choices=["auto", "device", "host"],
+                    help="where the headline run's admesh flags and fill plans are built "
+                         "(auto: timed both ways on the run, the faster kept)")
     ap.add_argument("--pre-steps", type=int, default=PRE_STEPS,
                     help="untimed steps before warm-up (smaller cases for profiling)")
     args = ap.parse_args()

@@ -159,13 +159,16 @@ int w2d_tstep(W2dCtx* ctx, double time, double dt);
 int w2d_criteria(W2dCtx* ctx, double* grad);
 /* The admesh flags on the device, for hosts that keep lp on the host but
  * want neither the per-block criteria download nor the flag loops over
- * nbmax.  w2d_set_links mirrors lp(nb,4:8) (son position and the four
- * neighbours) of the listed rows to the device: element (nb,k) of lp is
+ * nbmax.  w2d_set_links mirrors lp(nb,3:8) (first son, son position and
+ * the four neighbours) of the listed rows to the device: element (nb,k) of
+ * lp is
  * lp[(nb-1)*row_stride + (k-1)*col_stride] (Fortran lp(nbmin:,8) with
  * nbmin = 1: row_stride 1, col_stride = its leading dimension).  rows NULL
  * sends blocks 1..nbmax of the last w2d_set_topology; otherwise the nrows
  * IDs listed (duplicates allowed), e.g. those updatelpup/updatelpdown
- * changed.  Neighbours must be -1 or block IDs within the pool. */
+ * changed (and the parent whose lp(nb,3) admesh set).  Neighbours must be
+ * -1 or block IDs within the pool, lp(nb,3) 0 or the first of four IDs
+ * within it. */
 int w2d_set_links(W2dCtx* ctx, const int32_t* lp, int row_stride, int col_stride,
                   const int32_t* rows, int nrows);
 /* markref (src/markref.f90:23-44 with criteria's flags), critneighup
@@ -182,6 +185,12 @@ int w2d_set_links(W2dCtx* ctx, const int32_t* lp, int row_stride, int col_stride
  * list is longer than its capacity (the counts are still set). */
 int w2d_admesh_flags(W2dCtx* ctx, int32_t* refine, int cap_refine, int* nrefine,
                      int32_t* coarsen, int cap_coarsen, int* ncoarsen);
+/* locatebounds (src/locatebounds.f90:29-540) and the fill plans built from
+ * its list, on the device, from the tree of w2d_set_topology +
+ * w2d_set_links (lp(:,3:8)): the same plans as building innerbounds on the
+ * host and passing it to w2d_set_bounds, for hosts that do not need the
+ * list themselves.  Queued on the context's stream (no wait). */
+int w2d_locate_bounds(W2dCtx* ctx);
 /* The u motion of refine (src/refine.f90:30-38, 227-258): quads[k*5+0] is
  * the parent, quads[k*5+1..4] the four sons (BL, BR, TL, TR). */
 int w2d_refine(W2dCtx* ctx, const int32_t* quads, int n);
@@ -278,10 +287,26 @@ int w2d_sim_tree(W2dSim* sim, int32_t* lp, int32_t* leaf, int32_t* icoord,
                  int32_t* innerbounds, int32_t* ninternal);
 /* Enables/disables AMR (admesh after each step); on by default if nlevs>1. */
 int w2d_sim_set_amr(W2dSim* sim, int on);
-/* Where admesh takes its flags: 1 (default) on the device through
- * w2d_admesh_flags, 0 on the host from the w2d_criteria download.  Both
- * give the same refines and coarsenings. */
+/* Where the block tree's per-step integer work runs.  W2D_TREE_DEVICE:
+ * admesh takes its flags from w2d_admesh_flags and the fill plans come from
+ * w2d_locate_bounds; W2D_TREE_HOST: flags from the w2d_criteria download
+ * and the host's loops, plans from the host's locatebounds through
+ * w2d_set_bounds.  Both give the same refines, coarsenings and plans, so
+ * the same run.  W2D_TREE_AUTO (default): whenever the leaf count has moved
+ * by half since the last choice (and at the start), the driver times four
+ * steps each way (after one untimed step each) and keeps the faster; the
+ * device side wins on large trees, where the host's loops no longer hide
+ * behind the half step. */
+#define W2D_TREE_HOST   0
+#define W2D_TREE_DEVICE 1
+#define W2D_TREE_AUTO   2
+int w2d_sim_set_tree_mode(W2dSim* sim, int mode);
+/* The mode set and the side in use now (1 device, 0 host). */
+int w2d_sim_tree_mode(W2dSim* sim, int* mode, int* device);
+/* Each half alone (for tests; leaves W2D_TREE_AUTO): the flags (1 device,
+ * 0 host) and the plans (1 device, 0 host). */
 int w2d_sim_set_device_flags(W2dSim* sim, int on);
+int w2d_sim_set_device_plans(W2dSim* sim, int on);
 /* DMC table for the driver's context (as w2d_set_cooltab), then the
  * primitives and per-block partials of every leaf are recomputed with it. */
 int w2d_sim_set_cooltab(W2dSim* sim, const double* log_t, const double* neg_log_l, int n);

@@ -1,12 +1,21 @@
-"""admesh's flag loops on the device (w2d_admesh_flags: markref,
-critneighup and critneighdown with the effect of the pass's refines, then
-the refine and coarsen lists in admesh's order) against the same loops on
-the host from the criteria download (src/admesh.f90:23-105).
+"""The block tree's integer work on the device against the same work on
+the host:
 
-- the single-run driver with either source of flags takes the same refines
-  and coarsenings every step: identical lp, leaf and icoord after every
-  step, identical blocks at the end (AMR blast, jet, remnant with coolingh,
-  cylindrical jet);
+- admesh's flag loops (w2d_admesh_flags: markref, critneighup and
+  critneighdown with the effect of the pass's refines, then the refine and
+  coarsen lists in admesh's order) against the loops on the host from the
+  criteria download (src/admesh.f90:23-105);
+- locatebounds and the fill plans (w2d_locate_bounds) against the host's
+  locatebounds list handed to w2d_set_bounds (src/locatebounds.f90:29-540).
+
+Checks:
+
+- the single-run driver with the device's flags and plans and with the
+  host's takes the same refines and coarsenings and the same fills every
+  step: identical lp, leaf, icoord and dt after every step, identical
+  blocks at the end (AMR blast with and without the OUTFYB defect, jet,
+  remnant with coolingh, cylindrical jet with reflective walls), and each
+  device part alone against the host;
 - passes that refine or coarsen thousands of blocks at once (more than one
   download of the lists);
 - the device mirror of lp(:,4:8) rejects neighbours outside the pool.
@@ -21,12 +30,15 @@ from helpers import noncorner_mask
 pytestmark = pytest.mark.gpu
 
 
-def _pair(p, ic):
+def _pair(p, ic, flags=False, plans=False):
+    """a: the defaults (device flags and plans); b: the host's flags unless
+    `flags`, the host's plans unless `plans`."""
     from walicxe2d_b200.api import Simulation
     from walicxe2d_b200.params import COOLINGDMC
-    a = Simulation(p, ic)               # device flags (the default)
+    a = Simulation(p, ic)
     b = Simulation(p, ic)
-    b.set_device_flags(False)           # host loops over w2d_criteria
+    b.set_device_flags(flags)           # False: host loops over w2d_criteria
+    b.set_device_plans(plans)           # False: host locatebounds + w2d_set_bounds
     if p.cooling == COOLINGDMC:
         rows = np.loadtxt(os.path.join(os.path.dirname(__file__), "golden", "coolingDMC.tab"))
         for s in (a, b):
@@ -47,12 +59,16 @@ def _same_blocks(a, b):
     assert np.array_equal(ua[:, :, m], ub[:, :, m])
 
 
-@pytest.mark.parametrize("name,steps", [("sedov_amr_small", 80), ("jet_small", 80), ("snr_small", 40),
-                                        ("jet_cyl_small", 40)])
-def test_device_flags_equal_host_flags(name, steps):
+@pytest.mark.parametrize("name,steps", [("sedov_amr_small", 80), ("sedov_amr_small_nocompat", 240),
+                                        ("jet_small", 80), ("snr_small", 40), ("jet_cyl_small", 40)])
+@pytest.mark.parametrize("which", ["both", "flags", "plans"])
+def test_device_tree_work_equals_host(name, steps, which):
     from walicxe2d_b200.params import config
-    p, ic = config(name)
-    a, b = _pair(p, ic)
+    p, ic = config(name.replace("_nocompat", ""))
+    if name.endswith("_nocompat"):
+        p.compat = 0
+    # "flags": only the flags differ (both sides build plans on the device), etc.
+    a, b = _pair(p, ic, flags=(which == "plans"), plans=(which == "flags"))
     _same_tree(a, b)
     leaves = set()
     for _ in range(steps):
@@ -85,6 +101,24 @@ def test_passes_with_thousands_of_changes(mode):
         assert n0 == 2304 and n1 == 2304 * 16, (n0, n1)
     else:
         assert n0 == 2304 * 16 and n1 == 2304, (n0, n1)
+    _same_blocks(a, b)
+
+
+@pytest.mark.parametrize("mode", ["device", "host"])
+def test_fixed_tree_modes_equal_auto(mode):
+    """W2D_TREE_DEVICE and W2D_TREE_HOST against the default W2D_TREE_AUTO
+    (whose trials switch sides during the run): the same run."""
+    from walicxe2d_b200.api import Simulation
+    from walicxe2d_b200.params import config
+    p, ic = config("jet_small")
+    a = Simulation(p, ic)
+    b = Simulation(p, ic)
+    b.set_tree_mode(mode)
+    assert a.tree_mode()[0] == "auto" and b.tree_mode() == (mode, mode)
+    for _ in range(40):
+        a.run(1)
+        b.run(1)
+        _same_tree(a, b)
     _same_blocks(a, b)
 
 

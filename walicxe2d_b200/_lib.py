@@ -39,6 +39,7 @@ SIGNATURES = {
     "w2d_criteria": (_I, [_vp, _PD]),
     "w2d_set_links": (_I, [_vp, _PI32, _I, _I, _PI32, _I]),
     "w2d_admesh_flags": (_I, [_vp, _PI32, _I, C.POINTER(_I), _PI32, _I, C.POINTER(_I)]),
+    "w2d_locate_bounds": (_I, [_vp]),
     "w2d_refine": (_I, [_vp, _PI32, _I]),
     "w2d_coarse": (_I, [_vp, _PI32, _I]),
     "w2d_boundaryI": (_I, [_vp, _D]),
@@ -62,6 +63,9 @@ SIGNATURES = {
     "w2d_sim_tree": (_I, [_vp, _PI32, _PI32, _PI32, _PI32, _PI32]),
     "w2d_sim_set_amr": (_I, [_vp, _I]),
     "w2d_sim_set_device_flags": (_I, [_vp, _I]),
+    "w2d_sim_set_device_plans": (_I, [_vp, _I]),
+    "w2d_sim_set_tree_mode": (_I, [_vp, _I]),
+    "w2d_sim_tree_mode": (_I, [_vp, C.POINTER(_I), C.POINTER(_I)]),
     "w2d_sim_set_cooltab": (_I, [_vp, _PD, _PD, _I]),
     "w2d_sim_write_bin": (_I, [_vp, C.c_char_p, C.c_char_p, C.c_int32]),
     "w2d_sim_read_bin": (_I, [_vp, C.c_char_p, C.c_char_p, _D, _I]),

@@ -149,12 +149,16 @@ class Context:
         return g[:nbmax]
 
     def set_links(self, lp, rows=None):
-        """Device mirror of lp(:,4:8) (w2d_set_links); lp column-major
+        """Device mirror of lp(:,3:8) (w2d_set_links); lp column-major
         [nblocks, 8] as the reference holds it (block IDs from 1)."""
         lp = np.asfortranarray(lp, np.int32)
         r = None if rows is None else np.ascontiguousarray(rows, np.int32)
         self._check(self.L.w2d_set_links(self.h, _pi32(lp), 1, lp.shape[0], None if r is None else _pi32(r),
                                          0 if r is None else r.size), "w2d_set_links")
+
+    def locate_bounds(self):
+        """locatebounds and the fill plans on the device (w2d_locate_bounds)."""
+        self._check(self.L.w2d_locate_bounds(self.h), "w2d_locate_bounds")
 
     def admesh_flags(self, cap: int):
         """(refines, first sons of the families coarsened) of one admesh
@@ -283,6 +287,27 @@ class Simulation:
     def set_device_flags(self, on: bool):
         """admesh flags on the device (default) or on the host."""
         self.L.w2d_sim_set_device_flags(self.h, 1 if on else 0)
+
+    TREE_MODES = ("host", "device", "auto")
+
+    def set_tree_mode(self, mode: str):
+        """Where the tree's per-step integer work runs: 'host', 'device' or
+        'auto' (default: timed both ways on the live run, the faster kept)."""
+        rc = self.L.w2d_sim_set_tree_mode(self.h, self.TREE_MODES.index(mode))
+        if rc:
+            self.ctx._check(rc, "w2d_sim_set_tree_mode")
+
+    def tree_mode(self) -> tuple:
+        """(mode set, side in use now: 'device' or 'host')."""
+        m, d = C.c_int(0), C.c_int(0)
+        self.L.w2d_sim_tree_mode(self.h, C.byref(m), C.byref(d))
+        name = self.TREE_MODES[m.value] if 0 <= m.value < 3 else "manual"
+        return name, ("device" if d.value else "host")
+
+    def set_device_plans(self, on: bool):
+        """Fill plans built on the device (default) or by the host's
+        locatebounds."""
+        self.L.w2d_sim_set_device_plans(self.h, 1 if on else 0)
 
     PHASES = ("topology", "dt_half_launch", "plan", "dt_wait", "tstep_launch", "criteria_wait",
               "admesh_host", "amr_calls", "step_total")

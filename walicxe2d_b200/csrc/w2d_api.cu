@@ -706,12 +706,13 @@ int w2d_destroy(W2dCtx* c)
       if (c->tune_ev[k][q]) cudaEventDestroy(c->tune_ev[k][q]);
   if (c->h_nleaf) cudaFreeHost(c->h_nleaf);
   void* dev2[] = {c->d_run_of, c->d_runs, c->d_dt_run, c->d_loff, c->d_gradleaf, c->d_fb, c->d_fb_count,
-                  c->d_nn_counts, c->d_nleaf, c->d_links, c->d_son, c->d_mflags, c->d_mlists, c->d_rows6};
+                  c->d_nn_counts, c->d_nleaf, c->d_links, c->d_sons, c->d_mflags, c->d_mlists, c->d_rows7,
+                  c->d_posof, c->d_bcnt, c->d_blocal, c->d_bcta, c->d_wpos};
   for (void* d : dev2)
     if (d) cudaFree(d);
   if (c->h_dt_run) cudaFreeHost(c->h_dt_run);
   if (c->h_mlists) cudaFreeHost(c->h_mlists);
-  if (c->h_rows6) cudaFreeHost(c->h_rows6);
+  if (c->h_rows7) cudaFreeHost(c->h_rows7);
   if (c->h_loff) cudaFreeHost(c->h_loff);
   void* dev[] = {c->d_u, c->d_up, c->d_prim, c->d_lev, c->d_icoord, c->d_cfl, c->d_dtcool, c->d_grad,
                  c->d_err, c->d_dt, c->d_cooltab, c->d_leaves, c->d_fd1, c->d_fd2, c->d_stage, c->d_ids,
@@ -990,15 +991,27 @@ int ensure_mark(W2dCtx* c)
   if (c->d_links) return W2D_OK;
   const size_t slots = (size_t)c->cap + 1;
   CK(cudaMalloc(&c->d_links, sizeof(int4) * slots));
-  CK(cudaMalloc(&c->d_son, sizeof(int) * slots));
+  CK(cudaMalloc(&c->d_sons, sizeof(int2) * slots));
   CK(cudaMalloc(&c->d_mflags, 4 * slots));
   CK(cudaMalloc(&c->d_mlists, sizeof(int) * (4 + 2 * slots)));
-  CK(cudaMalloc(&c->d_rows6, sizeof(int) * 6 * slots));
+  CK(cudaMalloc(&c->d_rows7, sizeof(int) * 7 * slots));
   CK(cudaMallocHost(&c->h_mlists, sizeof(int) * (4 + 2 * slots)));
-  CK(cudaMallocHost(&c->h_rows6, sizeof(int) * 6 * slots));
+  CK(cudaMallocHost(&c->h_rows7, sizeof(int) * 7 * slots));
   CK(cudaEventCreateWithFlags(&c->ev_links, cudaEventDisableTiming));
   CK(cudaMemsetAsync(c->d_links, 0xff, sizeof(int4) * slots, c->st));   // -1: no neighbour
-  CK(cudaMemsetAsync(c->d_son, 0, sizeof(int) * slots, c->st));
+  CK(cudaMemsetAsync(c->d_sons, 0, sizeof(int2) * slots, c->st));
+  return W2D_OK;
+}
+
+int ensure_plan(W2dCtx* c)
+{
+  if (c->d_posof) return W2D_OK;
+  const size_t slots = (size_t)c->cap + 1;
+  CK(cudaMalloc(&c->d_posof, sizeof(int) * slots));
+  CK(cudaMalloc(&c->d_bcnt, sizeof(int) * slots));
+  CK(cudaMalloc(&c->d_blocal, sizeof(int) * slots));
+  CK(cudaMalloc(&c->d_bcta, sizeof(int) * (2 * (slots / 256 + 1) + 1)));
+  CK(cudaMalloc(&c->d_wpos, sizeof(int) * slots));
   return W2D_OK;
 }
 
@@ -1015,24 +1028,27 @@ int w2d_set_links(W2dCtx* c, const int32_t* lp, int row_stride, int col_stride, 
   for (int k0 = 0; k0 < n; k0 += chunk) {
     const int m = std::min(chunk, n - k0);
     CK(cudaEventSynchronize(c->ev_links));   // the previous chunk has left the staging
-    int* h = c->h_rows6;
+    int* h = c->h_rows7;
     for (int k = 0; k < m; ++k) {
       const int nb = rows ? rows[k0 + k] : k0 + k + 1;
       if (nb < 1 || nb > c->cap)
         return set_error(c, W2D_ERR_ARG, nb, 0, 0, "block ID %d outside 1..%d", nb, c->cap);
       const int32_t* r = lp + (size_t)(nb - 1) * row_stride;
-      int* o = h + 6 * (size_t)k;
+      int* o = h + 7 * (size_t)k;
       o[0] = nb;
-      o[1] = r[(size_t)3 * col_stride];
+      o[1] = r[(size_t)2 * col_stride];    // first son (0: none yet)
+      o[2] = r[(size_t)3 * col_stride];    // son position
+      if (o[1] < 0 || o[1] > c->cap - 3)
+        return set_error(c, W2D_ERR_ARG, nb, 3, 0, "lp(%d,3) = %d: no four sons fit in the pool", nb, o[1]);
       for (int s = 0; s < 4; ++s) {
         const int v = r[(size_t)(4 + s) * col_stride];
         if (v != -1 && (v < 1 || v > c->cap))
           return set_error(c, W2D_ERR_ARG, nb, 5 + s, 0, "lp(%d,%d) = %d is no block of the pool", nb, 5 + s, v);
-        o[2 + s] = v;
+        o[3 + s] = v;
       }
     }
-    CK(cudaMemcpyAsync(c->d_rows6, h, sizeof(int) * 6 * (size_t)m, cudaMemcpyHostToDevice, c->st));
-    if ((rc = launch(c, "set_links", [&] { return launch_set_links(c->d_rows6, m, c->d_links, c->d_son, c->st); })))
+    CK(cudaMemcpyAsync(c->d_rows7, h, sizeof(int) * 7 * (size_t)m, cudaMemcpyHostToDevice, c->st));
+    if ((rc = launch(c, "set_links", [&] { return launch_set_links(c->d_rows7, m, c->d_links, c->d_sons, c->st); })))
       return rc;
     CK(cudaEventRecord(c->ev_links, c->st));
   }
@@ -1061,7 +1077,7 @@ int w2d_admesh_flags(W2dCtx* c, int32_t* refine, int cap_refine, int* nrefine, i
   a.nlevs = c->p.nlevs;
   a.lev = c->d_lev;
   a.links = c->d_links;
-  a.son = c->d_son;
+  a.sons = c->d_sons;
   a.grad = c->d_grad;
   a.tol = c->p.tol;
   a.tol2 = c->p.tol2;
@@ -1111,6 +1127,55 @@ int w2d_admesh_flags(W2dCtx* c, int32_t* refine, int cap_refine, int* nrefine, i
                      cap_refine, cap_coarsen);
   if (nr) memcpy(refine, r, sizeof(int) * (size_t)nr);
   if (nc) memcpy(coarsen, q, sizeof(int) * (size_t)nc);
+  return W2D_OK;
+}
+
+int w2d_locate_bounds(W2dCtx* c)
+{
+  if (!c) return W2D_ERR_ARG;
+  if (!c->have_topology || !c->have_links)
+    return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology and w2d_set_links first");
+  if (c->nruns > 0) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "one run per context");
+  int rc = ensure_plan(c);
+  if (rc) return rc;
+  const size_t slots = (size_t)c->cap + 1;
+  const int nl = c->nleaf;
+  CK(cudaMemsetAsync(c->d_posof, 0xff, sizeof(int) * slots, c->st));    // -1: not a leaf
+  if (nl > 0) {
+    CK(cudaMemsetAsync(c->d_fd1, 0, sizeof(int2) * 4 * (size_t)nl, c->st));   // (0, FK_KEEP)
+    CK(cudaMemsetAsync(c->d_fd2, 0, sizeof(int2) * 4 * (size_t)nl, c->st));
+    CK(cudaMemsetAsync(c->d_wpos, 0, sizeof(int) * (size_t)nl, c->st));
+  }
+  PlanArgs a{};
+  a.leaves = c->d_leaves;
+  a.nleaf = nl;
+  a.nbmax = c->nbmax;
+  a.cap = c->cap;
+  a.lev = c->d_lev;
+  a.links = c->d_links;
+  a.sons = c->d_sons;
+  a.posof = c->d_posof;
+  a.cnt = c->d_bcnt;
+  a.local = c->d_blocal;
+  const int g = plan_ctas(nl);
+  a.ctatot = c->d_bcta;
+  a.ctaoff = c->d_bcta + (slots / 256 + 1);
+  a.total = c->d_bcta + 2 * (slots / 256 + 1);
+  a.fd1 = c->d_fd1;
+  a.fd2 = c->d_fd2;
+  a.wpos = c->d_wpos;
+  a.jetblk = c->d_jetblk;
+  a.bc[0] = c->p.bc_left;
+  a.bc[1] = c->p.bc_right;
+  a.bc[2] = c->p.bc_bottom;
+  a.bc[3] = c->p.bc_top;
+  a.f6b = (c->p.compat & W2D_COMPAT_OUTFYB) != 0;
+  a.jet = c->p.otherb == W2D_USERBC_JET;
+  if ((rc = launch(c, "locatebounds", [&] { return launch_locatebounds(a, c->st); }))) return rc;
+  if (nl > 0)   // the launcher issues up to six kernels; launch() counted one
+    c->nlaunch += 3 + (a.f6b && a.bc[2] != W2D_BC_REFLECTIVE) + a.jet;
+  (void)g;
+  c->have_bounds = true;
   return W2D_OK;
 }
 

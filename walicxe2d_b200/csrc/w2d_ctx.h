@@ -93,15 +93,23 @@ struct W2dCtx {
   cudaEvent_t ev_plan[2] = {nullptr, nullptr};
   int plan_buf = 0;
   // admesh flags on the device (allocated by the first w2d_set_links): the
-  // mirror of lp(:,4:8), four byte planes of cap+1 flags, the two lists
+  // mirror of lp(:,3:8), four byte planes of cap+1 flags, the two lists
   // behind two counters, and the pinned row staging of w2d_set_links
   int4* d_links = nullptr;
-  int* d_son = nullptr;
+  int2* d_sons = nullptr;     // lp(:,3), lp(:,4)
   unsigned char* d_mflags = nullptr;
   int* d_mlists = nullptr;    // [4 counters][cap+1 refines][cap+1 first sons]
   int* h_mlists = nullptr;    // pinned, same layout
-  int* d_rows6 = nullptr;     // (nb, lp(nb,4:8)) per row, cap+1 rows
-  int* h_rows6 = nullptr;     // pinned
+  int* d_rows7 = nullptr;     // (nb, lp(nb,3:8)) per row, cap+1 rows
+  int* h_rows7 = nullptr;     // pinned
+  // locatebounds on the device (allocated by the first w2d_locate_bounds):
+  // leaf position per slot, entries per leaf and their prefix sums, the
+  // writer position of each boundaryI bottom face
+  int* d_posof = nullptr;
+  int* d_bcnt = nullptr;
+  int* d_blocal = nullptr;
+  int* d_bcta = nullptr;      // CTA totals, then their offsets, then the list length
+  int* d_wpos = nullptr;
   cudaEvent_t ev_links = nullptr;
   bool have_links = false;
   // pinned staging of refine/coarse lists

@@ -117,9 +117,9 @@ void updatelpup(W2dSim* s, int nb, int s1, int s2, int s3, int s4)
   const int nlev2 = L.LP(nb, 1) + 1;
   int nsr;
   s->nbleafs += 3;
-  if (s->devflags) {   // rows whose lp(:,4:8) this call may change
-    const int rows[4] = {s1, s2, s3, s4};
-    s->touched.insert(s->touched.end(), rows, rows + 4);
+  if (s->tracks_links()) {   // rows whose lp(:,3:8) this pass may change
+    const int rows[5] = {nb, s1, s2, s3, s4};
+    s->touched.insert(s->touched.end(), rows, rows + 5);
     for (int k = 5; k <= 8; ++k) {
       const int n1 = L.LP(nb, k);
       if (n1 != -1 && !L.LEAF(n1))
@@ -170,7 +170,7 @@ void updatelpdown(W2dSim* s, int dad, int s1, int s2, int s3, int s4)
   L.LEAF(dad) = 1;
   L.LEAF(s1) = L.LEAF(s2) = L.LEAF(s3) = L.LEAF(s4) = 0;
   s->nbleafs -= 3;
-  if (s->devflags)     // the sons of dad's non-leaf neighbours get new links
+  if (s->tracks_links())   // the sons of dad's non-leaf neighbours get new links
     for (int k = 5; k <= 8; ++k) {
       const int n1 = L.LP(dad, k);
       if (n1 != -1 && !L.LEAF(n1))
@@ -261,8 +261,69 @@ double now_ms()
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+int push_links(W2dSim* s);
+
+// switches the tree work to the device (flags and plans) or to the host;
+// the mirror of lp is rebuilt and the next step plans again
+void set_tree_side(W2dSim* s, bool dev)
+{
+  if (dev != s->devflags) {
+    s->devflags = dev;
+    s->links_all = true;
+    s->touched.clear();
+  }
+  if (dev != s->devplans) {
+    s->devplans = dev;
+    s->links_all = true;
+    s->touched.clear();
+    s->dirty = true;
+  }
+}
+
+// W2D_TREE_AUTO: the step's side while a trial runs (one untimed and
+// kTrialSteps timed steps on the device, the same on the host), a new trial
+// when the leaf count has moved by half since the last choice
+constexpr int kTrialSteps = 4;
+
+void tree_trial_pre(W2dSim* s)
+{
+  if (s->tree_mode != W2D_TREE_AUTO || !s->amr) return;
+  if (s->trial_left == 0) {
+    const int n = s->nbleafs, c = s->chosen_nleaf;
+    if (c > 0 && 2 * n <= 3 * c && 3 * n >= 2 * c) return;
+    s->trial_left = 2 * (kTrialSteps + 1);
+    s->trial_ms[0] = s->trial_ms[1] = 0.0;
+    s->trial_n[0] = s->trial_n[1] = 0;
+  }
+  const int k = 2 * (kTrialSteps + 1) - s->trial_left;
+  set_tree_side(s, k <= kTrialSteps);
+}
+
+void tree_trial_post(W2dSim* s, double ms)
+{
+  if (s->tree_mode != W2D_TREE_AUTO || s->trial_left == 0) return;
+  const int k = 2 * (kTrialSteps + 1) - s->trial_left;
+  const int side = k <= kTrialSteps ? 1 : 0;
+  if (k % (kTrialSteps + 1) != 0) {
+    s->trial_ms[side] += ms;
+    s->trial_n[side] += 1;
+  }
+  if (--s->trial_left == 0) {
+    set_tree_side(s, s->trial_ms[1] / s->trial_n[1] <= s->trial_ms[0] / s->trial_n[0]);
+    s->chosen_nleaf = s->nbleafs;
+  }
+}
+
 int push_bounds(W2dSim* s)
 {
+  if (s->devplans) {
+    int rc = push_links(s);
+    if (rc) return rc;
+    if ((rc = w2d_locate_bounds(s->ctx))) return rc;
+    s->dirty = false;
+    s->ib_stale = true;
+    return W2D_OK;
+  }
   locatebounds(s);
   int rc = w2d_set_bounds(s->ctx, s->ib.data(), s->nib, s->nib);
   if (rc) return rc;
@@ -391,7 +452,7 @@ int admesh_apply(W2dSim* s, const int32_t* refine, int nr, const int32_t* first_
   return W2D_OK;
 }
 
-// the device mirror of lp(:,4:8): every row after a new tree, else the rows
+// the device mirror of lp(:,3:8): every row after a new tree, else the rows
 // the last pass changed
 int push_links(W2dSim* s)
 {
@@ -536,6 +597,8 @@ int w2d_sim_create(const W2dParams* p, const W2dInit* ic, W2dSim** out)
   W2dSim* s = new W2dSim();
   init_tree(s, p, ic);
   s->devflags = true;
+  s->devplans = true;
+  s->tree_mode = W2D_TREE_AUTO;
   int rc = w2d_create(p, &s->ctx);
   if (rc) { delete s; return rc; }
   if ((rc = basegrid(s))) { w2d_sim_destroy(s); return rc; }
@@ -566,6 +629,7 @@ int w2d_sim_run(W2dSim* s, int nsteps)
   for (int n = 0; n < nsteps && dev_dt; ++n) {
     // step graphs: dt stays on the device (the kernels read it there) and
     // comes to the host with the step's synchronization
+    tree_trial_pre(s);
     const double t0 = now_ms();
     const bool replan = s->dirty;
     if (replan && (rc = push_topology(s))) return rc;
@@ -589,9 +653,12 @@ int w2d_sim_run(W2dSim* s, int nsteps)
     s->dt = ctx_last_dt(s->ctx);
     s->time = s->time + s->dt;                               // src/main.f90:88
     s->steps++;
-    s->phase_ms[8] += now_ms() - t0;
+    const double ms = now_ms() - t0;
+    s->phase_ms[8] += ms;
+    tree_trial_post(s, ms);
   }
   for (int n = 0; n < nsteps && !dev_dt; ++n) {
+    tree_trial_pre(s);
     const double t0 = now_ms();
     const bool replan = s->dirty;
     if (replan && (rc = push_topology(s))) return rc;
@@ -616,7 +683,9 @@ int w2d_sim_run(W2dSim* s, int nsteps)
     s->zone_updates += (int64_t)s->nbleafs * s->p.nx * s->p.ny;
     if (s->amr && (rc = admesh(s))) return rc;              // src/main.f90:98
     s->steps++;
-    s->phase_ms[8] += now_ms() - t0;
+    const double ms = now_ms() - t0;
+    s->phase_ms[8] += ms;
+    tree_trial_post(s, ms);
   }
   // without AMR nothing has waited for the last step's kernels: check their
   // error word now (with AMR the criteria wait has done so)
@@ -656,7 +725,10 @@ int w2d_sim_tree(W2dSim* s, int32_t* lp, int32_t* leaf, int32_t* icoord, int32_t
       for (int nb = 1; nb <= s->cap; ++nb) lp[(size_t)(k - 1) * s->cap + (nb - 1)] = s->LP(nb, k);
   if (leaf) memcpy(leaf, s->leaf.data(), sizeof(int32_t) * s->leaf.size());
   if (icoord) memcpy(icoord, s->icoord.data(), sizeof(int32_t) * s->icoord.size());
-  if (s->dirty && (innerbounds || ninternal)) locatebounds(s);
+  if ((s->dirty || s->ib_stale) && (innerbounds || ninternal)) {
+    locatebounds(s);
+    s->ib_stale = false;
+  }
   if (innerbounds) memcpy(innerbounds, s->ib.data(), sizeof(int32_t) * s->ib.size());
   if (ninternal) *ninternal = s->nib;
   return W2D_OK;
@@ -669,13 +741,47 @@ int w2d_sim_set_amr(W2dSim* s, int on)
   return W2D_OK;
 }
 
+int w2d_sim_set_tree_mode(W2dSim* s, int mode)
+{
+  if (!s || mode < W2D_TREE_HOST || mode > W2D_TREE_AUTO) return W2D_ERR_ARG;
+  s->tree_mode = mode;
+  s->trial_left = 0;
+  s->chosen_nleaf = 0;     // auto: a trial at the next step
+  if (mode != W2D_TREE_AUTO) set_tree_side(s, mode == W2D_TREE_DEVICE);
+  return W2D_OK;
+}
+
+int w2d_sim_tree_mode(W2dSim* s, int* mode, int* device)
+{
+  if (!s) return W2D_ERR_ARG;
+  if (mode) *mode = s->tree_mode;
+  if (device) *device = (s->devflags && s->devplans) ? 1 : 0;
+  return W2D_OK;
+}
+
 int w2d_sim_set_device_flags(W2dSim* s, int on)
 {
   if (!s) return W2D_ERR_ARG;
+  s->tree_mode = -1;
+  s->trial_left = 0;
   if ((on != 0) != s->devflags) {
     s->devflags = on != 0;
     s->links_all = true;    // the mirror is rebuilt from the host tree
     s->touched.clear();
+  }
+  return W2D_OK;
+}
+
+int w2d_sim_set_device_plans(W2dSim* s, int on)
+{
+  if (!s) return W2D_ERR_ARG;
+  s->tree_mode = -1;
+  s->trial_left = 0;
+  if ((on != 0) != s->devplans) {
+    s->devplans = on != 0;
+    s->links_all = true;
+    s->touched.clear();
+    s->dirty = true;        // the next step builds its plans the new way
   }
   return W2D_OK;
 }

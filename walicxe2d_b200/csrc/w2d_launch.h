@@ -43,7 +43,8 @@ cudaError_t launch_dt_runs(const int* leaves, const int* loff, int nruns, const 
                            int use_cool, double courant, double psc, double tsc, double* dt_run, cudaStream_t st);
 
 // admesh flags on the device (w2d_mark.cu).  Per slot: lev, the mirror of
-// lp(:,4) (son) and lp(:,5:8) (links), the criteria maximum grad; byte
+// lp(:,3:4) (sons: first son, son position) and lp(:,5:8) (links), the
+// criteria maximum grad; byte
 // planes leafp, up, down, down2 zeroed before markref; counts[0..1] the
 // lengths of rlist (refines) and clist (first sons of coarsened families),
 // zeroed before, in atomic order.
@@ -52,7 +53,7 @@ struct MarkArgs {
   int nleaf, nbmax, cap, nlevs;
   const int* lev;
   const int4* links;
-  const int* son;
+  const int2* sons;
   const double* grad;
   double tol, tol2;
   unsigned char *leafp, *up, *down, *down2;
@@ -64,8 +65,32 @@ cudaError_t launch_markref(const MarkArgs& a, cudaStream_t st);
 cudaError_t launch_critneighup(const MarkArgs& a, int nl, cudaStream_t st);
 cudaError_t launch_critneighdown(const MarkArgs& a, cudaStream_t st);
 cudaError_t launch_coarsen_families(const MarkArgs& a, cudaStream_t st);
-// rows6: (nb, lp(nb,4), lp(nb,5..8)) per row
-cudaError_t launch_set_links(const int* rows6, int n, int4* links, int* son, cudaStream_t st);
+// rows7: (nb, lp(nb,3), lp(nb,4), lp(nb,5..8)) per row
+cudaError_t launch_set_links(const int* rows7, int n, int4* links, int2* sons, cudaStream_t st);
+
+// locatebounds and the fill plans on the device (w2d_mark.cu).  posof: per
+// slot, the leaf position or -1 (set to -1 before); cnt/local: per leaf
+// position, its entries and their exclusive prefix within its CTA of 256;
+// ctatot/ctaoff per CTA; total[0] the list length; fd1/fd2 (4 faces per
+// leaf position) and wpos (per leaf position) zeroed before; jetblk per
+// leaf position (jet runs).
+struct PlanArgs {
+  const int* leaves;
+  int nleaf, nbmax, cap;
+  const int* lev;
+  const int4* links;
+  const int2* sons;
+  int* posof;
+  int *cnt, *local, *ctatot, *ctaoff, *total;
+  int2 *fd1, *fd2;
+  int* wpos;
+  int* jetblk;
+  int bc[4];
+  int f6b, jet;
+};
+int plan_ctas(int nleaf);
+// six launches at most: positions, counts, scan, entries, OUTFYB, jet
+cudaError_t launch_locatebounds(const PlanArgs& a, cudaStream_t st);
 
 // one bounded wait that runs out (see w2d_wait_selftest)
 cudaError_t launch_wait_selftest(int* err, cudaStream_t st);

@@ -1,7 +1,10 @@
-// w2d_mark.cu -- the integer flag passes of admesh on the device: markref,
-// critneighup and critneighdown (src/admesh.f90:23-72), then the lists of
-// refines and coarsenings the pass makes.  The host keeps lp and applies
-// updatelpup / updatelpdown; the device holds a mirror of lp(:,4:8).
+// w2d_mark.cu -- integer work on the block tree, on the device: the flag
+// passes of admesh (markref, critneighup, critneighdown; src/admesh.f90:
+// 23-72) with the lists of refines and coarsenings the pass makes, and
+// locatebounds (src/locatebounds.f90:29-540) with the per-face fill plans
+// built from its list.  The host keeps lp and applies updatelpup /
+// updatelpdown; the device holds a mirror of lp(:,3:8).
+#include "../../include/w2d.h"
 #include "w2d_launch.h"
 
 namespace w2d {
@@ -93,7 +96,7 @@ __global__ void __launch_bounds__(kThreads) k_coarsen_families(MarkArgs a)
 {
   const int nb = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   if (nb > a.nbmax) return;
-  if (!a.down2[nb] || a.son[nb] != 1) return;
+  if (!a.down2[nb] || a.sons[nb].y != 1) return;
   const int l = a.lev[nb];
   if (l < 2 || l > a.nlevs) return;
   const int s2 = a.links[nb].y, s3 = a.links[nb].w;
@@ -106,20 +109,305 @@ __global__ void __launch_bounds__(kThreads) k_coarsen_families(MarkArgs a)
   }
 }
 
-// rows6[6k..6k+5] = (nb, lp(nb,4), lp(nb,5..8)); the host has checked nb.
-__global__ void __launch_bounds__(kThreads) k_set_links(const int* __restrict__ rows6, int n, int4* links, int* son)
+// rows7[7k..7k+6] = (nb, lp(nb,3), lp(nb,4), lp(nb,5..8)); the host has
+// checked every value.
+__global__ void __launch_bounds__(kThreads) k_set_links(const int* __restrict__ rows7, int n, int4* links,
+                                                        int2* sons)
 {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
-  const int* r = rows6 + 6 * (size_t)k;
+  const int* r = rows7 + 7 * (size_t)k;
   const int nb = r[0];
-  son[nb] = r[1];
-  links[nb] = make_int4(r[2], r[3], r[4], r[5]);
+  sons[nb] = make_int2(r[1], r[2]);
+  links[nb] = make_int4(r[3], r[4], r[5], r[6]);
+}
+
+// ---- locatebounds and the fill plans -------------------------------------
+//
+// locatebounds (src/locatebounds.f90:29-540, serial build) walks the leaves
+// in ascending ID and, per leaf, its sides left, right, bottom, top.  A side
+// adds an entry to innerbounds unless its bnd flag is already set:
+//   - a box wall: always (types -1..-4);
+//   - a same-level leaf neighbour n1: the entry (nb, n1, 1/4/7/10) sets
+//     the flag of n1's facing side, so of the pair only the lower ID adds
+//     it;
+//   - a same-level neighbour that has sons: the entry (nb, son, 2/5/8/11)
+//     with the son facing nb that has the lower ID (flags set on the sons,
+//     which never add entries toward a coarser block themselves);
+//   - a coarser neighbour: no entry (that neighbour adds the one above).
+// So each leaf's entries follow from its links alone, and their list
+// positions from a prefix sum of the counts over the leaves.  The plans are
+// those of the host walk (w2d_api.cu: plan_entries): every non-corner ghost
+// face has exactly one writer, except the bottom faces of boundaryI that
+// the OUTFYB defect also writes (resolved by list position in a second
+// pass), and the jet flags come from each block's first and last position
+// as nbs.
+
+__device__ __forceinline__ int pl_base(const PlanArgs& a, int k)
+{
+  return a.ctaoff[k / kThreads] + a.local[k];
+}
+
+// first and last list position (1-based) of block b as nbs, 0 if none
+__device__ __forceinline__ int2 pl_span(const PlanArgs& a, int b)
+{
+  if (b < 1 || b > a.nbmax) return make_int2(0, 0);
+  const int k = a.posof[b];
+  if (k < 0 || a.cnt[k] == 0) return make_int2(0, 0);
+  const int e0 = pl_base(a, k) + 1;
+  return make_int2(e0, e0 + a.cnt[k] - 1);
+}
+
+// The entries of leaf nb: (type, neighbour) per side, type 0 for none.
+__device__ __forceinline__ void pl_entries(const PlanArgs& a, int nb, int t[4], int n1[4])
+{
+  const int4 q = a.links[nb];
+  const int nn[4] = {q.x, q.y, q.z, q.w};
+  const int l = a.lev[nb];
+  const int same[4] = {1, 4, 7, 10}, rest[4] = {2, 5, 8, 11}, son_off[4] = {1, 0, 2, 0};
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    t[s] = 0;
+    n1[s] = 0;
+    const int m = nn[s];
+    if (m == -1) { t[s] = -(s + 1); continue; }
+    if (!in_pool(m, a.cap) || m > a.nbmax) continue;
+    if (a.lev[m] < l) continue;                          // coarser: its entry
+    if (a.posof[m] >= 0) {                               // same-level leaf
+      if (nb < m) { t[s] = same[s]; n1[s] = m; }
+    } else {                                             // same level, has sons
+      const int f = a.sons[m].x;
+      if (f < 1 || f + 3 > a.nbmax) continue;
+      t[s] = rest[s];
+      n1[s] = f + son_off[s];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_posof(PlanArgs a)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.nleaf) return;
+  const int nb = a.leaves[k];
+  if (in_pool(nb, a.cap)) a.posof[nb] = k;
+}
+
+// entries per leaf, their exclusive prefix sum within the CTA and the
+// CTA's total
+__global__ void __launch_bounds__(kThreads) k_bcount(PlanArgs a)
+{
+  __shared__ int wsum[kThreads / 32];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  int c = 0;
+  if (k < a.nleaf) {
+    const int nb = a.leaves[k];
+    if (in_pool(nb, a.cap)) {
+      int t[4], n1[4];
+      pl_entries(a, nb, t, n1);
+      c = (t[0] != 0) + (t[1] != 0) + (t[2] != 0) + (t[3] != 0);
+    }
+    a.cnt[k] = c;
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int v = lane < kThreads / 32 ? wsum[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
+    }
+    if (lane < kThreads / 32) wsum[lane] = v;   // inclusive over warps
+  }
+  __syncthreads();
+  const int before = (w > 0 ? wsum[w - 1] : 0) + x - c;
+  if (k < a.nleaf) a.local[k] = before;
+  if (threadIdx.x == kThreads - 1) a.ctatot[blockIdx.x] = wsum[kThreads / 32 - 1];
+}
+
+// exclusive prefix sum of the CTA totals (one CTA, tiles of 1024)
+__global__ void __launch_bounds__(1024) k_bscan(PlanArgs a, int nctas)
+{
+  __shared__ int wsum[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int t0 = 0; t0 < nctas; t0 += 1024) {
+    const int k = t0 + threadIdx.x;
+    const int c = k < nctas ? a.ctatot[k] : 0;
+    int x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      int v = wsum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
+      }
+      wsum[lane] = v;
+    }
+    __syncthreads();
+    if (k < nctas) a.ctaoff[k] = carry + (w > 0 ? wsum[w - 1] : 0) + x - c;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += wsum[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) a.total[0] = carry;
+}
+
+// put() of the host walk: one face descriptor of a leaf target, with the
+// jet flags for entry position e
+__device__ __forceinline__ void pl_put(const PlanArgs& a, int2* fd, bool is_fd1, int blk, int face, int nbr,
+                                       int kind, int off, int e)
+{
+  if (blk < 1 || blk > a.nbmax) return;
+  const int p = a.posof[blk];
+  if (p < 0) return;                       // non-leaf targets are rewritten before being read
+  int y = kind | (off << 8);
+  if (a.jet) {
+    const int s1 = (kind == FK_MIRROR || kind == FK_REFLECT) ? blk : nbr;
+    const int2 q1 = pl_span(a, s1);
+    if (q1.x && q1.x < e) y |= FD_SRC1_JET;
+    if (kind == FK_RESTRICT) {
+      const int2 q2 = pl_span(a, nbr + (face < 2 ? 2 : 1));
+      if (q2.x && q2.x < e) y |= FD_SRC2_JET;
+    }
+    if (pl_span(a, blk).y >= e) y |= FD_DST_JET;
+  }
+  fd[(size_t)p * 4 + face] = make_int2(nbr, y);
+  if (is_fd1 && face == 2) a.wpos[p] = e;
+}
+
+// every entry of every leaf, at its list position (the OUTFYB bottom-face
+// writes of boundaryI come in k_bplan_f6b)
+__global__ void __launch_bounds__(kThreads) k_bplan(PlanArgs a)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.nleaf) return;
+  const int nbs = a.leaves[k];
+  if (!in_pool(nbs, a.cap)) return;
+  int t[4], nn[4];
+  pl_entries(a, nbs, t, nn);
+  int e = pl_base(a, k);
+  const int H = W2D_NX / 2;
+#pragma unroll 1
+  for (int s = 0; s < 4; ++s) {
+    if (!t[s]) continue;
+    ++e;
+    const int n1 = nn[s];
+    auto both = [&](int blk, int face, int nbr, int kind, int off) {
+      pl_put(a, a.fd1, true, blk, face, nbr, kind, off, e);
+      pl_put(a, a.fd2, false, blk, face, nbr, kind, off, e);
+    };
+    switch (t[s]) {
+      case -1: case -2: case -4: {
+        const int f = (t[s] == -1) ? 0 : (t[s] == -2) ? 1 : 3;
+        both(nbs, f, nbs, a.bc[f] == W2D_BC_REFLECTIVE ? FK_REFLECT : FK_MIRROR, 0);
+        break;
+      }
+      case -3:
+        if (a.bc[2] == W2D_BC_REFLECTIVE) {
+          both(nbs, 2, nbs, FK_REFLECT, 0);
+        } else {
+          pl_put(a, a.fd2, false, nbs, 2, nbs, FK_MIRROR, 0, e);
+          if (!a.f6b) pl_put(a, a.fd1, true, nbs, 2, nbs, FK_MIRROR, 0, e);
+        }
+        break;
+      case 1:  both(nbs, 0, n1, FK_SAME, 0);  both(n1, 1, nbs, FK_SAME, 0); break;
+      case 4:  both(nbs, 1, n1, FK_SAME, 0);  both(n1, 0, nbs, FK_SAME, 0); break;
+      case 7:  both(nbs, 2, n1, FK_SAME, 0);  both(n1, 3, nbs, FK_SAME, 0); break;
+      case 10: both(nbs, 3, n1, FK_SAME, 0);  both(n1, 2, nbs, FK_SAME, 0); break;
+      case 2:
+        both(nbs, 0, n1, FK_RESTRICT, 0);
+        both(n1, 1, nbs, FK_INJECT, 0);
+        both(n1 + 2, 1, nbs, FK_INJECT, H);
+        break;
+      case 5:
+        both(nbs, 1, n1, FK_RESTRICT, 0);
+        both(n1, 0, nbs, FK_INJECT, 0);
+        both(n1 + 2, 0, nbs, FK_INJECT, H);
+        break;
+      case 8:
+        both(nbs, 2, n1, FK_RESTRICT, 0);
+        both(n1, 3, nbs, FK_INJECT, 0);
+        both(n1 + 1, 3, nbs, FK_INJECT, H);
+        break;
+      default:   // 11
+        both(nbs, 3, n1, FK_RESTRICT, 0);
+        both(n1, 2, nbs, FK_INJECT, 0);
+        both(n1 + 1, 2, nbs, FK_INJECT, H);
+        break;
+    }
+  }
+}
+
+// src/boundaryI.f90:87 (OUTFYB): the bottom-wall entry at list position e
+// fills the bottom face of block e; it wins over the face's own writer when
+// it comes later in the list
+__global__ void __launch_bounds__(kThreads) k_bplan_f6b(PlanArgs a)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.nleaf) return;
+  const int nbs = a.leaves[k];
+  if (!in_pool(nbs, a.cap) || a.links[nbs].z != -1) return;
+  int t[4], nn[4];
+  pl_entries(a, nbs, t, nn);
+  const int e = pl_base(a, k) + (t[0] != 0) + (t[1] != 0) + 1;   // the bottom entry's position
+  const int tb = e;
+  if (tb < 1 || tb > a.nbmax) return;
+  const int p = a.posof[tb];
+  if (p < 0 || a.wpos[p] > e) return;
+  pl_put(a, a.fd1, true, tb, 2, tb, FK_MIRROR, 0, e);
+}
+
+// faces no entry writes still get the jet if their block is ever nbs; the
+// interior of such a block always does (w2d_api.cu: w2d_set_bounds)
+__global__ void __launch_bounds__(kThreads) k_bplan_jet(PlanArgs a)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.nleaf) return;
+  const bool named = a.cnt[k] > 0;
+  a.jetblk[k] = named;
+  if (!named) return;
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    if ((a.fd1[(size_t)k * 4 + f].y & 0xff) == FK_KEEP) a.fd1[(size_t)k * 4 + f].y |= FD_DST_JET;
+    if ((a.fd2[(size_t)k * 4 + f].y & 0xff) == FK_KEEP) a.fd2[(size_t)k * 4 + f].y |= FD_DST_JET;
+  }
 }
 
 inline int ctas(int n) { return (n + kThreads - 1) / kThreads; }
 
 }  // namespace
+
+int plan_ctas(int nleaf) { return ctas(nleaf); }
+
+cudaError_t launch_locatebounds(const PlanArgs& a, cudaStream_t st)
+{
+  if (a.nleaf <= 0) return cudaSuccess;
+  const int g = ctas(a.nleaf);
+  k_posof<<<g, kThreads, 0, st>>>(a);
+  k_bcount<<<g, kThreads, 0, st>>>(a);
+  k_bscan<<<1, 1024, 0, st>>>(a, g);
+  k_bplan<<<g, kThreads, 0, st>>>(a);
+  if (a.f6b && a.bc[2] != W2D_BC_REFLECTIVE) k_bplan_f6b<<<g, kThreads, 0, st>>>(a);
+  if (a.jet) k_bplan_jet<<<g, kThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_markref(const MarkArgs& a, cudaStream_t st)
 {
@@ -149,10 +437,10 @@ cudaError_t launch_coarsen_families(const MarkArgs& a, cudaStream_t st)
   return cudaGetLastError();
 }
 
-cudaError_t launch_set_links(const int* rows6, int n, int4* links, int* son, cudaStream_t st)
+cudaError_t launch_set_links(const int* rows7, int n, int4* links, int2* sons, cudaStream_t st)
 {
   if (n <= 0) return cudaSuccess;
-  k_set_links<<<ctas(n), kThreads, 0, st>>>(rows6, n, links, son);
+  k_set_links<<<ctas(n), kThreads, 0, st>>>(rows7, n, links, sons);
   return cudaGetLastError();
 }
 

@@ -30,10 +30,19 @@ struct W2dSim {
   std::vector<std::vector<int32_t>> bucket;  // leaves per level, ascending ID
   std::vector<double> grad;
   std::vector<int32_t> rops, cops;
-  // admesh flags from the device (single-run driver): rows of lp(:,4:8)
+  // admesh flags from the device (single-run driver): rows of lp(:,3:8)
   // changed since the device mirror was last updated (all of them while
   // links_all), and the lists w2d_admesh_flags returns
   bool devflags = false, links_all = true;
+  // fill plans from the device (w2d_locate_bounds); ib is then built only
+  // when w2d_sim_tree asks for it
+  bool devplans = false, ib_stale = false;
+  bool tracks_links() const { return devflags || devplans; }
+  // W2D_TREE_* (-1: set half by half); the timing trial of W2D_TREE_AUTO
+  int tree_mode = -1;
+  int trial_left = 0, chosen_nleaf = 0;
+  double trial_ms[2] = {0.0, 0.0};
+  int trial_n[2] = {0, 0};
   std::vector<int32_t> touched, rlist, clist;
   std::vector<int32_t> ib1, ib2, ib3;
   double phase_ms[W2D_SIM_NPHASES] = {0};               // see w2d_sim_phase_ms
