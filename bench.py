@@ -625,7 +625,9 @@ def run_ours(args, ws, rank, local):
            "d2h_bytes_per_step": int(d2h),
            "how": "w2d_put_blocks of every leaf from pinned host memory, K main-loop steps "
                   "(topology and plans uploaded, dt and criteria read back each step), "
-                  "w2d_get_blocks of every leaf into pinned host memory; host wall clock"}
+                  "w2d_get_blocks of every leaf into pinned host memory; host wall clock; the steps run "
+                  "back to back, without the L2 flush that `value` puts before every step, and start "
+                  "where the timed and profiled steps left the blast (more leaves)"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:

@@ -984,6 +984,10 @@ int w2d_criteria(W2dCtx* c, double* grad)
 
 namespace {
 
+// bytes per flag plane: cap+1 rounded up, so that every plane starts on a
+// 256-byte boundary (k_markref_up sets flags with 32-bit atomics)
+size_t mark_plane(const W2dCtx* c) { return ((size_t)c->cap + 1 + 255) & ~(size_t)255; }
+
 // The device side of the admesh flags, allocated on first use (contexts
 // whose host takes the flags from w2d_criteria never hold it).
 int ensure_mark(W2dCtx* c)
@@ -992,7 +996,7 @@ int ensure_mark(W2dCtx* c)
   const size_t slots = (size_t)c->cap + 1;
   CK(cudaMalloc(&c->d_links, sizeof(int4) * slots));
   CK(cudaMalloc(&c->d_sons, sizeof(int2) * slots));
-  CK(cudaMalloc(&c->d_mflags, 4 * slots));
+  CK(cudaMalloc(&c->d_mflags, 4 * mark_plane(c)));
   CK(cudaMalloc(&c->d_mlists, sizeof(int) * (4 + 2 * slots)));
   CK(cudaMalloc(&c->d_rows7, sizeof(int) * 7 * slots));
   CK(cudaMallocHost(&c->h_mlists, sizeof(int) * (4 + 2 * slots)));
@@ -1067,7 +1071,8 @@ int w2d_admesh_flags(W2dCtx* c, int32_t* refine, int cap_refine, int* nrefine, i
     return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology and w2d_set_links first");
   if (c->nruns > 0) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "one run per context");
   const size_t slots = (size_t)c->cap + 1;
-  CK(cudaMemsetAsync(c->d_mflags, 0, 4 * slots, c->st));
+  const size_t plane = mark_plane(c);
+  CK(cudaMemsetAsync(c->d_mflags, 0, 4 * plane, c->st));
   CK(cudaMemsetAsync(c->d_mlists, 0, 4 * sizeof(int), c->st));
   MarkArgs a{};
   a.leaves = c->d_leaves;
@@ -1082,15 +1087,14 @@ int w2d_admesh_flags(W2dCtx* c, int32_t* refine, int cap_refine, int* nrefine, i
   a.tol = c->p.tol;
   a.tol2 = c->p.tol2;
   a.leafp = c->d_mflags;
-  a.up = c->d_mflags + slots;
-  a.down = c->d_mflags + 2 * slots;
-  a.down2 = c->d_mflags + 3 * slots;
+  a.up = c->d_mflags + plane;
+  a.down = c->d_mflags + 2 * plane;
+  a.down2 = c->d_mflags + 3 * plane;
   a.counts = c->d_mlists;
   a.rlist = c->d_mlists + 4;
   a.clist = c->d_mlists + 4 + slots;
-  int rc = launch(c, "markref", [&] { return launch_markref(a, c->st); });
-  for (int nl = c->p.nlevs - 1; nl >= 1 && !rc; --nl)
-    rc = launch(c, "critneighup", [&] { return launch_critneighup(a, nl, c->st); });
+  a.err = c->d_err;
+  int rc = launch(c, "markref_critneighup", [&] { return launch_markref_up(a, c->st); });
   if (!rc) rc = launch(c, "critneighdown", [&] { return launch_critneighdown(a, c->st); });
   if (!rc) rc = launch(c, "coarsen_families", [&] { return launch_coarsen_families(a, c->st); });
   if (rc) return rc;

@@ -60,9 +60,10 @@ struct MarkArgs {
   int* counts;
   int* rlist;
   int* clist;
+  int* err;      // the context's error word (W2D_ERR_TOPOLOGY on a malformed tree)
 };
-cudaError_t launch_markref(const MarkArgs& a, cudaStream_t st);
-cudaError_t launch_critneighup(const MarkArgs& a, int nl, cudaStream_t st);
+// markref and the whole critneighup cascade in one launch
+cudaError_t launch_markref_up(const MarkArgs& a, cudaStream_t st);
 cudaError_t launch_critneighdown(const MarkArgs& a, cudaStream_t st);
 cudaError_t launch_coarsen_families(const MarkArgs& a, cudaStream_t st);
 // rows7: (nb, lp(nb,3), lp(nb,4), lp(nb,5..8)) per row

@@ -15,11 +15,28 @@ constexpr int kThreads = 256;
 
 __device__ __forceinline__ bool in_pool(int n, int cap) { return n >= 1 && n <= cap; }
 
+// Sets byte n of a byte array to 1 and returns its old value (an atomic OR
+// on the aligned 32-bit word that holds it).
+__device__ __forceinline__ bool flag_set(unsigned char* f, int n)
+{
+  unsigned int* w = reinterpret_cast<unsigned int*>(f + (n & ~3));
+  const unsigned int bit = 1u << (8 * (n & 3));
+  return (atomicOr(w, bit) & bit) != 0;
+}
+
 // src/markref.f90:23-44 (every leaf of level >= 1) with the flags of
 // src/criteria.f90:36-50 on the device maximum grad[nb]: grad >= tol ->
-// irefup (only below nlevs), else grad <= tol2 -> irefdown.  Also marks the
-// leaves in leafp (the planes were zeroed before).
-__global__ void __launch_bounds__(kThreads) k_markref(MarkArgs a)
+// irefup (only below nlevs), else grad <= tol2 -> irefdown; also marks the
+// leaves in leafp (the planes were zeroed before).  Then critneighup
+// (src/critneighup.f90:19-58) in the same launch.  The reference visits the
+// levels from nlevs-1 down: a marked block of level nl marks its coarser
+// neighbours, which are visited at their own, later level.  The marks it
+// ends with are the closure of the markref marks under "a marked block marks
+// its coarser neighbours"; here each block that receives a mark first (the
+// atomic decides) walks on from it, so every block of the closure is
+// walked once.  The walk descends a level per edge, so its stack holds at
+// most 3 entries per level.
+__global__ void __launch_bounds__(kThreads) k_markref_up(MarkArgs a)
 {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= a.nleaf) return;
@@ -29,27 +46,33 @@ __global__ void __launch_bounds__(kThreads) k_markref(MarkArgs a)
   const int l = a.lev[nb];
   if (l < 1) return;
   const double g = a.grad[nb];
-  if (g >= a.tol) {
-    if (l < a.nlevs) a.up[nb] = 1;
-  } else if (g <= a.tol2) {
-    a.down[nb] = 1;
+  if (!(g >= a.tol)) {
+    if (g <= a.tol2) a.down[nb] = 1;
+    return;
   }
-}
-
-// src/critneighup.f90:19-58, one level nl per launch (nlevs-1 down to 1):
-// a block of level nl marked for refinement marks its coarser neighbours,
-// which the launches of the coarser levels then visit.  Several threads may
-// store the same 1 into one flag.
-__global__ void __launch_bounds__(kThreads) k_critneighup(MarkArgs a, int nl)
-{
-  const int nb = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (nb > a.nbmax) return;
-  if (!a.up[nb] || a.lev[nb] != nl) return;
-  const int4 q = a.links[nb];
-  const int n[4] = {q.x, q.y, q.z, q.w};
+  if (l >= a.nlevs) return;
+  if (flag_set(a.up, nb)) return;           // reached already by another walk
+  constexpr int kStack = 3 * W2D_MAXLEV + 4;
+  int stack[kStack];
+  int top = 0;
+  stack[top++] = nb;
+  while (top > 0) {
+    const int x = stack[--top];
+    const int lx = a.lev[x];
+    const int4 q = a.links[x];
+    const int n[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-  for (int s = 0; s < 4; ++s)
-    if (in_pool(n[s], a.cap) && a.lev[n[s]] < nl) a.up[n[s]] = 1;
+    for (int s = 0; s < 4; ++s) {
+      const int n1 = n[s];
+      if (!in_pool(n1, a.cap) || a.lev[n1] >= lx) continue;
+      if (flag_set(a.up, n1)) continue;
+      if (top < kStack) {
+        stack[top++] = n1;
+      } else {                               // not reachable in a tree of nlevs levels
+        set_err(a.err, W2D_ERR_TOPOLOGY, x, 0, 0);
+      }
+    }
+  }
 }
 
 // The refine list (src/admesh.f90:29-65 refines every block of level
@@ -409,17 +432,10 @@ cudaError_t launch_locatebounds(const PlanArgs& a, cudaStream_t st)
   return cudaGetLastError();
 }
 
-cudaError_t launch_markref(const MarkArgs& a, cudaStream_t st)
+cudaError_t launch_markref_up(const MarkArgs& a, cudaStream_t st)
 {
   if (a.nleaf <= 0) return cudaSuccess;
-  k_markref<<<ctas(a.nleaf), kThreads, 0, st>>>(a);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_critneighup(const MarkArgs& a, int nl, cudaStream_t st)
-{
-  if (a.nbmax <= 0) return cudaSuccess;
-  k_critneighup<<<ctas(a.nbmax), kThreads, 0, st>>>(a, nl);
+  k_markref_up<<<ctas(a.nleaf), kThreads, 0, st>>>(a);
   return cudaGetLastError();
 }
 
