@@ -186,6 +186,7 @@ KArgs kargs(W2dCtx* c, const int2* fd)
   a.dtcool = c->d_dtcool;
   a.grad = c->d_grad;
   a.err = c->d_err;
+  a.leafflag = c->nruns > 0 ? nullptr : c->d_leafflag;
   a.cooltab = c->d_cooltab;
   a.nlevs = c->p.nlevs;
   a.eta = c->p.eta;
@@ -622,6 +623,8 @@ int w2d_create(const W2dParams* p, W2dCtx** out)
   CKC(cudaMalloc(&c->d_dt, sizeof(double) * 4));
   CKC(cudaMalloc(&c->d_cooltab, sizeof(double) * 82));
   CKC(cudaMalloc(&c->d_leaves, sizeof(int) * slots));
+  CKC(cudaMalloc(&c->d_leafflag, sizeof(int) * slots));
+  CKC(cudaMemsetAsync(c->d_leafflag, 0, sizeof(int) * slots, c->st));
   CKC(cudaMalloc(&c->d_fb_count, sizeof(int)));
   CKC(cudaMalloc(&c->d_nleaf, sizeof(int)));
   CKC(cudaMemsetAsync(c->d_nleaf, 0, sizeof(int), c->st));
@@ -716,7 +719,7 @@ int w2d_destroy(W2dCtx* c)
   if (c->h_loff) cudaFreeHost(c->h_loff);
   void* dev[] = {c->d_u, c->d_up, c->d_prim, c->d_lev, c->d_icoord, c->d_cfl, c->d_dtcool, c->d_grad,
                  c->d_err, c->d_dt, c->d_cooltab, c->d_leaves, c->d_fd1, c->d_fd2, c->d_stage, c->d_ids,
-                 c->d_flush, c->d_dtwork, c->d_dtcount, c->d_jetblk};
+                 c->d_flush, c->d_dtwork, c->d_dtcount, c->d_jetblk, c->d_leafflag};
   for (void* d : dev)
     if (d) cudaFree(d);
   void* host[] = {c->h_small, c->h_grad, c->h_err, c->h_fd1[0], c->h_fd2[0], c->h_leaflist,
@@ -794,10 +797,47 @@ int w2d_set_topology(W2dCtx* c, const int32_t* lp, int ld_lp, const int32_t* lea
     CK(cudaMemcpyAsync(c->d_leaves, c->h_leaflist, sizeof(int) * nl, cudaMemcpyHostToDevice, c->st));
   }
   CK(cudaEventRecord(c->ev_topo, c->st));
+  // the device's leaf flags, which k_amr keeps from here on
+  CK(cudaMemsetAsync(c->d_leafflag, 0, sizeof(int) * ((size_t)c->cap + 1), c->st));
+  int rc = launch(c, "leaf_flags", [&] { return launch_flag_leaves(c->d_leaves, (int)nl, c->d_leafflag, c->st); });
+  if (rc) return rc;
   c->have_topology = true;
+  c->have_bounds = false;
+  c->host_leaves_stale = false;
+  return W2D_OK;
+}
+
+namespace {
+int ensure_plan(W2dCtx* c);   // (defined with the other lazily allocated parts below)
+}  // namespace
+
+}  // extern "C"
+
+// After refines and coarsenings through k_amr only (which keep the device's
+// lev, icoord and leaf flags): the leaf list rebuilt on the device from the
+// flags, in ascending ID as w2d_set_topology builds it.  The host's copies
+// of leaf and the list are stale until the next w2d_set_topology.
+int ctx_topology_device(W2dCtx* c, int nbmax, int nleaf)
+{
+  if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
+  if (nbmax < 0 || nbmax > c->cap || nleaf < 0 || nleaf > nbmax) return W2D_ERR_ARG;
+  int rc = ensure_plan(c);
+  if (rc) return rc;
+  const size_t slots = (size_t)c->cap + 1;
+  c->nbmax = nbmax;
+  c->nleaf = nleaf;
+  rc = launch(c, "leaf_list", [&] {
+    return launch_leaf_list(c->d_leafflag, nbmax, c->d_blocal, c->d_bcta, c->d_bcta + (slots / 256 + 1),
+                            c->d_leaves, c->d_nleaf, c->st);
+  });
+  if (rc) return rc;
+  if (nbmax > 0) c->nlaunch += 2;   // three kernels, launch() counted one
+  c->host_leaves_stale = true;
   c->have_bounds = false;
   return W2D_OK;
 }
+
+extern "C" {
 
 // Builds the two fill plans from the list (src/locatebounds.f90:29-540
 // output) in list order: for every leaf face the last entry that writes it
@@ -805,7 +845,8 @@ int w2d_set_topology(W2dCtx* c, const int32_t* lp, int ld_lp, const int32_t* lea
 int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
 {
   if (!c || (!ib && n > 0) || n < 0 || ld < n) return W2D_ERR_ARG;
-  if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
+  if (!c->have_topology || c->host_leaves_stale)
+    return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
   // alternate pinned buffers; wait only for the upload that last used this one
   const int q = c->plan_buf;
   c->plan_buf ^= 1;
@@ -974,11 +1015,21 @@ int w2d_tstep(W2dCtx* c, double time, double dt)
 int w2d_criteria(W2dCtx* c, double* grad)
 {
   if (!c || !grad) return W2D_ERR_ARG;
-  if (c->nbmax > 0)
+  // the leaf flags come from the device when the leaf list was built there
+  const bool dev_leaf = c->host_leaves_stale;
+  if (dev_leaf) CK(cudaEventSynchronize(c->ev_topo));   // h_leaflist is free
+  if (c->nbmax > 0) {
     CK(cudaMemcpyAsync(c->h_grad, c->d_grad + 1, sizeof(double) * (size_t)c->nbmax, cudaMemcpyDeviceToHost, c->st));
+    if (dev_leaf)
+      CK(cudaMemcpyAsync(c->h_leaflist, c->d_leafflag + 1, sizeof(int) * (size_t)c->nbmax, cudaMemcpyDeviceToHost,
+                         c->st));
+  }
   int rc = sync_and_check(c);
   if (rc) return rc;
-  for (int nb = 1; nb <= c->nbmax; ++nb) grad[nb - 1] = c->leaf[nb] ? c->h_grad[nb - 1] : -1.0;
+  for (int nb = 1; nb <= c->nbmax; ++nb) {
+    const bool is_leaf = dev_leaf ? c->h_leaflist[nb - 1] != 0 : c->leaf[nb] != 0;
+    grad[nb - 1] = is_leaf ? c->h_grad[nb - 1] : -1.0;
+  }
   return W2D_OK;
 }
 

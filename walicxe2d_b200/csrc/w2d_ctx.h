@@ -36,6 +36,10 @@ struct W2dCtx {
   double* d_cooltab = nullptr;
   // leaf list (uploaded with the topology) and per-step plan
   int* d_leaves = nullptr;  // one per slot
+  int* d_leafflag = nullptr; // per slot: 1 for a leaf (set with the topology, kept by k_amr)
+  // the leaf list was last built on the device (ctx_topology_device): the
+  // host copies leaf/leaves/pos_of are stale until the next w2d_set_topology
+  bool host_leaves_stale = false;
   int* h_leaflist = nullptr; // pinned staging of d_leaves (guarded by ev_topo)
   int2* d_fd1 = nullptr;   // boundaryI (layer 0 of u)
   int2* d_fd2 = nullptr;   // boundaryII (two layers of up)

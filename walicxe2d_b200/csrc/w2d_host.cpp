@@ -190,6 +190,8 @@ void updatelpdown(W2dSim* s, int dad, int s1, int s2, int s3, int s4)
 // column is passed on its own.
 int push_topology(W2dSim* s)
 {
+  if (s->devplans && s->topo_dev_ok) return ctx_topology_device(s->ctx, s->nbmax, s->nbleafs);
+  s->topo_dev_ok = true;
   for (int nb = 1; nb <= s->nbmax; ++nb) s->levbuf[nb - 1] = s->LP(nb, 1);
   return w2d_set_topology(s->ctx, s->levbuf.data(), s->cap, s->leaf.data(), s->icoord.data(), s->cap,
                           s->nbmax, s->dx.data(), s->dy.data());
@@ -545,6 +547,7 @@ int basegrid_tree(W2dSim* s, std::vector<int32_t>& ids, std::vector<double>& blo
   for (size_t q = 0; q < ids.size(); ++q) initial_block(s, ids[q], blocks.data() + q * bs);
   s->dirty = true;
   s->links_all = true;
+  s->topo_dev_ok = false;
   return W2D_OK;
 }
 
@@ -904,6 +907,7 @@ int w2d_sim_read_bin(W2dSim* s, const char* pointers, const char* blocks, double
   s->dirty = true;
   s->links_all = true;
   s->touched.clear();
+  s->topo_dev_ok = false;
   int rc = push_topology(s);
   if (rc) return rc;
   if ((rc = w2d_put_blocks(s->ctx, ids.data(), (int)ids.size(), u.data()))) return rc;

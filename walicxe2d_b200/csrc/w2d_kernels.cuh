@@ -59,6 +59,7 @@ struct KArgs {
   double* dtcool;     // per slot: DMC cooling-time limit
   double* grad;       // per slot: criteria maximum jump
   int* err;           // device error word {code, block, i, j}
+  int* leafflag;      // per slot: 1 for a leaf, kept by k_amr (null: not kept)
   const double* cooltab;  // [2][41] DMC table (T, Lambda)
   int nlevs;
   int jet;                // impose_jet is active (OTHERB)
@@ -1034,6 +1035,15 @@ __global__ void __launch_bounds__(W2D_THREADS) k_amr(KArgs a, PhysArgs pa, const
     const_cast<int*>(a.lev)[b] = tup[4 * k + 1];
     const_cast<int*>(a.icoord)[2 * b] = tup[4 * k + 2];
     const_cast<int*>(a.icoord)[2 * b + 1] = tup[4 * k + 3];
+    if (a.leafflag) {          // leaf(:) as updatelpup / updatelpdown leave it
+      a.leafflag[b] = 1;
+      if (k < 4 * nr) {
+        if ((k & 3) == 0) a.leafflag[ops[(k >> 2) * 5]] = 0;
+      } else {
+        const int op = nr + (k - 4 * nr);
+        for (int s = 1; s <= 4; ++s) a.leafflag[ops[op * 5 + s]] = 0;
+      }
+    }
   }
   const int NX = W2D_NX, H = W2D_NX / 2;
   if (k < 4 * nr) {

@@ -93,6 +93,13 @@ int plan_ctas(int nleaf);
 // six launches at most: positions, counts, scan, entries, OUTFYB, jet
 cudaError_t launch_locatebounds(const PlanArgs& a, cudaStream_t st);
 
+// flag[leaves[k]] = 1 for k < nl (flag zeroed before)
+cudaError_t launch_flag_leaves(const int* leaves, int nl, int* flag, cudaStream_t st);
+// leaves[] = the slots 1..nbmax whose flag is set, ascending; *nleaf their
+// count (three launches; local per slot, ctatot/ctaoff per CTA of 256)
+cudaError_t launch_leaf_list(const int* flag, int nbmax, int* local, int* ctatot, int* ctaoff, int* leaves,
+                             int* nleaf, cudaStream_t st);
+
 // one bounded wait that runs out (see w2d_wait_selftest)
 cudaError_t launch_wait_selftest(int* err, cudaStream_t st);
 

@@ -413,9 +413,78 @@ __global__ void __launch_bounds__(kThreads) k_bplan_jet(PlanArgs a)
   }
 }
 
+// ---- the leaf list from the leaf flags --------------------------------------
+// flag[1..n] -> the slots with flag 1 in ascending order (the order of the
+// reference's loops over nb with leaf(nb)), and their count
+
+__global__ void __launch_bounds__(kThreads) k_flag_leaves(const int* __restrict__ leaves, int nl, int* flag)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nl) flag[leaves[k]] = 1;
+}
+
+__global__ void __launch_bounds__(kThreads) k_lscan_local(const int* __restrict__ flag, int n, int* local,
+                                                          int* ctatot)
+{
+  __shared__ int wsum[kThreads / 32];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (k < n) ? (flag[k + 1] != 0) : 0;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int v = lane < kThreads / 32 ? wsum[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
+    }
+    if (lane < kThreads / 32) wsum[lane] = v;
+  }
+  __syncthreads();
+  if (k < n) local[k] = (w > 0 ? wsum[w - 1] : 0) + x - c;
+  if (threadIdx.x == kThreads - 1) ctatot[blockIdx.x] = wsum[kThreads / 32 - 1];
+}
+
+__global__ void __launch_bounds__(kThreads) k_lcompact(const int* __restrict__ flag, int n,
+                                                       const int* __restrict__ local,
+                                                       const int* __restrict__ ctaoff, int* leaves)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n && flag[k + 1]) leaves[ctaoff[k / kThreads] + local[k]] = k + 1;
+}
+
 inline int ctas(int n) { return (n + kThreads - 1) / kThreads; }
 
 }  // namespace
+
+cudaError_t launch_flag_leaves(const int* leaves, int nl, int* flag, cudaStream_t st)
+{
+  if (nl <= 0) return cudaSuccess;
+  k_flag_leaves<<<ctas(nl), kThreads, 0, st>>>(leaves, nl, flag);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_leaf_list(const int* flag, int nbmax, int* local, int* ctatot, int* ctaoff, int* leaves,
+                             int* nleaf, cudaStream_t st)
+{
+  if (nbmax <= 0) return cudaMemsetAsync(nleaf, 0, sizeof(int), st);
+  const int g = ctas(nbmax);
+  k_lscan_local<<<g, kThreads, 0, st>>>(flag, nbmax, local, ctatot);
+  PlanArgs a{};
+  a.ctatot = ctatot;
+  a.ctaoff = ctaoff;
+  a.total = nleaf;
+  k_bscan<<<1, 1024, 0, st>>>(a, g);
+  k_lcompact<<<g, kThreads, 0, st>>>(flag, nbmax, local, ctaoff, leaves);
+  return cudaGetLastError();
+}
 
 int plan_ctas(int nleaf) { return ctas(nleaf); }
 

@@ -37,6 +37,10 @@ struct W2dSim {
   // fill plans from the device (w2d_locate_bounds); ib is then built only
   // when w2d_sim_tree asks for it
   bool devplans = false, ib_stale = false;
+  // the device's tree has followed every change since the last full
+  // topology upload (k_amr keeps lev, icoord and the leaf flags), so the
+  // leaf list can be rebuilt there
+  bool topo_dev_ok = false;
   bool tracks_links() const { return devflags || devplans; }
   // W2D_TREE_* (-1: set half by half); the timing trial of W2D_TREE_AUTO
   int tree_mode = -1;
