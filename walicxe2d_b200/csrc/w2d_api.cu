@@ -828,7 +828,7 @@ int ctx_topology_device(W2dCtx* c, int nbmax, int nleaf)
   c->nleaf = nleaf;
   rc = launch(c, "leaf_list", [&] {
     return launch_leaf_list(c->d_leafflag, nbmax, c->d_blocal, c->d_bcta, c->d_bcta + (slots / 256 + 1),
-                            c->d_leaves, c->d_nleaf, c->st);
+                            c->d_leaves, c->d_nleaf, c->d_posof, c->st);
   });
   if (rc) return rc;
   if (nbmax > 0) c->nlaunch += 2;   // three kernels, launch() counted one
@@ -1195,7 +1195,10 @@ int w2d_locate_bounds(W2dCtx* c)
   if (rc) return rc;
   const size_t slots = (size_t)c->cap + 1;
   const int nl = c->nleaf;
-  CK(cudaMemsetAsync(c->d_posof, 0xff, sizeof(int) * slots, c->st));    // -1: not a leaf
+  // a leaf list built on the device came with the positions of all slots
+  // 1..nbmax (the only ones the plan kernels look up)
+  const bool posof_ready = c->host_leaves_stale;
+  if (!posof_ready) CK(cudaMemsetAsync(c->d_posof, 0xff, sizeof(int) * slots, c->st));    // -1: not a leaf
   if (nl > 0) {
     CK(cudaMemsetAsync(c->d_fd1, 0, sizeof(int2) * 4 * (size_t)nl, c->st));   // (0, FK_KEEP)
     CK(cudaMemsetAsync(c->d_fd2, 0, sizeof(int2) * 4 * (size_t)nl, c->st));
@@ -1226,9 +1229,9 @@ int w2d_locate_bounds(W2dCtx* c)
   a.bc[3] = c->p.bc_top;
   a.f6b = (c->p.compat & W2D_COMPAT_OUTFYB) != 0;
   a.jet = c->p.otherb == W2D_USERBC_JET;
-  if ((rc = launch(c, "locatebounds", [&] { return launch_locatebounds(a, c->st); }))) return rc;
+  if ((rc = launch(c, "locatebounds", [&] { return launch_locatebounds(a, posof_ready, c->st); }))) return rc;
   if (nl > 0)   // the launcher issues up to six kernels; launch() counted one
-    c->nlaunch += 3 + (a.f6b && a.bc[2] != W2D_BC_REFLECTIVE) + a.jet;
+    c->nlaunch += 2 + !posof_ready + (a.f6b && a.bc[2] != W2D_BC_REFLECTIVE) + a.jet;
   (void)g;
   c->have_bounds = true;
   return W2D_OK;

@@ -90,15 +90,18 @@ struct PlanArgs {
   int f6b, jet;
 };
 int plan_ctas(int nleaf);
-// six launches at most: positions, counts, scan, entries, OUTFYB, jet
-cudaError_t launch_locatebounds(const PlanArgs& a, cudaStream_t st);
+// six launches at most: positions (unless posof_ready: posof already holds
+// the leaf position of every slot 1..nbmax, -1 for the others), counts,
+// scan, entries, OUTFYB, jet
+cudaError_t launch_locatebounds(const PlanArgs& a, bool posof_ready, cudaStream_t st);
 
 // flag[leaves[k]] = 1 for k < nl (flag zeroed before)
 cudaError_t launch_flag_leaves(const int* leaves, int nl, int* flag, cudaStream_t st);
 // leaves[] = the slots 1..nbmax whose flag is set, ascending; *nleaf their
-// count (three launches; local per slot, ctatot/ctaoff per CTA of 256)
+// count; posof[1..nbmax] their positions (-1: not a leaf).  Three launches;
+// local per slot, ctatot/ctaoff per CTA of 256.
 cudaError_t launch_leaf_list(const int* flag, int nbmax, int* local, int* ctatot, int* ctaoff, int* leaves,
-                             int* nleaf, cudaStream_t st);
+                             int* nleaf, int* posof, cudaStream_t st);
 
 // one bounded wait that runs out (see w2d_wait_selftest)
 cudaError_t launch_wait_selftest(int* err, cudaStream_t st);

@@ -452,12 +452,19 @@ __global__ void __launch_bounds__(kThreads) k_lscan_local(const int* __restrict_
   if (threadIdx.x == kThreads - 1) ctatot[blockIdx.x] = wsum[kThreads / 32 - 1];
 }
 
+// also posof[1..n]: the leaf position of every leaf slot, -1 for the others
 __global__ void __launch_bounds__(kThreads) k_lcompact(const int* __restrict__ flag, int n,
                                                        const int* __restrict__ local,
-                                                       const int* __restrict__ ctaoff, int* leaves)
+                                                       const int* __restrict__ ctaoff, int* leaves, int* posof)
 {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n && flag[k + 1]) leaves[ctaoff[k / kThreads] + local[k]] = k + 1;
+  if (k >= n) return;
+  int p = -1;
+  if (flag[k + 1]) {
+    p = ctaoff[k / kThreads] + local[k];
+    leaves[p] = k + 1;
+  }
+  posof[k + 1] = p;
 }
 
 inline int ctas(int n) { return (n + kThreads - 1) / kThreads; }
@@ -472,7 +479,7 @@ cudaError_t launch_flag_leaves(const int* leaves, int nl, int* flag, cudaStream_
 }
 
 cudaError_t launch_leaf_list(const int* flag, int nbmax, int* local, int* ctatot, int* ctaoff, int* leaves,
-                             int* nleaf, cudaStream_t st)
+                             int* nleaf, int* posof, cudaStream_t st)
 {
   if (nbmax <= 0) return cudaMemsetAsync(nleaf, 0, sizeof(int), st);
   const int g = ctas(nbmax);
@@ -482,17 +489,17 @@ cudaError_t launch_leaf_list(const int* flag, int nbmax, int* local, int* ctatot
   a.ctaoff = ctaoff;
   a.total = nleaf;
   k_bscan<<<1, 1024, 0, st>>>(a, g);
-  k_lcompact<<<g, kThreads, 0, st>>>(flag, nbmax, local, ctaoff, leaves);
+  k_lcompact<<<g, kThreads, 0, st>>>(flag, nbmax, local, ctaoff, leaves, posof);
   return cudaGetLastError();
 }
 
 int plan_ctas(int nleaf) { return ctas(nleaf); }
 
-cudaError_t launch_locatebounds(const PlanArgs& a, cudaStream_t st)
+cudaError_t launch_locatebounds(const PlanArgs& a, bool posof_ready, cudaStream_t st)
 {
   if (a.nleaf <= 0) return cudaSuccess;
   const int g = ctas(a.nleaf);
-  k_posof<<<g, kThreads, 0, st>>>(a);
+  if (!posof_ready) k_posof<<<g, kThreads, 0, st>>>(a);
   k_bcount<<<g, kThreads, 0, st>>>(a);
   k_bscan<<<1, 1024, 0, st>>>(a, g);
   k_bplan<<<g, kThreads, 0, st>>>(a);
