@@ -94,3 +94,51 @@ def test_oracle_reader_refuses_bad_files(oracle_lib, tmp_path):
     with pytest.raises(RuntimeError):
         q.read_bin(fp, fb, 0.0)
     assert os.path.getsize(fp) == 16 + 44 * o.nbmax
+
+
+def test_reference_reader_sees_the_oracle_state(oracle_lib, tmp_path):
+    """tests/golden/bin_reader_sedov.json holds what the reference's own
+    reader (py/walicxe2d_utils.py, run by tests/golden/make_bin_golden.py)
+    made of the oracle's BIN files after 12 steps of the small AMR blast:
+    the mesh table (corners and level of every leaf), per-leaf sums of the
+    decoded blocks, and the sum of the density map at the finest
+    resolution.  The oracle's state gives the same, so the files carry
+    that state as the reference's post-processing reads it."""
+    import json
+
+    from scipy import ndimage
+
+    from walicxe2d_b200.params import config
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "bin_reader_sedov.json")))
+    p, ic = config("sedov_amr_small")
+    o = oracle_lib.Oracle(p, ic, threads=4)
+    o.startup()
+    o.run(12)
+    ids = o.leaves()
+    assert len(ids) == g["nleaf"]
+    lp, icd = o.lp, o.icoord
+    mesh = []
+    for nb in ids:
+        lev = int(lp[nb, 0])
+        dx = p.xmax / p.nbroot_x / p.nx / (2.0 ** (lev - 1))
+        dy = p.ymax / p.nbroot_y / p.ny / (2.0 ** (lev - 1))
+        mesh.append([icd[nb, 0] * dx, icd[nb, 1] * dy, (icd[nb, 0] + p.nx) * dx, (icd[nb, 1] + p.ny) * dy,
+                     float(lev), 0.0])
+    assert mesh == g["mesh"]
+    # the reader's blocks[a, b, eq, leaf] is u(leaf, eq, i=a, j=b)
+    blk = np.zeros((W, W, p.neq, len(ids)))
+    for q, nb in enumerate(ids):
+        for k in range(p.neq):
+            blk[:, :, k, q] = o.u[nb, k].T
+    sums = [[float(blk[:, :, k, q].sum()) for k in range(p.neq)] for q in range(len(ids))]
+    assert sums == g["block_sums"]
+    # density at the finest resolution, coarser leaves zoomed (order 1)
+    nxt, nyt = p.nbroot_x * p.nx * 2 ** (p.nlevs - 1), p.nbroot_y * p.ny * 2 ** (p.nlevs - 1)
+    rho = np.zeros((nxt, nyt))
+    for q, nb in enumerate(ids):
+        f = 2 ** (p.nlevs - int(lp[nb, 0]))
+        x0, y0 = int(icd[nb, 0]) * f, int(icd[nb, 1]) * f
+        a = blk[2:p.ny + 2, 2:p.nx + 2, 0, q]
+        rho[x0:x0 + f * p.nx, y0:y0 + f * p.ny] = a if f == 1 else ndimage.zoom(a, f, order=1)
+    assert list(rho.T.shape) == g["map_shape"]
+    assert abs(rho.sum() - g["map_sum"]) <= 1e-12 * abs(g["map_sum"])
