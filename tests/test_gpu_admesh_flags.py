@@ -136,3 +136,41 @@ def test_links_reject_blocks_outside_the_pool():
         s.ctx.set_links(bad, rows=[nb])
     s.ctx.set_links(good)                    # the real tree is accepted again
     s.run(5)
+
+
+@pytest.mark.parametrize("mode", ["device", "host"])
+def test_pool_exhaustion_is_reported_by_both_sides(mode):
+    """src/admesh.f90:44-47 stops when the sons do not fit in the pool; both
+    sides report W2D_ERR_CAPACITY at the same step (no device fault)."""
+    from walicxe2d_b200._lib import W2dException
+    from walicxe2d_b200.api import Simulation
+    from walicxe2d_b200.params import sedov
+    p, ic = sedov(nbroot=4, nlevs=4, tol=0.1, nblocks=16 + 64 + 40, startup_admesh=0)
+    p.tol = -1.0                        # every leaf below nlevs refines
+    s = Simulation(p, ic)
+    s.set_tree_mode(mode)
+    s.run(1)                            # 16 roots -> 64 leaves (80 blocks)
+    with pytest.raises(W2dException) as e:
+        s.run(1)                        # 64 more families do not fit in 120 slots
+    assert e.value.code == 4            # W2D_ERR_CAPACITY
+
+
+def test_single_root_block_against_the_oracle(oracle_lib):
+    """One root block (1x1 roots, 4 levels): the tree grows from a single
+    block; the device's tree work and the host's give the oracle's tree and
+    blocks after every few steps."""
+    from walicxe2d_b200.params import sedov
+    p, ic = sedov(nbroot=1, nlevs=4, tol=0.1, nblocks=4000)
+    o = oracle_lib.Oracle(p, ic, threads=4)
+    o.startup()
+    a, b = _pair(p, ic)
+    m = noncorner_mask()
+    for _ in range(6):
+        o.run(10)
+        a.run(10)
+        b.run(10)
+        _same_tree(a, b)
+        ids = o.leaves()
+        assert np.array_equal(np.nonzero(a.tree()[1])[0], ids)
+        u = a.ctx.get_blocks(ids)
+        assert np.array_equal(u[:, :, m], o.u[ids][:, :, m])
