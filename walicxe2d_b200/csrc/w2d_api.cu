@@ -1146,8 +1146,7 @@ int w2d_admesh_flags(W2dCtx* c, int32_t* refine, int cap_refine, int* nrefine, i
   a.clist = c->d_mlists + 4 + slots;
   a.err = c->d_err;
   int rc = launch(c, "markref_critneighup", [&] { return launch_markref_up(a, c->st); });
-  if (!rc) rc = launch(c, "critneighdown", [&] { return launch_critneighdown(a, c->st); });
-  if (!rc) rc = launch(c, "coarsen_families", [&] { return launch_coarsen_families(a, c->st); });
+  if (!rc) rc = launch(c, "critneighdown_coarsen", [&] { return launch_refine_coarsen(a, c->st); });
   if (rc) return rc;
   // the counters and the heads of both lists in one wait; longer lists
   // (rare: a pass that remeshes thousands of blocks) in a second one

@@ -45,7 +45,7 @@ cudaError_t launch_dt_runs(const int* leaves, const int* loff, int nruns, const 
 // admesh flags on the device (w2d_mark.cu).  Per slot: lev, the mirror of
 // lp(:,3:4) (sons: first son, son position) and lp(:,5:8) (links), the
 // criteria maximum grad; byte
-// planes leafp, up, down, down2 zeroed before markref; counts[0..1] the
+// planes leafp, up, down (down2 unused) zeroed before markref; counts[0..1] the
 // lengths of rlist (refines) and clist (first sons of coarsened families),
 // zeroed before, in atomic order.
 struct MarkArgs {
@@ -64,8 +64,8 @@ struct MarkArgs {
 };
 // markref and the whole critneighup cascade in one launch
 cudaError_t launch_markref_up(const MarkArgs& a, cudaStream_t st);
-cudaError_t launch_critneighdown(const MarkArgs& a, cudaStream_t st);
-cudaError_t launch_coarsen_families(const MarkArgs& a, cudaStream_t st);
+// the refine list, then critneighdown and the coarsened families in one launch
+cudaError_t launch_refine_coarsen(const MarkArgs& a, cudaStream_t st);
 // rows7: (nb, lp(nb,3), lp(nb,4), lp(nb,5..8)) per row
 cudaError_t launch_set_links(const int* rows7, int n, int4* links, int2* sons, cudaStream_t st);
 

@@ -75,58 +75,61 @@ __global__ void __launch_bounds__(kThreads) k_markref_up(MarkArgs a)
   }
 }
 
-// The refine list (src/admesh.f90:29-65 refines every block of level
-// 1..nlevs-1 still marked) and critneighdown (src/critneighdown.f90:22-48)
-// as it sees the tree after those refines: updatelpup has cleared irefdown
-// of the refined blocks (src/updatelpup.f90:182-188), a refined neighbour of
-// the same level is no longer a leaf, and a refined coarser neighbour has
-// been replaced in lp by one of its new sons, a leaf
-// (src/updatelpup.f90:20-175 redirects the finer neighbours).
-__global__ void __launch_bounds__(kThreads) k_critneighdown(MarkArgs a)
+// a block refined by this pass (src/admesh.f90:29-65 refines every block of
+// level 1..nlevs-1 still marked)
+__device__ __forceinline__ bool refined_now(const MarkArgs& a, int nb)
 {
-  const int nb = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (nb > a.nbmax) return;
   const int l = a.lev[nb];
-  const bool refined = a.up[nb] && l >= 1 && l <= a.nlevs - 1;
-  if (refined) {
-    const int k = atomicAdd(&a.counts[0], 1);
-    if (k < a.cap) a.rlist[k] = nb;
-  }
-  unsigned char d = (a.down[nb] && !refined) ? 1 : 0;
-  if (d) {
-    const int4 q = a.links[nb];
-    const int n[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      const int n1 = n[s];
-      if (n1 == -1) continue;
-      if (!in_pool(n1, a.cap)) { d = 0; continue; }
-      const int l1 = a.lev[n1];
-      const bool r1 = a.up[n1] && l1 >= 1 && l1 <= a.nlevs - 1;
-      if (r1 && l1 < l) continue;            // now points to a new son
-      if (!a.leafp[n1] || r1) d = 0;
-    }
-  }
-  a.down2[nb] = d;
+  return a.up[nb] && l >= 1 && l <= a.nlevs - 1;
 }
 
-// src/admesh.f90:75-105: a first son (lp(nb,4) = 1) of level 2..nlevs whose
-// family is marked for coarsening throughout.  The sibling links of a
-// family (lp(s1,6), lp(s1,8), lp(lp(s1,6),8)) are never changed by the
-// updatelpup / updatelpdown calls of other families, so the decisions do
-// not depend on the order in which admesh takes them.
-__global__ void __launch_bounds__(kThreads) k_coarsen_families(MarkArgs a)
+// irefdown of block nb after critneighdown (src/critneighdown.f90:22-48)
+// as it sees the tree after the pass's refines: updatelpup has cleared
+// irefdown of the refined blocks (src/updatelpup.f90:182-188), a refined
+// neighbour of the same level is no longer a leaf, and a refined coarser
+// neighbour has been replaced in lp by one of its new sons, a leaf
+// (src/updatelpup.f90:20-175 redirects the finer neighbours).
+__device__ __forceinline__ bool down_after(const MarkArgs& a, int nb)
+{
+  if (!a.down[nb] || refined_now(a, nb)) return false;
+  const int l = a.lev[nb];
+  const int4 q = a.links[nb];
+  const int n[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    const int n1 = n[s];
+    if (n1 == -1) continue;
+    if (!in_pool(n1, a.cap)) return false;
+    const bool r1 = refined_now(a, n1);
+    if (r1 && a.lev[n1] < l) continue;       // now points to a new son
+    if (!a.leafp[n1] || r1) return false;
+  }
+  return true;
+}
+
+// The refine list, and the families the pass coarsens (src/admesh.f90:
+// 75-105): a first son (lp(nb,4) = 1) of level 2..nlevs whose four members
+// all keep irefdown.  The sibling links of a family (lp(s1,6), lp(s1,8),
+// lp(lp(s1,6),8)) are never changed by the updatelpup / updatelpdown calls
+// of other families, so the decisions do not depend on the order in which
+// admesh takes them.
+__global__ void __launch_bounds__(kThreads) k_refine_coarsen(MarkArgs a)
 {
   const int nb = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   if (nb > a.nbmax) return;
-  if (!a.down2[nb] || a.sons[nb].y != 1) return;
+  if (refined_now(a, nb)) {
+    const int k = atomicAdd(&a.counts[0], 1);
+    if (k < a.cap) a.rlist[k] = nb;
+    return;
+  }
+  if (!a.down[nb] || a.sons[nb].y != 1) return;
   const int l = a.lev[nb];
   if (l < 2 || l > a.nlevs) return;
   const int s2 = a.links[nb].y, s3 = a.links[nb].w;
   if (!in_pool(s2, a.cap) || !in_pool(s3, a.cap)) return;
   const int s4 = a.links[s2].w;
   if (!in_pool(s4, a.cap)) return;
-  if (a.down2[s2] && a.down2[s3] && a.down2[s4]) {
+  if (down_after(a, nb) && down_after(a, s2) && down_after(a, s3) && down_after(a, s4)) {
     const int k = atomicAdd(&a.counts[1], 1);
     if (k < a.cap) a.clist[k] = nb;
   }
@@ -515,17 +518,10 @@ cudaError_t launch_markref_up(const MarkArgs& a, cudaStream_t st)
   return cudaGetLastError();
 }
 
-cudaError_t launch_critneighdown(const MarkArgs& a, cudaStream_t st)
+cudaError_t launch_refine_coarsen(const MarkArgs& a, cudaStream_t st)
 {
   if (a.nbmax <= 0) return cudaSuccess;
-  k_critneighdown<<<ctas(a.nbmax), kThreads, 0, st>>>(a);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_coarsen_families(const MarkArgs& a, cudaStream_t st)
-{
-  if (a.nbmax <= 0) return cudaSuccess;
-  k_coarsen_families<<<ctas(a.nbmax), kThreads, 0, st>>>(a);
+  k_refine_coarsen<<<ctas(a.nbmax), kThreads, 0, st>>>(a);
   return cudaGetLastError();
 }
 
