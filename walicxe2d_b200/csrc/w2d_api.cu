@@ -710,7 +710,7 @@ int w2d_destroy(W2dCtx* c)
   if (c->h_nleaf) cudaFreeHost(c->h_nleaf);
   void* dev2[] = {c->d_run_of, c->d_runs, c->d_dt_run, c->d_loff, c->d_gradleaf, c->d_fb, c->d_fb_count,
                   c->d_nn_counts, c->d_nleaf, c->d_links, c->d_sons, c->d_mflags, c->d_mlists, c->d_rows7,
-                  c->d_posof, c->d_bcnt, c->d_blocal, c->d_bcta, c->d_wpos};
+                  c->d_posof, c->d_bent, c->d_bspan, c->d_blocal, c->d_bcta, c->d_wpos};
   for (void* d : dev2)
     if (d) cudaFree(d);
   if (c->h_dt_run) cudaFreeHost(c->h_dt_run);
@@ -809,6 +809,9 @@ int w2d_set_topology(W2dCtx* c, const int32_t* lp, int ld_lp, const int32_t* lea
 
 namespace {
 int ensure_plan(W2dCtx* c);   // (defined with the other lazily allocated parts below)
+// CTAs of 256 the plan build may use (one thread per leaf and side), so the
+// stride between the CTA totals and their offsets in d_bcta
+inline size_t bcta_half(const W2dCtx* c) { return (4 * ((size_t)c->cap + 1)) / 256 + 1; }
 }  // namespace
 
 }  // extern "C"
@@ -823,11 +826,10 @@ int ctx_topology_device(W2dCtx* c, int nbmax, int nleaf)
   if (nbmax < 0 || nbmax > c->cap || nleaf < 0 || nleaf > nbmax) return W2D_ERR_ARG;
   int rc = ensure_plan(c);
   if (rc) return rc;
-  const size_t slots = (size_t)c->cap + 1;
   c->nbmax = nbmax;
   c->nleaf = nleaf;
   rc = launch(c, "leaf_list", [&] {
-    return launch_leaf_list(c->d_leafflag, nbmax, c->d_blocal, c->d_bcta, c->d_bcta + (slots / 256 + 1),
+    return launch_leaf_list(c->d_leafflag, nbmax, c->d_blocal, c->d_bcta, c->d_bcta + bcta_half(c),
                             c->d_leaves, c->d_nleaf, c->d_posof, c->st);
   });
   if (rc) return rc;
@@ -1063,9 +1065,10 @@ int ensure_plan(W2dCtx* c)
   if (c->d_posof) return W2D_OK;
   const size_t slots = (size_t)c->cap + 1;
   CK(cudaMalloc(&c->d_posof, sizeof(int) * slots));
-  CK(cudaMalloc(&c->d_bcnt, sizeof(int) * slots));
-  CK(cudaMalloc(&c->d_blocal, sizeof(int) * slots));
-  CK(cudaMalloc(&c->d_bcta, sizeof(int) * (2 * (slots / 256 + 1) + 1)));
+  CK(cudaMalloc(&c->d_bent, sizeof(int2) * 4 * slots));
+  CK(cudaMalloc(&c->d_bspan, sizeof(int2) * slots));
+  CK(cudaMalloc(&c->d_blocal, sizeof(int) * 4 * slots));
+  CK(cudaMalloc(&c->d_bcta, sizeof(int) * (2 * bcta_half(c) + 1)));
   CK(cudaMalloc(&c->d_wpos, sizeof(int) * slots));
   return W2D_OK;
 }
@@ -1212,12 +1215,13 @@ int w2d_locate_bounds(W2dCtx* c)
   a.links = c->d_links;
   a.sons = c->d_sons;
   a.posof = c->d_posof;
-  a.cnt = c->d_bcnt;
+  a.entries = c->d_bent;
+  a.span = c->d_bspan;
   a.local = c->d_blocal;
   const int g = plan_ctas(nl);
   a.ctatot = c->d_bcta;
-  a.ctaoff = c->d_bcta + (slots / 256 + 1);
-  a.total = c->d_bcta + 2 * (slots / 256 + 1);
+  a.ctaoff = c->d_bcta + bcta_half(c);
+  a.total = c->d_bcta + 2 * bcta_half(c);
   a.fd1 = c->d_fd1;
   a.fd2 = c->d_fd2;
   a.wpos = c->d_wpos;
@@ -1229,8 +1233,8 @@ int w2d_locate_bounds(W2dCtx* c)
   a.f6b = (c->p.compat & W2D_COMPAT_OUTFYB) != 0;
   a.jet = c->p.otherb == W2D_USERBC_JET;
   if ((rc = launch(c, "locatebounds", [&] { return launch_locatebounds(a, posof_ready, c->st); }))) return rc;
-  if (nl > 0)   // the launcher issues up to six kernels; launch() counted one
-    c->nlaunch += 2 + !posof_ready + (a.f6b && a.bc[2] != W2D_BC_REFLECTIVE) + a.jet;
+  if (nl > 0)   // the launcher issues up to seven kernels; launch() counted one
+    c->nlaunch += 2 + !posof_ready + (a.f6b && a.bc[2] != W2D_BC_REFLECTIVE) + 2 * a.jet;
   (void)g;
   c->have_bounds = true;
   return W2D_OK;

@@ -107,12 +107,14 @@ struct W2dCtx {
   int* d_rows7 = nullptr;     // (nb, lp(nb,3:8)) per row, cap+1 rows
   int* h_rows7 = nullptr;     // pinned
   // locatebounds on the device (allocated by the first w2d_locate_bounds):
-  // leaf position per slot, entries per leaf and their prefix sums, the
+  // leaf position per slot, the entry of every (leaf, side) and the prefix
+  // sums of their count, each slot's first and last list position (jet), the
   // writer position of each boundaryI bottom face
   int* d_posof = nullptr;
-  int* d_bcnt = nullptr;
-  int* d_blocal = nullptr;
-  int* d_bcta = nullptr;      // CTA totals, then their offsets, then the list length
+  int2* d_bent = nullptr;     // 4 per leaf position
+  int2* d_bspan = nullptr;    // per slot
+  int* d_blocal = nullptr;    // 4 per leaf position (the leaf list uses 1 per slot)
+  int* d_bcta = nullptr;      // CTA totals, then their offsets (bcta_half apart), then the list length
   int* d_wpos = nullptr;
   cudaEvent_t ev_links = nullptr;
   bool have_links = false;

@@ -70,11 +70,13 @@ cudaError_t launch_refine_coarsen(const MarkArgs& a, cudaStream_t st);
 cudaError_t launch_set_links(const int* rows7, int n, int4* links, int2* sons, cudaStream_t st);
 
 // locatebounds and the fill plans on the device (w2d_mark.cu).  posof: per
-// slot, the leaf position or -1 (set to -1 before); cnt/local: per leaf
-// position, its entries and their exclusive prefix within its CTA of 256;
-// ctatot/ctaoff per CTA; total[0] the list length; fd1/fd2 (4 faces per
-// leaf position) and wpos (per leaf position) zeroed before; jetblk per
-// leaf position (jet runs).
+// slot, the leaf position or -1 (set to -1 before); entries/local: per
+// (leaf position, side), its innerbounds entry (type, neighbour) and the
+// exclusive prefix of the entry count within its CTA of 256; ctatot/ctaoff
+// per CTA; total[0] the list length; span (jet runs): per slot, the first
+// and last list position as nbs; fd1/fd2 (4 faces per leaf position) and
+// wpos (per leaf position) zeroed before; jetblk per leaf position (jet
+// runs).
 struct PlanArgs {
   const int* leaves;
   int nleaf, nbmax, cap;
@@ -82,7 +84,9 @@ struct PlanArgs {
   const int4* links;
   const int2* sons;
   int* posof;
-  int *cnt, *local, *ctatot, *ctaoff, *total;
+  int2* entries;
+  int2* span;
+  int *local, *ctatot, *ctaoff, *total;
   int2 *fd1, *fd2;
   int* wpos;
   int* jetblk;
@@ -90,9 +94,9 @@ struct PlanArgs {
   int f6b, jet;
 };
 int plan_ctas(int nleaf);
-// six launches at most: positions (unless posof_ready: posof already holds
-// the leaf position of every slot 1..nbmax, -1 for the others), counts,
-// scan, entries, OUTFYB, jet
+// seven launches at most: positions (unless posof_ready: posof already
+// holds the leaf position of every slot 1..nbmax, -1 for the others),
+// entries and counts, scan, spans (jet), plans, OUTFYB, jet
 cudaError_t launch_locatebounds(const PlanArgs& a, bool posof_ready, cudaStream_t st);
 
 // flag[leaves[k]] = 1 for k < nl (flag zeroed before)

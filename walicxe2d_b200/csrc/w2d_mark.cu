@@ -162,52 +162,36 @@ __global__ void __launch_bounds__(kThreads) k_set_links(const int* __restrict__ 
 //     which never add entries toward a coarser block themselves);
 //   - a coarser neighbour: no entry (that neighbour adds the one above).
 // So each leaf's entries follow from its links alone, and their list
-// positions from a prefix sum of the counts over the leaves.  The plans are
-// those of the host walk (w2d_api.cu: plan_entries): every non-corner ghost
-// face has exactly one writer, except the bottom faces of boundaryI that
-// the OUTFYB defect also writes (resolved by list position in a second
-// pass), and the jet flags come from each block's first and last position
-// as nbs.
+// positions from a prefix sum over (leaf, side) in list order: one thread
+// per leaf and side finds its entry, the prefix sum gives its position, and
+// one thread per entry writes the plans.  The plans are those of the host
+// walk (w2d_api.cu: plan_entries): every non-corner ghost face has exactly
+// one writer, except the bottom faces of boundaryI that the OUTFYB defect
+// also writes (resolved by list position in a second pass), and the jet
+// flags come from each block's first and last position as nbs (a per-slot
+// table built before the plans).
 
-__device__ __forceinline__ int pl_base(const PlanArgs& a, int k)
+// The entry of side s of leaf nb: (type, neighbour), type 0 for none.
+__device__ __forceinline__ int2 pl_entry(const PlanArgs& a, int nb, int s)
 {
-  return a.ctaoff[k / kThreads] + a.local[k];
+  const int4 q = a.links[nb];
+  const int m = s == 0 ? q.x : s == 1 ? q.y : s == 2 ? q.z : q.w;
+  if (m == -1) return make_int2(-(s + 1), 0);
+  if (!in_pool(m, a.cap) || m > a.nbmax) return make_int2(0, 0);
+  if (a.lev[m] < a.lev[nb]) return make_int2(0, 0);          // coarser: its entry
+  if (a.posof[m] >= 0)                                        // same-level leaf
+    return nb < m ? make_int2(1 + 3 * s, m) : make_int2(0, 0);
+  const int f = a.sons[m].x;                                  // same level, has sons
+  if (f < 1 || f + 3 > a.nbmax) return make_int2(0, 0);
+  const int son_off = (s == 0) ? 1 : (s == 2) ? 2 : 0;
+  return make_int2(2 + 3 * s, f + son_off);
 }
 
 // first and last list position (1-based) of block b as nbs, 0 if none
 __device__ __forceinline__ int2 pl_span(const PlanArgs& a, int b)
 {
   if (b < 1 || b > a.nbmax) return make_int2(0, 0);
-  const int k = a.posof[b];
-  if (k < 0 || a.cnt[k] == 0) return make_int2(0, 0);
-  const int e0 = pl_base(a, k) + 1;
-  return make_int2(e0, e0 + a.cnt[k] - 1);
-}
-
-// The entries of leaf nb: (type, neighbour) per side, type 0 for none.
-__device__ __forceinline__ void pl_entries(const PlanArgs& a, int nb, int t[4], int n1[4])
-{
-  const int4 q = a.links[nb];
-  const int nn[4] = {q.x, q.y, q.z, q.w};
-  const int l = a.lev[nb];
-  const int same[4] = {1, 4, 7, 10}, rest[4] = {2, 5, 8, 11}, son_off[4] = {1, 0, 2, 0};
-#pragma unroll
-  for (int s = 0; s < 4; ++s) {
-    t[s] = 0;
-    n1[s] = 0;
-    const int m = nn[s];
-    if (m == -1) { t[s] = -(s + 1); continue; }
-    if (!in_pool(m, a.cap) || m > a.nbmax) continue;
-    if (a.lev[m] < l) continue;                          // coarser: its entry
-    if (a.posof[m] >= 0) {                               // same-level leaf
-      if (nb < m) { t[s] = same[s]; n1[s] = m; }
-    } else {                                             // same level, has sons
-      const int f = a.sons[m].x;
-      if (f < 1 || f + 3 > a.nbmax) continue;
-      t[s] = rest[s];
-      n1[s] = f + son_off[s];
-    }
-  }
+  return a.span[b];
 }
 
 __global__ void __launch_bounds__(kThreads) k_posof(PlanArgs a)
@@ -218,43 +202,40 @@ __global__ void __launch_bounds__(kThreads) k_posof(PlanArgs a)
   if (in_pool(nb, a.cap)) a.posof[nb] = k;
 }
 
-// entries per leaf, their exclusive prefix sum within the CTA and the
-// CTA's total
+// thread x = 4 * leaf position + side: the entry, and the exclusive prefix
+// of the entry count within the CTA (list order), and the CTA's total
 __global__ void __launch_bounds__(kThreads) k_bcount(PlanArgs a)
 {
   __shared__ int wsum[kThreads / 32];
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
   int c = 0;
-  if (k < a.nleaf) {
-    const int nb = a.leaves[k];
-    if (in_pool(nb, a.cap)) {
-      int t[4], n1[4];
-      pl_entries(a, nb, t, n1);
-      c = (t[0] != 0) + (t[1] != 0) + (t[2] != 0) + (t[3] != 0);
-    }
-    a.cnt[k] = c;
+  if (x < 4 * a.nleaf) {
+    const int nb = a.leaves[x >> 2];
+    int2 en = make_int2(0, 0);
+    if (in_pool(nb, a.cap)) en = pl_entry(a, nb, x & 3);
+    a.entries[x] = en;
+    c = en.x != 0;
   }
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int x = c;
+  int v = c;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
+    const int y = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += y;
   }
-  if (lane == 31) wsum[w] = x;
+  if (lane == 31) wsum[w] = v;
   __syncthreads();
   if (w == 0) {
-    int v = lane < kThreads / 32 ? wsum[lane] : 0;
+    int u = lane < kThreads / 32 ? wsum[lane] : 0;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, v, o);
-      if (lane >= o) v += y;
+      const int y = __shfl_up_sync(0xffffffffu, u, o);
+      if (lane >= o) u += y;
     }
-    if (lane < kThreads / 32) wsum[lane] = v;   // inclusive over warps
+    if (lane < kThreads / 32) wsum[lane] = u;   // inclusive over warps
   }
   __syncthreads();
-  const int before = (w > 0 ? wsum[w - 1] : 0) + x - c;
-  if (k < a.nleaf) a.local[k] = before;
+  if (x < 4 * a.nleaf) a.local[x] = (w > 0 ? wsum[w - 1] : 0) + v - c;
   if (threadIdx.x == kThreads - 1) a.ctatot[blockIdx.x] = wsum[kThreads / 32 - 1];
 }
 
@@ -295,6 +276,31 @@ __global__ void __launch_bounds__(1024) k_bscan(PlanArgs a, int nctas)
   if (threadIdx.x == 0) a.total[0] = carry;
 }
 
+// list position (1-based) of the entry of thread x (if it has one)
+__device__ __forceinline__ int pl_pos(const PlanArgs& a, int x)
+{
+  return a.ctaoff[x / kThreads] + a.local[x] + 1;
+}
+
+// jet runs: first and last position of every leaf as nbs, per slot (the
+// slots 1..nbmax that are not leaves get none)
+__global__ void __launch_bounds__(kThreads) k_bspan(PlanArgs a)
+{
+  const int nb = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (nb > a.nbmax) return;
+  const int k = a.posof[nb];
+  int2 sp = make_int2(0, 0);
+  if (k >= 0) {
+    for (int s = 0; s < 4; ++s) {
+      if (a.entries[4 * k + s].x == 0) continue;
+      const int e = pl_pos(a, 4 * k + s);
+      if (!sp.x) sp.x = e;
+      sp.y = e;
+    }
+  }
+  a.span[nb] = sp;
+}
+
 // put() of the host walk: one face descriptor of a leaf target, with the
 // jet flags for entry position e
 __device__ __forceinline__ void pl_put(const PlanArgs& a, int2* fd, bool is_fd1, int blk, int face, int nbr,
@@ -318,81 +324,73 @@ __device__ __forceinline__ void pl_put(const PlanArgs& a, int2* fd, bool is_fd1,
   if (is_fd1 && face == 2) a.wpos[p] = e;
 }
 
-// every entry of every leaf, at its list position (the OUTFYB bottom-face
-// writes of boundaryI come in k_bplan_f6b)
+// every entry at its list position, one thread per (leaf, side) (the
+// OUTFYB bottom-face writes of boundaryI come in k_bplan_f6b)
 __global__ void __launch_bounds__(kThreads) k_bplan(PlanArgs a)
 {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= a.nleaf) return;
-  const int nbs = a.leaves[k];
-  if (!in_pool(nbs, a.cap)) return;
-  int t[4], nn[4];
-  pl_entries(a, nbs, t, nn);
-  int e = pl_base(a, k);
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= 4 * a.nleaf) return;
+  const int2 en = a.entries[x];
+  if (en.x == 0) return;
+  const int nbs = a.leaves[x >> 2];
+  const int e = pl_pos(a, x);
+  const int n1 = en.y;
   const int H = W2D_NX / 2;
-#pragma unroll 1
-  for (int s = 0; s < 4; ++s) {
-    if (!t[s]) continue;
-    ++e;
-    const int n1 = nn[s];
-    auto both = [&](int blk, int face, int nbr, int kind, int off) {
-      pl_put(a, a.fd1, true, blk, face, nbr, kind, off, e);
-      pl_put(a, a.fd2, false, blk, face, nbr, kind, off, e);
-    };
-    switch (t[s]) {
-      case -1: case -2: case -4: {
-        const int f = (t[s] == -1) ? 0 : (t[s] == -2) ? 1 : 3;
-        both(nbs, f, nbs, a.bc[f] == W2D_BC_REFLECTIVE ? FK_REFLECT : FK_MIRROR, 0);
-        break;
-      }
-      case -3:
-        if (a.bc[2] == W2D_BC_REFLECTIVE) {
-          both(nbs, 2, nbs, FK_REFLECT, 0);
-        } else {
-          pl_put(a, a.fd2, false, nbs, 2, nbs, FK_MIRROR, 0, e);
-          if (!a.f6b) pl_put(a, a.fd1, true, nbs, 2, nbs, FK_MIRROR, 0, e);
-        }
-        break;
-      case 1:  both(nbs, 0, n1, FK_SAME, 0);  both(n1, 1, nbs, FK_SAME, 0); break;
-      case 4:  both(nbs, 1, n1, FK_SAME, 0);  both(n1, 0, nbs, FK_SAME, 0); break;
-      case 7:  both(nbs, 2, n1, FK_SAME, 0);  both(n1, 3, nbs, FK_SAME, 0); break;
-      case 10: both(nbs, 3, n1, FK_SAME, 0);  both(n1, 2, nbs, FK_SAME, 0); break;
-      case 2:
-        both(nbs, 0, n1, FK_RESTRICT, 0);
-        both(n1, 1, nbs, FK_INJECT, 0);
-        both(n1 + 2, 1, nbs, FK_INJECT, H);
-        break;
-      case 5:
-        both(nbs, 1, n1, FK_RESTRICT, 0);
-        both(n1, 0, nbs, FK_INJECT, 0);
-        both(n1 + 2, 0, nbs, FK_INJECT, H);
-        break;
-      case 8:
-        both(nbs, 2, n1, FK_RESTRICT, 0);
-        both(n1, 3, nbs, FK_INJECT, 0);
-        both(n1 + 1, 3, nbs, FK_INJECT, H);
-        break;
-      default:   // 11
-        both(nbs, 3, n1, FK_RESTRICT, 0);
-        both(n1, 2, nbs, FK_INJECT, 0);
-        both(n1 + 1, 2, nbs, FK_INJECT, H);
-        break;
+  auto both = [&](int blk, int face, int nbr, int kind, int off) {
+    pl_put(a, a.fd1, true, blk, face, nbr, kind, off, e);
+    pl_put(a, a.fd2, false, blk, face, nbr, kind, off, e);
+  };
+  switch (en.x) {
+    case -1: case -2: case -4: {
+      const int f = (en.x == -1) ? 0 : (en.x == -2) ? 1 : 3;
+      both(nbs, f, nbs, a.bc[f] == W2D_BC_REFLECTIVE ? FK_REFLECT : FK_MIRROR, 0);
+      break;
     }
+    case -3:
+      if (a.bc[2] == W2D_BC_REFLECTIVE) {
+        both(nbs, 2, nbs, FK_REFLECT, 0);
+      } else {
+        pl_put(a, a.fd2, false, nbs, 2, nbs, FK_MIRROR, 0, e);
+        if (!a.f6b) pl_put(a, a.fd1, true, nbs, 2, nbs, FK_MIRROR, 0, e);
+      }
+      break;
+    case 1:  both(nbs, 0, n1, FK_SAME, 0);  both(n1, 1, nbs, FK_SAME, 0); break;
+    case 4:  both(nbs, 1, n1, FK_SAME, 0);  both(n1, 0, nbs, FK_SAME, 0); break;
+    case 7:  both(nbs, 2, n1, FK_SAME, 0);  both(n1, 3, nbs, FK_SAME, 0); break;
+    case 10: both(nbs, 3, n1, FK_SAME, 0);  both(n1, 2, nbs, FK_SAME, 0); break;
+    case 2:
+      both(nbs, 0, n1, FK_RESTRICT, 0);
+      both(n1, 1, nbs, FK_INJECT, 0);
+      both(n1 + 2, 1, nbs, FK_INJECT, H);
+      break;
+    case 5:
+      both(nbs, 1, n1, FK_RESTRICT, 0);
+      both(n1, 0, nbs, FK_INJECT, 0);
+      both(n1 + 2, 0, nbs, FK_INJECT, H);
+      break;
+    case 8:
+      both(nbs, 2, n1, FK_RESTRICT, 0);
+      both(n1, 3, nbs, FK_INJECT, 0);
+      both(n1 + 1, 3, nbs, FK_INJECT, H);
+      break;
+    default:   // 11
+      both(nbs, 3, n1, FK_RESTRICT, 0);
+      both(n1, 2, nbs, FK_INJECT, 0);
+      both(n1 + 1, 2, nbs, FK_INJECT, H);
+      break;
   }
 }
 
 // src/boundaryI.f90:87 (OUTFYB): the bottom-wall entry at list position e
 // fills the bottom face of block e; it wins over the face's own writer when
-// it comes later in the list
+// it comes later in the list.  One thread per leaf (its bottom side).
 __global__ void __launch_bounds__(kThreads) k_bplan_f6b(PlanArgs a)
 {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= a.nleaf) return;
-  const int nbs = a.leaves[k];
-  if (!in_pool(nbs, a.cap) || a.links[nbs].z != -1) return;
-  int t[4], nn[4];
-  pl_entries(a, nbs, t, nn);
-  const int e = pl_base(a, k) + (t[0] != 0) + (t[1] != 0) + 1;   // the bottom entry's position
+  const int x = 4 * k + 2;
+  if (a.entries[x].x != -3) return;
+  const int e = pl_pos(a, x);
   const int tb = e;
   if (tb < 1 || tb > a.nbmax) return;
   const int p = a.posof[tb];
@@ -406,7 +404,7 @@ __global__ void __launch_bounds__(kThreads) k_bplan_jet(PlanArgs a)
 {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= a.nleaf) return;
-  const bool named = a.cnt[k] > 0;
+  const bool named = a.span[a.leaves[k]].x > 0;
   a.jetblk[k] = named;
   if (!named) return;
 #pragma unroll
@@ -501,11 +499,12 @@ int plan_ctas(int nleaf) { return ctas(nleaf); }
 cudaError_t launch_locatebounds(const PlanArgs& a, bool posof_ready, cudaStream_t st)
 {
   if (a.nleaf <= 0) return cudaSuccess;
-  const int g = ctas(a.nleaf);
+  const int g = ctas(a.nleaf), g4 = ctas(4 * a.nleaf);
   if (!posof_ready) k_posof<<<g, kThreads, 0, st>>>(a);
-  k_bcount<<<g, kThreads, 0, st>>>(a);
-  k_bscan<<<1, 1024, 0, st>>>(a, g);
-  k_bplan<<<g, kThreads, 0, st>>>(a);
+  k_bcount<<<g4, kThreads, 0, st>>>(a);
+  k_bscan<<<1, 1024, 0, st>>>(a, g4);
+  if (a.jet) k_bspan<<<ctas(a.nbmax), kThreads, 0, st>>>(a);
+  k_bplan<<<g4, kThreads, 0, st>>>(a);
   if (a.f6b && a.bc[2] != W2D_BC_REFLECTIVE) k_bplan_f6b<<<g, kThreads, 0, st>>>(a);
   if (a.jet) k_bplan_jet<<<g, kThreads, 0, st>>>(a);
   return cudaGetLastError();
