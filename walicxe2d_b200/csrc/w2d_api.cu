@@ -1201,11 +1201,7 @@ int w2d_locate_bounds(W2dCtx* c)
   // 1..nbmax (the only ones the plan kernels look up)
   const bool posof_ready = c->host_leaves_stale;
   if (!posof_ready) CK(cudaMemsetAsync(c->d_posof, 0xff, sizeof(int) * slots, c->st));    // -1: not a leaf
-  if (nl > 0) {
-    CK(cudaMemsetAsync(c->d_fd1, 0, sizeof(int2) * 4 * (size_t)nl, c->st));   // (0, FK_KEEP)
-    CK(cudaMemsetAsync(c->d_fd2, 0, sizeof(int2) * 4 * (size_t)nl, c->st));
-    CK(cudaMemsetAsync(c->d_wpos, 0, sizeof(int) * (size_t)nl, c->st));
-  }
+  // (the plans and the bottom-face writer positions are cleared by k_bcount)
   PlanArgs a{};
   a.leaves = c->d_leaves;
   a.nleaf = nl;

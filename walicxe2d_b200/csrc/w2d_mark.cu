@@ -203,13 +203,18 @@ __global__ void __launch_bounds__(kThreads) k_posof(PlanArgs a)
 }
 
 // thread x = 4 * leaf position + side: the entry, and the exclusive prefix
-// of the entry count within the CTA (list order), and the CTA's total
+// of the entry count within the CTA (list order), and the CTA's total; it
+// also clears face x of both plans (FK_KEEP) and, for side 0, the leaf's
+// bottom-face writer position, before k_bplan writes them
 __global__ void __launch_bounds__(kThreads) k_bcount(PlanArgs a)
 {
   __shared__ int wsum[kThreads / 32];
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   int c = 0;
   if (x < 4 * a.nleaf) {
+    a.fd1[x] = make_int2(0, FK_KEEP);
+    a.fd2[x] = make_int2(0, FK_KEEP);
+    if ((x & 3) == 0) a.wpos[x >> 2] = 0;
     const int nb = a.leaves[x >> 2];
     int2 en = make_int2(0, 0);
     if (in_pool(nb, a.cap)) en = pl_entry(a, nb, x & 3);
