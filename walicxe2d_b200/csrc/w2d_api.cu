@@ -1049,7 +1049,7 @@ int ensure_mark(W2dCtx* c)
   const size_t slots = (size_t)c->cap + 1;
   CK(cudaMalloc(&c->d_links, sizeof(int4) * slots));
   CK(cudaMalloc(&c->d_sons, sizeof(int2) * slots));
-  CK(cudaMalloc(&c->d_mflags, 4 * mark_plane(c)));
+  CK(cudaMalloc(&c->d_mflags, 3 * mark_plane(c)));
   CK(cudaMalloc(&c->d_mlists, sizeof(int) * (4 + 2 * slots)));
   CK(cudaMalloc(&c->d_rows7, sizeof(int) * 7 * slots));
   CK(cudaMallocHost(&c->h_mlists, sizeof(int) * (4 + 2 * slots)));
@@ -1126,7 +1126,7 @@ int w2d_admesh_flags(W2dCtx* c, int32_t* refine, int cap_refine, int* nrefine, i
   if (c->nruns > 0) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "one run per context");
   const size_t slots = (size_t)c->cap + 1;
   const size_t plane = mark_plane(c);
-  CK(cudaMemsetAsync(c->d_mflags, 0, 4 * plane, c->st));
+  CK(cudaMemsetAsync(c->d_mflags, 0, 3 * plane, c->st));
   CK(cudaMemsetAsync(c->d_mlists, 0, 4 * sizeof(int), c->st));
   MarkArgs a{};
   a.leaves = c->d_leaves;
@@ -1143,7 +1143,6 @@ int w2d_admesh_flags(W2dCtx* c, int32_t* refine, int cap_refine, int* nrefine, i
   a.leafp = c->d_mflags;
   a.up = c->d_mflags + plane;
   a.down = c->d_mflags + 2 * plane;
-  a.down2 = c->d_mflags + 3 * plane;
   a.counts = c->d_mlists;
   a.rlist = c->d_mlists + 4;
   a.clist = c->d_mlists + 4 + slots;

@@ -97,7 +97,7 @@ struct W2dCtx {
   cudaEvent_t ev_plan[2] = {nullptr, nullptr};
   int plan_buf = 0;
   // admesh flags on the device (allocated by the first w2d_set_links): the
-  // mirror of lp(:,3:8), four byte planes of cap+1 flags, the two lists
+  // mirror of lp(:,3:8), three byte planes of cap+1 flags, the two lists
   // behind two counters, and the pinned row staging of w2d_set_links
   int4* d_links = nullptr;
   int2* d_sons = nullptr;     // lp(:,3), lp(:,4)

@@ -45,7 +45,7 @@ cudaError_t launch_dt_runs(const int* leaves, const int* loff, int nruns, const 
 // admesh flags on the device (w2d_mark.cu).  Per slot: lev, the mirror of
 // lp(:,3:4) (sons: first son, son position) and lp(:,5:8) (links), the
 // criteria maximum grad; byte
-// planes leafp, up, down (down2 unused) zeroed before markref; counts[0..1] the
+// planes leafp, up, down zeroed before markref; counts[0..1] the
 // lengths of rlist (refines) and clist (first sons of coarsened families),
 // zeroed before, in atomic order.
 struct MarkArgs {
@@ -56,7 +56,7 @@ struct MarkArgs {
   const int2* sons;
   const double* grad;
   double tol, tol2;
-  unsigned char *leafp, *up, *down, *down2;
+  unsigned char *leafp, *up, *down;
   int* counts;
   int* rlist;
   int* clist;
