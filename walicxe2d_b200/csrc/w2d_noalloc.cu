@@ -15,30 +15,26 @@
 // allocated per call.  Built with --fmad=false like the FP64 kernels.
 #include <cuda_runtime.h>
 
-#include <cstdio>
-#include <mutex>
-
 #include "../../include/w2d.h"
 #include "w2d_phys.cuh"
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-
-// Per-block partials, then the result at index W2D_NOALLOC_MAX_BLOCKS.
+// Per-block partials, then the result at index W2D_NOALLOC_MAX_BLOCKS and
+// the first block with a level outside 1..nlevs (0: none) at the index after.
 static __device__ __align__(256) double g_noalloc_scratch[W2D_NOALLOC_MAX_BLOCKS + 32];
-
-double* g_scratch_dev[kMaxDevices] = {nullptr};  // device address, per device
-std::mutex g_setup_mutex;
 
 struct Spacing {
   double dx[W2D_MAXLEV_NOALLOC + 1];
   double dy[W2D_MAXLEV_NOALLOC + 1];
 };
 
+// A block whose level lies outside 1..nlevs gets the partial -(b+1): the
+// true partials are positive, so the reduction can tell them apart.
 template <int NEQ>
 __global__ void __launch_bounds__(256) k_cfl_partials(const double* __restrict__ u, const int32_t* __restrict__ lev,
-                                                      Spacing sp, w2d::Phys<double> ph, double* __restrict__ part)
+                                                      int nlevs, Spacing sp, w2d::Phys<double> ph,
+                                                      double* __restrict__ part)
 {
   __shared__ double red[8];
   const int b = blockIdx.x;
@@ -51,9 +47,15 @@ __global__ void __launch_bounds__(256) k_cfl_partials(const double* __restrict__
   w2d::uprim<NEQ>(ph, q, uu, T);
   const double cs = w2d::sound(ph, q[3], q[0]);
   const int l = lev[b];
+  if (l < 1 || l > nlevs) {
+    if (t == 0) part[b] = -(double)(b + 1);
+    return;
+  }
   const double t1 = sp.dx[l] / (fabs(q[1]) + cs);
   const double t2 = sp.dy[l] / (fabs(q[2]) + cs);
-  double m = (t1 < t2) ? t1 : t2;
+  // fmin here as in the reduction below: a NaN cell is ignored, as the
+  // context's max over |u|+cs ignores it
+  double m = fmin(t1, t2);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((t & 31) == 0) red[t >> 5] = m;
@@ -68,35 +70,47 @@ __global__ void __launch_bounds__(256) k_cfl_partials(const double* __restrict__
 __global__ void __launch_bounds__(1024) k_cfl_reduce(const double* __restrict__ part, int n, double courant,
                                                      double psc, double tsc, double* __restrict__ out)
 {
-  __shared__ double red[32];
-  double m = 1.e30;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) m = fmin(m, part[k]);
+  __shared__ double red[32], bad[32];
+  double m = 1.e30, worst = 0.0;   // worst: most negative partial (a bad level)
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const double v = part[k];
+    if (v < 0.0) worst = fmin(worst, v);
+    else m = fmin(m, v);
+  }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  for (int o = 16; o > 0; o >>= 1) {
+    m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+    worst = fmin(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = m;
+    bad[threadIdx.x >> 5] = worst;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     m = red[0];
-    for (int w = 1; w < 32; ++w) m = fmin(m, red[w]);
+    worst = bad[0];
+    for (int w = 1; w < 32; ++w) {
+      m = fmin(m, red[w]);
+      worst = fmin(worst, bad[w]);
+    }
     const double a = courant * m;
     const double c = 0.4 * 1e30 * psc / tsc;
     out[0] = (a < c) ? a : c;
+    out[1] = -worst;   // a block ID + 1 with a bad level, or 0
   }
 }
 
-// Device address of the scratch array for the current device, looked up
-// once per device with that device current.
+// Device address of the scratch array in the caller's current device and
+// context.  Looked up on every call (the lookup allocates nothing): after a
+// device reset, or when an offload runtime tears its context down and builds
+// a new one, the module is loaded again and the array can move, so an
+// address kept from an earlier call could point at freed memory.
 int scratch_for_current_device(double** out)
 {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return W2D_ERR_CUDA;
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_dev[dev]) {
-    void* ptr = nullptr;
-    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return W2D_ERR_CUDA;
-    g_scratch_dev[dev] = static_cast<double*>(ptr);
-  }
-  *out = g_scratch_dev[dev];
+  void* ptr = nullptr;
+  if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return W2D_ERR_CUDA;
+  *out = static_cast<double*>(ptr);
   return W2D_OK;
 }
 
@@ -128,13 +142,16 @@ extern "C" int w2d_timestep_noalloc(const W2dParams* p, const double* u, const i
   ph.solver = p->solver;
   ph.limiter = p->limiter;
   switch (p->neq) {
-    case 4: k_cfl_partials<4><<<nblocks, 256>>>(u, lev, sp, ph, scratch); break;
-    case 5: k_cfl_partials<5><<<nblocks, 256>>>(u, lev, sp, ph, scratch); break;
-    default: k_cfl_partials<6><<<nblocks, 256>>>(u, lev, sp, ph, scratch); break;
+    case 4: k_cfl_partials<4><<<nblocks, 256>>>(u, lev, p->nlevs, sp, ph, scratch); break;
+    case 5: k_cfl_partials<5><<<nblocks, 256>>>(u, lev, p->nlevs, sp, ph, scratch); break;
+    default: k_cfl_partials<6><<<nblocks, 256>>>(u, lev, p->nlevs, sp, ph, scratch); break;
   }
   k_cfl_reduce<<<1, 1024>>>(scratch, nblocks, p->cfl, p->psc, p->tsc, scratch + W2D_NOALLOC_MAX_BLOCKS);
   if (cudaGetLastError() != cudaSuccess) return W2D_ERR_CUDA;
-  if (cudaMemcpy(dt, scratch + W2D_NOALLOC_MAX_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+  double res[2];
+  if (cudaMemcpy(res, scratch + W2D_NOALLOC_MAX_BLOCKS, sizeof(res), cudaMemcpyDeviceToHost) != cudaSuccess)
     return W2D_ERR_CUDA;
+  if (res[1] != 0.0) return W2D_ERR_TOPOLOGY;   // a level outside 1..nlevs
+  *dt = res[0];
   return W2D_OK;
 }
