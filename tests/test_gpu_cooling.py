@@ -3,8 +3,10 @@
 coolingh (src/coolingh.f90) and coolingdmc (src/coolingdmc.f90) use exp,
 pow, log and log10; CUDA's versions differ from glibc's by a few ulp, so
 these runs are held to a relative L1 tolerance per conserved field of
-1e-10 (the plain adiabatic path is exact).  The FP32 path is held to the
-target of its design: density L1 <= 1e-3 against the FP64 oracle.
+1e-12, the relative L1 the task asks of the FP64 path (measured: up to
+3e-13 on these runs; the plain adiabatic path is exact).  The FP32 path is
+held to the target of its design: density L1 <= 1e-3 against the FP64
+oracle.
 """
 import os
 
@@ -12,11 +14,12 @@ import numpy as np
 import pytest
 
 from helpers import compare_blocks, noncorner_mask
+from parity_log import record
 from walicxe2d_b200.params import COOLINGDMC, COOLINGH, config, scalings, sedov
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-COOL_RTOL = 1e-10
+COOL_RTOL = 1e-12
 
 
 def _dmc_table():
@@ -43,9 +46,10 @@ def _pair(p, ic, oracle_lib, table=False):
     return o, s
 
 
-def _compare(o, s, rtol):
+def _compare(o, s, rtol, test=""):
     ids = o.leaves()
     dmax, l1, n = compare_blocks(s.ctx.get_blocks(ids), o.u[ids], noncorner_mask())
+    record(test, s.status()["steps"], l1, dmax, n)
     assert np.all(l1 <= rtol), (l1, dmax, n)
     return l1
 
@@ -61,7 +65,7 @@ def test_coolingh_snr_blast(oracle_lib):
         dto = o.run(1, amr=False)
         s.run(1)
         assert abs(s.status()["dt"] - dto) <= 1e-12 * dto
-    l1 = _compare(o, s, COOL_RTOL)
+    l1 = _compare(o, s, COOL_RTOL, "coolingh_snr_blast")
     # the cooling did act: the neutral density differs from pure advection
     assert np.isfinite(l1).all()
 
@@ -77,7 +81,7 @@ def test_coolingdmc_blast(oracle_lib):
         dto = o.run(1, amr=False)
         s.run(1)
         assert abs(s.status()["dt"] - dto) <= 1e-12 * dto
-    _compare(o, s, COOL_RTOL)
+    _compare(o, s, COOL_RTOL, "coolingdmc_blast")
     ids = o.leaves()
     pg = s.ctx.get_primit(ids)
     m = np.zeros((20, 20), bool)
