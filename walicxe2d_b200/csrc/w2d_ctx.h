@@ -40,6 +40,10 @@ struct W2dCtx {
   // the leaf list was last built on the device (ctx_topology_device): the
   // host copies leaf/leaves/pos_of are stale until the next w2d_set_topology
   bool host_leaves_stale = false;
+  // w2d_refine / w2d_coarse changed the device's leaf flags (and nbmax,
+  // nleaf) since the leaf list was last built: the list is rebuilt on the
+  // device before its next use (ensure_leaf_list)
+  bool leaves_dirty = false;
   int* h_leaflist = nullptr; // pinned staging of d_leaves (guarded by ev_topo)
   int2* d_fd1 = nullptr;   // boundaryI (layer 0 of u)
   int2* d_fd2 = nullptr;   // boundaryII (two layers of up)

@@ -23,9 +23,14 @@ int ctx_tstep_rest(W2dCtx* c, double time, double dt);  // full step, boundaryI,
 // The refines (rq, nr quads) and coarsenings (cq, nc quads) of one admesh
 // pass in one launch; equal to w2d_refine(rq) followed by w2d_coarse(cq).
 int ctx_amr(W2dCtx* c, const int32_t* rq, int nr, const int32_t* cq, int nc);
+// FP64 conserved totals of the interiors of the blocks in slots[0..n-1]
+int ctx_totals(W2dCtx* c, const int32_t* slots, int n, double* tot);
 // the leaf list rebuilt on the device after tree changes made only through
 // ctx_amr since the last w2d_set_topology (nbmax and the leaf count given)
 int ctx_topology_device(W2dCtx* c, int nbmax, int nleaf);
+// the same, when w2d_refine / w2d_coarse changed the leaves since the list
+// was last built (no-op otherwise)
+int ensure_leaf_list(W2dCtx* c);
 
 // ---- ensembles: runs share one context; run r owns slots base[r]+1 ..
 // base[r]+cap[r] and numbers its blocks 1..cap[r] as a single run does.
