@@ -143,6 +143,15 @@ int w2d_get_u_fortran(W2dCtx* ctx, double* u, int ld, int nbmin,
                       const int32_t* ids, int n);
 /* primit (block-major, like w2d_get_blocks) as the reference holds it. */
 int w2d_get_primit(W2dCtx* ctx, const int32_t* ids, int n, double* prim);
+/* Conserved totals (no counterpart in the reference, which writes no
+ * totals): tot[q] = sum over the interior cells of every leaf of u(q) dV
+ * for q = 1..neq (mass, the two momenta, energy, passives), dV = dx dy of
+ * the cell's level, times the radius in cylindrical geometry (volume per
+ * radian).  Per-block partials are formed on the device in FP64, in a
+ * fixed order, and summed on the host in leaf order, so the totals are
+ * FP64 whatever the precision of the state (the FP32 path keeps them in
+ * FP64) and repeat exactly for the same state. */
+int w2d_totals(W2dCtx* ctx, double* tot);
 
 /* ---- the per-step block update (src/main.f90:87-98) --------------------- */
 /* timestep(dt), src/timestep.f90:7-61: CFL minimum over interior leaf cells
@@ -239,11 +248,19 @@ int w2d_flush_l2(W2dCtx* ctx);
  * COOLINGDMC.  Nothing is allocated: the per-block partials live in a
  * file-scope device array of W2D_NOALLOC_MAX_BLOCKS doubles that every GPU
  * loading the library keeps until exit; nblocks above that is rejected with
- * W2D_ERR_CAPACITY.  The first call on a device looks up that array's device
- * address (cudaGetSymbolAddress) with the device current; make that first
- * call before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race.  Work is queued on the legacy default stream and
- * the call returns once dt has been copied back. */
+ * W2D_ERR_CAPACITY.  Every call looks up that array's device address
+ * (cudaGetSymbolAddress, which allocates nothing) in the caller's current
+ * device and context, so a host that resets its device or has its context
+ * rebuilt by an offload runtime still gets a valid address; the first call
+ * in a context may load the library's device code, so make it before any
+ * stream capture.  A block whose level lies outside 1..nlevs makes the call
+ * return W2D_ERR_TOPOLOGY (dt untouched).  Cells whose values give NaN are
+ * ignored, as w2d_timestep ignores them.  All calls share the array: calls
+ * that overlap on the GPU race.  Work is queued on the legacy default
+ * stream, which waits for the other blocking streams of the device but not
+ * for streams created non-blocking: a host that wrote u or lev on such a
+ * stream (an OpenACC async queue, for one) synchronises it first.  The call
+ * returns once dt has been copied back. */
 #define W2D_NOALLOC_MAX_BLOCKS 65536
 #define W2D_MAXLEV_NOALLOC 16
 int w2d_timestep_noalloc(const W2dParams* p, const double* u, const int32_t* lev, int nblocks,
@@ -360,6 +377,8 @@ W2dCtx* w2d_ens_ctx(W2dEns* ens);
 int w2d_ens_run_slots(W2dEns* ens, int run, int32_t* base, int32_t* cap);
 /* leaf block IDs of a run (ascending, run numbering); ids may be NULL */
 int w2d_ens_leaves(W2dEns* ens, int run, int32_t* ids, int32_t* n);
+/* w2d_totals of run `run` */
+int w2d_ens_totals(W2dEns* ens, int run, double* tot);
 int w2d_ens_set_amr(W2dEns* ens, int on);
 /* Host wall-clock ms per phase of w2d_ens_run: [0] leaf lists, [1] dt and
  * half-step launches with locatebounds + fill plans of the changed runs,
@@ -420,15 +439,19 @@ int w2d_nn_params(W2dNN* nn, float* params, int set);   /* get (0) / set (1) */
 int w2d_nn_grad(W2dNN* nn, const float* feat, const float* targ, int n, float* grad, float* loss);
 int w2d_nn_forward(W2dNN* nn, const float* feat, int n, float* out);   /* out [2][n] */
 /* The exact routine judges the surrogate on n fresh samples: [0] share
- * the surrogate serves (inputs in range, predicted |dT/T| <= 10%), [1]
- * median, [2] 99th percentile and [3] maximum relative error of T and [4]
- * mean and [5] maximum error of the neutral fraction over those, [6] share
- * whose exact |dT/T| <= 10%.  stats holds 8 doubles.  coolingh networks
- * only: W2D_ERR_STATE for a coolingdmc network. */
-int w2d_nn_judge(W2dNN* nn, int64_t n, uint64_t seed, double* stats);
+ * the surrogate serves at the serve tolerance tol (in (0, 0.1]: inputs in
+ * range, predicted relative changes of T and of the thermal pressure and
+ * predicted change of the neutral fraction within tol, the test of the
+ * cooling kernel), [1] median, [2] 99th percentile and [3] maximum
+ * relative error of T and [4] mean and [5] maximum error of the neutral
+ * fraction over those, [6] share whose exact |dT/T| <= 10%.  stats holds 8
+ * doubles.  coolingh networks only: W2D_ERR_STATE for a coolingdmc
+ * network. */
+int w2d_nn_judge(W2dNN* nn, int64_t n, uint64_t seed, double tol, double* stats);
 /* coolingh of an FP32 context (or ensemble context) through the network:
  * cells whose inputs lie outside the training ranges or whose predicted
- * relative change exceeds the serve tolerance (below) take the exact
+ * relative change of T or of the thermal pressure, or predicted change of
+ * the neutral fraction, exceeds the serve tolerance (below) take the exact
  * routine.  The network must outlive its
  * use by the context; nn = NULL detaches it. */
 int w2d_set_surrogate(W2dCtx* ctx, W2dNN* nn);

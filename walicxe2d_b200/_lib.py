@@ -34,6 +34,8 @@ SIGNATURES = {
     "w2d_put_u_fortran": (_I, [_vp, _PD, _I, _I, _PI32, _I]),
     "w2d_get_u_fortran": (_I, [_vp, _PD, _I, _I, _PI32, _I]),
     "w2d_get_primit": (_I, [_vp, _PI32, _I, _PD]),
+    "w2d_totals": (_I, [_vp, _PD]),
+    "w2d_ens_totals": (_I, [_vp, _I, _PD]),
     "w2d_timestep": (_I, [_vp, _PD]),
     "w2d_tstep": (_I, [_vp, _D, _D]),
     "w2d_criteria": (_I, [_vp, _PD]),
@@ -89,7 +91,7 @@ SIGNATURES = {
     "w2d_nn_grad": (_I, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float), _I, C.POINTER(C.c_float),
                          C.POINTER(C.c_float)]),
     "w2d_nn_forward": (_I, [_vp, C.POINTER(C.c_float), _I, C.POINTER(C.c_float)]),
-    "w2d_nn_judge": (_I, [_vp, C.c_int64, C.c_uint64, _PD]),
+    "w2d_nn_judge": (_I, [_vp, C.c_int64, C.c_uint64, _D, _PD]),
     "w2d_autotune": (_I, [_vp, _I]),
     "w2d_tuning": (_I, [_vp, _PI32, _PD, C.POINTER(_I)]),
     "w2d_set_graphs": (_I, [_vp, _I]),

@@ -119,6 +119,13 @@ class Context:
         self._check(self.L.w2d_get_primit(self.h, _pi32(ids), ids.size, _pd(u)), "w2d_get_primit")
         return u
 
+    def totals(self) -> np.ndarray:
+        """FP64 totals of u over the leaf interiors, per conserved field
+        (w2d_totals)."""
+        t = np.zeros(self.neq)
+        self._check(self.L.w2d_totals(self.h, _pd(t)), "w2d_totals")
+        return t
+
     # ---- the reference's routines -------------------------------------------
     def timestep(self) -> float:
         dt = C.c_double()
@@ -460,6 +467,14 @@ class Ensemble:
         base, _ = self.slots(run)
         return ids, self.ctx.get_blocks(ids + base)
 
+    def totals(self, run: int) -> np.ndarray:
+        """FP64 conserved totals of run `run` (w2d_ens_totals)."""
+        t = np.zeros(self.members[run][0].neq)
+        rc = self.L.w2d_ens_totals(self.h, run, _pd(t))
+        if rc:
+            self.ctx._check(rc, "w2d_ens_totals")
+        return t
+
     def phase_ms(self, reset: bool = False) -> dict:
         ms = np.zeros(len(self.PHASES))
         self.L.w2d_ens_phase_ms(self.h, _pd(ms), 1 if reset else 0)
@@ -541,8 +556,10 @@ class Surrogate:
                     "w2d_nn_forward")
         return out.T.copy()
 
-    def judge(self, n: int = 1 << 20, seed: int = 7) -> dict:
+    def judge(self, n: int = 1 << 20, seed: int = 7, tol: float = 0.002) -> dict:
+        """The exact routine rates the network on n fresh samples, at the
+        serve test of the cooling kernel with tolerance tol (w2d_nn_judge)."""
         st = np.zeros(8)
-        self._check(self.L.w2d_nn_judge(self.h, n, seed, _pd(st)), "w2d_nn_judge")
+        self._check(self.L.w2d_nn_judge(self.h, n, seed, tol, _pd(st)), "w2d_nn_judge")
         return {k: float(st[i]) for i, k in enumerate(self.JUDGE)}
 

@@ -505,6 +505,8 @@ int half_step(W2dCtx* c, double dt, const double* dt_dev)
 int ctx_dt_launch(W2dCtx* c)
 {
   if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
+  int rc0 = ensure_leaf_list(c);
+  if (rc0) return rc0;
   const int nl = c->nleaf;
   const bool dev = c->want_graphs && c->p.otherb == W2D_USERBC_NONE;   // count on the device, fixed grid
   int rc = launch(c, "timestep", [&] {
@@ -548,13 +550,17 @@ int ctx_tstep_rest(W2dCtx* c, double time, double dt)
   set_jet_state(c, a2, time);   // both fills impose the jet at tstep's time
   set_jet_state(c, a1, time);
   const bool jet = a1.jet != 0;
+  // adiabatic runs without the jet: the full step computes the block
+  // statistics of its new interior, fill I those of the filled faces; with
+  // the jet its interior writes and the statistics follow in a second pass,
+  // after every fill read of the interiors; with cooling, after cooling
+  const int stats = c->p.cooling == W2D_ADIABATIC && !jet;
   KArgs af = a2;
+  af.split_stats = stats;
   apply_shape(c, af, TK_FULL);
   if ((rc = launch_tk(c, TK_FULL, "full_step", [&] { return c->L->full(c->neq, af, pa, dt, c->st); }))) return rc;
-  // boundaryI; with the jet its interior writes and the statistics follow in
-  // a second pass, after every fill read of the interiors
-  const int stats = c->p.cooling == W2D_ADIABATIC && !jet;
   KArgs ai = a1;
+  ai.split_stats = stats;
   apply_shape(c, ai, TK_FILL1);
   if ((rc = launch_tk(c, TK_FILL1, "fill_I", [&] { return c->L->fill1(c->neq, ai, pa, stats, c->st); }))) return rc;
   if (jet && c->p.cooling == W2D_ADIABATIC) {
@@ -804,6 +810,7 @@ int w2d_set_topology(W2dCtx* c, const int32_t* lp, int ld_lp, const int32_t* lea
   c->have_topology = true;
   c->have_bounds = false;
   c->host_leaves_stale = false;
+  c->leaves_dirty = false;
   return W2D_OK;
 }
 
@@ -835,8 +842,20 @@ int ctx_topology_device(W2dCtx* c, int nbmax, int nleaf)
   if (rc) return rc;
   if (nbmax > 0) c->nlaunch += 2;   // three kernels, launch() counted one
   c->host_leaves_stale = true;
+  c->leaves_dirty = false;
   c->have_bounds = false;
   return W2D_OK;
+}
+
+// A host that calls w2d_refine / w2d_coarse in admesh and then, as the
+// reference's main loop does (src/main.f90:87-98), timestep before tstep's
+// locatebounds, has changed the leaves without a new w2d_set_topology: the
+// device's leaf flags are current (k_amr keeps them), its leaf list is not.
+// Every entry point that walks the leaves rebuilds the list from the flags
+// here first.
+int ensure_leaf_list(W2dCtx* c)
+{
+  return c->leaves_dirty ? ctx_topology_device(c, c->nbmax, c->nleaf) : W2D_OK;
 }
 
 extern "C" {
@@ -847,6 +866,8 @@ extern "C" {
 int w2d_set_bounds(W2dCtx* c, const int32_t* ib, int ld, int n)
 {
   if (!c || (!ib && n > 0) || n < 0 || ld < n) return W2D_ERR_ARG;
+  int rc0 = ensure_leaf_list(c);   // (then stale on the host: the error below)
+  if (rc0) return rc0;
   if (!c->have_topology || c->host_leaves_stale)
     return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
   // alternate pinned buffers; wait only for the upload that last used this one
@@ -956,6 +977,41 @@ int w2d_get_blocks(W2dCtx* c, const int32_t* ids, int n, double* u)
   return get_pool(c, c->d_u, ids, n, u);
 }
 
+// Conserved totals of the interiors of n blocks (device list d_ids): the
+// per-block FP64 partials of k_totals, summed here in list order.
+static int totals_of(W2dCtx* c, const int* d_ids, int n, double* tot)
+{
+  for (int q = 0; q < c->neq; ++q) tot[q] = 0.0;
+  if (n == 0) return W2D_OK;
+  int rc = ensure_stage(c, (size_t)n * c->neq * sizeof(double));
+  if (rc) return rc;
+  KArgs a = kargs(c, c->d_fd1);
+  const int cyl = c->p.geometry == W2D_GEOM_CYLINDRICAL;
+  double* part_d = static_cast<double*>(c->d_stage);
+  const int chunk = (int)std::max<size_t>(1, c->stage_bytes / (c->neq * sizeof(double)));
+  std::vector<double> part((size_t)std::min(n, chunk) * c->neq);
+  for (int k0 = 0; k0 < n; k0 += chunk) {   // (the staging is bounded)
+    const int m = std::min(chunk, n - k0);
+    if ((rc = launch(c, "totals", [&] { return c->L->totals(c->neq, a, cyl, d_ids + k0, m, part_d, c->st); })))
+      return rc;
+    CK(cudaMemcpyAsync(part.data(), part_d, sizeof(double) * (size_t)m * c->neq, cudaMemcpyDeviceToHost, c->st));
+    if ((rc = sync_and_check(c))) return rc;
+    for (int k = 0; k < m; ++k)
+      for (int q = 0; q < c->neq; ++q) tot[q] += part[(size_t)k * c->neq + q];
+  }
+  return W2D_OK;
+}
+
+int w2d_totals(W2dCtx* c, double* tot)
+{
+  if (!c || !tot) return W2D_ERR_ARG;
+  if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
+  if (c->nruns > 0) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "one run per context (w2d_ens_totals)");
+  int rc = ensure_leaf_list(c);
+  if (rc) return rc;
+  return totals_of(c, c->d_leaves, c->nleaf, tot);
+}
+
 int w2d_get_primit(W2dCtx* c, const int32_t* ids, int n, double* prim)
 {
   if (!c || n < 0 || (n > 0 && (!ids || !prim))) return W2D_ERR_ARG;
@@ -1017,6 +1073,8 @@ int w2d_tstep(W2dCtx* c, double time, double dt)
 int w2d_criteria(W2dCtx* c, double* grad)
 {
   if (!c || !grad) return W2D_ERR_ARG;
+  int rc0 = ensure_leaf_list(c);
+  if (rc0) return rc0;
   // the leaf flags come from the device when the leaf list was built there
   const bool dev_leaf = c->host_leaves_stale;
   if (dev_leaf) CK(cudaEventSynchronize(c->ev_topo));   // h_leaflist is free
@@ -1124,6 +1182,8 @@ int w2d_admesh_flags(W2dCtx* c, int32_t* refine, int cap_refine, int* nrefine, i
   if (!c->have_topology || !c->have_links)
     return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology and w2d_set_links first");
   if (c->nruns > 0) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "one run per context");
+  int rc0 = ensure_leaf_list(c);
+  if (rc0) return rc0;
   const size_t slots = (size_t)c->cap + 1;
   const size_t plane = mark_plane(c);
   CK(cudaMemsetAsync(c->d_mflags, 0, 3 * plane, c->st));
@@ -1192,7 +1252,9 @@ int w2d_locate_bounds(W2dCtx* c)
   if (!c->have_topology || !c->have_links)
     return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology and w2d_set_links first");
   if (c->nruns > 0) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "one run per context");
-  int rc = ensure_plan(c);
+  int rc = ensure_leaf_list(c);
+  if (rc) return rc;
+  rc = ensure_plan(c);
   if (rc) return rc;
   const size_t slots = (size_t)c->cap + 1;
   const int nl = c->nleaf;
@@ -1293,8 +1355,29 @@ static int amr_pass(W2dCtx* c, const int32_t* rq, int nr, const int32_t* cq, int
   });
 }
 
-int w2d_refine(W2dCtx* c, const int32_t* quads, int n) { return amr_pass(c, quads, n, nullptr, 0); }
-int w2d_coarse(W2dCtx* c, const int32_t* quads, int n) { return amr_pass(c, nullptr, 0, quads, n); }
+// The public refine / coarse of a host's admesh: after the data motion the
+// leaves have changed (a refine makes one leaf four, a coarsening four
+// leaves one, sons may lie above nbmax) and the fill plans are stale.  The
+// leaf list is rebuilt on the device at its next use (ensure_leaf_list), so
+// that w2d_timestep may follow directly, as timestep follows admesh in the
+// reference's main loop; the plans come with the next w2d_set_bounds or
+// w2d_locate_bounds, as locatebounds starts tstep.
+static int amr_public(W2dCtx* c, const int32_t* rq, int nr, const int32_t* cq, int nc)
+{
+  int rc = amr_pass(c, rq, nr, cq, nc);
+  if (rc || nr + nc == 0 || c->nruns > 0) return rc;
+  int mx = c->nbmax;
+  for (int q = 0; q < nr; ++q)
+    for (int s = 1; s <= 4; ++s) mx = std::max(mx, (int)rq[5 * q + s]);
+  c->nbmax = mx;
+  c->nleaf += 3 * (nr - nc);
+  c->leaves_dirty = true;
+  c->have_bounds = false;
+  return W2D_OK;
+}
+
+int w2d_refine(W2dCtx* c, const int32_t* quads, int n) { return amr_public(c, quads, n, nullptr, 0); }
+int w2d_coarse(W2dCtx* c, const int32_t* quads, int n) { return amr_public(c, nullptr, 0, quads, n); }
 
 int w2d_boundaryI(W2dCtx* c, double time)
 {
@@ -1418,6 +1501,16 @@ int w2d_flush_l2(W2dCtx* c)
 }  // extern "C"
 
 int ctx_amr(W2dCtx* c, const int32_t* rq, int nr, const int32_t* cq, int nc) { return amr_pass(c, rq, nr, cq, nc); }
+
+int ctx_totals(W2dCtx* c, const int32_t* slots, int n, double* tot)
+{
+  if (n < 0 || (n > 0 && !slots) || !tot) return W2D_ERR_ARG;
+  int rc = valid_ids(c, slots, n);
+  if (rc) return rc;
+  if ((rc = ensure_ids(c, n))) return rc;
+  if (n > 0) CK(cudaMemcpyAsync(c->d_ids, slots, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, c->st));
+  return totals_of(c, c->d_ids, n, tot);
+}
 
 // ---------------------------------------------------------------------------
 // ensembles (w2d_internal.h)

@@ -181,6 +181,43 @@ __global__ void __launch_bounds__(W2D_THREADS, 2) k_cool(KArgs a, PhysArgs pa, d
 
 // primitives of whole blocks into a staging buffer (w2d_get_primit when
 // the pool does not store them)
+// Conserved totals in FP64 (the FP32 path keeps its state in FP32, its
+// totals in FP64): CTA k sums u_q dV over the 256 interior cells of block
+// ids[k] into out[k*NEQ + q], dV = dx dy of the block's level, times the
+// cell's radius r = (j + icoord(nb,2) - 0.5) dy in cylindrical geometry
+// (volume per radian).  The sum runs in a fixed order (warp trees, then the
+// warps in order), so the partials do not depend on scheduling.
+template <typename R, int NEQ>
+__global__ void __launch_bounds__(256) k_totals(KArgs a, int cyl, const int* __restrict__ ids,
+                                                double* __restrict__ out)
+{
+  __shared__ double red[8][NEQ];
+  const int b = ids[blockIdx.x];
+  const int t = threadIdx.x, i = 1 + t % 16, j = 1 + t / 16;
+  const int lev = a.lev[b];
+  const double dy = geo_dy(a, b, lev);
+  double dv = geo_dx(a, b, lev) * dy;
+  if (cyl) dv = dv * (((double)(j + a.icoord[2 * b + 1]) - 0.5) * dy);
+  const R* ub = (const R*)a.u + (size_t)b * NEQ * W2D_CELLS;
+  double v[NEQ];
+#pragma unroll
+  for (int q = 0; q < NEQ; ++q) {
+    v[q] = (double)ub[q * W2D_CELLS + cidx(i, j)] * dv;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+  }
+  if ((t & 31) == 0) {
+#pragma unroll
+    for (int q = 0; q < NEQ; ++q) red[t >> 5][q] = v[q];
+  }
+  __syncthreads();
+  if (t < NEQ) {
+    double s = 0.;
+    for (int w = 0; w < 8; ++w) s += red[w][t];
+    out[(size_t)blockIdx.x * NEQ + t] = s;
+  }
+}
+
 template <typename R, int NEQ>
 __global__ void k_to_prim(PhysArgs pa, const R* __restrict__ u, double* __restrict__ out,
                           const int* __restrict__ ids)

@@ -407,6 +407,16 @@ int w2d_ens_leaves(W2dEns* e, int run, int32_t* ids, int32_t* n)
   return W2D_OK;
 }
 
+int w2d_ens_totals(W2dEns* e, int run, double* tot)
+{
+  if (!e || !tot || run < 0 || run >= (int)e->runs.size()) return W2D_ERR_ARG;
+  const W2dSim& s = e->runs[run];
+  std::vector<int32_t> slots;
+  for (int nb = 1; nb <= s.nbmax; ++nb)
+    if (s.leaf[(size_t)nb - 1]) slots.push_back(e->base[run] + nb);
+  return ctx_totals(e->ctx, slots.data(), (int)slots.size(), tot);
+}
+
 int w2d_ens_set_amr(W2dEns* e, int on)
 {
   if (!e) return W2D_ERR_ARG;

@@ -83,6 +83,11 @@ struct KArgs {
   // (a launch captured in a CUDA graph reads the current count from it).
   int grid, sched;
   const int* nleaf_dev;
+  // block statistics split between the full step and fill I (adiabatic
+  // runs without the jet): the full step writes the CFL partial and the
+  // criteria maximum over interior neighbour pairs, fill I folds in the
+  // pairs with a ghost cell
+  int split_stats;
 };
 
 struct LeafRange {
@@ -539,6 +544,75 @@ __device__ __forceinline__ void block_stats(const R (*sp)[W2D_W][W2D_W], const P
   }
 }
 
+// The block statistics of block_stats computed from the new interior of a
+// full step, before fill I: each of threads 0..255 has written its cell's
+// new u into the interior of st.  The CFL partial is complete (timestep reads interior cells only,
+// src/timestep.f90:21-47).  The criteria maximum (src/criteria.f90:16-50)
+// covers the neighbour pairs inside the interior here; fill I folds in the
+// pairs of edge cells with their layer-0 ghosts (fill_face_stats).  The
+// two parts combine exactly: for am > 0, max(RN(x/am), RN(y/am)) =
+// RN(max(x, y)/am).  st (its interior) and sred are overwritten.
+template <typename R, int NEQ>
+__device__ __forceinline__ void interior_stats(R (*st)[W2D_W][W2D_W], double* sred, const Phys<R>& ph,
+                                               const KArgs& a, int b, int lev)
+{
+  const int tid = threadIdx.x;
+  const int i = 1 + tid % 16, j = 1 + tid / 16;
+  const int ti = i + 1, tj = j + 1;
+  double au = 0., av = 0., grad = 0.;
+  R rho = R(0.), p = R(0.);
+  if (tid < 256) {
+    R q[NEQ], nv[NEQ], T;
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) nv[k] = st[k][tj][ti];
+    uprim<NEQ>(ph, q, nv, T);
+    const R cs = sound(ph, q[3], q[0]);
+    au = (double)(absr(q[1]) + cs);
+    av = (double)(absr(q[2]) + cs);
+    rho = q[0];
+    p = q[3];
+    // (this cell's entries of st are read by no other thread before the
+    // barrier below)
+    st[0][tj][ti] = rho;
+    st[3][tj][ti] = p;
+  }
+  __syncthreads();
+  if (tid < 256) {
+    const R fl = R(1e-15);
+    const R am = fmaxr(fl, absr(p)), am2 = fmaxr(fl, absr(rho));
+    R dp = R(0.), dr = R(0.);
+    if (i < W2D_NX) { dp = fmaxr(dp, absr(st[3][tj][ti + 1] - p)); dr = fmaxr(dr, absr(st[0][tj][ti + 1] - rho)); }
+    if (i > 1) { dp = fmaxr(dp, absr(st[3][tj][ti - 1] - p)); dr = fmaxr(dr, absr(st[0][tj][ti - 1] - rho)); }
+    if (j < W2D_NX) { dp = fmaxr(dp, absr(st[3][tj + 1][ti] - p)); dr = fmaxr(dr, absr(st[0][tj + 1][ti] - rho)); }
+    if (j > 1) { dp = fmaxr(dp, absr(st[3][tj - 1][ti] - p)); dr = fmaxr(dr, absr(st[0][tj - 1][ti] - rho)); }
+    grad = (double)fmaxr(dp / am, dr / am2);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    au = fmax(au, __shfl_xor_sync(0xffffffffu, au, o));
+    av = fmax(av, __shfl_xor_sync(0xffffffffu, av, o));
+    grad = fmax(grad, __shfl_xor_sync(0xffffffffu, grad, o));
+  }
+  if ((tid & 31) == 0) {
+    sred[tid >> 5] = au;
+    sred[16 + (tid >> 5)] = av;
+    sred[32 + (tid >> 5)] = grad;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double m0 = sred[0], m1 = sred[16], m2 = sred[32];
+    for (int w = 1; w < W2D_THREADS / 32; ++w) {
+      m0 = fmax(m0, sred[w]);
+      m1 = fmax(m1, sred[16 + w]);
+      m2 = fmax(m2, sred[32 + w]);
+    }
+    const R t1 = R(geo_dx(a, b, lev)) / R(m0);
+    const R t2 = R(geo_dy(a, b, lev)) / R(m1);
+    a.cfl[b] = (double)fminr(t1, t2);
+    a.grad[b] = m2;
+  }
+}
+
 // Geometric source terms of cylindrical coordinates (x -> z, y -> r) for
 // cell (ti, tj) of a primitive tile, src/step.f90:46-73 (prims): with
 // r = (j + icoord(nb,2) - 0.5) dy(lev) and H = rho (vz^2 + vr^2)/2 +
@@ -790,8 +864,15 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_full(KArgs a, P
       if (visc)
         v = v + eta * (so[k][tj][ti + 1] + so[k][tj][ti - 1] + so[k][tj + 1][ti] + so[k][tj - 1][ti] - R(4.) * uo);
       u[k * W2D_CELLS + cidx(i, j)] = v;
+      // the new u of this cell, for the statistics below (the flux phase
+      // that read the other cells' primitives in st passed its barrier;
+      // this cell's entries were last read for its own source terms)
+      if (a.split_stats) st[k][tj][ti] = v;
     }
   }
+  // the statistics of the new interior (timestep's partial, most of
+  // criteria); sf is free once every thread has passed the next barrier
+  if (a.split_stats) interior_stats<R, NEQ>(st, reinterpret_cast<double*>(&sf[0][0][0]), ph, a, b, lev);
   leaf_end();
   }
 }
@@ -861,13 +942,15 @@ __global__ void __launch_bounds__(W2D_THREADS, 4) k_fill1(KArgs a, PhysArgs pa, 
   }
 }
 
-// Fill of layer 0 without the statistics (cooling runs and the jet, whose
-// statistics follow in a later pass): 64 threads per leaf, four leaves per
-// 256-thread CTA.  Persistent (P): the CTA walks its leaves as leaf_range
-// gives them, four at a time (li, li + step, li + 2 step, li + 3 step);
-// otherwise CTA k takes leaves 4k .. 4k + 3.
+// Fill of layer 0 without the block statistics (cooling runs and the jet,
+// whose statistics follow in a later pass), or with the criteria terms of
+// the filled faces (a.split_stats: the full step computed the rest):
+// 64 threads per leaf, four leaves per 256-thread CTA.  Persistent (P):
+// the CTA walks its leaves as leaf_range gives them, four at a time (li,
+// li + step, li + 2 step, li + 3 step); otherwise CTA k takes leaves
+// 4k .. 4k + 3.  A warp serves two faces of one leaf.
 template <typename R, int NEQ, bool P>
-__global__ void __launch_bounds__(256) k_fill1g(KArgs a)
+__global__ void __launch_bounds__(256) k_fill1g(KArgs a, PhysArgs pa)
 {
   const int tid = threadIdx.x, g = tid >> 6, t = tid & 63;
   const int f = t / 16, m = 1 + t % 16;
@@ -882,20 +965,45 @@ __global__ void __launch_bounds__(256) k_fill1g(KArgs a)
   }
   int gi, gj;
   ghost_ij(f, 0, m, gi, gj);
+  // the edge cell next to this ghost
+  const int ci = gi < 1 ? 1 : (gi > W2D_NX ? W2D_NX : gi);
+  const int cj = gj < 1 ? 1 : (gj > W2D_NX ? W2D_NX : gj);
   for (; lr.li < lr.end; lr.li += 4 * lr.step) {
     const int li = lr.li + g * lr.step;
-    if (li >= lr.end) continue;
+    if (li >= lr.end) continue;     // (the whole warp: one leaf per warp)
     const int b = a.leaves[li];
     const int2 d = a.fd[li * 4 + f];
     R gv[NEQ];
     bool w = false;
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) w = ghost_value<R>(upool, bs, a, b, d, f, 0, m, k, gv[k]);
+    R* __restrict__ u = upool + (size_t)b * bs;
     if (w) {
-      R* __restrict__ u = upool + (size_t)b * bs;
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) u[k * W2D_CELLS + cidx(gi, gj)] = gv[k];
     }
+    if (!a.split_stats) continue;
+    // src/criteria.f90:16-50 for the pair (edge cell, its ghost), from the
+    // primitives of both as calcprim gives them; a face no entry writes
+    // keeps the ghost value it has
+    const Phys<R> ph = make_phys<R, -1, -1>(pa);
+    R uc[NEQ], qc[NEQ], qg[NEQ], T;
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) {
+      if (!w) gv[k] = u[k * W2D_CELLS + cidx(gi, gj)];
+      uc[k] = u[k * W2D_CELLS + cidx(ci, cj)];
+    }
+    uprim<NEQ>(ph, qg, gv, T);
+    uprim<NEQ>(ph, qc, uc, T);
+    const R fl = R(1e-15);
+    const R am = fmaxr(fl, absr(qc[3])), am2 = fmaxr(fl, absr(qc[0]));
+    double gr = (double)fmaxr(absr(qg[3] - qc[3]) / am, absr(qg[0] - qc[0]) / am2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) gr = fmax(gr, __shfl_xor_sync(0xffffffffu, gr, o));
+    // the full step wrote the interior maximum; both are >= 0, so their
+    // bit patterns order as the values
+    if ((tid & 31) == 0)
+      atomicMax(reinterpret_cast<unsigned long long*>(a.grad + b), (unsigned long long)__double_as_longlong(gr));
   }
 }
 

@@ -104,11 +104,11 @@ static cudaError_t fill1_p(const KArgs& a, const PhysArgs& pa, int stats, cudaSt
 template <int NEQ>
 static cudaError_t fill1_t(const KArgs& a, const PhysArgs& pa, int stats, cudaStream_t st)
 {
-  if (!stats) {   // ghost faces only: four leaves per CTA
+  if (!stats || a.split_stats) {   // ghost faces (and their criteria terms): four leaves per CTA
     if (a.grid > 0)
-      k_fill1g<R, NEQ, true><<<a.grid, 256, 0, st>>>(a);
+      k_fill1g<R, NEQ, true><<<a.grid, 256, 0, st>>>(a, pa);
     else
-      k_fill1g<R, NEQ, false><<<(a.nleaf + 3) / 4, 256, 0, st>>>(a);
+      k_fill1g<R, NEQ, false><<<(a.nleaf + 3) / 4, 256, 0, st>>>(a, pa);
     return cudaGetLastError();
   }
   return a.grid > 0 ? fill1_p<NEQ, true>(a, pa, stats, st) : fill1_p<NEQ, false>(a, pa, stats, st);
@@ -228,8 +228,15 @@ static cudaError_t to_prim(int neq, const PhysArgs& pa, const void* u, void* out
   return cudaGetLastError();
 }
 
-static const Launchers table = {half, full,    fill1,  fill_only, calcprim, jet_only,
-                                amr,  cool,    scatter, gather,   to_prim,  sizeof(R)};
+static cudaError_t totals(int neq, const KArgs& a, int cyl, const int* ids, int n, double* out, cudaStream_t st)
+{
+  if (n == 0) return cudaSuccess;
+  W2D_NEQ_SWITCH(neq, (k_totals<R, NEQ><<<n, 256, 0, st>>>(a, cyl, ids, out)));
+  return cudaGetLastError();
+}
+
+static const Launchers table = {half,    full,   fill1,   fill_only, calcprim, jet_only, amr,
+                                cool,    scatter, gather, to_prim,   totals,   sizeof(R)};
 
 }  // namespace W2D_INST_NS
 }  // namespace w2d

@@ -24,6 +24,8 @@ struct Launchers {
   cudaError_t (*scatter)(void* pool, const void* stage, const int* ids, int n, size_t bs, cudaStream_t);
   cudaError_t (*gather)(const void* pool, void* stage, const int* ids, int n, size_t bs, cudaStream_t);
   cudaError_t (*to_prim)(int neq, const PhysArgs&, const void* u, void* out, const int* ids, int n, cudaStream_t);
+  // FP64 conserved totals of the interiors of blocks ids[0..n-1]: out[k*neq+q]
+  cudaError_t (*totals)(int neq, const KArgs&, int cyl, const int* ids, int n, double* out, cudaStream_t);
   size_t elem;  // sizeof(R)
 };
 

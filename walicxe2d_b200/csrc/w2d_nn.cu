@@ -492,9 +492,11 @@ __global__ void __launch_bounds__(128, 1) k_nn_forward(const float* __restrict__
 
 // The exact routine judges the surrogate on fresh samples: per sample the
 // relative error of T, the absolute error of the neutral fraction, whether
-// the surrogate would be used (in range, |dT/T| <= 10%).
+// the surrogate would be used (the serve test of the cooling kernel at
+// tolerance tol: predicted changes of T, of the thermal pressure and of the
+// neutral fraction within tol).
 __global__ void k_nn_judge(int64_t n, uint64_t seed, const float* __restrict__ out, float* __restrict__ feat,
-                           int64_t ld, int pass, float* __restrict__ res)
+                           int64_t ld, int pass, double tol, float* __restrict__ res)
 {
   const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
@@ -508,7 +510,7 @@ __global__ void k_nn_judge(int64_t n, uint64_t seed, const float* __restrict__ o
   }
   double y1, ce, t1, y1p, t1p;
   d_atomic_core(T, y0, dn, dts, y1, ce, t1);
-  const bool use = nn_update(out[k], out[n + k], dn, T, y0, dts, y1p, t1p);
+  const bool use = nn_update(out[k], out[n + k], dn, T, y0, dts, y1p, t1p, tol);
   res[k] = use ? 1.f : 0.f;
   res[n + k] = (float)fabs(t1p / t1 - 1.);
   res[2 * n + k] = (float)fabs(y1p - y1);
@@ -1083,20 +1085,20 @@ int w2d_nn_forward(W2dNN* nn, const float* feat, int n, float* out)
   return rc;
 }
 
-int w2d_nn_judge(W2dNN* nn, int64_t n, uint64_t seed, double* stats)
+int w2d_nn_judge(W2dNN* nn, int64_t n, uint64_t seed, double tol, double* stats)
 {
-  if (!nn || !stats || n < 128) return W2D_ERR_ARG;
+  if (!nn || !stats || n < 128 || !(tol > 0.0 && tol <= 0.1)) return W2D_ERR_ARG;
   if (nn->kind != W2D_COOLINGH) return W2D_ERR_STATE;   // the judge runs coolingh's routine
   float *df = nullptr, *dout = nullptr, *dres = nullptr;
   NCK(cudaMalloc(&df, sizeof(float) * 4 * (size_t)n));
   NCK(cudaMalloc(&dout, sizeof(float) * 2 * (size_t)n));
   NCK(cudaMalloc(&dres, sizeof(float) * 4 * (size_t)n));
   const unsigned g = (unsigned)((n + 255) / 256);
-  k_nn_judge<<<g, 256, 0, nn->st>>>(n, seed, dout, df, n, 0, dres);
+  k_nn_judge<<<g, 256, 0, nn->st>>>(n, seed, dout, df, n, 0, tol, dres);
   int rc = cudaGetLastError() == cudaSuccess ? W2D_OK : W2D_ERR_CUDA;
   if (!rc) rc = nn_forward_launch(nn, df, n, n, dout);
   if (!rc) {
-    k_nn_judge<<<g, 256, 0, nn->st>>>(n, seed, dout, df, n, 1, dres);
+    k_nn_judge<<<g, 256, 0, nn->st>>>(n, seed, dout, df, n, 1, tol, dres);
     if (cudaGetLastError() != cudaSuccess) rc = W2D_ERR_CUDA;
   }
   std::vector<float> h(4 * (size_t)n);

@@ -99,10 +99,10 @@ __device__ __forceinline__ void nn_targets(double n, double y0, double dt_s, dou
 
 // The update from the outputs, with atomic's clamps (src/coolingh.f90:
 // 227-228, 250-253); returns false when the predicted relative change of T
-// or of the thermal pressure exceeds 10% (the cell then takes the exact
-// routine).
+// or of the thermal pressure, or the predicted change of the neutral
+// fraction, exceeds tol (the cell then takes the exact routine).
 __device__ __forceinline__ bool nn_update(float o0, float o1, double n, double T, double y0, double dt_s, double& y1,
-                                          double& t1)
+                                          double& t1, double tol)
 {
   y1 = y0 + n * dt_s * (double)NN_SY * sinh((double)NN_AY * (double)o0);
   y1 = y1 < 1. ? y1 : 1.;
@@ -113,7 +113,7 @@ __device__ __forceinline__ bool nn_update(float o0, float o1, double n, double T
   t1 = t1 < 10. * T ? t1 : 10. * T;
   t1 = t1 > 10. ? t1 : 10.;
   const double dp = ((2. - y1) * t1) / ((2. - y0) * T) - 1.;
-  return fabs(t1 / T - 1.) <= 0.1 && fabs(dp) <= 0.1;
+  return fabs(t1 / T - 1.) <= tol && fabs(dp) <= tol && fabs(y1 - y0) <= tol;
 }
 
 // nn_features / nn_in_range / nn_update in single precision for the
@@ -139,9 +139,10 @@ __device__ __forceinline__ bool nn_update_f(float o0, float o1, float n, float T
   t1 = t1 < 10.f * T ? t1 : 10.f * T;
   t1 = t1 > 10.f ? t1 : 10.f;
   // served when the predicted relative changes of T and of the thermal
-  // pressure (2 - y) T both stay within tol (at most 10%)
+  // pressure (2 - y) T and the predicted change of the neutral fraction
+  // all stay within tol (at most 10%)
   const float dp = ((2.f - y1) * t1) / ((2.f - y0) * T) - 1.f;
-  return fabsf(t1 / T - 1.f) <= tol && fabsf(dp) <= tol;
+  return fabsf(t1 / T - 1.f) <= tol && fabsf(dp) <= tol && fabsf(y1 - y0) <= tol;
 }
 
 // coolingdmc mode (src/coolingdmc.f90:30-40): above 1e4 K the pressure

@@ -137,10 +137,10 @@ __device__ __forceinline__ void hll_flux(const Phys<R>& ph, const R* ql, const R
 //   HLL-HLLC  src/hll_hllcfluxes.f90:98-210
 // csl/csr are the sound speeds of the two states (callers that reuse a
 // cell's sound speed pass it in; the value is the one sound() returns).
+// pl is overwritten (it holds the star side's state on return).
 // Returns false on the NaN contact speed that stops the reference.
 template <int NEQ, typename R>
-__device__ __forceinline__ bool riemann(const Phys<R>& ph, const R* pl, const R* pr, R csl, R csr,
-                                        R* ff)
+__device__ __forceinline__ bool riemann(const Phys<R>& ph, R* pl, const R* pr, R csl, R csr, R* ff)
 {
   R beta1 = R(1.), beta2 = R(0.);
   if (ph.solver == SOLVER_HLL_HLLC) {              // hll_hllcfluxes.f90:110-129
@@ -161,6 +161,9 @@ __device__ __forceinline__ bool riemann(const Phys<R>& ph, const R* pl, const R*
   if (sl > R(0)) { primf<NEQ>(ph, pl, ff); return true; }
   if (sr < R(0)) { primf<NEQ>(ph, pr, ff); return true; }
   if (ph.solver == SOLVER_HLL) { hll_flux<NEQ>(ph, pl, pr, sl, sr, ff); return true; }
+  // the HLL part of the hybrid, from the states before pl is overwritten
+  R fh[NEQ];
+  if (ph.solver == SOLVER_HLL_HLLC) hll_flux<NEQ>(ph, pl, pr, sl, sr, fh);
   R slmul = sl - pl[1];
   R srmur = sr - pr[1];
   R rholul = pl[0] * pl[1];
@@ -168,11 +171,14 @@ __device__ __forceinline__ bool riemann(const Phys<R>& ph, const R* pl, const R*
   R sst = (srmur * rhorur - slmul * rholul - pr[3] + pl[3]) / (srmur * pr[0] - slmul * pl[0]);
   bool left = sst >= R(0.);
   if (!left && !(sst <= R(0.))) return false;
-  if (left) hllc_star<NEQ>(ph, pl, sl, slmul, sst, pl[0], ff);
-  else      hllc_star<NEQ>(ph, pr, sr, srmur, sst, ph.hllc_compat ? pr[3] : pr[0], ff);
+  // the star state of the side the contact leaves behind: the side's inputs
+  // are selected into pl and one star computation follows, so that the
+  // threads of a warp on both sides of a contact do not run it twice
+  const R den = left ? pl[0] : (ph.hllc_compat ? pr[3] : pr[0]);
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k) pl[k] = left ? pl[k] : pr[k];
+  hllc_star<NEQ>(ph, pl, left ? sl : sr, left ? slmul : srmur, sst, den, ff);
   if (ph.solver == SOLVER_HLL_HLLC) {
-    R fh[NEQ];
-    hll_flux<NEQ>(ph, pl, pr, sl, sr, fh);
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) ff[k] = beta1 * (ff[k]) + beta2 * (fh[k]);
   }
