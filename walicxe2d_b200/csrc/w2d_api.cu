@@ -245,12 +245,14 @@ PhysArgs pargs(W2dCtx* c)
   return pa;
 }
 
+// Block-ID staging on the device: at least a pool's worth of IDs from the
+// first use (transfers of up to every block then never reallocate it)
 int ensure_ids(W2dCtx* c, int n)
 {
   if (n <= c->ids_cap) return W2D_OK;
   if (c->d_ids) cudaFree(c->d_ids);
   c->d_ids = nullptr;
-  int cap = std::max(n, 1024);
+  int cap = std::max({n, 1024, c->cap + 1});
   CK(cudaMalloc(&c->d_ids, sizeof(int) * (size_t)cap));
   c->ids_cap = cap;
   return W2D_OK;
@@ -263,17 +265,14 @@ int ensure_ids(W2dCtx* c, int n)
 // into it (at full speed when the caller's memory is pinned).
 constexpr size_t kStageBytes = (size_t)64 << 20;
 
+// Allocated at its bound on first use (a growing stage would be freed and
+// allocated again, with a device synchronisation, whenever a run's transfers
+// grow); `bytes` only says whether any staging is needed.
 int ensure_stage(W2dCtx* c, size_t bytes)
 {
-  bytes = std::min(bytes, kStageBytes);
-  if (bytes > c->stage_bytes) {
-    CK(cudaStreamSynchronize(c->st));
-    if (c->d_stage) cudaFree(c->d_stage);
-    c->d_stage = nullptr;
-    c->stage_bytes = 0;
-    CK(cudaMalloc(&c->d_stage, bytes));
-    c->stage_bytes = bytes;
-  }
+  if (bytes == 0 || c->d_stage) return W2D_OK;
+  CK(cudaMalloc(&c->d_stage, kStageBytes));
+  c->stage_bytes = kStageBytes;
   return W2D_OK;
 }
 
@@ -291,6 +290,8 @@ int check_device(W2dCtx* c)
                                                  : "device error");
     c->h_err[0] = 0;
     cudaMemsetAsync(c->d_err, 0, 4 * sizeof(int), c->st);
+    // a grid barrier that ran out left its words behind
+    if (c->d_gbar) cudaMemsetAsync(c->d_gbar, 0, 2 * sizeof(unsigned int), c->st);
     return rc;
   }
   return W2D_OK;
@@ -562,7 +563,7 @@ int ctx_tstep_rest(W2dCtx* c, double time, double dt)
   KArgs ai = a1;
   ai.split_stats = stats;
   apply_shape(c, ai, TK_FILL1);
-  if ((rc = launch_tk(c, TK_FILL1, "fill_I", [&] { return c->L->fill1(c->neq, ai, pa, stats, c->st); }))) return rc;
+  if ((rc = launch_tk(c, TK_FILL1, "fill_I", [&] { return c->L->fill1(c->neq, ai, pa, c->st); }))) return rc;
   if (jet && c->p.cooling == W2D_ADIABATIC) {
     const int nl = c->nleaf;
     if ((rc = launch(c, "jet_calcprim", [&] { return c->L->calcprim(c->neq, a1, pa, c->d_leaves, nl, 1, c->st); })))
@@ -631,6 +632,8 @@ int w2d_create(const W2dParams* p, W2dCtx** out)
   CKC(cudaMalloc(&c->d_leaves, sizeof(int) * slots));
   CKC(cudaMalloc(&c->d_leafflag, sizeof(int) * slots));
   CKC(cudaMemsetAsync(c->d_leafflag, 0, sizeof(int) * slots, c->st));
+  CKC(cudaMalloc(&c->d_gbar, 2 * sizeof(unsigned int)));
+  CKC(cudaMemsetAsync(c->d_gbar, 0, 2 * sizeof(unsigned int), c->st));
   CKC(cudaMalloc(&c->d_fb_count, sizeof(int)));
   CKC(cudaMalloc(&c->d_nleaf, sizeof(int)));
   CKC(cudaMemsetAsync(c->d_nleaf, 0, sizeof(int), c->st));
@@ -725,7 +728,7 @@ int w2d_destroy(W2dCtx* c)
   if (c->h_loff) cudaFreeHost(c->h_loff);
   void* dev[] = {c->d_u, c->d_up, c->d_prim, c->d_lev, c->d_icoord, c->d_cfl, c->d_dtcool, c->d_grad,
                  c->d_err, c->d_dt, c->d_cooltab, c->d_leaves, c->d_fd1, c->d_fd2, c->d_stage, c->d_ids,
-                 c->d_flush, c->d_dtwork, c->d_dtcount, c->d_jetblk, c->d_leafflag};
+                 c->d_flush, c->d_dtwork, c->d_dtcount, c->d_jetblk, c->d_leafflag, c->d_gbar, c->d_lrank};
   for (void* d : dev)
     if (d) cudaFree(d);
   void* host[] = {c->h_small, c->h_grad, c->h_err, c->h_fd1[0], c->h_fd2[0], c->h_leaflist,
@@ -819,6 +822,42 @@ int ensure_plan(W2dCtx* c);   // (defined with the other lazily allocated parts 
 // CTAs of 256 the plan build may use (one thread per leaf and side), so the
 // stride between the CTA totals and their offsets in d_bcta
 inline size_t bcta_half(const W2dCtx* c) { return (4 * ((size_t)c->cap + 1)) / 256 + 1; }
+
+// arguments of a tree build over the context's slots 1..nbmax
+TreeArgs tree_args(W2dCtx* c, bool plans)
+{
+  TreeArgs t{};
+  PlanArgs& a = t.p;
+  a.leaves = c->d_leaves;
+  a.nbmax = c->nbmax;
+  a.cap = c->cap;
+  a.lev = c->d_lev;
+  a.links = c->d_links;
+  a.sons = c->d_sons;
+  a.posof = c->d_posof;
+  a.entries = c->d_bent;
+  a.span = c->d_bspan;
+  a.local = c->d_blocal;
+  a.total = c->d_bcta + 2 * bcta_half(c);
+  a.fd1 = c->d_fd1;
+  a.fd2 = c->d_fd2;
+  a.wpos = c->d_wpos;
+  a.jetblk = c->d_jetblk;
+  a.bc[0] = c->p.bc_left;
+  a.bc[1] = c->p.bc_right;
+  a.bc[2] = c->p.bc_bottom;
+  a.bc[3] = c->p.bc_top;
+  a.f6b = (c->p.compat & W2D_COMPAT_OUTFYB) != 0;
+  a.jet = c->p.otherb == W2D_USERBC_JET;
+  t.flag = c->d_leafflag;
+  t.lrank = c->d_lrank;
+  t.tcnt = c->d_bcta;
+  t.nleaf_dev = c->d_nleaf;
+  t.plans = plans ? 1 : 0;
+  t.bar = c->d_gbar;
+  t.err = c->d_err;
+  return t;
+}
 }  // namespace
 
 }  // extern "C"
@@ -835,15 +874,30 @@ int ctx_topology_device(W2dCtx* c, int nbmax, int nleaf)
   if (rc) return rc;
   c->nbmax = nbmax;
   c->nleaf = nleaf;
-  rc = launch(c, "leaf_list", [&] {
-    return launch_leaf_list(c->d_leafflag, nbmax, c->d_blocal, c->d_bcta, c->d_bcta + bcta_half(c),
-                            c->d_leaves, c->d_nleaf, c->d_posof, c->st);
-  });
-  if (rc) return rc;
-  if (nbmax > 0) c->nlaunch += 2;   // three kernels, launch() counted one
+  TreeArgs t = tree_args(c, false);
+  if ((rc = launch(c, "leaf_list", [&] { return launch_tree_build(t, c->st); }))) return rc;
   c->host_leaves_stale = true;
   c->leaves_dirty = false;
   c->have_bounds = false;
+  return W2D_OK;
+}
+
+// The leaf list and the fill plans (locatebounds) of the tree of the leaf
+// flags and the lp(:,3:8) mirror, in one launch.
+int ctx_tree_device(W2dCtx* c, int nbmax, int nleaf)
+{
+  if (!c->have_topology || !c->have_links)
+    return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology and w2d_set_links first");
+  if (nbmax < 0 || nbmax > c->cap || nleaf < 0 || nleaf > nbmax) return W2D_ERR_ARG;
+  int rc = ensure_plan(c);
+  if (rc) return rc;
+  c->nbmax = nbmax;
+  c->nleaf = nleaf;
+  TreeArgs t = tree_args(c, true);
+  if ((rc = launch(c, "tree_build", [&] { return launch_tree_build(t, c->st); }))) return rc;
+  c->host_leaves_stale = true;
+  c->leaves_dirty = false;
+  c->have_bounds = true;
   return W2D_OK;
 }
 
@@ -1126,6 +1180,7 @@ int ensure_plan(W2dCtx* c)
   CK(cudaMalloc(&c->d_bent, sizeof(int2) * 4 * slots));
   CK(cudaMalloc(&c->d_bspan, sizeof(int2) * slots));
   CK(cudaMalloc(&c->d_blocal, sizeof(int) * 4 * slots));
+  CK(cudaMalloc(&c->d_lrank, sizeof(int) * slots));
   CK(cudaMalloc(&c->d_bcta, sizeof(int) * (2 * bcta_half(c) + 1)));
   CK(cudaMalloc(&c->d_wpos, sizeof(int) * slots));
   return W2D_OK;
@@ -1186,8 +1241,6 @@ int w2d_admesh_flags(W2dCtx* c, int32_t* refine, int cap_refine, int* nrefine, i
   if (rc0) return rc0;
   const size_t slots = (size_t)c->cap + 1;
   const size_t plane = mark_plane(c);
-  CK(cudaMemsetAsync(c->d_mflags, 0, 3 * plane, c->st));
-  CK(cudaMemsetAsync(c->d_mlists, 0, 4 * sizeof(int), c->st));
   MarkArgs a{};
   a.leaves = c->d_leaves;
   a.nleaf = c->nleaf;
@@ -1207,8 +1260,9 @@ int w2d_admesh_flags(W2dCtx* c, int32_t* refine, int cap_refine, int* nrefine, i
   a.rlist = c->d_mlists + 4;
   a.clist = c->d_mlists + 4 + slots;
   a.err = c->d_err;
-  int rc = launch(c, "markref_critneighup", [&] { return launch_markref_up(a, c->st); });
-  if (!rc) rc = launch(c, "critneighdown_coarsen", [&] { return launch_refine_coarsen(a, c->st); });
+  // the planes and counters zeroed, markref + critneighup, then the refine
+  // list, critneighdown and the coarsened families: one launch
+  int rc = launch(c, "admesh_flags", [&] { return launch_admesh_flags(a, plane, c->d_gbar, c->st); });
   if (rc) return rc;
   // the counters and the heads of both lists in one wait; longer lists
   // (rare: a pass that remeshes thousands of blocks) in a second one
@@ -1252,49 +1306,9 @@ int w2d_locate_bounds(W2dCtx* c)
   if (!c->have_topology || !c->have_links)
     return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology and w2d_set_links first");
   if (c->nruns > 0) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "one run per context");
-  int rc = ensure_leaf_list(c);
-  if (rc) return rc;
-  rc = ensure_plan(c);
-  if (rc) return rc;
-  const size_t slots = (size_t)c->cap + 1;
-  const int nl = c->nleaf;
-  // a leaf list built on the device came with the positions of all slots
-  // 1..nbmax (the only ones the plan kernels look up)
-  const bool posof_ready = c->host_leaves_stale;
-  if (!posof_ready) CK(cudaMemsetAsync(c->d_posof, 0xff, sizeof(int) * slots, c->st));    // -1: not a leaf
-  // (the plans and the bottom-face writer positions are cleared by k_bcount)
-  PlanArgs a{};
-  a.leaves = c->d_leaves;
-  a.nleaf = nl;
-  a.nbmax = c->nbmax;
-  a.cap = c->cap;
-  a.lev = c->d_lev;
-  a.links = c->d_links;
-  a.sons = c->d_sons;
-  a.posof = c->d_posof;
-  a.entries = c->d_bent;
-  a.span = c->d_bspan;
-  a.local = c->d_blocal;
-  const int g = plan_ctas(nl);
-  a.ctatot = c->d_bcta;
-  a.ctaoff = c->d_bcta + bcta_half(c);
-  a.total = c->d_bcta + 2 * bcta_half(c);
-  a.fd1 = c->d_fd1;
-  a.fd2 = c->d_fd2;
-  a.wpos = c->d_wpos;
-  a.jetblk = c->d_jetblk;
-  a.bc[0] = c->p.bc_left;
-  a.bc[1] = c->p.bc_right;
-  a.bc[2] = c->p.bc_bottom;
-  a.bc[3] = c->p.bc_top;
-  a.f6b = (c->p.compat & W2D_COMPAT_OUTFYB) != 0;
-  a.jet = c->p.otherb == W2D_USERBC_JET;
-  if ((rc = launch(c, "locatebounds", [&] { return launch_locatebounds(a, posof_ready, c->st); }))) return rc;
-  if (nl > 0)   // the launcher issues up to seven kernels; launch() counted one
-    c->nlaunch += 2 + !posof_ready + (a.f6b && a.bc[2] != W2D_BC_REFLECTIVE) + 2 * a.jet;
-  (void)g;
-  c->have_bounds = true;
-  return W2D_OK;
+  // the list is rebuilt from the leaf flags in the same launch (the same
+  // list w2d_set_topology uploaded, or the one refine/coarse left)
+  return ctx_tree_device(c, c->nbmax, c->nleaf);
 }
 
 // One admesh pass worth of refines and coarsenings: host levels/icoord of

@@ -110,16 +110,21 @@ struct W2dCtx {
   int* h_mlists = nullptr;    // pinned, same layout
   int* d_rows7 = nullptr;     // (nb, lp(nb,3:8)) per row, cap+1 rows
   int* h_rows7 = nullptr;     // pinned
-  // locatebounds on the device (allocated by the first w2d_locate_bounds):
-  // leaf position per slot, the entry of every (leaf, side) and the prefix
-  // sums of their count, each slot's first and last list position (jet), the
-  // writer position of each boundaryI bottom face
+  // the leaf list and locatebounds on the device (allocated by the first
+  // use): leaf position per slot, the entry of every (slot, side) and its
+  // rank in its tile of 256, each slot's rank among the leaves of its tile,
+  // each slot's first and last list position (jet), the writer position of
+  // each boundaryI bottom face
   int* d_posof = nullptr;
-  int2* d_bent = nullptr;     // 4 per leaf position
+  int2* d_bent = nullptr;     // 4 per slot
   int2* d_bspan = nullptr;    // per slot
-  int* d_blocal = nullptr;    // 4 per leaf position (the leaf list uses 1 per slot)
-  int* d_bcta = nullptr;      // CTA totals, then their offsets (bcta_half apart), then the list length
+  int* d_blocal = nullptr;    // 4 per slot
+  int* d_lrank = nullptr;     // per slot
+  int* d_bcta = nullptr;      // tile counts (entry tiles, then slot tiles), the list length at bcta_half(c) * 2
   int* d_wpos = nullptr;
+  // the two words of the grid barrier of the cooperative tree kernels
+  // (count, generation); zero between launches, reset after a device error
+  unsigned int* d_gbar = nullptr;
   cudaEvent_t ev_links = nullptr;
   bool have_links = false;
   // pinned staging of refine/coarse lists

@@ -333,6 +333,26 @@ int push_bounds(W2dSim* s)
   return W2D_OK;
 }
 
+// The tree's upload at the start of a step after a mesh change: with the
+// plans on the device (and the device's leaf flags current), the changed
+// lp rows and then the leaf list with the plans in one launch (*planned);
+// otherwise the leaf list alone, the plans following the half step's
+// launch (push_bounds) so that a host walk overlaps it
+int push_tree(W2dSim* s, bool* planned)
+{
+  *planned = false;
+  if (s->devplans && s->topo_dev_ok) {
+    int rc = push_links(s);
+    if (rc) return rc;
+    if ((rc = ctx_tree_device(s->ctx, s->nbmax, s->nbleafs))) return rc;
+    s->dirty = false;
+    s->ib_stale = true;
+    *planned = true;
+    return W2D_OK;
+  }
+  return push_topology(s);
+}
+
 int refresh_plan(W2dSim* s)
 {
   const double t0 = now_ms();
@@ -458,10 +478,15 @@ int admesh_apply(W2dSim* s, const int32_t* refine, int nr, const int32_t* first_
 // the last pass changed
 int push_links(W2dSim* s)
 {
-  const int32_t* rows = s->links_all ? nullptr : s->touched.data();
-  const int n = s->links_all ? 0 : (int)s->touched.size();
-  if (!s->links_all && n == 0) return W2D_OK;
-  int rc = w2d_set_links(s->ctx, s->lp.data() + 8, 8, 1, rows, n);
+  if (!s->links_all && s->touched.empty()) return W2D_OK;
+  // every block of the run's tree: listed explicitly, since the context's
+  // own nbmax is that of its last topology upload, which a refine pass
+  // since then has outgrown
+  if (s->links_all) {
+    s->touched.resize((size_t)s->nbmax);
+    for (int nb = 1; nb <= s->nbmax; ++nb) s->touched[(size_t)nb - 1] = nb;
+  }
+  int rc = w2d_set_links(s->ctx, s->lp.data() + 8, 8, 1, s->touched.data(), (int)s->touched.size());
   if (rc) return rc;
   s->links_all = false;
   s->touched.clear();
@@ -635,11 +660,12 @@ int w2d_sim_run(W2dSim* s, int nsteps)
     tree_trial_pre(s);
     const double t0 = now_ms();
     const bool replan = s->dirty;
-    if (replan && (rc = push_topology(s))) return rc;
+    bool planned = false;
+    if (replan && (rc = push_tree(s, &planned))) return rc;
     const double t1 = now_ms();
     if ((rc = ctx_step_first(s->ctx))) return rc;           // src/main.f90:87, then tstep's first pass
     const double t2 = now_ms();
-    if (replan && (rc = push_bounds(s))) return rc;
+    if (replan && !planned && (rc = push_bounds(s))) return rc;
     const double t3 = now_ms();
     if ((rc = ctx_step_rest(s->ctx))) return rc;            // the rest of tstep
     const double t4 = now_ms();
@@ -664,12 +690,13 @@ int w2d_sim_run(W2dSim* s, int nsteps)
     tree_trial_pre(s);
     const double t0 = now_ms();
     const bool replan = s->dirty;
-    if (replan && (rc = push_topology(s))) return rc;
+    bool planned = false;
+    if (replan && (rc = push_tree(s, &planned))) return rc;
     const double t1 = now_ms();
     if ((rc = ctx_dt_launch(s->ctx))) return rc;            // src/main.f90:87
     if ((rc = ctx_half_step(s->ctx))) return rc;            // src/main.f90:95 (first pass)
     const double t2 = now_ms();
-    if (replan && (rc = push_bounds(s))) return rc;
+    if (replan && !planned && (rc = push_bounds(s))) return rc;
     const double t3 = now_ms();
     double dt = 0.0;
     if ((rc = ctx_dt_wait(s->ctx, &dt))) return rc;

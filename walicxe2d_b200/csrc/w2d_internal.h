@@ -31,6 +31,9 @@ int ctx_topology_device(W2dCtx* c, int nbmax, int nleaf);
 // the same, when w2d_refine / w2d_coarse changed the leaves since the list
 // was last built (no-op otherwise)
 int ensure_leaf_list(W2dCtx* c);
+// the leaf list and the fill plans (w2d_locate_bounds) in one launch, from
+// the leaf flags and the lp(:,3:8) mirror (nbmax and the leaf count given)
+int ctx_tree_device(W2dCtx* c, int nbmax, int nleaf);
 
 // ---- ensembles: runs share one context; run r owns slots base[r]+1 ..
 // base[r]+cap[r] and numbers its blocks 1..cap[r] as a single run does.

@@ -644,17 +644,20 @@ __device__ __forceinline__ double cyl_radius(const KArgs& a, int b, int lev, int
 template <typename R, int NEQ>
 __host__ __device__ constexpr size_t smem_half()
 {
-  return 128 + sizeof(R) * (NEQ * W2D_CELLS + W2D_CELLS + 2 * NEQ * 272);
+  return 128 + sizeof(R) * (2 * NEQ * W2D_CELLS + W2D_CELLS + 2 * NEQ * 272);
 }
 
 template <typename R, int NEQ, int SOLVER, bool P>
 __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_half(KArgs a, PhysArgs pa, double dt)
 {
+  // su: the tile as loaded (u, or the stored primitives under DMC); st:
+  // the primitives of cells 0..17; scs: their sound speeds
   uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
-  R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
-  R(*scs)[W2D_W] = reinterpret_cast<R(*)[W2D_W]>(w2d_smem + 128 + sizeof(R) * NEQ * W2D_CELLS);
-  R(*sf)[16][17] = reinterpret_cast<R(*)[16][17]>(w2d_smem + 128 + sizeof(R) * (NEQ + 1) * W2D_CELLS);
-  R(*sg)[17][16] = reinterpret_cast<R(*)[17][16]>(w2d_smem + 128 + sizeof(R) * ((NEQ + 1) * W2D_CELLS + NEQ * 272));
+  R(*su)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
+  R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128 + sizeof(R) * NEQ * W2D_CELLS);
+  R(*scs)[W2D_W] = reinterpret_cast<R(*)[W2D_W]>(w2d_smem + 128 + sizeof(R) * 2 * NEQ * W2D_CELLS);
+  R(*sf)[16][17] = reinterpret_cast<R(*)[16][17]>(w2d_smem + 128 + sizeof(R) * (2 * NEQ + 1) * W2D_CELLS);
+  R(*sg)[17][16] = reinterpret_cast<R(*)[17][16]>(w2d_smem + 128 + sizeof(R) * ((2 * NEQ + 1) * W2D_CELLS + NEQ * 272));
   const Phys<R> ph = make_phys<R, SOLVER, -1>(pa);
   const int tid = threadIdx.x;
   const size_t bs = (size_t)NEQ * W2D_CELLS;
@@ -665,7 +668,7 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_half(KArgs a, P
   const int b = a.leaves[lr.li];
   const R* __restrict__ u = (const R*)a.u + (size_t)b * bs;
   R* __restrict__ up = (R*)a.up + (size_t)b * bs;
-  if (tid == 0) tile_issue<R, NEQ>(&st[0][0][0], dmc ? (const R*)a.prim + (size_t)b * bs : u, bar);
+  if (tid == 0) tile_issue<R, NEQ>(&su[0][0][0], dmc ? (const R*)a.prim + (size_t)b * bs : u, bar);
   const int lev = a.lev[b];
   const double dtm = step_dt(a, b, dt) / 2.;
   const R dtdx = R(dtm / geo_dx(a, b, lev));
@@ -678,15 +681,15 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_half(KArgs a, P
     if ((ti == 1 || ti == 18) && (tj == 1 || tj == 18)) continue;
     R q[NEQ];
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) q[k] = st[k][tj][ti];
+    for (int k = 0; k < NEQ; ++k) q[k] = su[k][tj][ti];
     if (!dmc) {
       R uu[NEQ], T;
 #pragma unroll
       for (int k = 0; k < NEQ; ++k) uu[k] = q[k];
       uprim<NEQ>(ph, q, uu, T);
-#pragma unroll
-      for (int k = 0; k < NEQ; ++k) st[k][tj][ti] = q[k];
     }
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) st[k][tj][ti] = q[k];
     scs[tj][ti] = sound(ph, q[3], q[0]);
   }
   __syncthreads();
@@ -721,7 +724,8 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_half(KArgs a, P
     if (pa.cyl) cyl_sources<R, NEQ>(st, i + 1, j + 1, R(cyl_radius(a, b, lev, j)), ph.cv, S);
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) {
-      const R uo = u[k * W2D_CELLS + cidx(i, j)];
+      // u from the tile (under DMC the tile holds the primitives: u from HBM)
+      const R uo = dmc ? u[k * W2D_CELLS + cidx(i, j)] : su[k][j + 1][i + 1];
       R v = uo - dtdx * (sf[k][j - 1][i] - sf[k][j - 1][i - 1]) - dtdy * (sg[k][j][i - 1] - sg[k][j - 1][i - 1]);
       if (pa.cyl) v = v + R(dtm) * S[k];
       up[k * W2D_CELLS + cidx(i, j)] = v;
@@ -879,73 +883,10 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_full(KArgs a, P
 
 // ---------------------------------------------------------------------------
 // Fill of layer 0 of u: the non-MPI walk of src/boundaryI.f90:34-396 as
-// per-face last writers.  With stats != 0 (ADIABATIC) it also computes,
-// from calcprim(u) of the filled block, the CFL partial of timestep and the
-// criteria maximum.
-template <typename R, int NEQ>
-__host__ __device__ constexpr size_t smem_fill1()
-{
-  return 128 + sizeof(R) * NEQ * W2D_CELLS + 64 * sizeof(double);
-}
-
-template <typename R, int NEQ, bool P>
-__global__ void __launch_bounds__(W2D_THREADS, 4) k_fill1(KArgs a, PhysArgs pa, int stats)
-{
-  uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
-  R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
-  double* sred = reinterpret_cast<double*>(w2d_smem + 128 + sizeof(R) * NEQ * W2D_CELLS);
-  const Phys<R> ph = make_phys<R, -1, -1>(pa);
-  const int tid = threadIdx.x;
-  const size_t bs = (size_t)NEQ * W2D_CELLS;
-  R* __restrict__ upool = (R*)a.u;
-  bar_init_once(bar);
-  uint32_t par = 0;
-  for (LeafRange lr = leaf_range<P>(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
-  const int li = lr.li;
-  const int b = a.leaves[li];
-  R* __restrict__ u = upool + (size_t)b * bs;
-  if (stats && tid == 0) tile_issue<R, NEQ>(&st[0][0][0], u, bar);
-  R gv[NEQ];
-  bool w = false;
-  int gi = 0, gj = 0;
-  if (tid < 64) {
-    const int f = tid / 16, m = 1 + tid % 16;
-    ghost_ij(f, 0, m, gi, gj);
-    const int2 d = a.fd[li * 4 + f];
-#pragma unroll
-    for (int k = 0; k < NEQ; ++k) w = ghost_value<R>(upool, bs, a, b, d, f, 0, m, k, gv[k]);
-    if (w) {
-#pragma unroll
-      for (int k = 0; k < NEQ; ++k) u[k * W2D_CELLS + cidx(gi, gj)] = gv[k];
-    }
-  }
-  if (!stats) continue;
-  if (!wait_tiles_p(bar, a.err, b, par)) return;
-  if (tid < 64 && w) {
-#pragma unroll
-    for (int k = 0; k < NEQ; ++k) st[k][gj + 1][gi + 1] = gv[k];
-  }
-  __syncthreads();
-  for (int c = tid; c < 18 * 18; c += W2D_THREADS) {   // calcprim of cells 0..17
-    const int ti = 1 + c % 18, tj = 1 + c / 18;
-    if ((ti == 1 || ti == 18) && (tj == 1 || tj == 18)) continue;
-    R uu[NEQ], q[NEQ], T;
-#pragma unroll
-    for (int k = 0; k < NEQ; ++k) uu[k] = st[k][tj][ti];
-    uprim<NEQ>(ph, q, uu, T);
-#pragma unroll
-    for (int k = 0; k < NEQ; ++k) st[k][tj][ti] = q[k];
-  }
-  __syncthreads();
-  block_stats<R, NEQ>(st, ph, a, pa, b, sred);
-  leaf_end();
-  }
-}
-
-// Fill of layer 0 without the block statistics (cooling runs and the jet,
-// whose statistics follow in a later pass), or with the criteria terms of
-// the filled faces (a.split_stats: the full step computed the rest):
-// 64 threads per leaf, four leaves per 256-thread CTA.  Persistent (P):
+// per-face last writers, without the block statistics (cooling runs and
+// the jet, whose statistics follow in a later pass), or with the criteria
+// terms of the filled faces (a.split_stats: the full step computed the
+// rest): 64 threads per leaf, four leaves per 256-thread CTA.  Persistent (P):
 // the CTA walks its leaves as leaf_range gives them, four at a time (li,
 // li + step, li + 2 step, li + 3 step); otherwise CTA k takes leaves
 // 4k .. 4k + 3.  A warp serves two faces of one leaf.

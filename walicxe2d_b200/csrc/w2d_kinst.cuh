@@ -91,33 +91,22 @@ static cudaError_t full(int neq, const KArgs& a, const PhysArgs& pa, double dt, 
   return cudaSuccess;
 }
 
-template <int NEQ, bool P>
-static cudaError_t fill1_p(const KArgs& a, const PhysArgs& pa, int stats, cudaStream_t st)
+// the ghost faces (and, with a.split_stats, their criteria terms): four
+// leaves per CTA
+template <int NEQ>
+static cudaError_t fill1_t(const KArgs& a, const PhysArgs& pa, cudaStream_t st)
 {
-  static bool done = false;
-  constexpr size_t sm = smem_fill1<R, NEQ>();
-  cudaError_t e = smem_opt_in(k_fill1<R, NEQ, P>, sm, done);
-  if (e != cudaSuccess) return e;
-  k_fill1<R, NEQ, P><<<launch_grid(a), W2D_THREADS, sm, st>>>(a, pa, stats);
+  if (a.grid > 0)
+    k_fill1g<R, NEQ, true><<<a.grid, 256, 0, st>>>(a, pa);
+  else
+    k_fill1g<R, NEQ, false><<<(a.nleaf + 3) / 4, 256, 0, st>>>(a, pa);
   return cudaGetLastError();
 }
-template <int NEQ>
-static cudaError_t fill1_t(const KArgs& a, const PhysArgs& pa, int stats, cudaStream_t st)
-{
-  if (!stats || a.split_stats) {   // ghost faces (and their criteria terms): four leaves per CTA
-    if (a.grid > 0)
-      k_fill1g<R, NEQ, true><<<a.grid, 256, 0, st>>>(a, pa);
-    else
-      k_fill1g<R, NEQ, false><<<(a.nleaf + 3) / 4, 256, 0, st>>>(a, pa);
-    return cudaGetLastError();
-  }
-  return a.grid > 0 ? fill1_p<NEQ, true>(a, pa, stats, st) : fill1_p<NEQ, false>(a, pa, stats, st);
-}
 
-static cudaError_t fill1(int neq, const KArgs& a, const PhysArgs& pa, int stats, cudaStream_t st)
+static cudaError_t fill1(int neq, const KArgs& a, const PhysArgs& pa, cudaStream_t st)
 {
   if (a.nleaf == 0) return cudaSuccess;
-  W2D_NEQ_SWITCH(neq, return (fill1_t<NEQ>(a, pa, stats, st)));
+  W2D_NEQ_SWITCH(neq, return (fill1_t<NEQ>(a, pa, st)));
   return cudaSuccess;
 }
 

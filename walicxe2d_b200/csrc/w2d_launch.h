@@ -11,7 +11,8 @@ namespace w2d {
 struct Launchers {
   cudaError_t (*half)(int neq, const KArgs&, const PhysArgs&, double dt, cudaStream_t);
   cudaError_t (*full)(int neq, const KArgs&, const PhysArgs&, double dt, cudaStream_t);
-  cudaError_t (*fill1)(int neq, const KArgs&, const PhysArgs&, int stats, cudaStream_t);
+  // boundaryI's fill of layer 0 (with a.split_stats, the criteria terms of the filled faces)
+  cudaError_t (*fill1)(int neq, const KArgs&, const PhysArgs&, cudaStream_t);
   cudaError_t (*fill_only)(int neq, const KArgs&, void* pool, int layers, cudaStream_t);
   cudaError_t (*calcprim)(int neq, const KArgs&, const PhysArgs&, const int* list, int n, int mode,
                           cudaStream_t);
@@ -64,50 +65,54 @@ struct MarkArgs {
   int* clist;
   int* err;      // the context's error word (W2D_ERR_TOPOLOGY on a malformed tree)
 };
-// markref and the whole critneighup cascade in one launch
-cudaError_t launch_markref_up(const MarkArgs& a, cudaStream_t st);
-// the refine list, then critneighdown and the coarsened families in one launch
-cudaError_t launch_refine_coarsen(const MarkArgs& a, cudaStream_t st);
+// the flag planes and counts zeroed, markref with the whole critneighup
+// cascade, then the refine list, critneighdown and the coarsened families:
+// one cooperative launch (bar: the context's two grid-barrier words, zero)
+cudaError_t launch_admesh_flags(const MarkArgs& a, size_t plane_bytes, unsigned int* bar, cudaStream_t st);
 // rows7: (nb, lp(nb,3), lp(nb,4), lp(nb,5..8)) per row
 cudaError_t launch_set_links(const int* rows7, int n, int4* links, int2* sons, cudaStream_t st);
 
 // locatebounds and the fill plans on the device (w2d_mark.cu).  posof: per
-// slot, the leaf position or -1 (set to -1 before); entries/local: per
-// (leaf position, side), its innerbounds entry (type, neighbour) and the
-// exclusive prefix of the entry count within its CTA of 256; ctatot/ctaoff
-// per CTA; total[0] the list length; span (jet runs): per slot, the first
-// and last list position as nbs; fd1/fd2 (4 faces per leaf position) and
-// wpos (per leaf position) zeroed before; jetblk per leaf position (jet
-// runs).
+// slot, the leaf position or -1; entries/local: per x = 4 nb + side, its
+// innerbounds entry (type, neighbour) and its rank among the entries of its
+// tile of 256; total[0] the list length; span (jet runs): per slot, the
+// first and last list position as nbs; fd1/fd2 (4 faces per leaf
+// position), wpos (per leaf position) and jetblk (jet runs) written.
 struct PlanArgs {
-  const int* leaves;
-  int nleaf, nbmax, cap;
+  int* leaves;
+  int nbmax, cap;
   const int* lev;
   const int4* links;
   const int2* sons;
   int* posof;
   int2* entries;
   int2* span;
-  int *local, *ctatot, *ctaoff, *total;
+  int *local, *total;
   int2 *fd1, *fd2;
   int* wpos;
   int* jetblk;
   int bc[4];
   int f6b, jet;
 };
-int plan_ctas(int nleaf);
-// seven launches at most: positions (unless posof_ready: posof already
-// holds the leaf position of every slot 1..nbmax, -1 for the others),
-// entries and counts, scan, spans (jet), plans, OUTFYB, jet
-cudaError_t launch_locatebounds(const PlanArgs& a, bool posof_ready, cudaStream_t st);
+// The leaf list from the leaf flags (ascending ID) with every slot's leaf
+// position and the leaf count, and with plans != 0 locatebounds and the
+// plans too: one cooperative launch (bar: the two grid-barrier words, zero).
+struct TreeArgs {
+  PlanArgs p;
+  const int* flag;       // per slot: 1 for a leaf
+  int* lrank;            // per slot: rank among the leaves of its tile of 256
+  int* tcnt;             // per tile: entry tiles, then slot tiles
+  int* nleaf_dev;        // the leaf count
+  int plans;
+  unsigned int* bar;
+  int* err;
+};
+// tiles of 256 a tree build over slots 1..nbmax uses (entries and slots)
+inline int tree_tiles(int nbmax) { return (4 * (nbmax + 1) + 255) / 256 + (nbmax + 1 + 255) / 256; }
+cudaError_t launch_tree_build(const TreeArgs& t, cudaStream_t st);
 
 // flag[leaves[k]] = 1 for k < nl (flag zeroed before)
 cudaError_t launch_flag_leaves(const int* leaves, int nl, int* flag, cudaStream_t st);
-// leaves[] = the slots 1..nbmax whose flag is set, ascending; *nleaf their
-// count; posof[1..nbmax] their positions (-1: not a leaf).  Three launches;
-// local per slot, ctatot/ctaoff per CTA of 256.
-cudaError_t launch_leaf_list(const int* flag, int nbmax, int* local, int* ctatot, int* ctaoff, int* leaves,
-                             int* nleaf, int* posof, cudaStream_t st);
 
 // one bounded wait that runs out (see w2d_wait_selftest)
 cudaError_t launch_wait_selftest(int* err, cudaStream_t st);

@@ -4,6 +4,8 @@
 // locatebounds (src/locatebounds.f90:29-540) with the per-face fill plans
 // built from its list.  The host keeps lp and applies updatelpup /
 // updatelpdown; the device holds a mirror of lp(:,3:8).
+#include <algorithm>
+
 #include "../../include/w2d.h"
 #include "w2d_launch.h"
 
@@ -36,10 +38,8 @@ __device__ __forceinline__ bool flag_set(unsigned char* f, int n)
 // atomic decides) walks on from it, so every block of the closure is
 // walked once.  The walk descends a level per edge, so its stack holds at
 // most 3 entries per level.
-__global__ void __launch_bounds__(kThreads) k_markref_up(MarkArgs a)
+__device__ void markref_up_one(const MarkArgs& a, int k)
 {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= a.nleaf) return;
   const int nb = a.leaves[k];
   if (!in_pool(nb, a.cap)) return;
   a.leafp[nb] = 1;
@@ -76,11 +76,12 @@ __global__ void __launch_bounds__(kThreads) k_markref_up(MarkArgs a)
 }
 
 // a block refined by this pass (src/admesh.f90:29-65 refines every block of
-// level 1..nlevs-1 still marked)
+// level 1..nlevs-1 still marked); the planes were written by other CTAs
+// before the barrier, so they are read from L2
 __device__ __forceinline__ bool refined_now(const MarkArgs& a, int nb)
 {
   const int l = a.lev[nb];
-  return a.up[nb] && l >= 1 && l <= a.nlevs - 1;
+  return __ldcg(a.up + nb) && l >= 1 && l <= a.nlevs - 1;
 }
 
 // irefdown of block nb after critneighdown (src/critneighdown.f90:22-48)
@@ -91,7 +92,7 @@ __device__ __forceinline__ bool refined_now(const MarkArgs& a, int nb)
 // (src/updatelpup.f90:20-175 redirects the finer neighbours).
 __device__ __forceinline__ bool down_after(const MarkArgs& a, int nb)
 {
-  if (!a.down[nb] || refined_now(a, nb)) return false;
+  if (!__ldcg(a.down + nb) || refined_now(a, nb)) return false;
   const int l = a.lev[nb];
   const int4 q = a.links[nb];
   const int n[4] = {q.x, q.y, q.z, q.w};
@@ -102,7 +103,7 @@ __device__ __forceinline__ bool down_after(const MarkArgs& a, int nb)
     if (!in_pool(n1, a.cap)) return false;
     const bool r1 = refined_now(a, n1);
     if (r1 && a.lev[n1] < l) continue;       // now points to a new son
-    if (!a.leafp[n1] || r1) return false;
+    if (!__ldcg(a.leafp + n1) || r1) return false;
   }
   return true;
 }
@@ -113,16 +114,14 @@ __device__ __forceinline__ bool down_after(const MarkArgs& a, int nb)
 // lp(lp(s1,6),8)) are never changed by the updatelpup / updatelpdown calls
 // of other families, so the decisions do not depend on the order in which
 // admesh takes them.
-__global__ void __launch_bounds__(kThreads) k_refine_coarsen(MarkArgs a)
+__device__ void refine_coarsen_one(const MarkArgs& a, int nb)
 {
-  const int nb = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (nb > a.nbmax) return;
   if (refined_now(a, nb)) {
     const int k = atomicAdd(&a.counts[0], 1);
     if (k < a.cap) a.rlist[k] = nb;
     return;
   }
-  if (!a.down[nb] || a.sons[nb].y != 1) return;
+  if (!__ldcg(a.down + nb) || a.sons[nb].y != 1) return;
   const int l = a.lev[nb];
   if (l < 2 || l > a.nlevs) return;
   const int s2 = a.links[nb].y, s3 = a.links[nb].w;
@@ -148,79 +147,53 @@ __global__ void __launch_bounds__(kThreads) k_set_links(const int* __restrict__ 
   links[nb] = make_int4(r[3], r[4], r[5], r[6]);
 }
 
-// ---- locatebounds and the fill plans -------------------------------------
-//
-// locatebounds (src/locatebounds.f90:29-540, serial build) walks the leaves
-// in ascending ID and, per leaf, its sides left, right, bottom, top.  A side
-// adds an entry to innerbounds unless its bnd flag is already set:
-//   - a box wall: always (types -1..-4);
-//   - a same-level leaf neighbour n1: the entry (nb, n1, 1/4/7/10) sets
-//     the flag of n1's facing side, so of the pair only the lower ID adds
-//     it;
-//   - a same-level neighbour that has sons: the entry (nb, son, 2/5/8/11)
-//     with the son facing nb that has the lower ID (flags set on the sons,
-//     which never add entries toward a coarser block themselves);
-//   - a coarser neighbour: no entry (that neighbour adds the one above).
-// So each leaf's entries follow from its links alone, and their list
-// positions from a prefix sum over (leaf, side) in list order: one thread
-// per leaf and side finds its entry, the prefix sum gives its position, and
-// one thread per entry writes the plans.  The plans are those of the host
-// walk (w2d_api.cu: plan_entries): every non-corner ghost face has exactly
-// one writer, except the bottom faces of boundaryI that the OUTFYB defect
-// also writes (resolved by list position in a second pass), and the jet
-// flags come from each block's first and last position as nbs (a per-slot
-// table built before the plans).
+// ---- bounded grid barrier of the one-launch kernels ------------------------
+// The tree kernels below run as cooperative launches (every CTA resident at
+// once) and separate their phases with this barrier.  bar[0] counts the
+// CTAs that have arrived, bar[1] is the generation: the last CTA to arrive
+// resets the count and moves the generation, the others wait for it to
+// move.  The wait is bounded (2^22 polls, about a second): a barrier that
+// runs out records W2D_ERR_TIMEOUT and returns false, the CTA leaves the
+// kernel, and the host resets both words before its next launch.  Data
+// that other CTAs wrote before a barrier is read after it with __ldcg (from
+// L2), never from a line this SM's L1 may hold.
+constexpr long kBarPolls = 1L << 22;
 
-// The entry of side s of leaf nb: (type, neighbour), type 0 for none.
-__device__ __forceinline__ int2 pl_entry(const PlanArgs& a, int nb, int s)
+__device__ bool grid_barrier(unsigned int* bar, int* err)
 {
-  const int4 q = a.links[nb];
-  const int m = s == 0 ? q.x : s == 1 ? q.y : s == 2 ? q.z : q.w;
-  if (m == -1) return make_int2(-(s + 1), 0);
-  if (!in_pool(m, a.cap) || m > a.nbmax) return make_int2(0, 0);
-  if (a.lev[m] < a.lev[nb]) return make_int2(0, 0);          // coarser: its entry
-  if (a.posof[m] >= 0)                                        // same-level leaf
-    return nb < m ? make_int2(1 + 3 * s, m) : make_int2(0, 0);
-  const int f = a.sons[m].x;                                  // same level, has sons
-  if (f < 1 || f + 3 > a.nbmax) return make_int2(0, 0);
-  const int son_off = (s == 0) ? 1 : (s == 2) ? 2 : 0;
-  return make_int2(2 + 3 * s, f + son_off);
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* gen = bar + 1;
+    const unsigned int g0 = *gen;
+    __threadfence();
+    int good = 1;
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long polls = 0;
+      while (*gen == g0) {
+        if (++polls > kBarPolls) {
+          set_err(err, W2D_ERR_TIMEOUT, 0, -1, -1);
+          good = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    ok = good;
+  }
+  __syncthreads();
+  return ok != 0;
 }
 
-// first and last list position (1-based) of block b as nbs, 0 if none
-__device__ __forceinline__ int2 pl_span(const PlanArgs& a, int b)
-{
-  if (b < 1 || b > a.nbmax) return make_int2(0, 0);
-  return a.span[b];
-}
-
-__global__ void __launch_bounds__(kThreads) k_posof(PlanArgs a)
-{
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= a.nleaf) return;
-  const int nb = a.leaves[k];
-  if (in_pool(nb, a.cap)) a.posof[nb] = k;
-}
-
-// thread x = 4 * leaf position + side: the entry, and the exclusive prefix
-// of the entry count within the CTA (list order), and the CTA's total; it
-// also clears face x of both plans (FK_KEEP) and, for side 0, the leaf's
-// bottom-face writer position, before k_bplan writes them
-__global__ void __launch_bounds__(kThreads) k_bcount(PlanArgs a)
+// Exclusive prefix of c over the 256 threads of the CTA; *total gets the sum.
+__device__ __forceinline__ int cta_scan(int c, int* total)
 {
   __shared__ int wsum[kThreads / 32];
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int c = 0;
-  if (x < 4 * a.nleaf) {
-    a.fd1[x] = make_int2(0, FK_KEEP);
-    a.fd2[x] = make_int2(0, FK_KEEP);
-    if ((x & 3) == 0) a.wpos[x >> 2] = 0;
-    const int nb = a.leaves[x >> 2];
-    int2 en = make_int2(0, 0);
-    if (in_pool(nb, a.cap)) en = pl_entry(a, nb, x & 3);
-    a.entries[x] = en;
-    c = en.x != 0;
-  }
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   int v = c;
 #pragma unroll
@@ -240,110 +213,122 @@ __global__ void __launch_bounds__(kThreads) k_bcount(PlanArgs a)
     if (lane < kThreads / 32) wsum[lane] = u;   // inclusive over warps
   }
   __syncthreads();
-  if (x < 4 * a.nleaf) a.local[x] = (w > 0 ? wsum[w - 1] : 0) + v - c;
-  if (threadIdx.x == kThreads - 1) a.ctatot[blockIdx.x] = wsum[kThreads / 32 - 1];
+  const int ex = (w > 0 ? wsum[w - 1] : 0) + v - c;
+  *total = wsum[kThreads / 32 - 1];
+  __syncthreads();   // wsum is reused by the next call
+  return ex;
 }
 
-// exclusive prefix sum of the CTA totals (one CTA, tiles of 1024)
-__global__ void __launch_bounds__(1024) k_bscan(PlanArgs a, int nctas)
+// out[0..n] = exclusive prefix sums of the n counts cnt[0..n) (out[n]: the
+// total), every CTA for itself, in chunks of 256.
+__device__ void cta_scan_counts(const int* cnt, int n, int* out)
 {
-  __shared__ int wsum[32];
-  __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
+  int carry = 0;
+  for (int k0 = 0; k0 < n; k0 += kThreads) {
+    const int k = k0 + (int)threadIdx.x;
+    const int c = k < n ? __ldcg(cnt + k) : 0;
+    int tot;
+    const int ex = cta_scan(c, &tot);
+    if (k < n) out[k] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) out[n] = carry;
   __syncthreads();
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int t0 = 0; t0 < nctas; t0 += 1024) {
-    const int k = t0 + threadIdx.x;
-    const int c = k < nctas ? a.ctatot[k] : 0;
-    int x = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) wsum[w] = x;
-    __syncthreads();
-    if (w == 0) {
-      int v = wsum[lane];
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += y;
-      }
-      wsum[lane] = v;
-    }
-    __syncthreads();
-    if (k < nctas) a.ctaoff[k] = carry + (w > 0 ? wsum[w - 1] : 0) + x - c;
-    __syncthreads();
-    if (threadIdx.x == 0) carry += wsum[31];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) a.total[0] = carry;
 }
 
-// list position (1-based) of the entry of thread x (if it has one)
-__device__ __forceinline__ int pl_pos(const PlanArgs& a, int x)
+// ---- locatebounds and the fill plans -------------------------------------
+//
+// locatebounds (src/locatebounds.f90:29-540, serial build) walks the leaves
+// in ascending ID and, per leaf, its sides left, right, bottom, top.  A side
+// adds an entry to innerbounds unless its bnd flag is already set:
+//   - a box wall: always (types -1..-4);
+//   - a same-level leaf neighbour n1: the entry (nb, n1, 1/4/7/10) sets
+//     the flag of n1's facing side, so of the pair only the lower ID adds
+//     it;
+//   - a same-level neighbour that has sons: the entry (nb, son, 2/5/8/11)
+//     with the son facing nb that has the lower ID (flags set on the sons,
+//     which never add entries toward a coarser block themselves);
+//   - a coarser neighbour: no entry (that neighbour adds the one above).
+// So each leaf's entries follow from its links and the leaf flags alone,
+// and, the walk going by ascending ID, the list position of the entry of
+// (slot nb, side s) is the number of entries at x = 4 nb + s' before it: a
+// prefix sum over x = 4 nb + s, independent of the leaf list.  One launch
+// (k_tree_build) builds the leaf list and these positions in its first
+// phases and the plans after a barrier; the plans are those of the host
+// walk (w2d_api.cu: plan_entries): every non-corner ghost face has exactly
+// one writer, except the bottom faces of boundaryI that the OUTFYB defect
+// also writes (resolved by list position after a second barrier), and the
+// jet flags come from each block's first and last position as nbs.
+
+struct TreeCtx {
+  const TreeArgs& t;
+  const int* sl;       // exclusive prefix of the leaves over the 256-slot tiles (shared memory)
+  // leaf position of block blk, -1 if it is no leaf
+  __device__ __forceinline__ int leafpos(int blk) const
+  {
+    if (blk < 1 || blk > t.p.nbmax || !t.flag[blk]) return -1;
+    return sl[blk >> 8] + __ldcg(t.lrank + blk);
+  }
+};
+
+// The entry of side s of leaf nb: (type, neighbour), type 0 for none.
+__device__ __forceinline__ int2 tb_entry(const TreeArgs& t, int nb, int s)
 {
-  return a.ctaoff[x / kThreads] + a.local[x] + 1;
+  const PlanArgs& a = t.p;
+  const int4 q = a.links[nb];
+  const int m = s == 0 ? q.x : s == 1 ? q.y : s == 2 ? q.z : q.w;
+  if (m == -1) return make_int2(-(s + 1), 0);
+  if (!in_pool(m, a.cap) || m > a.nbmax) return make_int2(0, 0);
+  if (a.lev[m] < a.lev[nb]) return make_int2(0, 0);          // coarser: its entry
+  if (t.flag[m])                                              // same-level leaf
+    return nb < m ? make_int2(1 + 3 * s, m) : make_int2(0, 0);
+  const int f = a.sons[m].x;                                  // same level, has sons
+  if (f < 1 || f + 3 > a.nbmax) return make_int2(0, 0);
+  const int son_off = (s == 0) ? 1 : (s == 2) ? 2 : 0;
+  return make_int2(2 + 3 * s, f + son_off);
 }
 
-// jet runs: first and last position of every leaf as nbs, per slot (the
-// slots 1..nbmax that are not leaves get none)
-__global__ void __launch_bounds__(kThreads) k_bspan(PlanArgs a)
+// first and last list position (1-based) of block b as nbs, 0 if none
+__device__ __forceinline__ int2 tb_span(const PlanArgs& a, int b)
 {
-  const int nb = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (nb > a.nbmax) return;
-  const int k = a.posof[nb];
-  int2 sp = make_int2(0, 0);
-  if (k >= 0) {
-    for (int s = 0; s < 4; ++s) {
-      if (a.entries[4 * k + s].x == 0) continue;
-      const int e = pl_pos(a, 4 * k + s);
-      if (!sp.x) sp.x = e;
-      sp.y = e;
-    }
-  }
-  a.span[nb] = sp;
+  if (b < 1 || b > a.nbmax) return make_int2(0, 0);
+  return __ldcg(a.span + b);
 }
 
 // put() of the host walk: one face descriptor of a leaf target, with the
 // jet flags for entry position e
-__device__ __forceinline__ void pl_put(const PlanArgs& a, int2* fd, bool is_fd1, int blk, int face, int nbr,
+__device__ __forceinline__ void tb_put(const TreeCtx& tc, int2* fd, bool is_fd1, int blk, int face, int nbr,
                                        int kind, int off, int e)
 {
-  if (blk < 1 || blk > a.nbmax) return;
-  const int p = a.posof[blk];
+  const PlanArgs& a = tc.t.p;
+  const int p = tc.leafpos(blk);
   if (p < 0) return;                       // non-leaf targets are rewritten before being read
   int y = kind | (off << 8);
   if (a.jet) {
     const int s1 = (kind == FK_MIRROR || kind == FK_REFLECT) ? blk : nbr;
-    const int2 q1 = pl_span(a, s1);
+    const int2 q1 = tb_span(a, s1);
     if (q1.x && q1.x < e) y |= FD_SRC1_JET;
     if (kind == FK_RESTRICT) {
-      const int2 q2 = pl_span(a, nbr + (face < 2 ? 2 : 1));
+      const int2 q2 = tb_span(a, nbr + (face < 2 ? 2 : 1));
       if (q2.x && q2.x < e) y |= FD_SRC2_JET;
     }
-    if (pl_span(a, blk).y >= e) y |= FD_DST_JET;
+    if (tb_span(a, blk).y >= e) y |= FD_DST_JET;
   }
   fd[(size_t)p * 4 + face] = make_int2(nbr, y);
   if (is_fd1 && face == 2) a.wpos[p] = e;
 }
 
-// every entry at its list position, one thread per (leaf, side) (the
-// OUTFYB bottom-face writes of boundaryI come in k_bplan_f6b)
-__global__ void __launch_bounds__(kThreads) k_bplan(PlanArgs a)
+// every entry at its list position (the OUTFYB bottom-face writes of
+// boundaryI come after the next barrier)
+__device__ __forceinline__ void tb_plan(const TreeCtx& tc, int x, int2 en, int e)
 {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  if (x >= 4 * a.nleaf) return;
-  const int2 en = a.entries[x];
-  if (en.x == 0) return;
-  const int nbs = a.leaves[x >> 2];
-  const int e = pl_pos(a, x);
+  const PlanArgs& a = tc.t.p;
+  const int nbs = x >> 2;
   const int n1 = en.y;
   const int H = W2D_NX / 2;
   auto both = [&](int blk, int face, int nbr, int kind, int off) {
-    pl_put(a, a.fd1, true, blk, face, nbr, kind, off, e);
-    pl_put(a, a.fd2, false, blk, face, nbr, kind, off, e);
+    tb_put(tc, a.fd1, true, blk, face, nbr, kind, off, e);
+    tb_put(tc, a.fd2, false, blk, face, nbr, kind, off, e);
   };
   switch (en.x) {
     case -1: case -2: case -4: {
@@ -355,8 +340,8 @@ __global__ void __launch_bounds__(kThreads) k_bplan(PlanArgs a)
       if (a.bc[2] == W2D_BC_REFLECTIVE) {
         both(nbs, 2, nbs, FK_REFLECT, 0);
       } else {
-        pl_put(a, a.fd2, false, nbs, 2, nbs, FK_MIRROR, 0, e);
-        if (!a.f6b) pl_put(a, a.fd1, true, nbs, 2, nbs, FK_MIRROR, 0, e);
+        tb_put(tc, a.fd2, false, nbs, 2, nbs, FK_MIRROR, 0, e);
+        if (!a.f6b) tb_put(tc, a.fd1, true, nbs, 2, nbs, FK_MIRROR, 0, e);
       }
       break;
     case 1:  both(nbs, 0, n1, FK_SAME, 0);  both(n1, 1, nbs, FK_SAME, 0); break;
@@ -386,42 +371,131 @@ __global__ void __launch_bounds__(kThreads) k_bplan(PlanArgs a)
   }
 }
 
-// src/boundaryI.f90:87 (OUTFYB): the bottom-wall entry at list position e
-// fills the bottom face of block e; it wins over the face's own writer when
-// it comes later in the list.  One thread per leaf (its bottom side).
-__global__ void __launch_bounds__(kThreads) k_bplan_f6b(PlanArgs a)
+// The leaf list (ascending ID, the order of the reference's loops over nb
+// with leaf(nb)) from the leaf flags, every slot's leaf position, and, with
+// t.plans, locatebounds and the fill plans, in one cooperative launch.
+// Tiles of 256: entry tiles u < nte (x = 256 u + thread, x = 4 nb + side),
+// then slot tiles (slot = 256 (u - nte) + thread); CTA k owns tiles k,
+// k + grid, ... in every phase, so it reads back its own first-phase
+// results directly.  Dynamic shared memory: the prefix sums over the entry
+// tiles (nte + 1 ints) and over the slot tiles (ntl + 1 ints).
+__global__ void __launch_bounds__(kThreads) k_tree_build(TreeArgs t, int nte, int ntl)
 {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= a.nleaf) return;
-  const int x = 4 * k + 2;
-  if (a.entries[x].x != -3) return;
-  const int e = pl_pos(a, x);
-  const int tb = e;
-  if (tb < 1 || tb > a.nbmax) return;
-  const int p = a.posof[tb];
-  if (p < 0 || a.wpos[p] > e) return;
-  pl_put(a, a.fd1, true, tb, 2, tb, FK_MIRROR, 0, e);
-}
-
-// faces no entry writes still get the jet if their block is ever nbs; the
-// interior of such a block always does (w2d_api.cu: w2d_set_bounds)
-__global__ void __launch_bounds__(kThreads) k_bplan_jet(PlanArgs a)
-{
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= a.nleaf) return;
-  const bool named = a.span[a.leaves[k]].x > 0;
-  a.jetblk[k] = named;
-  if (!named) return;
+  extern __shared__ int tb_smem[];
+  int* se = tb_smem;              // nte + 1
+  int* sl = tb_smem + nte + 1;    // ntl + 1
+  const PlanArgs& a = t.p;
+  const int nbmax = a.nbmax;
+  const int tid = threadIdx.x;
+  const int gtid = blockIdx.x * blockDim.x + tid, gsz = gridDim.x * blockDim.x;
+  // phase 1: entries and their ranks within the entry tiles; leaf ranks
+  // within the slot tiles; the plans cleared (FK_KEEP) for every position
+  // a leaf may take
+  for (int u = blockIdx.x; u < nte + ntl; u += gridDim.x) {
+    int c = 0, tot;
+    if (u < nte) {
+      const int x = 256 * u + tid;
+      int2 en = make_int2(0, 0);
+      if (x < 4 * (nbmax + 1)) {
+        const int nb = x >> 2;
+        if (nb >= 1 && t.flag[nb]) en = tb_entry(t, nb, x & 3);
+        a.entries[x] = en;
+      }
+      c = en.x != 0;
+      const int ex = cta_scan(c, &tot);
+      if (x < 4 * (nbmax + 1)) a.local[x] = ex;
+    } else {
+      const int slot = 256 * (u - nte) + tid;
+      c = slot >= 1 && slot <= nbmax && t.flag[slot] != 0;
+      const int ex = cta_scan(c, &tot);
+      if (slot <= nbmax) t.lrank[slot] = ex;
+    }
+    if (tid == 0) t.tcnt[u] = tot;
+  }
+  if (t.plans) {
+    for (int x = gtid; x < 4 * nbmax; x += gsz) {
+      a.fd1[x] = make_int2(0, FK_KEEP);
+      a.fd2[x] = make_int2(0, FK_KEEP);
+    }
+    for (int k = gtid; k < nbmax; k += gsz) a.wpos[k] = 0;
+  }
+  if (!grid_barrier(t.bar, t.err)) return;
+  // phase 2: offsets of every tile; the list and the positions
+  cta_scan_counts(t.tcnt, nte, se);
+  cta_scan_counts(t.tcnt + nte, ntl, sl);
+  if (blockIdx.x == 0 && tid == 0) {
+    *t.nleaf_dev = sl[ntl];
+    if (t.plans) a.total[0] = se[nte];
+  }
+  for (int u = blockIdx.x; u < nte + ntl; u += gridDim.x) {
+    if (u < nte) continue;
+    const int slot = 256 * (u - nte) + tid;
+    if (slot < 1 || slot > nbmax) continue;
+    const int p = t.flag[slot] ? sl[u - nte] + t.lrank[slot] : -1;
+    a.posof[slot] = p;
+    if (p >= 0) a.leaves[p] = slot;
+  }
+  if (!t.plans) return;
+  const TreeCtx tc{t, sl};
+  if (a.jet) {
+    // first and last position of every slot as nbs (its entries lie in
+    // one entry tile), then a barrier: the plans read other slots' spans
+    for (int u = blockIdx.x; u < nte; u += gridDim.x) {
+      const int nb = 64 * u + (tid >> 2);
+      if ((tid & 3) != 0 || nb < 1 || nb > nbmax) continue;
+      int2 sp = make_int2(0, 0);
+      for (int s = 0; s < 4; ++s) {
+        const int x = 4 * nb + s;
+        if (a.entries[x].x == 0) continue;
+        const int e = se[u] + a.local[x] + 1;
+        if (!sp.x) sp.x = e;
+        sp.y = e;
+      }
+      a.span[nb] = sp;
+    }
+    if (!grid_barrier(t.bar, t.err)) return;
+  }
+  for (int u = blockIdx.x; u < nte; u += gridDim.x) {
+    const int x = 256 * u + tid;
+    if (x >= 4 * (nbmax + 1)) continue;
+    const int2 en = a.entries[x];
+    if (en.x != 0) tb_plan(tc, x, en, se[u] + a.local[x] + 1);
+  }
+  const bool f6b = a.f6b && a.bc[2] != W2D_BC_REFLECTIVE;
+  if (!f6b && !a.jet) return;
+  if (!grid_barrier(t.bar, t.err)) return;
+  // phase 3, src/boundaryI.f90:87 (OUTFYB): the bottom-wall entry at list
+  // position e fills the bottom face of block e; it wins over the face's
+  // own writer when it comes later in the list
+  if (f6b) {
+    for (int u = blockIdx.x; u < nte; u += gridDim.x) {
+      const int x = 256 * u + tid;
+      if (x >= 4 * (nbmax + 1) || (x & 3) != 2 || a.entries[x].x != -3) continue;
+      const int e = se[u] + a.local[x] + 1;
+      const int p = tc.leafpos(e);
+      if (p < 0 || __ldcg(a.wpos + p) > e) continue;
+      tb_put(tc, a.fd1, true, e, 2, e, FK_MIRROR, 0, e);
+    }
+  }
+  if (!a.jet) return;
+  if (!grid_barrier(t.bar, t.err)) return;
+  // phase 4: faces no entry writes still get the jet if their block is
+  // ever nbs; the interior of such a block always does
+  const int nl = sl[ntl];
+  for (int k = gtid; k < nl; k += gsz) {
+    const bool named = tb_span(a, __ldcg(a.leaves + k)).x > 0;
+    a.jetblk[k] = named;
+    if (!named) continue;
 #pragma unroll
-  for (int f = 0; f < 4; ++f) {
-    if ((a.fd1[(size_t)k * 4 + f].y & 0xff) == FK_KEEP) a.fd1[(size_t)k * 4 + f].y |= FD_DST_JET;
-    if ((a.fd2[(size_t)k * 4 + f].y & 0xff) == FK_KEEP) a.fd2[(size_t)k * 4 + f].y |= FD_DST_JET;
+    for (int f = 0; f < 4; ++f) {
+      int2 d1 = __ldcg(a.fd1 + (size_t)k * 4 + f), d2 = __ldcg(a.fd2 + (size_t)k * 4 + f);
+      if ((d1.y & 0xff) == FK_KEEP) a.fd1[(size_t)k * 4 + f].y = d1.y | FD_DST_JET;
+      if ((d2.y & 0xff) == FK_KEEP) a.fd2[(size_t)k * 4 + f].y = d2.y | FD_DST_JET;
+    }
   }
 }
 
-// ---- the leaf list from the leaf flags --------------------------------------
-// flag[1..n] -> the slots with flag 1 in ascending order (the order of the
-// reference's loops over nb with leaf(nb)), and their count
+// ---- the leaf flags of a list -------------------------------------------------
 
 __global__ void __launch_bounds__(kThreads) k_flag_leaves(const int* __restrict__ leaves, int nl, int* flag)
 {
@@ -429,48 +503,20 @@ __global__ void __launch_bounds__(kThreads) k_flag_leaves(const int* __restrict_
   if (k < nl) flag[leaves[k]] = 1;
 }
 
-__global__ void __launch_bounds__(kThreads) k_lscan_local(const int* __restrict__ flag, int n, int* local,
-                                                          int* ctatot)
+// ---- admesh flags in one launch ------------------------------------------------
+// The three flag planes and the list counters zeroed, markref with the
+// critneighup closure, then the refine list, critneighdown and the
+// coarsened families, with a barrier between the phases.
+__global__ void __launch_bounds__(kThreads) k_admesh_flags(MarkArgs a, size_t plane_words, unsigned int* bar)
 {
-  __shared__ int wsum[kThreads / 32];
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int c = (k < n) ? (flag[k + 1] != 0) : 0;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int x = c;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) wsum[w] = x;
-  __syncthreads();
-  if (w == 0) {
-    int v = lane < kThreads / 32 ? wsum[lane] : 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, v, o);
-      if (lane >= o) v += y;
-    }
-    if (lane < kThreads / 32) wsum[lane] = v;
-  }
-  __syncthreads();
-  if (k < n) local[k] = (w > 0 ? wsum[w - 1] : 0) + x - c;
-  if (threadIdx.x == kThreads - 1) ctatot[blockIdx.x] = wsum[kThreads / 32 - 1];
-}
-
-// also posof[1..n]: the leaf position of every leaf slot, -1 for the others
-__global__ void __launch_bounds__(kThreads) k_lcompact(const int* __restrict__ flag, int n,
-                                                       const int* __restrict__ local,
-                                                       const int* __restrict__ ctaoff, int* leaves, int* posof)
-{
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  int p = -1;
-  if (flag[k + 1]) {
-    p = ctaoff[k / kThreads] + local[k];
-    leaves[p] = k + 1;
-  }
-  posof[k + 1] = p;
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsz = gridDim.x * blockDim.x;
+  unsigned int* w = reinterpret_cast<unsigned int*>(a.leafp);   // leafp, up, down are contiguous
+  for (size_t k = gtid; k < 3 * plane_words; k += gsz) w[k] = 0u;
+  if (gtid < 4) a.counts[gtid] = 0;
+  if (!grid_barrier(bar, a.err)) return;
+  for (int k = gtid; k < a.nleaf; k += gsz) markref_up_one(a, k);
+  if (!grid_barrier(bar, a.err)) return;
+  for (int nb = 1 + gtid; nb <= a.nbmax; nb += gsz) refine_coarsen_one(a, nb);
 }
 
 inline int ctas(int n) { return (n + kThreads - 1) / kThreads; }
@@ -484,49 +530,62 @@ cudaError_t launch_flag_leaves(const int* leaves, int nl, int* flag, cudaStream_
   return cudaGetLastError();
 }
 
-cudaError_t launch_leaf_list(const int* flag, int nbmax, int* local, int* ctatot, int* ctaoff, int* leaves,
-                             int* nleaf, int* posof, cudaStream_t st)
+// CTAs of a cooperative launch of `kernel` with at most `smem` bytes of
+// dynamic shared memory that are resident at once on this device (0 on
+// failure).  The answer is kept per kernel, device and 4 KB step of smem.
+template <typename K>
+static int coop_capacity(K kernel, size_t smem, int (&cache)[8][41])
 {
-  if (nbmax <= 0) return cudaMemsetAsync(nleaf, 0, sizeof(int), st);
-  const int g = ctas(nbmax);
-  k_lscan_local<<<g, kThreads, 0, st>>>(flag, nbmax, local, ctatot);
-  PlanArgs a{};
-  a.ctatot = ctatot;
-  a.ctaoff = ctaoff;
-  a.total = nleaf;
-  k_bscan<<<1, 1024, 0, st>>>(a, g);
-  k_lcompact<<<g, kThreads, 0, st>>>(flag, nbmax, local, ctaoff, leaves, posof);
-  return cudaGetLastError();
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  const size_t step = (smem + 4095) / 4096;
+  if (dev < 0 || dev >= 8 || step > 40) return 0;
+  int& c = cache[dev][step];
+  if (c > 0) return c;
+  int nsm = 0, per = 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kThreads, step * 4096) != cudaSuccess) return 0;
+  c = per * nsm;
+  return c;
 }
 
-int plan_ctas(int nleaf) { return ctas(nleaf); }
-
-cudaError_t launch_locatebounds(const PlanArgs& a, bool posof_ready, cudaStream_t st)
+cudaError_t launch_tree_build(const TreeArgs& t, cudaStream_t st)
 {
-  if (a.nleaf <= 0) return cudaSuccess;
-  const int g = ctas(a.nleaf), g4 = ctas(4 * a.nleaf);
-  if (!posof_ready) k_posof<<<g, kThreads, 0, st>>>(a);
-  k_bcount<<<g4, kThreads, 0, st>>>(a);
-  k_bscan<<<1, 1024, 0, st>>>(a, g4);
-  if (a.jet) k_bspan<<<ctas(a.nbmax), kThreads, 0, st>>>(a);
-  k_bplan<<<g4, kThreads, 0, st>>>(a);
-  if (a.f6b && a.bc[2] != W2D_BC_REFLECTIVE) k_bplan_f6b<<<g, kThreads, 0, st>>>(a);
-  if (a.jet) k_bplan_jet<<<g, kThreads, 0, st>>>(a);
-  return cudaGetLastError();
+  const int nbmax = t.p.nbmax;
+  if (nbmax <= 0) return cudaMemsetAsync(t.nleaf_dev, 0, sizeof(int), st);
+  const int ntl = (nbmax + 1 + kThreads - 1) / kThreads;
+  const int nte = t.plans ? (4 * (nbmax + 1) + kThreads - 1) / kThreads : 0;
+  const size_t smem = sizeof(int) * (size_t)(nte + ntl + 2);
+  static bool opted = false;
+  if (smem > 48 * 1024 && !opted) {
+    cudaError_t e = cudaFuncSetAttribute(k_tree_build, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    if (e != cudaSuccess) return e;
+    opted = true;
+  }
+  if (smem > 160 * 1024) return cudaErrorInvalidValue;
+  static int cache[8][41] = {};
+  const int cap = coop_capacity(k_tree_build, smem, cache);
+  if (cap <= 0) return cudaErrorLaunchOutOfResources;
+  const int grid = std::min(nte + ntl, cap);
+  TreeArgs targ = t;
+  int nte_a = nte, ntl_a = ntl;
+  void* args[] = {&targ, &nte_a, &ntl_a};
+  return cudaLaunchCooperativeKernel((const void*)k_tree_build, dim3(grid), dim3(kThreads), args, smem, st);
 }
 
-cudaError_t launch_markref_up(const MarkArgs& a, cudaStream_t st)
+cudaError_t launch_admesh_flags(const MarkArgs& a, size_t plane_bytes, unsigned int* bar, cudaStream_t st)
 {
-  if (a.nleaf <= 0) return cudaSuccess;
-  k_markref_up<<<ctas(a.nleaf), kThreads, 0, st>>>(a);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_refine_coarsen(const MarkArgs& a, cudaStream_t st)
-{
-  if (a.nbmax <= 0) return cudaSuccess;
-  k_refine_coarsen<<<ctas(a.nbmax), kThreads, 0, st>>>(a);
-  return cudaGetLastError();
+  const size_t words = plane_bytes / 4;
+  const int want = std::max(ctas(std::max(a.nleaf, a.nbmax)), 1);
+  static int cache[8][41] = {};
+  const int cap = coop_capacity(k_admesh_flags, 0, cache);
+  if (cap <= 0) return cudaErrorLaunchOutOfResources;
+  const int grid = std::min(want, cap);
+  MarkArgs marg = a;
+  size_t w = words;
+  unsigned int* b = bar;
+  void* args[] = {&marg, &w, &b};
+  return cudaLaunchCooperativeKernel((const void*)k_admesh_flags, dim3(grid), dim3(kThreads), args, 0, st);
 }
 
 cudaError_t launch_set_links(const int* rows7, int n, int4* links, int2* sons, cudaStream_t st)
