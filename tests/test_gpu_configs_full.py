@@ -11,8 +11,10 @@ and configuration 4 (planar jet with coolingdmc, 32x8 roots, 7 levels) run
 their plain FP64 path from the initial conditions against the oracle, with
 the same block tree at every check and each conserved field within a
 relative L1 of COOL_RTOL (the cooling routines use CUDA's exp, pow, log and
-log10 where the oracle uses glibc's; the adiabatic path is exact).  The
-measured figures go to W2D_PARITY_LOG when it is set.
+log10 where the oracle uses glibc's; the adiabatic path is exact).  Both
+are also checked at their developed states (about 5.6k and 11k leaves),
+warm-started on both sides from the reference's BIN files of a device run.
+The measured figures go to W2D_PARITY_LOG when it is set.
 """
 import os
 
@@ -98,4 +100,54 @@ def test_config_cooling_fp64_vs_oracle(oracle_lib, name, nsteps, every):
             record(name, step, l1, dmax, n, leaves=int(o.leaves().size), dt_rel=abs(dtd - dto) / dto)
             worst = max(worst, float(np.max(l1)))
             assert np.all(l1 <= COOL_RTOL), (step, l1, dmax, n)
+    assert worst >= 0.0
+
+
+# the developed states of the bench (leaves after the steps from the initial
+# conditions: the remnant ~5.6k, the jet ~11k, inside the 10k-20k blocks of
+# configuration 4)
+@pytest.mark.parametrize("name,pre,nsteps,cap", [("snr", 4000, 30, 100000), ("jet_dmc", 15000, 30, 60000)])
+def test_developed_state_fp64_vs_oracle(oracle_lib, tmp_path, name, pre, nsteps, cap):
+    """The device advances the configuration from its initial conditions to
+    its developed state and writes the reference's BIN files
+    (src/output.f90:39-67); the oracle and a fresh device run both warm
+    start from them (src/basegrid.f90:167-251) and take the main loop side
+    by side: same tree, dt every step, each field within COOL_RTOL."""
+    from walicxe2d_b200.api import Simulation
+    p, ic = config(name)
+    p.nblocks = cap
+    table = p.cooling == 2
+
+    def device():
+        s = Simulation(p, ic)
+        if table:
+            s.set_cooltab(*_dmc_table())
+        s.ctx.set_graphs(True)
+        return s
+
+    a = device()
+    a.run(pre)
+    files = (str(tmp_path / "pointers.bin"), str(tmp_path / "blocks.bin"))
+    a.write_bin(*files)
+    t0 = a.status()["time"]
+    a.close()
+    o = oracle_lib.Oracle(p, ic, threads=THREADS)
+    if table:
+        o.set_cooltab(*_dmc_table())
+    o.read_bin(*files, t0)
+    s = device()
+    s.read_bin(*files, time=t0)
+    _check_tree(o, s)
+    nleaf = int(o.leaves().size)
+    worst = 0.0
+    for step in range(1, nsteps + 1):
+        dto = o.run(1)
+        s.run(1)
+        dtd = s.status()["dt"]
+        assert abs(dtd - dto) <= COOL_RTOL * dto, (step, dtd, dto)
+    _check_tree(o, s)
+    dmax, l1, n = _state(o, s)
+    record(name + "_developed", nsteps, l1, dmax, n, leaves=nleaf, pre_steps=pre)
+    worst = float(np.max(l1))
+    assert np.all(l1 <= COOL_RTOL), (l1, dmax, n)
     assert worst >= 0.0

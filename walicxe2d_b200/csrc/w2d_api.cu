@@ -290,8 +290,9 @@ int check_device(W2dCtx* c)
                                                  : "device error");
     c->h_err[0] = 0;
     cudaMemsetAsync(c->d_err, 0, 4 * sizeof(int), c->st);
-    // a grid barrier that ran out left its words behind
+    // a grid barrier that ran out left its count behind
     if (c->d_gbar) cudaMemsetAsync(c->d_gbar, 0, 2 * sizeof(unsigned int), c->st);
+    c->gbar_count = 0;
     return rc;
   }
   return W2D_OK;
@@ -855,7 +856,12 @@ TreeArgs tree_args(W2dCtx* c, bool plans)
   t.nleaf_dev = c->d_nleaf;
   t.plans = plans ? 1 : 0;
   t.bar = c->d_gbar;
+  t.bar_base = c->gbar_count;
   t.err = c->d_err;
+  t.rows7 = c->d_rows7;
+  t.nrows = plans ? c->tree_rows : 0;
+  t.links = c->d_links;
+  t.sons = c->d_sons;
   return t;
 }
 }  // namespace
@@ -875,7 +881,12 @@ int ctx_topology_device(W2dCtx* c, int nbmax, int nleaf)
   c->nbmax = nbmax;
   c->nleaf = nleaf;
   TreeArgs t = tree_args(c, false);
-  if ((rc = launch(c, "leaf_list", [&] { return launch_tree_build(t, c->st); }))) return rc;
+  if ((rc = launch(c, "leaf_list", [&] {
+    unsigned int n = 0;
+    const cudaError_t e = launch_tree_build(t, &n, c->st);
+    c->gbar_count += n;
+    return e;
+  }))) return rc;
   c->host_leaves_stale = true;
   c->leaves_dirty = false;
   c->have_bounds = false;
@@ -894,7 +905,12 @@ int ctx_tree_device(W2dCtx* c, int nbmax, int nleaf)
   c->nbmax = nbmax;
   c->nleaf = nleaf;
   TreeArgs t = tree_args(c, true);
-  if ((rc = launch(c, "tree_build", [&] { return launch_tree_build(t, c->st); }))) return rc;
+  if ((rc = launch(c, "tree_build", [&] {
+    unsigned int n = 0;
+    const cudaError_t e = launch_tree_build(t, &n, c->st);
+    c->gbar_count += n;
+    return e;
+  }))) return rc;
   c->host_leaves_stale = true;
   c->leaves_dirty = false;
   c->have_bounds = true;
@@ -1188,6 +1204,63 @@ int ensure_plan(W2dCtx* c)
 
 }  // namespace
 
+}  // extern "C"
+
+// Validates rows k0 .. k0+m-1 of the list (or blocks k0+1 .. k0+m) of lp and
+// writes them, 7 ints each, into the pinned staging and sends them to d_rows7
+// (after the previous send has left the staging).
+static int stage_link_rows(W2dCtx* c, const int32_t* lp, int row_stride, int col_stride, const int32_t* rows,
+                           int k0, int m)
+{
+  CK(cudaEventSynchronize(c->ev_links));
+  int* h = c->h_rows7;
+  for (int k = 0; k < m; ++k) {
+    const int nb = rows ? rows[k0 + k] : k0 + k + 1;
+    if (nb < 1 || nb > c->cap)
+      return set_error(c, W2D_ERR_ARG, nb, 0, 0, "block ID %d outside 1..%d", nb, c->cap);
+    const int32_t* r = lp + (size_t)(nb - 1) * row_stride;
+    int* o = h + 7 * (size_t)k;
+    o[0] = nb;
+    o[1] = r[(size_t)2 * col_stride];    // first son (0: none yet)
+    o[2] = r[(size_t)3 * col_stride];    // son position
+    if (o[1] < 0 || o[1] > c->cap - 3)
+      return set_error(c, W2D_ERR_ARG, nb, 3, 0, "lp(%d,3) = %d: no four sons fit in the pool", nb, o[1]);
+    for (int s = 0; s < 4; ++s) {
+      const int v = r[(size_t)(4 + s) * col_stride];
+      if (v != -1 && (v < 1 || v > c->cap))
+        return set_error(c, W2D_ERR_ARG, nb, 5 + s, 0, "lp(%d,%d) = %d is no block of the pool", nb, 5 + s, v);
+      o[3 + s] = v;
+    }
+  }
+  CK(cudaMemcpyAsync(c->d_rows7, h, sizeof(int) * 7 * (size_t)m, cudaMemcpyHostToDevice, c->st));
+  return W2D_OK;
+}
+
+// The tree's changed lp rows, the leaf list and the fill plans in one
+// launch: the rows staged here are applied by the tree build's first phase.
+// More rows than the staging holds go through w2d_set_links first.
+int ctx_tree_device_rows(W2dCtx* c, const int32_t* lp, int row_stride, int col_stride, const int32_t* rows,
+                         int nrows, int nbmax, int nleaf)
+{
+  if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
+  int rc = ensure_mark(c);
+  if (rc) return rc;
+  if (nrows > c->cap + 1) {
+    if ((rc = w2d_set_links(c, lp, row_stride, col_stride, rows, nrows))) return rc;
+    nrows = 0;
+  } else if (nrows > 0 && (rc = stage_link_rows(c, lp, row_stride, col_stride, rows, 0, nrows))) {
+    return rc;
+  }
+  c->have_links = true;
+  c->tree_rows = nrows;
+  rc = ctx_tree_device(c, nbmax, nleaf);
+  c->tree_rows = 0;
+  if (nrows > 0) CK(cudaEventRecord(c->ev_links, c->st));
+  return rc;
+}
+
+extern "C" {
+
 int w2d_set_links(W2dCtx* c, const int32_t* lp, int row_stride, int col_stride, const int32_t* rows, int nrows)
 {
   if (!c || !lp || (rows && nrows < 0) || (!rows && nrows != 0)) return W2D_ERR_ARG;
@@ -1198,27 +1271,7 @@ int w2d_set_links(W2dCtx* c, const int32_t* lp, int row_stride, int col_stride, 
   const int chunk = c->cap + 1;
   for (int k0 = 0; k0 < n; k0 += chunk) {
     const int m = std::min(chunk, n - k0);
-    CK(cudaEventSynchronize(c->ev_links));   // the previous chunk has left the staging
-    int* h = c->h_rows7;
-    for (int k = 0; k < m; ++k) {
-      const int nb = rows ? rows[k0 + k] : k0 + k + 1;
-      if (nb < 1 || nb > c->cap)
-        return set_error(c, W2D_ERR_ARG, nb, 0, 0, "block ID %d outside 1..%d", nb, c->cap);
-      const int32_t* r = lp + (size_t)(nb - 1) * row_stride;
-      int* o = h + 7 * (size_t)k;
-      o[0] = nb;
-      o[1] = r[(size_t)2 * col_stride];    // first son (0: none yet)
-      o[2] = r[(size_t)3 * col_stride];    // son position
-      if (o[1] < 0 || o[1] > c->cap - 3)
-        return set_error(c, W2D_ERR_ARG, nb, 3, 0, "lp(%d,3) = %d: no four sons fit in the pool", nb, o[1]);
-      for (int s = 0; s < 4; ++s) {
-        const int v = r[(size_t)(4 + s) * col_stride];
-        if (v != -1 && (v < 1 || v > c->cap))
-          return set_error(c, W2D_ERR_ARG, nb, 5 + s, 0, "lp(%d,%d) = %d is no block of the pool", nb, 5 + s, v);
-        o[3 + s] = v;
-      }
-    }
-    CK(cudaMemcpyAsync(c->d_rows7, h, sizeof(int) * 7 * (size_t)m, cudaMemcpyHostToDevice, c->st));
+    if ((rc = stage_link_rows(c, lp, row_stride, col_stride, rows, k0, m))) return rc;
     if ((rc = launch(c, "set_links", [&] { return launch_set_links(c->d_rows7, m, c->d_links, c->d_sons, c->st); })))
       return rc;
     CK(cudaEventRecord(c->ev_links, c->st));
@@ -1262,7 +1315,12 @@ int w2d_admesh_flags(W2dCtx* c, int32_t* refine, int cap_refine, int* nrefine, i
   a.err = c->d_err;
   // the planes and counters zeroed, markref + critneighup, then the refine
   // list, critneighdown and the coarsened families: one launch
-  int rc = launch(c, "admesh_flags", [&] { return launch_admesh_flags(a, plane, c->d_gbar, c->st); });
+  int rc = launch(c, "admesh_flags", [&] {
+    unsigned int n = 0;
+    const cudaError_t e = launch_admesh_flags(a, plane, c->d_gbar, c->gbar_count, &n, c->st);
+    c->gbar_count += n;
+    return e;
+  });
   if (rc) return rc;
   // the counters and the heads of both lists in one wait; longer lists
   // (rare: a pass that remeshes thousands of blocks) in a second one

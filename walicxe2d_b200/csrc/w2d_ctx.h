@@ -122,9 +122,11 @@ struct W2dCtx {
   int* d_lrank = nullptr;     // per slot
   int* d_bcta = nullptr;      // tile counts (entry tiles, then slot tiles), the list length at bcta_half(c) * 2
   int* d_wpos = nullptr;
-  // the two words of the grid barrier of the cooperative tree kernels
-  // (count, generation); zero between launches, reset after a device error
+  // the arrival count of the grid barriers of the cooperative tree kernels
+  // and the host's copy of it (both reset after a device error)
   unsigned int* d_gbar = nullptr;
+  unsigned int gbar_count = 0;
+  int tree_rows = 0;   // lp rows staged in d_rows7 for the next tree build to apply
   cudaEvent_t ev_links = nullptr;
   bool have_links = false;
   // pinned staging of refine/coarse lists

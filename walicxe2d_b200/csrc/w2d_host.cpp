@@ -342,9 +342,17 @@ int push_tree(W2dSim* s, bool* planned)
 {
   *planned = false;
   if (s->devplans && s->topo_dev_ok) {
-    int rc = push_links(s);
+    // the changed lp rows (all of them after a side switch), listed by ID
+    // and applied by the same launch
+    if (s->links_all) {
+      s->touched.resize((size_t)s->nbmax);
+      for (int nb = 1; nb <= s->nbmax; ++nb) s->touched[(size_t)nb - 1] = nb;
+    }
+    int rc = ctx_tree_device_rows(s->ctx, s->lp.data() + 8, 8, 1, s->touched.data(), (int)s->touched.size(),
+                                  s->nbmax, s->nbleafs);
     if (rc) return rc;
-    if ((rc = ctx_tree_device(s->ctx, s->nbmax, s->nbleafs))) return rc;
+    s->links_all = false;
+    s->touched.clear();
     s->dirty = false;
     s->ib_stale = true;
     *planned = true;

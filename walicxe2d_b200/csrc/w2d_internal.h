@@ -34,6 +34,10 @@ int ensure_leaf_list(W2dCtx* c);
 // the leaf list and the fill plans (w2d_locate_bounds) in one launch, from
 // the leaf flags and the lp(:,3:8) mirror (nbmax and the leaf count given)
 int ctx_tree_device(W2dCtx* c, int nbmax, int nleaf);
+// the same with the changed rows of lp (as w2d_set_links takes them) applied
+// in the same launch
+int ctx_tree_device_rows(W2dCtx* c, const int32_t* lp, int row_stride, int col_stride, const int32_t* rows,
+                         int nrows, int nbmax, int nleaf);
 
 // ---- ensembles: runs share one context; run r owns slots base[r]+1 ..
 // base[r]+cap[r] and numbers its blocks 1..cap[r] as a single run does.

@@ -67,8 +67,11 @@ struct MarkArgs {
 };
 // the flag planes and counts zeroed, markref with the whole critneighup
 // cascade, then the refine list, critneighdown and the coarsened families:
-// one cooperative launch (bar: the context's two grid-barrier words, zero)
-cudaError_t launch_admesh_flags(const MarkArgs& a, size_t plane_bytes, unsigned int* bar, cudaStream_t st);
+// one cooperative launch
+// bar_base: the barrier count when the launch begins; *arrivals: the count
+// it adds (the host keeps the running count)
+cudaError_t launch_admesh_flags(const MarkArgs& a, size_t plane_bytes, unsigned int* bar, unsigned int bar_base,
+                                unsigned int* arrivals, cudaStream_t st);
 // rows7: (nb, lp(nb,3), lp(nb,4), lp(nb,5..8)) per row
 cudaError_t launch_set_links(const int* rows7, int n, int4* links, int2* sons, cudaStream_t st);
 
@@ -96,7 +99,7 @@ struct PlanArgs {
 };
 // The leaf list from the leaf flags (ascending ID) with every slot's leaf
 // position and the leaf count, and with plans != 0 locatebounds and the
-// plans too: one cooperative launch (bar: the two grid-barrier words, zero).
+// plans too: one cooperative launch.
 struct TreeArgs {
   PlanArgs p;
   const int* flag;       // per slot: 1 for a leaf
@@ -104,12 +107,20 @@ struct TreeArgs {
   int* tcnt;             // per tile: entry tiles, then slot tiles
   int* nleaf_dev;        // the leaf count
   int plans;
-  unsigned int* bar;
+  unsigned int* bar;     // the grid-barrier count ...
+  unsigned int bar_base; // ... when the launch begins
   int* err;
+  // lp rows to apply first (7 ints each, as w2d_set_links sends them): the
+  // mirror's links and sons of those blocks
+  const int* rows7;
+  int nrows;
+  int4* links;
+  int2* sons;
 };
 // tiles of 256 a tree build over slots 1..nbmax uses (entries and slots)
 inline int tree_tiles(int nbmax) { return (4 * (nbmax + 1) + 255) / 256 + (nbmax + 1 + 255) / 256; }
-cudaError_t launch_tree_build(const TreeArgs& t, cudaStream_t st);
+// *arrivals: what the launch adds to the grid-barrier count
+cudaError_t launch_tree_build(const TreeArgs& t, unsigned int* arrivals, cudaStream_t st);
 
 // flag[leaves[k]] = 1 for k < nl (flag zeroed before)
 cudaError_t launch_flag_leaves(const int* leaves, int nl, int* flag, cudaStream_t st);

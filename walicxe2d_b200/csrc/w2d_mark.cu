@@ -92,20 +92,25 @@ __device__ __forceinline__ bool refined_now(const MarkArgs& a, int nb)
 // (src/updatelpup.f90:20-175 redirects the finer neighbours).
 __device__ __forceinline__ bool down_after(const MarkArgs& a, int nb)
 {
-  if (!__ldcg(a.down + nb) || refined_now(a, nb)) return false;
+  // every load first (a neighbour -1 or outside the pool reads nb's own
+  // entries, unused), then the rule: a neighbour passes if it is none, or
+  // a refined coarser block, or a leaf that is not refined
   const int l = a.lev[nb];
+  const bool ok0 = __ldcg(a.down + nb) != 0 && !refined_now(a, nb);
   const int4 q = a.links[nb];
   const int n[4] = {q.x, q.y, q.z, q.w};
+  bool ok = ok0;
 #pragma unroll
   for (int s = 0; s < 4; ++s) {
     const int n1 = n[s];
-    if (n1 == -1) continue;
-    if (!in_pool(n1, a.cap)) return false;
-    const bool r1 = refined_now(a, n1);
-    if (r1 && a.lev[n1] < l) continue;       // now points to a new son
-    if (!__ldcg(a.leafp + n1) || r1) return false;
+    const bool inp = in_pool(n1, a.cap);
+    const int m = inp ? n1 : nb;
+    const int lm = a.lev[m];
+    const bool r1 = __ldcg(a.up + m) != 0 && lm >= 1 && lm <= a.nlevs - 1;
+    const bool leafm = __ldcg(a.leafp + m) != 0;
+    ok = ok && (n1 == -1 || (inp && ((r1 && lm < l) || (leafm && !r1))));
   }
-  return true;
+  return ok;
 }
 
 // The refine list, and the families the pass coarsens (src/admesh.f90:
@@ -128,7 +133,10 @@ __device__ void refine_coarsen_one(const MarkArgs& a, int nb)
   if (!in_pool(s2, a.cap) || !in_pool(s3, a.cap)) return;
   const int s4 = a.links[s2].w;
   if (!in_pool(s4, a.cap)) return;
-  if (down_after(a, nb) && down_after(a, s2) && down_after(a, s3) && down_after(a, s4)) {
+  // the four members evaluated side by side (their loads overlap), not as a
+  // chain of short-circuits
+  const bool d1 = down_after(a, nb), d2 = down_after(a, s2), d3 = down_after(a, s3), d4 = down_after(a, s4);
+  if (d1 && d2 && d3 && d4) {
     const int k = atomicAdd(&a.counts[1], 1);
     if (k < a.cap) a.clist[k] = nb;
   }
@@ -149,39 +157,44 @@ __global__ void __launch_bounds__(kThreads) k_set_links(const int* __restrict__ 
 
 // ---- bounded grid barrier of the one-launch kernels ------------------------
 // The tree kernels below run as cooperative launches (every CTA resident at
-// once) and separate their phases with this barrier.  bar[0] counts the
-// CTAs that have arrived, bar[1] is the generation: the last CTA to arrive
-// resets the count and moves the generation, the others wait for it to
-// move.  The wait is bounded (2^22 polls, about a second): a barrier that
-// runs out records W2D_ERR_TIMEOUT and returns false, the CTA leaves the
-// kernel, and the host resets both words before its next launch.  Data
-// that other CTAs wrote before a barrier is read after it with __ldcg (from
-// L2), never from a line this SM's L1 may hold.
+// once) and separate their phases with this barrier.  bar[0] counts
+// arrivals over the context's life: the host keeps its own copy of the
+// count (it knows every launch's grid size and number of barriers), passes
+// it in as the launch's base, and the k-th barrier of a launch of G CTAs
+// is passed once the count reaches base + k G; one atomic per CTA and
+// barrier, nothing to reset between barriers or launches.  The wait is
+// bounded (2^22 polls, about a second): a barrier that runs out records
+// W2D_ERR_TIMEOUT and returns false, the CTA leaves the kernel, and the host
+// resets the count (and its copy) when it reports the error.  Data other
+// CTAs wrote before a barrier is read after it with __ldcg (from L2), never
+// from a line this SM's L1 may hold.
 constexpr long kBarPolls = 1L << 22;
 
-__device__ bool grid_barrier(unsigned int* bar, int* err)
+struct GridBar {
+  unsigned int* count;
+  unsigned int base;   // the count when the launch began
+  int* err;
+};
+
+// the k-th barrier of the launch (k = 1, 2, ...)
+__device__ bool grid_barrier(const GridBar& g, int k)
 {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int* gen = bar + 1;
-    const unsigned int g0 = *gen;
     __threadfence();
+    atomicAdd(g.count, 1u);
+    const unsigned int target = g.base + (unsigned int)k * gridDim.x;
+    volatile unsigned int* cnt = g.count;
     int good = 1;
-    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      long polls = 0;
-      while (*gen == g0) {
-        if (++polls > kBarPolls) {
-          set_err(err, W2D_ERR_TIMEOUT, 0, -1, -1);
-          good = 0;
-          break;
-        }
-        __nanosleep(32);
+    long polls = 0;
+    while ((int)(*cnt - target) < 0) {   // (wraps around safely)
+      if (++polls > kBarPolls) {
+        set_err(g.err, W2D_ERR_TIMEOUT, 0, -1, -1);
+        good = 0;
+        break;
       }
+      __nanosleep(32);
     }
     __threadfence();
     ok = good;
@@ -275,14 +288,14 @@ struct TreeCtx {
 __device__ __forceinline__ int2 tb_entry(const TreeArgs& t, int nb, int s)
 {
   const PlanArgs& a = t.p;
-  const int4 q = a.links[nb];
+  const int4 q = __ldcg(a.links + nb);     // (phase 0 may have written it)
   const int m = s == 0 ? q.x : s == 1 ? q.y : s == 2 ? q.z : q.w;
   if (m == -1) return make_int2(-(s + 1), 0);
   if (!in_pool(m, a.cap) || m > a.nbmax) return make_int2(0, 0);
   if (a.lev[m] < a.lev[nb]) return make_int2(0, 0);          // coarser: its entry
   if (t.flag[m])                                              // same-level leaf
     return nb < m ? make_int2(1 + 3 * s, m) : make_int2(0, 0);
-  const int f = a.sons[m].x;                                  // same level, has sons
+  const int f = __ldcg(a.sons + m).x;                        // same level, has sons
   if (f < 1 || f + 3 > a.nbmax) return make_int2(0, 0);
   const int son_off = (s == 0) ? 1 : (s == 2) ? 2 : 0;
   return make_int2(2 + 3 * s, f + son_off);
@@ -295,13 +308,13 @@ __device__ __forceinline__ int2 tb_span(const PlanArgs& a, int b)
   return __ldcg(a.span + b);
 }
 
-// put() of the host walk: one face descriptor of a leaf target, with the
-// jet flags for entry position e
-__device__ __forceinline__ void tb_put(const TreeCtx& tc, int2* fd, bool is_fd1, int blk, int face, int nbr,
+// put() of the host walk: one face descriptor of leaf target blk at leaf
+// position p (< 0: not a leaf, nothing written), with the jet flags for
+// entry position e
+__device__ __forceinline__ void tb_put(const TreeCtx& tc, int2* fd, bool is_fd1, int blk, int p, int face, int nbr,
                                        int kind, int off, int e)
 {
   const PlanArgs& a = tc.t.p;
-  const int p = tc.leafpos(blk);
   if (p < 0) return;                       // non-leaf targets are rewritten before being read
   int y = kind | (off << 8);
   if (a.jet) {
@@ -319,54 +332,59 @@ __device__ __forceinline__ void tb_put(const TreeCtx& tc, int2* fd, bool is_fd1,
 }
 
 // every entry at its list position (the OUTFYB bottom-face writes of
-// boundaryI come after the next barrier)
+// boundaryI come after the next barrier); the leaf positions of the
+// entry's targets are looked up together, before any write
 __device__ __forceinline__ void tb_plan(const TreeCtx& tc, int x, int2 en, int e)
 {
   const PlanArgs& a = tc.t.p;
   const int nbs = x >> 2;
   const int n1 = en.y;
   const int H = W2D_NX / 2;
-  auto both = [&](int blk, int face, int nbr, int kind, int off) {
-    tb_put(tc, a.fd1, true, blk, face, nbr, kind, off, e);
-    tb_put(tc, a.fd2, false, blk, face, nbr, kind, off, e);
+  const int t2 = (en.x == 2 || en.x == 5) ? n1 + 2 : n1 + 1;   // the second son of a restriction
+  const int pn = tc.leafpos(nbs);
+  const int p1 = en.x > 0 ? tc.leafpos(n1) : -1;
+  const int p2 = (en.x == 2 || en.x == 5 || en.x == 8 || en.x == 11) ? tc.leafpos(t2) : -1;
+  auto both = [&](int blk, int p, int face, int nbr, int kind, int off) {
+    tb_put(tc, a.fd1, true, blk, p, face, nbr, kind, off, e);
+    tb_put(tc, a.fd2, false, blk, p, face, nbr, kind, off, e);
   };
   switch (en.x) {
     case -1: case -2: case -4: {
       const int f = (en.x == -1) ? 0 : (en.x == -2) ? 1 : 3;
-      both(nbs, f, nbs, a.bc[f] == W2D_BC_REFLECTIVE ? FK_REFLECT : FK_MIRROR, 0);
+      both(nbs, pn, f, nbs, a.bc[f] == W2D_BC_REFLECTIVE ? FK_REFLECT : FK_MIRROR, 0);
       break;
     }
     case -3:
       if (a.bc[2] == W2D_BC_REFLECTIVE) {
-        both(nbs, 2, nbs, FK_REFLECT, 0);
+        both(nbs, pn, 2, nbs, FK_REFLECT, 0);
       } else {
-        tb_put(tc, a.fd2, false, nbs, 2, nbs, FK_MIRROR, 0, e);
-        if (!a.f6b) tb_put(tc, a.fd1, true, nbs, 2, nbs, FK_MIRROR, 0, e);
+        tb_put(tc, a.fd2, false, nbs, pn, 2, nbs, FK_MIRROR, 0, e);
+        if (!a.f6b) tb_put(tc, a.fd1, true, nbs, pn, 2, nbs, FK_MIRROR, 0, e);
       }
       break;
-    case 1:  both(nbs, 0, n1, FK_SAME, 0);  both(n1, 1, nbs, FK_SAME, 0); break;
-    case 4:  both(nbs, 1, n1, FK_SAME, 0);  both(n1, 0, nbs, FK_SAME, 0); break;
-    case 7:  both(nbs, 2, n1, FK_SAME, 0);  both(n1, 3, nbs, FK_SAME, 0); break;
-    case 10: both(nbs, 3, n1, FK_SAME, 0);  both(n1, 2, nbs, FK_SAME, 0); break;
+    case 1:  both(nbs, pn, 0, n1, FK_SAME, 0);  both(n1, p1, 1, nbs, FK_SAME, 0); break;
+    case 4:  both(nbs, pn, 1, n1, FK_SAME, 0);  both(n1, p1, 0, nbs, FK_SAME, 0); break;
+    case 7:  both(nbs, pn, 2, n1, FK_SAME, 0);  both(n1, p1, 3, nbs, FK_SAME, 0); break;
+    case 10: both(nbs, pn, 3, n1, FK_SAME, 0);  both(n1, p1, 2, nbs, FK_SAME, 0); break;
     case 2:
-      both(nbs, 0, n1, FK_RESTRICT, 0);
-      both(n1, 1, nbs, FK_INJECT, 0);
-      both(n1 + 2, 1, nbs, FK_INJECT, H);
+      both(nbs, pn, 0, n1, FK_RESTRICT, 0);
+      both(n1, p1, 1, nbs, FK_INJECT, 0);
+      both(t2, p2, 1, nbs, FK_INJECT, H);
       break;
     case 5:
-      both(nbs, 1, n1, FK_RESTRICT, 0);
-      both(n1, 0, nbs, FK_INJECT, 0);
-      both(n1 + 2, 0, nbs, FK_INJECT, H);
+      both(nbs, pn, 1, n1, FK_RESTRICT, 0);
+      both(n1, p1, 0, nbs, FK_INJECT, 0);
+      both(t2, p2, 0, nbs, FK_INJECT, H);
       break;
     case 8:
-      both(nbs, 2, n1, FK_RESTRICT, 0);
-      both(n1, 3, nbs, FK_INJECT, 0);
-      both(n1 + 1, 3, nbs, FK_INJECT, H);
+      both(nbs, pn, 2, n1, FK_RESTRICT, 0);
+      both(n1, p1, 3, nbs, FK_INJECT, 0);
+      both(t2, p2, 3, nbs, FK_INJECT, H);
       break;
     default:   // 11
-      both(nbs, 3, n1, FK_RESTRICT, 0);
-      both(n1, 2, nbs, FK_INJECT, 0);
-      both(n1 + 1, 2, nbs, FK_INJECT, H);
+      both(nbs, pn, 3, n1, FK_RESTRICT, 0);
+      both(n1, p1, 2, nbs, FK_INJECT, 0);
+      both(t2, p2, 2, nbs, FK_INJECT, H);
       break;
   }
 }
@@ -388,6 +406,18 @@ __global__ void __launch_bounds__(kThreads) k_tree_build(TreeArgs t, int nte, in
   const int nbmax = a.nbmax;
   const int tid = threadIdx.x;
   const int gtid = blockIdx.x * blockDim.x + tid, gsz = gridDim.x * blockDim.x;
+  // phase 0: the lp rows the host changed, into the mirror
+  const GridBar gb{t.bar, t.bar_base, t.err};
+  int nbar = 0;
+  if (t.nrows > 0) {
+    for (int k = gtid; k < t.nrows; k += gsz) {
+      const int* r = t.rows7 + 7 * (size_t)k;
+      const int nb = r[0];
+      t.sons[nb] = make_int2(r[1], r[2]);
+      t.links[nb] = make_int4(r[3], r[4], r[5], r[6]);
+    }
+    if (!grid_barrier(gb, ++nbar)) return;
+  }
   // phase 1: entries and their ranks within the entry tiles; leaf ranks
   // within the slot tiles; the plans cleared (FK_KEEP) for every position
   // a leaf may take
@@ -419,7 +449,7 @@ __global__ void __launch_bounds__(kThreads) k_tree_build(TreeArgs t, int nte, in
     }
     for (int k = gtid; k < nbmax; k += gsz) a.wpos[k] = 0;
   }
-  if (!grid_barrier(t.bar, t.err)) return;
+  if (!grid_barrier(gb, ++nbar)) return;
   // phase 2: offsets of every tile; the list and the positions
   cta_scan_counts(t.tcnt, nte, se);
   cta_scan_counts(t.tcnt + nte, ntl, sl);
@@ -453,7 +483,7 @@ __global__ void __launch_bounds__(kThreads) k_tree_build(TreeArgs t, int nte, in
       }
       a.span[nb] = sp;
     }
-    if (!grid_barrier(t.bar, t.err)) return;
+    if (!grid_barrier(gb, ++nbar)) return;
   }
   for (int u = blockIdx.x; u < nte; u += gridDim.x) {
     const int x = 256 * u + tid;
@@ -463,7 +493,7 @@ __global__ void __launch_bounds__(kThreads) k_tree_build(TreeArgs t, int nte, in
   }
   const bool f6b = a.f6b && a.bc[2] != W2D_BC_REFLECTIVE;
   if (!f6b && !a.jet) return;
-  if (!grid_barrier(t.bar, t.err)) return;
+  if (!grid_barrier(gb, ++nbar)) return;
   // phase 3, src/boundaryI.f90:87 (OUTFYB): the bottom-wall entry at list
   // position e fills the bottom face of block e; it wins over the face's
   // own writer when it comes later in the list
@@ -474,11 +504,11 @@ __global__ void __launch_bounds__(kThreads) k_tree_build(TreeArgs t, int nte, in
       const int e = se[u] + a.local[x] + 1;
       const int p = tc.leafpos(e);
       if (p < 0 || __ldcg(a.wpos + p) > e) continue;
-      tb_put(tc, a.fd1, true, e, 2, e, FK_MIRROR, 0, e);
+      tb_put(tc, a.fd1, true, e, p, 2, e, FK_MIRROR, 0, e);
     }
   }
   if (!a.jet) return;
-  if (!grid_barrier(t.bar, t.err)) return;
+  if (!grid_barrier(gb, ++nbar)) return;
   // phase 4: faces no entry writes still get the jet if their block is
   // ever nbs; the interior of such a block always does
   const int nl = sl[ntl];
@@ -507,15 +537,17 @@ __global__ void __launch_bounds__(kThreads) k_flag_leaves(const int* __restrict_
 // The three flag planes and the list counters zeroed, markref with the
 // critneighup closure, then the refine list, critneighdown and the
 // coarsened families, with a barrier between the phases.
-__global__ void __launch_bounds__(kThreads) k_admesh_flags(MarkArgs a, size_t plane_words, unsigned int* bar)
+__global__ void __launch_bounds__(kThreads) k_admesh_flags(MarkArgs a, size_t plane_words, unsigned int* bar,
+                                                           unsigned int bar_base)
 {
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsz = gridDim.x * blockDim.x;
+  const GridBar gb{bar, bar_base, a.err};
   unsigned int* w = reinterpret_cast<unsigned int*>(a.leafp);   // leafp, up, down are contiguous
   for (size_t k = gtid; k < 3 * plane_words; k += gsz) w[k] = 0u;
   if (gtid < 4) a.counts[gtid] = 0;
-  if (!grid_barrier(bar, a.err)) return;
+  if (!grid_barrier(gb, 1)) return;
   for (int k = gtid; k < a.nleaf; k += gsz) markref_up_one(a, k);
-  if (!grid_barrier(bar, a.err)) return;
+  if (!grid_barrier(gb, 2)) return;
   for (int nb = 1 + gtid; nb <= a.nbmax; nb += gsz) refine_coarsen_one(a, nb);
 }
 
@@ -549,8 +581,9 @@ static int coop_capacity(K kernel, size_t smem, int (&cache)[8][41])
   return c;
 }
 
-cudaError_t launch_tree_build(const TreeArgs& t, cudaStream_t st)
+cudaError_t launch_tree_build(const TreeArgs& t, unsigned int* arrivals, cudaStream_t st)
 {
+  *arrivals = 0;
   const int nbmax = t.p.nbmax;
   if (nbmax <= 0) return cudaMemsetAsync(t.nleaf_dev, 0, sizeof(int), st);
   const int ntl = (nbmax + 1 + kThreads - 1) / kThreads;
@@ -570,11 +603,20 @@ cudaError_t launch_tree_build(const TreeArgs& t, cudaStream_t st)
   TreeArgs targ = t;
   int nte_a = nte, ntl_a = ntl;
   void* args[] = {&targ, &nte_a, &ntl_a};
-  return cudaLaunchCooperativeKernel((const void*)k_tree_build, dim3(grid), dim3(kThreads), args, smem, st);
+  const cudaError_t e =
+      cudaLaunchCooperativeKernel((const void*)k_tree_build, dim3(grid), dim3(kThreads), args, smem, st);
+  // the barriers the launch passes (the same conditions as in the kernel)
+  const bool f6b = t.p.f6b && t.p.bc[2] != W2D_BC_REFLECTIVE;
+  int nb = (t.nrows > 0) + 1;
+  if (t.plans) nb += (t.p.jet ? 1 : 0) + ((f6b || t.p.jet) ? 1 : 0) + (t.p.jet ? 1 : 0);
+  if (e == cudaSuccess) *arrivals = (unsigned int)(nb * grid);
+  return e;
 }
 
-cudaError_t launch_admesh_flags(const MarkArgs& a, size_t plane_bytes, unsigned int* bar, cudaStream_t st)
+cudaError_t launch_admesh_flags(const MarkArgs& a, size_t plane_bytes, unsigned int* bar, unsigned int bar_base,
+                                unsigned int* arrivals, cudaStream_t st)
 {
+  *arrivals = 0;
   const size_t words = plane_bytes / 4;
   const int want = std::max(ctas(std::max(a.nleaf, a.nbmax)), 1);
   static int cache[8][41] = {};
@@ -584,8 +626,12 @@ cudaError_t launch_admesh_flags(const MarkArgs& a, size_t plane_bytes, unsigned 
   MarkArgs marg = a;
   size_t w = words;
   unsigned int* b = bar;
-  void* args[] = {&marg, &w, &b};
-  return cudaLaunchCooperativeKernel((const void*)k_admesh_flags, dim3(grid), dim3(kThreads), args, 0, st);
+  unsigned int base = bar_base;
+  void* args[] = {&marg, &w, &b, &base};
+  const cudaError_t e =
+      cudaLaunchCooperativeKernel((const void*)k_admesh_flags, dim3(grid), dim3(kThreads), args, 0, st);
+  if (e == cudaSuccess) *arrivals = 2u * (unsigned int)grid;
+  return e;
 }
 
 cudaError_t launch_set_links(const int* rows7, int n, int4* links, int2* sons, cudaStream_t st)
