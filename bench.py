@@ -613,8 +613,14 @@ def run_ours(args, ws, rank, local):
     achieved = bytes_per_zone * per_launch_zones / (tot_ms / nl / 1000.0) / 1e9
     peak, peak_kind = _measured_peaks()
     tpz = _traffic_per_zone(dom, args.precision)
+    # the whole step too: both passes' algorithmic traffic (5.125 x neq x
+    # sizeof(real) per zone-update) at the measured zone-update rate
+    step_bytes_per_zone = 5.125 * p.neq * elem
+    step_achieved = step_bytes_per_zone * value / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
+                "step_achieved": step_achieved, "step_frac": step_achieved / peak,
+                "step_algorithmic_bytes_per_zone": step_bytes_per_zone,
                 "traffic": (tpz * per_launch_zones) if tpz is not None else None,
                 "algorithmic_bytes_per_launch": bytes_per_zone * per_launch_zones,
                 "mean_launch_us": 1000.0 * tot_ms / nl,

@@ -4,12 +4,17 @@ program runs its compiled-in set-up.
 
     python -m walicxe2d_b200.run CONFIG STEPS [--precision 64|32]
         [--tree auto|device|host] [--nblocks N] [--no-graphs]
+        [--surrogate-epochs E]
 
 CONFIG is one of the names of walicxe2d_b200.params.config (sedov64,
-sedov_amr, snr, jet_dmc, ...).  The DMC table of coolingdmc runs is read
-from tests/golden/coolingDMC.tab (the reference's src/DMClib/coolingDMC.tab).
-Prints the final status as one JSON line.  Used, for one, as the workload of
-profiler captures of single kernels.
+sedov_amr, snr, jet_dmc, ...), or ensemble:N for the first N runs of the
+ensemble preset (Sedov-with-coolingh runs of uneven size, one device
+context).  The DMC table of coolingdmc runs is read from
+tests/golden/coolingDMC.tab (the reference's src/DMClib/coolingDMC.tab).
+With --surrogate-epochs E > 0 an FP32 coolingh run cools through the
+learned surrogate, trained first for E epochs on 2M samples that the exact
+routine labels.  Prints the final status as one JSON line.  Used, for one,
+as the workload of profiler captures of single kernels.
 """
 from __future__ import annotations
 
@@ -27,28 +32,48 @@ def main(argv=None) -> int:
     ap.add_argument("--tree", default="auto", choices=["auto", "device", "host"])
     ap.add_argument("--nblocks", type=int, default=0, help="pool capacity (0: the config's own)")
     ap.add_argument("--no-graphs", action="store_true")
+    ap.add_argument("--surrogate-epochs", type=int, default=0,
+                    help="cool an FP32 coolingh run through the learned surrogate trained for this many epochs")
     args = ap.parse_args(argv)
 
     import numpy as np
 
-    from .api import Simulation
-    from .params import COOLINGDMC, config
-    p, ic = config(args.config)
-    p.precision = args.precision
-    if args.nblocks > 0:
-        p.nblocks = args.nblocks
-    sim = Simulation(p, ic)
-    if p.cooling == COOLINGDMC:
-        tab = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden",
-                           "coolingDMC.tab")
-        rows = np.loadtxt(tab)
-        sim.set_cooltab(rows[:, 0], rows[:, 1])
-    sim.set_tree_mode(args.tree)
-    sim.ctx.set_graphs(not args.no_graphs)
-    sim.run(args.steps)
-    sim.ctx.sync()
-    print(json.dumps({"config": args.config, **sim.status()}), flush=True)
-    sim.close()
+    from .api import Ensemble, Simulation, Surrogate
+    from .params import COOLINGDMC, config, ensemble_members
+
+    nn = None
+    if args.surrogate_epochs > 0:
+        nn = Surrogate(20261203)
+        nn.samples(2_000_000, seed=20261203)
+        nn.train(args.surrogate_epochs, batch=8192, lr=2e-3, lr_end=2e-5)
+
+    if args.config.startswith("ensemble:"):
+        mem = ensemble_members(count=int(args.config.split(":")[1]), precision=args.precision)
+        for p, _ in mem:
+            if args.nblocks > 0:
+                p.nblocks = args.nblocks
+        run = Ensemble(mem, threads=0)
+        status = lambda: run.status(-1)   # noqa: E731
+    else:
+        p, ic = config(args.config)
+        p.precision = args.precision
+        if args.nblocks > 0:
+            p.nblocks = args.nblocks
+        run = Simulation(p, ic)
+        if p.cooling == COOLINGDMC:
+            tab = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden",
+                               "coolingDMC.tab")
+            rows = np.loadtxt(tab)
+            run.set_cooltab(rows[:, 0], rows[:, 1])
+        run.set_tree_mode(args.tree)
+        status = run.status
+    if nn is not None:
+        run.ctx.set_surrogate(nn)
+    run.ctx.set_graphs(not args.no_graphs)
+    run.run(args.steps)
+    run.ctx.sync()
+    print(json.dumps({"config": args.config, **status()}), flush=True)
+    run.close()
     return 0
 
 
