@@ -504,7 +504,7 @@ __device__ __forceinline__ void block_stats(const R (*sp)[W2D_W][W2D_W], const P
     dr = fmaxr(dr, absr(sp[0][tj][ti - 1] - rho));
     dr = fmaxr(dr, absr(sp[0][tj + 1][ti] - rho));
     dr = fmaxr(dr, absr(sp[0][tj - 1][ti] - rho));
-    grad = (double)fmaxr(dp / am, dr / am2);
+    grad = (double)fmaxr(divr(dp, am), divr(dr, am2));
     if (pa.cooling == COOL_DMC) {                    // src/timestep.f90:34-41
       const double T = ((double)p / (double)rho) * pa.tempsc;
       if (T > 1e4) {
@@ -585,7 +585,7 @@ __device__ __forceinline__ void interior_stats(R (*st)[W2D_W][W2D_W], double* sr
     if (i > 1) { dp = fmaxr(dp, absr(st[3][tj][ti - 1] - p)); dr = fmaxr(dr, absr(st[0][tj][ti - 1] - rho)); }
     if (j < W2D_NX) { dp = fmaxr(dp, absr(st[3][tj + 1][ti] - p)); dr = fmaxr(dr, absr(st[0][tj + 1][ti] - rho)); }
     if (j > 1) { dp = fmaxr(dp, absr(st[3][tj - 1][ti] - p)); dr = fmaxr(dr, absr(st[0][tj - 1][ti] - rho)); }
-    grad = (double)fmaxr(dp / am, dr / am2);
+    grad = (double)fmaxr(divr(dp, am), divr(dr, am2));
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -938,7 +938,7 @@ __global__ void __launch_bounds__(256) k_fill1g(KArgs a, PhysArgs pa)
     uprim<NEQ>(ph, qc, uc, T);
     const R fl = R(1e-15);
     const R am = fmaxr(fl, absr(qc[3])), am2 = fmaxr(fl, absr(qc[0]));
-    double gr = (double)fmaxr(absr(qg[3] - qc[3]) / am, absr(qg[0] - qc[0]) / am2);
+    double gr = (double)fmaxr(divr(absr(qg[3] - qc[3]), am), divr(absr(qg[0] - qc[0]), am2));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) gr = fmax(gr, __shfl_xor_sync(0xffffffffu, gr, o));
     // the full step wrote the interior maximum; both are >= 0, so their

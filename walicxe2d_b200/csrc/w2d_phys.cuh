@@ -21,6 +21,9 @@ template <typename R> __device__ __forceinline__ R fmaxr(R a, R b) { return (a >
 template <typename R> __device__ __forceinline__ R fminr(R a, R b) { return (a < b) ? a : b; }
 __device__ __forceinline__ double sqrtr(double x) { return sqrt(x); }
 __device__ __forceinline__ float sqrtr(float x) { return sqrtf(x); }
+// the divisions of the update (IEEE in FP64, the build's division in FP32)
+__device__ __forceinline__ double divr(double a, double b) { return a / b; }
+__device__ __forceinline__ float divr(float a, float b) { return a / b; }
 __device__ __forceinline__ double absr(double x) { return fabs(x); }
 __device__ __forceinline__ float absr(float x) { return fabsf(x); }
 __device__ __forceinline__ double signr(double a) { return copysign(1.0, a); }
@@ -46,23 +49,23 @@ __device__ __forceinline__ void uprim(const Phys<R>& ph, R* prim, const R* uu, R
   const R tiny = R(1e-15);
   R r = uu[0] > tiny ? uu[0] : tiny;
   prim[0] = r;
-  prim[1] = uu[1] / r;
-  prim[2] = uu[2] / r;
+  prim[1] = divr(uu[1], r);
+  prim[2] = divr(uu[2], r);
 #pragma unroll
   for (int k = 4; k < NEQ; ++k) prim[k] = uu[k];
-  prim[3] = (uu[3] - R(0.5) * r * (prim[1] * prim[1] + prim[2] * prim[2])) / ph.cv;
+  prim[3] = divr(uu[3] - R(0.5) * r * (prim[1] * prim[1] + prim[2] * prim[2]), ph.cv);
   prim[3] = fmaxr(prim[3], tiny);
   if (ph.cooling == COOL_NONE) {
-    T = prim[3] / r;
+    T = divr(prim[3], r);
   } else if (ph.cooling == COOL_H) {
     R dentot = (R(2.) * r - prim[NEQ > 4 ? 4 : 0]);
     dentot = fmaxr(dentot, tiny);
-    T = fmaxr(R(1.), (prim[3] / dentot) * ph.tempsc);
-    prim[3] = dentot * T / ph.tempsc;
+    T = fmaxr(R(1.), divr(prim[3], dentot) * ph.tempsc);
+    prim[3] = divr(dentot * T, ph.tempsc);
   } else {
     r = fmaxr(r, tiny);
-    T = fmaxr(R(1.), (prim[3] / (r)) * ph.tempsc);
-    prim[3] = r * T / ph.tempsc;
+    T = fmaxr(R(1.), divr(prim[3], r) * ph.tempsc);
+    prim[3] = divr(r * T, ph.tempsc);
   }
 }
 
@@ -93,7 +96,7 @@ __device__ __forceinline__ void primf(const Phys<R>& ph, const R* p, R* ff)
 
 // src/sound.f90:4-13
 template <typename R>
-__device__ __forceinline__ R sound(const Phys<R>& ph, R p, R d) { return sqrtr(ph.gamma * p / d); }
+__device__ __forceinline__ R sound(const Phys<R>& ph, R p, R d) { return sqrtr(divr(ph.gamma * p, d)); }
 
 // Star-region state of HLLC, src/hllcfluxes.f90:127-160, for the side
 // "s" (left: s = sl, smus = sl - u_l; right: s = sr, smus = sr - u_r).
@@ -102,14 +105,14 @@ __device__ __forceinline__ void hllc_star(const Phys<R>& ph, const R* q, R s, R 
                                           R den, R* ff)
 {
   R uu[NEQ], uuk[NEQ];
-  R rhost = q[0] * (smus) / (s - sst);
+  R rhost = divr(q[0] * smus, s - sst);
   R ek = R(0.5) * q[0] * (q[1] * q[1] + q[2] * q[2]) + ph.cv * q[3];
   uuk[0] = rhost;
   uuk[1] = rhost * sst;
   uuk[2] = rhost * q[2];
-  uuk[3] = rhost * (ek / q[0] + (sst - q[1]) * (sst + q[3] / (den * smus)));
+  uuk[3] = rhost * (divr(ek, q[0]) + (sst - q[1]) * (sst + divr(q[3], den * smus)));
 #pragma unroll
-  for (int k = 4; k < NEQ; ++k) uuk[k] = rhost * q[k] / q[0];
+  for (int k = 4; k < NEQ; ++k) uuk[k] = divr(rhost * q[k], q[0]);
   primf<NEQ>(ph, q, ff);
   primu<NEQ>(ph, q, uu);
 #pragma unroll
@@ -128,7 +131,7 @@ __device__ __forceinline__ void hll_flux(const Phys<R>& ph, const R* ql, const R
   primu<NEQ>(ph, qr, ur);
 #pragma unroll
   for (int k = 0; k < NEQ; ++k)
-    ff[k] = (sr * fl[k] - sl * fr[k] + sl * sr * (ur[k] - ul[k])) / (sr - sl);
+    ff[k] = divr(sr * fl[k] - sl * fr[k] + sl * sr * (ur[k] - ul[k]), sr - sl);
 }
 
 // Riemann flux of the selected solver:
@@ -151,7 +154,7 @@ __device__ __forceinline__ bool riemann(const Phys<R>& ph, R* pl, const R* pr, R
       beta1 = R(1.0);
       beta2 = R(0.0);
     } else {
-      R alpha1 = absr(dq1) / mag;
+      R alpha1 = divr(absr(dq1), mag);
       beta1 = sqrtr(alpha1);
       beta2 = R(1.) - beta1;
     }
@@ -168,7 +171,7 @@ __device__ __forceinline__ bool riemann(const Phys<R>& ph, R* pl, const R* pr, R
   R srmur = sr - pr[1];
   R rholul = pl[0] * pl[1];
   R rhorur = pr[0] * pr[1];
-  R sst = (srmur * rhorur - slmul * rholul - pr[3] + pl[3]) / (srmur * pr[0] - slmul * pl[0]);
+  R sst = divr(srmur * rhorur - slmul * rholul - pr[3] + pl[3], srmur * pr[0] - slmul * pl[0]);
   bool left = sst >= R(0.);
   if (!left && !(sst <= R(0.))) return false;
   // the star state of the side the contact leaves behind: the side's inputs
@@ -195,10 +198,10 @@ __device__ __forceinline__ R average(int limiter, R a, R b)
     case 1: { R s = signr(a); return s * fmaxr(R(0.), fminr(absr(a), s * b)); }
     case 2:
       if (a * b <= R(0.)) return R(0.);
-      return a * b * (a + b) / (a * a + b * b);
+      return divr(a * b * (a + b), a * a + b * b);
     case 3: {
       const R delta = R(1.e-7);
-      return (a * (b * b + delta) + b * (a * a + delta)) / (a * a + b * b + delta);
+      return divr(a * (b * b + delta) + b * (a * a + delta), a * a + b * b + delta);
     }
     case 4: {
       R s = signr(a);
