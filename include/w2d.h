@@ -400,10 +400,20 @@ int w2d_ens_phase_ms(W2dEns* ens, double* ms, int reset);
  * makes an ensemble context, or the context of a single run without the
  * jet (w2d_sim_ctx), replay each step's two launch sequences as CUDA
  * graphs (persistent shapes only; leaf count and dt are read on the
- * device, dt reaches the host with the step's synchronization). */
+ * device, dt reaches the host with the step's synchronization).
+ * w2d_set_step_kernel(ctx, 1) lets such a single adiabatic run take each
+ * step -- timestep, tstep and the block statistics -- as ONE cooperative
+ * persistent kernel whose phases wait on per-block flags instead of kernel
+ * boundaries, once the autotuner is done and while the fill plans are
+ * current (w2d_sim_set_device_plans); the results equal those of the
+ * separate kernels bit for bit.  The default, 0, keeps the separate
+ * kernels, which measured faster on the B200 (the FP64 phases are latency
+ * bound, and a CTA waiting for its neighbours' flags idles its warps at
+ * least as long as a kernel boundary does). */
 int w2d_autotune(W2dCtx* ctx, int reps);
 int w2d_tuning(W2dCtx* ctx, int32_t* shape, double* ms, int* tuning_left);
 int w2d_set_graphs(W2dCtx* ctx, int on);
+int w2d_set_step_kernel(W2dCtx* ctx, int fused);
 
 /* ---- Learned coolingh surrogate (no counterpart in the reference) ---------
  * A 4 -> 64 -> 64 -> 2 tanh MLP with BF16 weights on the tensor cores

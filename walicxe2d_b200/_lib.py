@@ -95,6 +95,7 @@ SIGNATURES = {
     "w2d_autotune": (_I, [_vp, _I]),
     "w2d_tuning": (_I, [_vp, _PI32, _PD, C.POINTER(_I)]),
     "w2d_set_graphs": (_I, [_vp, _I]),
+    "w2d_set_step_kernel": (_I, [_vp, _I]),
     "w2d_set_surrogate": (_I, [_vp, _vp]),
     "w2d_set_surrogate_tol": (_I, [_vp, _D]),
     "w2d_surrogate_counts": (_I, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),

@@ -239,6 +239,11 @@ class Context:
     def set_graphs(self, on: bool = True):
         self._check(self.L.w2d_set_graphs(self.h, 1 if on else 0), "w2d_set_graphs")
 
+    def set_step_kernel(self, fused: bool = True):
+        """The whole step of a single adiabatic run as one fused kernel, or
+        the separate kernels (the context's default)."""
+        self._check(self.L.w2d_set_step_kernel(self.h, 1 if fused else 0), "w2d_set_step_kernel")
+
     def set_surrogate(self, nn):
         """coolingh through a trained Surrogate (None detaches it)."""
         self._check(self.L.w2d_set_surrogate(self.h, nn.h if nn is not None else None), "w2d_set_surrogate")

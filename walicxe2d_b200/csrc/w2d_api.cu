@@ -293,6 +293,11 @@ int check_device(W2dCtx* c)
     // a grid barrier that ran out left its count behind
     if (c->d_gbar) cudaMemsetAsync(c->d_gbar, 0, 2 * sizeof(unsigned int), c->st);
     c->gbar_count = 0;
+    // so may the fused step's; its flags restart with its epoch
+    if (c->d_step_sync) {
+      cudaMemsetAsync(c->d_step_sync, 0, 4 * sizeof(unsigned), c->st);
+      cudaMemsetAsync(c->d_step_flags, 0, 2 * ((size_t)c->cap + 1) * sizeof(unsigned), c->st);
+    }
     return rc;
   }
   return W2D_OK;
@@ -714,13 +719,15 @@ int w2d_destroy(W2dCtx* c)
     if (e) cudaEventDestroy(e);
   if (c->gx_first) cudaGraphExecDestroy(c->gx_first);
   if (c->gx_rest) cudaGraphExecDestroy(c->gx_rest);
+  if (c->gx_step) cudaGraphExecDestroy(c->gx_step);
   for (int k = 0; k < 5; ++k)
     for (int q = 0; q < 2; ++q)
       if (c->tune_ev[k][q]) cudaEventDestroy(c->tune_ev[k][q]);
   if (c->h_nleaf) cudaFreeHost(c->h_nleaf);
   void* dev2[] = {c->d_run_of, c->d_runs, c->d_dt_run, c->d_loff, c->d_gradleaf, c->d_fb, c->d_fb_count,
                   c->d_nn_counts, c->d_nleaf, c->d_links, c->d_sons, c->d_mflags, c->d_mlists, c->d_rows7,
-                  c->d_posof, c->d_bent, c->d_bspan, c->d_blocal, c->d_bcta, c->d_wpos};
+                  c->d_posof, c->d_bent, c->d_bspan, c->d_blocal, c->d_bcta, c->d_wpos,
+                  c->d_step_flags, c->d_step_sync, c->d_step_part};
   for (void* d : dev2)
     if (d) cudaFree(d);
   if (c->h_dt_run) cudaFreeHost(c->h_dt_run);
@@ -1817,10 +1824,85 @@ bool graphs_now(const W2dCtx* c)
 bool ctx_device_dt(W2dCtx* c) { return c->want_graphs && c->p.otherb == W2D_USERBC_NONE; }
 double ctx_last_dt(W2dCtx* c) { return c->h_small[0]; }
 
+namespace {
+
+// The fused step kernel applies to a single adiabatic run without the jet
+// whose dt stays on the device, once the fill plans are current and the
+// autotuner is done with the separate kernels.
+bool step_fused_ok(const W2dCtx* c)
+{
+  return c->step_fused && c->nruns == 0 && c->p.cooling == W2D_ADIABATIC && c->p.otherb == W2D_USERBC_NONE &&
+         c->want_graphs && c->have_topology && c->have_bounds && c->tune_left == 0;
+}
+
+int ensure_step(W2dCtx* c)
+{
+  if (c->step_grid < 0) {
+    const int per = c->L->step_per_sm(c->neq, pargs(c));
+    c->step_grid = per >= 1 ? (per < 4 ? per : 4) * c->nsm : 0;
+  }
+  if (c->step_grid == 0 || c->d_step_flags) return W2D_OK;
+  const size_t slots = (size_t)c->cap + 1;
+  CK(cudaMalloc(&c->d_step_flags, 2 * slots * sizeof(unsigned)));
+  CK(cudaMemsetAsync(c->d_step_flags, 0, 2 * slots * sizeof(unsigned), c->st));
+  CK(cudaMalloc(&c->d_step_sync, 4 * sizeof(unsigned)));
+  CK(cudaMemsetAsync(c->d_step_sync, 0, 4 * sizeof(unsigned), c->st));
+  CK(cudaMalloc(&c->d_step_part, (size_t)c->step_grid * sizeof(double)));
+  return W2D_OK;
+}
+
+// timestep and tstep in one launch (w2d_step.cuh); dt and the error word
+// follow to pinned memory as after the separate dt reduction
+int step_launch(W2dCtx* c)
+{
+  int rc = ensure_leaf_list(c);
+  if (rc) return rc;
+  const PhysArgs pa = pargs(c);
+  KArgs a = kargs(c, c->d_fd2);
+  a.dt_dev = nullptr;   // the kernel forms dt itself
+  a.split_stats = 1;
+  a.grid = c->step_grid;
+  a.sched = 0;
+  const size_t slots = (size_t)c->cap + 1;
+  StepArgs s;
+  s.fd1 = c->d_fd1;
+  s.flag_half = c->d_step_flags;
+  s.flag_full = c->d_step_flags + slots;
+  s.sync = c->d_step_sync;
+  s.part = c->d_step_part;
+  s.dt_out = c->d_dt;
+  s.courant = c->p.cfl;
+  s.psc = c->p.psc;
+  s.tsc = c->p.tsc;
+  rc = launch(c, "step", [&] { return c->L->step(c->neq, a, pa, s, c->step_grid, c->st); });
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(c->h_small, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(c->h_err, c->d_err, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  if (!c->capturing) CK(cudaEventRecord(c->ev_dt, c->st));
+  return W2D_OK;
+}
+
+}  // namespace
+
 // first part of a step: dt (of every run of an ensemble) and its copy to
-// the host, the half step
+// the host, the half step; or, where it applies, the whole step as the one
+// fused kernel (the rest of the step is then done)
 int ctx_step_first(W2dCtx* c)
 {
+  c->step_fused_now = false;
+  if (step_fused_ok(c)) {
+    int rc = ensure_step(c);
+    if (rc) return rc;
+    if (c->step_grid > 0) {
+      c->step_fused_now = true;
+      auto body = [&] { return step_launch(c); };
+      if (!graphs_now(c)) return body();
+      if (!c->gx_step && (rc = capture(c, &c->gx_step, &c->nlaunch_graph_step, body))) return rc;
+      CK(cudaGraphLaunch(c->gx_step, c->st));
+      c->nlaunch += c->nlaunch_graph_step;
+      return W2D_OK;
+    }
+  }
   auto body = [&] {
     int rc = c->nruns > 0 ? ctx_ens_dt_launch(c) : ctx_dt_launch(c);
     return rc ? rc : ctx_half_step(c);
@@ -1838,6 +1920,10 @@ int ctx_step_first(W2dCtx* c)
 // the rest of the step: full step, boundaryI, cooling, statistics
 int ctx_step_rest(W2dCtx* c)
 {
+  if (c->step_fused_now) {
+    c->step_fused_now = false;
+    return W2D_OK;
+  }
   auto body = [&] { return ctx_tstep_rest(c, 0.0, 0.0); };
   if (!graphs_now(c)) return body();
   if (c->nn_img) {
@@ -1891,7 +1977,15 @@ int w2d_set_graphs(W2dCtx* c, int on)
       if (kShapes[c->tshape[k]].per_sm == 0) c->tshape[k] = 2;
   if (c->gx_first) cudaGraphExecDestroy(c->gx_first);
   if (c->gx_rest) cudaGraphExecDestroy(c->gx_rest);
-  c->gx_first = c->gx_rest = nullptr;
+  if (c->gx_step) cudaGraphExecDestroy(c->gx_step);
+  c->gx_first = c->gx_rest = c->gx_step = nullptr;
+  return W2D_OK;
+}
+
+int w2d_set_step_kernel(W2dCtx* c, int fused)
+{
+  if (!c) return W2D_ERR_ARG;
+  c->step_fused = fused != 0;
   return W2D_OK;
 }
 

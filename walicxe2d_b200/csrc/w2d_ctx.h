@@ -76,6 +76,19 @@ struct W2dCtx {
   bool want_graphs = false, capturing = false;
   cudaGraphExec_t gx_first = nullptr, gx_rest = nullptr;
   int64_t nlaunch_graph_first = 0, nlaunch_graph_rest = 0;
+  // the fused step kernel (w2d_step.cuh), allocated by its first use: per
+  // slot the epochs of the last half and full step, the epoch and barrier
+  // words, the CTAs' CFL minima; its grid (-1: not sized yet, 0: it does
+  // not fit), whether to use it (w2d_set_step_kernel; off by default: the
+  // separate kernels measured faster), whether the current step ran it,
+  // its graph
+  unsigned* d_step_flags = nullptr;   // 2 (cap + 1)
+  unsigned* d_step_sync = nullptr;    // 4
+  double* d_step_part = nullptr;      // step_grid
+  int step_grid = -1;
+  bool step_fused = false, step_fused_now = false;
+  cudaGraphExec_t gx_step = nullptr;
+  int64_t nlaunch_graph_step = 0;
   int nruns = 0;
   int* d_run_of = nullptr;
   w2d::RunGeo* d_runs = nullptr;

@@ -90,6 +90,17 @@ struct KArgs {
   int split_stats;
 };
 
+// The fused step kernel's state (w2d_step.cuh)
+struct StepArgs {
+  const int2* fd1;        // fill I plans (KArgs.fd holds fill II's)
+  unsigned* flag_half;    // [slot]: epoch of the block's last half step
+  unsigned* flag_full;    // [slot]: epoch of its last full step
+  unsigned* sync;         // [0] epoch, [1] barrier count, [2] barrier generation, [3] CTAs done
+  double* part;           // [grid]: the CTAs' CFL minima
+  double* dt_out;         // the step's dt, for the host
+  double courant, psc, tsc;
+};
+
 struct LeafRange {
   int li, end, step;
 };
@@ -440,12 +451,18 @@ __device__ __forceinline__ void tiles_issue2(R* d1, const R* s1, R* d2, const R*
   bulk_g2s(d1, s1, bytes, bar);
   bulk_g2s(d2, s2, bytes, bar);
 }
+// U (the fused step kernel, whose threads go on after a failed leaf): the
+// CTA agrees on the outcome, so that all of its threads skip together.
+template <bool U = false>
 __device__ __forceinline__ bool wait_tiles_p(uint64_t* bar, int* err, int b, uint32_t parity)
 {
-  if (mbar_wait(bar, parity)) return true;
-  if (threadIdx.x == 0) set_err(err, ERR_TIMEOUT, b, -1, -1);
-  mbar_wait(bar, parity);
-  return false;
+  const bool got = mbar_wait(bar, parity);
+  if (!got) {
+    if (threadIdx.x == 0) set_err(err, ERR_TIMEOUT, b, -1, -1);
+    mbar_wait(bar, parity);
+  }
+  if (U) return !__syncthreads_or(!got);
+  return got;
 }
 // end of one leaf: the shared tiles this thread wrote are ordered before the
 // next leaf's tile copies into them
@@ -647,8 +664,11 @@ __host__ __device__ constexpr size_t smem_half()
   return 128 + sizeof(R) * (2 * NEQ * W2D_CELLS + W2D_CELLS + 2 * NEQ * 272);
 }
 
-template <typename R, int NEQ, int SOLVER, bool P>
-__global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_half(KArgs a, PhysArgs pa, double dt)
+// One leaf of the half step (position li of the leaf list); the tile
+// barrier completes with phase parity `par`.  Returns false when the tile
+// copy timed out (recorded in the error word).
+template <typename R, int NEQ, int SOLVER, bool U = false>
+__device__ __forceinline__ bool half_leaf(const KArgs& a, const PhysArgs& pa, double dt, int li, uint32_t par)
 {
   // su: the tile as loaded (u, or the stored primitives under DMC); st:
   // the primitives of cells 0..17; scs: their sound speeds
@@ -662,10 +682,7 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_half(KArgs a, P
   const int tid = threadIdx.x;
   const size_t bs = (size_t)NEQ * W2D_CELLS;
   const bool dmc = pa.cooling == COOL_DMC;
-  bar_init_once(bar);
-  uint32_t par = 0;
-  for (LeafRange lr = leaf_range<P>(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
-  const int b = a.leaves[lr.li];
+  const int b = a.leaves[li];
   const R* __restrict__ u = (const R*)a.u + (size_t)b * bs;
   R* __restrict__ up = (R*)a.up + (size_t)b * bs;
   if (tid == 0) tile_issue<R, NEQ>(&su[0][0][0], dmc ? (const R*)a.prim + (size_t)b * bs : u, bar);
@@ -673,7 +690,7 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_half(KArgs a, P
   const double dtm = step_dt(a, b, dt) / 2.;
   const R dtdx = R(dtm / geo_dx(a, b, lev));
   const R dtdy = R(dtm / geo_dy(a, b, lev));
-  if (!wait_tiles_p(bar, a.err, b, par)) return;
+  if (!wait_tiles_p<U>(bar, a.err, b, par)) return false;
 
   // primitives (in place) and sound speed of cells 0..17 (corners skipped)
   for (int c = tid; c < 18 * 18; c += W2D_THREADS) {
@@ -732,7 +749,16 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_half(KArgs a, P
     }
   }
   leaf_end();
-  }
+  return true;
+}
+
+template <typename R, int NEQ, int SOLVER, bool P>
+__global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_half(KArgs a, PhysArgs pa, double dt)
+{
+  bar_init_once(reinterpret_cast<uint64_t*>(w2d_smem));
+  uint32_t par = 0;
+  for (LeafRange lr = leaf_range<P>(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u)
+    if (!half_leaf<R, NEQ, SOLVER>(a, pa, dt, lr.li, par)) return;
 }
 
 // ---------------------------------------------------------------------------
@@ -746,8 +772,10 @@ __host__ __device__ constexpr size_t smem_full()
   return 128 + sizeof(R) * (2 * NEQ * W2D_CELLS + 2 * NEQ * 272);
 }
 
-template <typename R, int NEQ, int SOLVER, int LIMITER, bool P>
-__global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_full(KArgs a, PhysArgs pa, double dt)
+// One leaf of the full step (position li of the leaf list).  Returns false
+// when the tile copies timed out (recorded in the error word).
+template <typename R, int NEQ, int SOLVER, int LIMITER, bool U = false>
+__device__ __forceinline__ bool full_leaf(const KArgs& a, const PhysArgs& pa, double dt, int li, uint32_t par)
 {
   uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
   R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
@@ -758,10 +786,6 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_full(KArgs a, P
   const int tid = threadIdx.x;
   const size_t bs = (size_t)NEQ * W2D_CELLS;
   const R* __restrict__ upool = (const R*)a.up;
-  bar_init_once(bar);
-  uint32_t par = 0;
-  for (LeafRange lr = leaf_range<P>(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u) {
-  const int li = lr.li;
   const int b = a.leaves[li];
   R* __restrict__ u = (R*)a.u + (size_t)b * bs;
   if (tid == 0) tiles_issue2<R, NEQ>(&st[0][0][0], upool + (size_t)b * bs, &so[0][0][0], u, bar);
@@ -782,7 +806,7 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_full(KArgs a, P
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) gw = ghost_value<R>(upool, bs, a, b, d, gf, gg, gm, k, gv[k]);
   }
-  if (!wait_tiles_p(bar, a.err, b, par)) return;
+  if (!wait_tiles_p<U>(bar, a.err, b, par)) return false;
   if (tid < 128 && gw) {
     int i, j;
     ghost_ij(gf, gg, gm, i, j);
@@ -878,7 +902,16 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_full(KArgs a, P
   // criteria); sf is free once every thread has passed the next barrier
   if (a.split_stats) interior_stats<R, NEQ>(st, reinterpret_cast<double*>(&sf[0][0][0]), ph, a, b, lev);
   leaf_end();
-  }
+  return true;
+}
+
+template <typename R, int NEQ, int SOLVER, int LIMITER, bool P>
+__global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_full(KArgs a, PhysArgs pa, double dt)
+{
+  bar_init_once(reinterpret_cast<uint64_t*>(w2d_smem));
+  uint32_t par = 0;
+  for (LeafRange lr = leaf_range<P>(a); lr.li < lr.end; lr.li += lr.step, par ^= 1u)
+    if (!full_leaf<R, NEQ, SOLVER, LIMITER>(a, pa, dt, lr.li, par)) return;
 }
 
 // ---------------------------------------------------------------------------
@@ -890,13 +923,59 @@ __global__ void __launch_bounds__(W2D_THREADS, w2d_minb<R>(P)) k_full(KArgs a, P
 // the CTA walks its leaves as leaf_range gives them, four at a time (li,
 // li + step, li + 2 step, li + 3 step); otherwise CTA k takes leaves
 // 4k .. 4k + 3.  A warp serves two faces of one leaf.
+// Thread t (0..63) of the 64 that fill leaf position li: face t/16, cell
+// 1 + t%16 along it.
+template <typename R, int NEQ>
+__device__ __forceinline__ void fill1_leaf(const KArgs& a, const PhysArgs& pa, const int2* __restrict__ fd, int li,
+                                           int t)
+{
+  const int f = t / 16, m = 1 + t % 16;
+  const size_t bs = (size_t)NEQ * W2D_CELLS;
+  R* __restrict__ upool = (R*)a.u;
+  int gi, gj;
+  ghost_ij(f, 0, m, gi, gj);
+  // the edge cell next to this ghost
+  const int ci = gi < 1 ? 1 : (gi > W2D_NX ? W2D_NX : gi);
+  const int cj = gj < 1 ? 1 : (gj > W2D_NX ? W2D_NX : gj);
+  const int b = a.leaves[li];
+  const int2 d = fd[li * 4 + f];
+  R gv[NEQ];
+  bool w = false;
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k) w = ghost_value<R>(upool, bs, a, b, d, f, 0, m, k, gv[k]);
+  R* __restrict__ u = upool + (size_t)b * bs;
+  if (w) {
+#pragma unroll
+    for (int k = 0; k < NEQ; ++k) u[k * W2D_CELLS + cidx(gi, gj)] = gv[k];
+  }
+  if (!a.split_stats) return;
+  // src/criteria.f90:16-50 for the pair (edge cell, its ghost), from the
+  // primitives of both as calcprim gives them; a face no entry writes
+  // keeps the ghost value it has
+  const Phys<R> ph = make_phys<R, -1, -1>(pa);
+  R uc[NEQ], qc[NEQ], qg[NEQ], T;
+#pragma unroll
+  for (int k = 0; k < NEQ; ++k) {
+    if (!w) gv[k] = u[k * W2D_CELLS + cidx(gi, gj)];
+    uc[k] = u[k * W2D_CELLS + cidx(ci, cj)];
+  }
+  uprim<NEQ>(ph, qg, gv, T);
+  uprim<NEQ>(ph, qc, uc, T);
+  const R fl = R(1e-15);
+  const R am = fmaxr(fl, absr(qc[3])), am2 = fmaxr(fl, absr(qc[0]));
+  double gr = (double)fmaxr(divr(absr(qg[3] - qc[3]), am), divr(absr(qg[0] - qc[0]), am2));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) gr = fmax(gr, __shfl_xor_sync(0xffffffffu, gr, o));
+  // the full step wrote the interior maximum; both are >= 0, so their
+  // bit patterns order as the values
+  if ((t & 31) == 0)
+    atomicMax(reinterpret_cast<unsigned long long*>(a.grad + b), (unsigned long long)__double_as_longlong(gr));
+}
+
 template <typename R, int NEQ, bool P>
 __global__ void __launch_bounds__(256) k_fill1g(KArgs a, PhysArgs pa)
 {
   const int tid = threadIdx.x, g = tid >> 6, t = tid & 63;
-  const int f = t / 16, m = 1 + t % 16;
-  const size_t bs = (size_t)NEQ * W2D_CELLS;
-  R* __restrict__ upool = (R*)a.u;
   LeafRange lr;
   if (P) {
     lr = leaf_range<true>(a);
@@ -904,47 +983,10 @@ __global__ void __launch_bounds__(256) k_fill1g(KArgs a, PhysArgs pa)
     const int lo = 4 * (int)blockIdx.x;
     lr = {lo, lo + 4 < a.nleaf ? lo + 4 : a.nleaf, 1};
   }
-  int gi, gj;
-  ghost_ij(f, 0, m, gi, gj);
-  // the edge cell next to this ghost
-  const int ci = gi < 1 ? 1 : (gi > W2D_NX ? W2D_NX : gi);
-  const int cj = gj < 1 ? 1 : (gj > W2D_NX ? W2D_NX : gj);
   for (; lr.li < lr.end; lr.li += 4 * lr.step) {
     const int li = lr.li + g * lr.step;
     if (li >= lr.end) continue;     // (the whole warp: one leaf per warp)
-    const int b = a.leaves[li];
-    const int2 d = a.fd[li * 4 + f];
-    R gv[NEQ];
-    bool w = false;
-#pragma unroll
-    for (int k = 0; k < NEQ; ++k) w = ghost_value<R>(upool, bs, a, b, d, f, 0, m, k, gv[k]);
-    R* __restrict__ u = upool + (size_t)b * bs;
-    if (w) {
-#pragma unroll
-      for (int k = 0; k < NEQ; ++k) u[k * W2D_CELLS + cidx(gi, gj)] = gv[k];
-    }
-    if (!a.split_stats) continue;
-    // src/criteria.f90:16-50 for the pair (edge cell, its ghost), from the
-    // primitives of both as calcprim gives them; a face no entry writes
-    // keeps the ghost value it has
-    const Phys<R> ph = make_phys<R, -1, -1>(pa);
-    R uc[NEQ], qc[NEQ], qg[NEQ], T;
-#pragma unroll
-    for (int k = 0; k < NEQ; ++k) {
-      if (!w) gv[k] = u[k * W2D_CELLS + cidx(gi, gj)];
-      uc[k] = u[k * W2D_CELLS + cidx(ci, cj)];
-    }
-    uprim<NEQ>(ph, qg, gv, T);
-    uprim<NEQ>(ph, qc, uc, T);
-    const R fl = R(1e-15);
-    const R am = fmaxr(fl, absr(qc[3])), am2 = fmaxr(fl, absr(qc[0]));
-    double gr = (double)fmaxr(divr(absr(qg[3] - qc[3]), am), divr(absr(qg[0] - qc[0]), am2));
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) gr = fmax(gr, __shfl_xor_sync(0xffffffffu, gr, o));
-    // the full step wrote the interior maximum; both are >= 0, so their
-    // bit patterns order as the values
-    if ((tid & 31) == 0)
-      atomicMax(reinterpret_cast<unsigned long long*>(a.grad + b), (unsigned long long)__double_as_longlong(gr));
+    fill1_leaf<R, NEQ>(a, pa, a.fd, li, t);
   }
 }
 

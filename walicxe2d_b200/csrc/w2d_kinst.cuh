@@ -8,6 +8,7 @@
 #pragma once
 
 #include "w2d_cool.cuh"
+#include "w2d_step.cuh"
 #include "w2d_launch.h"
 
 namespace w2d {
@@ -224,8 +225,83 @@ static cudaError_t totals(int neq, const KArgs& a, int cyl, const int* ids, int 
   return cudaGetLastError();
 }
 
+template <int NEQ>
+constexpr size_t smem_step()
+{
+  return smem_half<R, NEQ>() > smem_full<R, NEQ>() ? smem_half<R, NEQ>() : smem_full<R, NEQ>();
+}
+
+template <int NEQ, int S, int L>
+static cudaError_t step_t(const KArgs& a, const PhysArgs& pa, const StepArgs& s, int grid, cudaStream_t st)
+{
+  static bool done = false;
+  constexpr size_t sm = smem_step<NEQ>();
+  cudaError_t e = smem_opt_in(k_step<R, NEQ, S, L>, sm, done);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(W2D_THREADS);
+  cfg.dynamicSmemBytes = sm;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_step<R, NEQ, S, L>, a, pa, s);
+}
+template <int NEQ, int S, int L>
+static int step_occ_t()
+{
+  static bool done = false;
+  constexpr size_t sm = smem_step<NEQ>();
+  if (smem_opt_in(k_step<R, NEQ, S, L>, sm, done) != cudaSuccess) return 0;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_step<R, NEQ, S, L>, W2D_THREADS, sm) != cudaSuccess) return 0;
+  return n;
+}
+
+// the same solver/limiter forms as the full step's launcher (the half step
+// runs the solver's form, generic where the full step is)
+static cudaError_t step(int neq, const KArgs& a, const PhysArgs& pa, const StepArgs& s, int grid, cudaStream_t st)
+{
+  if (pa.solver == SOLVER_HLLC && pa.limiter == 1) {
+    W2D_NEQ_SWITCH(neq, return (step_t<NEQ, SOLVER_HLLC, 1>(a, pa, s, grid, st)));
+  }
+  if (pa.solver == SOLVER_HLLC && pa.limiter == 2) {
+    W2D_NEQ_SWITCH(neq, return (step_t<NEQ, SOLVER_HLLC, 2>(a, pa, s, grid, st)));
+  }
+  W2D_NEQ_SWITCH(neq, return (step_t<NEQ, -1, -99>(a, pa, s, grid, st)));
+  return cudaSuccess;
+}
+static int step_per_sm(int neq, const PhysArgs& pa)
+{
+  if (pa.solver == SOLVER_HLLC && pa.limiter == 1) {
+    switch (neq) {
+      case 4: return step_occ_t<4, SOLVER_HLLC, 1>();
+      case 5: return step_occ_t<5, SOLVER_HLLC, 1>();
+      case 6: return step_occ_t<6, SOLVER_HLLC, 1>();
+      default: return 0;
+    }
+  }
+  if (pa.solver == SOLVER_HLLC && pa.limiter == 2) {
+    switch (neq) {
+      case 4: return step_occ_t<4, SOLVER_HLLC, 2>();
+      case 5: return step_occ_t<5, SOLVER_HLLC, 2>();
+      case 6: return step_occ_t<6, SOLVER_HLLC, 2>();
+      default: return 0;
+    }
+  }
+  switch (neq) {
+    case 4: return step_occ_t<4, -1, -99>();
+    case 5: return step_occ_t<5, -1, -99>();
+    case 6: return step_occ_t<6, -1, -99>();
+    default: return 0;
+  }
+}
+
 static const Launchers table = {half,    full,   fill1,   fill_only, calcprim, jet_only, amr,
-                                cool,    scatter, gather, to_prim,   totals,   sizeof(R)};
+                                cool,    scatter, gather, to_prim,   totals,   sizeof(R), step, step_per_sm};
 
 }  // namespace W2D_INST_NS
 }  // namespace w2d

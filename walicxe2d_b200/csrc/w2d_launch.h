@@ -28,6 +28,10 @@ struct Launchers {
   // FP64 conserved totals of the interiors of blocks ids[0..n-1]: out[k*neq+q]
   cudaError_t (*totals)(int neq, const KArgs&, int cyl, const int* ids, int n, double* out, cudaStream_t);
   size_t elem;  // sizeof(R)
+  // one step of a single adiabatic run as one cooperative kernel of `grid`
+  // CTAs (w2d_step.cuh); step_per_sm: how many of its CTAs fit on an SM
+  cudaError_t (*step)(int neq, const KArgs&, const PhysArgs&, const StepArgs&, int grid, cudaStream_t);
+  int (*step_per_sm)(int neq, const PhysArgs&);
 };
 
 const Launchers& launchers64();

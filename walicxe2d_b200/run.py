@@ -4,7 +4,7 @@ program runs its compiled-in set-up.
 
     python -m walicxe2d_b200.run CONFIG STEPS [--precision 64|32]
         [--tree auto|device|host] [--nblocks N] [--no-graphs]
-        [--surrogate-epochs E]
+        [--step-kernel fused|separate] [--surrogate-epochs E]
 
 CONFIG is one of the names of walicxe2d_b200.params.config (sedov64,
 sedov_amr, snr, jet_dmc, ...), or ensemble:N for the first N runs of the
@@ -32,6 +32,8 @@ def main(argv=None) -> int:
     ap.add_argument("--tree", default="auto", choices=["auto", "device", "host"])
     ap.add_argument("--nblocks", type=int, default=0, help="pool capacity (0: the config's own)")
     ap.add_argument("--no-graphs", action="store_true")
+    ap.add_argument("--step-kernel", default="separate", choices=["fused", "separate"],
+                    help="a single adiabatic run's step as one fused kernel, or the separate kernels")
     ap.add_argument("--surrogate-epochs", type=int, default=0,
                     help="cool an FP32 coolingh run through the learned surrogate trained for this many epochs")
     args = ap.parse_args(argv)
@@ -70,6 +72,7 @@ def main(argv=None) -> int:
     if nn is not None:
         run.ctx.set_surrogate(nn)
     run.ctx.set_graphs(not args.no_graphs)
+    run.ctx.set_step_kernel(args.step_kernel == "fused")
     run.run(args.steps)
     run.ctx.sync()
     print(json.dumps({"config": args.config, **status()}), flush=True)
