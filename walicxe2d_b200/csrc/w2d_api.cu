@@ -242,6 +242,8 @@ PhysArgs pargs(W2dCtx* c)
   pa.solver = c->p.solver;
   pa.limiter = c->p.limiter;
   pa.cyl = c->p.geometry == W2D_GEOM_CYLINDRICAL;
+  pa.cvh = pa.cvl = 0.0;
+  pa.cv_split = cv_split(c->p.cv, &pa.cvh, &pa.cvl) ? 1 : 0;
   return pa;
 }
 

@@ -144,6 +144,8 @@ struct PhysArgs {
   double cv, gamma, tempsc;
   int cooling, hllc_compat, solver, limiter;
   int cyl;   // CYLINDRICAL geometric source terms in step
+  double cvh, cvl;   // x / cv in two operations when cv_split (w2d_phys.cuh)
+  int cv_split;
 };
 
 __device__ __forceinline__ int cidx(int i, int j) { return (j + 1) * W2D_W + (i + 1); }
@@ -379,6 +381,9 @@ __device__ __forceinline__ Phys<R> make_phys(const PhysArgs& pa)
   ph.hllc_compat = pa.hllc_compat;
   ph.solver = (SOLVER >= 0) ? SOLVER : pa.solver;
   ph.limiter = (LIMITER >= -1) ? LIMITER : pa.limiter;
+  ph.cvh = pa.cvh;
+  ph.cvl = pa.cvl;
+  ph.cv_split = pa.cv_split;
   return ph;
 }
 

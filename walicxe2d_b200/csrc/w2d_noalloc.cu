@@ -141,6 +141,8 @@ extern "C" int w2d_timestep_noalloc(const W2dParams* p, const double* u, const i
   ph.hllc_compat = 0;
   ph.solver = p->solver;
   ph.limiter = p->limiter;
+  ph.cvh = ph.cvl = 0.0;
+  ph.cv_split = w2d::cv_split(p->cv, &ph.cvh, &ph.cvl) ? 1 : 0;
   switch (p->neq) {
     case 4: k_cfl_partials<4><<<nblocks, 256>>>(u, lev, p->nlevs, sp, ph, scratch); break;
     case 5: k_cfl_partials<5><<<nblocks, 256>>>(u, lev, p->nlevs, sp, ph, scratch); break;

@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cmath>
+
 #define W2D_NX 16               // interior cells per block side
 #define W2D_W 20                // with two ghost layers
 #define W2D_CELLS (W2D_W * W2D_W)
@@ -40,7 +42,41 @@ struct Phys {
   int hllc_compat;     // primr(4)/(primr(4)*srmur), src/hllcfluxes.f90:157
   int solver;
   int limiter;
+  // x / cv by two FP64 operations when cv_split (see cv_split below)
+  double cvh, cvl;
+  int cv_split;
 };
+
+// Division by cv = 1/(gamma-1) as fma(x, h, x*l), h = RN(1/cv) and
+// l = RN(1/cv - h), when the odd part C of cv's integer significand is
+// below 2^20 (cv = 1.5 for gamma = 5/3: C = 3).  Then x/cv = (X 2^s)/C times
+// a power of two (X: x's significand, s >= 1), so x/cv minus any midpoint
+// between neighbouring doubles is an odd multiple of ulp/(2C): x/cv lies at
+// least ulp/(2C) from every midpoint.  fma(x, h, x*l) rounds once a value
+// within about 2^-104 |x/cv| of x/cv (h + l carries 1/cv to about 2^-107,
+// x*l is rounded at 2^-53 of a term 2^-53 below the result), far inside
+// that margin, so it returns the correctly rounded x/cv -- for |x| >= 2^-960
+// (x*l stays normal); other x, zeros among them (-0 * h + +0 would lose the
+// sign of -0/cv when l < 0), take the division.
+inline bool cv_split(double cv, double* h, double* l)
+{
+  if (!(cv > 0.0) || !std::isfinite(cv)) return false;
+  int e;
+  const double m = std::frexp(cv, &e);                        // [0.5, 1)
+  uint64_t M = (uint64_t)std::ldexp(m, 53);                   // the 53-bit significand
+  while ((M & 1u) == 0u) M >>= 1;
+  if (M >= (1u << 20)) return false;
+  *h = 1.0 / cv;
+  *l = std::fma(-cv, *h, 1.0) / cv;                           // (1 - cv h exactly) / cv
+  return true;
+}
+
+__device__ __forceinline__ double div_cv(const Phys<double>& ph, double x)
+{
+  if (ph.cv_split && fabs(x) >= 0x1p-960) return fma(x, ph.cvh, x * ph.cvl);
+  return x / ph.cv;
+}
+__device__ __forceinline__ float div_cv(const Phys<float>& ph, float x) { return x / ph.cv; }
 
 // src/uprim.f90:5-63 -- prim from u; T is returned for the cooling modes.
 template <int NEQ, typename R>
@@ -53,7 +89,7 @@ __device__ __forceinline__ void uprim(const Phys<R>& ph, R* prim, const R* uu, R
   prim[2] = divr(uu[2], r);
 #pragma unroll
   for (int k = 4; k < NEQ; ++k) prim[k] = uu[k];
-  prim[3] = divr(uu[3] - R(0.5) * r * (prim[1] * prim[1] + prim[2] * prim[2]), ph.cv);
+  prim[3] = div_cv(ph, uu[3] - R(0.5) * r * (prim[1] * prim[1] + prim[2] * prim[2]));
   prim[3] = fmaxr(prim[3], tiny);
   if (ph.cooling == COOL_NONE) {
     T = divr(prim[3], r);
