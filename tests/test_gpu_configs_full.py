@@ -81,7 +81,7 @@ def test_config2_sedov_amr_exact_300_steps(oracle_lib):
     assert o.leaves().size > 3000   # the developed blast of the bench
 
 
-# measured (B200, this build): the remnant 8.8e-15 worst field after 400
+# measured (B200, this build): the remnant 2.8e-14 worst field after 400
 # steps; the jet 6.9e-13 after 400 (the y momentum, whose total is small),
 # 1.3e-12 after 500: libm differences of a few ulp grow with the flow
 @pytest.mark.parametrize("name,nsteps,every", [("snr", 400, 50), ("jet_dmc", 400, 50)])

@@ -12,22 +12,39 @@
 
 namespace w2d {
 
-__device__ __forceinline__ double d_alpha(double T) { return 2.55e-13 * pow((1.e4 / T), 0.79); }
+// The powers of coolingh (src/coolingh.f90:5-259) in forms equal to them
+// as real functions that share one logarithm per cell: x**y as
+// exp(y*log(x)), with log(c*x) = log(c) + log(x) for the constant factors;
+// x**0.5 as sqrt(x); 10**x as exp10(x).  CUDA's exp, log and exp10 are
+// within a few ulp; the products y*log(x) are below ~20 in magnitude here,
+// so their rounding moves a power by < 5e-15 relative, far inside the
+// path's tolerance against the CPU restatement (relative L1 1e-12 per
+// field), and it replaces seven general pow calls per cell.
+constexpr double kLn1e3 = 6.907755278982137;      // log(1000)
+constexpr double kLn1e4 = 9.210340371976184;      // log(10000)
+constexpr double kLn1e5 = 11.512925464970229;     // log(100000)
+constexpr double kLn157890 = 11.969653867015934;  // log(157890)
+
+// alpha (src/coolingh.f90: 2.55e-13 (1e4/T)**0.79), from lT = log(T)
+__device__ __forceinline__ double d_alpha(double lT) { return 2.55e-13 * exp(0.79 * (kLn1e4 - lT)); }
 __device__ __forceinline__ double d_colf(double T) { return 5.83e-11 * sqrt(T) * exp(-157828. / T); }
-__device__ __forceinline__ double d_betah(double T)
+// betah: a = 157890/T, 1.133e-24/sqrt(a) (-0.0713 + 0.5 log a + 0.640 a**(-0.33333))
+__device__ __forceinline__ double d_betah(double T, double lT)
 {
-  double a = 157890. / T;
-  return 1.133e-24 / sqrt(a) * (-0.0713 + 0.5 * log(a) + 0.640 * pow(a, (-0.33333)));
+  const double a = 157890. / T;
+  const double la = kLn157890 - lT;
+  return 1.133e-24 / sqrt(a) * (-0.0713 + 0.5 * la + 0.640 * exp(-0.33333 * la));
 }
 
-// src/coolingh.f90:88-165
-__device__ __forceinline__ double d_aloss(double x1, double den, double dh0, double te0)
+// src/coolingh.f90:88-165 (ALOSS), with lte0 = log(te0)
+__device__ __forceinline__ double d_aloss(double x1, double den, double dh0, double te0, double lte0)
 {
   const double XO = 1.e-3, XION = 2.179e-11;
   const double C0 = 0.5732, C1 = 1.8288e-5, C2 = -1.15822e-10, C3 = 9.4288e-16;
   const double D0 = 0.5856, D1 = 1.55083e-5, D2 = -9.669e-12, D3 = 5.716e-19;
   const double ENK = 118409., EN = 1.634E-11;
   double te = fmaxr(te0, 1000.);
+  const double lte = te0 > 1000. ? lte0 : kLn1e3;
   double dh = den;
   double dhp = (1. - x1) * dh;
   double de = dhp + 1.E-4 * dh;
@@ -46,14 +63,14 @@ __device__ __forceinline__ double d_aloss(double x1, double den, double dh0, dou
   double ecoll = fmaxr(de * dh0 * qla * EN, 0.);
   double cion = 5.834E-11 * sqrt(te) * exp(-1.579E5 / te);
   double eion = de * dh0 * cion * XION;
-  double erec = fmaxr(de * dhp * (d_betah(te)), 0.);
+  double erec = fmaxr(de * dhp * (d_betah(te, lte)), 0.);
   double tm = 1. / te;
   double t2 = tm * tm;
-  double eoi = fmaxr(de * doi * pow(10., (1381465. * t2 - 12328.69 * tm - 19.82621)), 0.);
-  double eoii = fmaxr(de * doii * pow(10., (-2061075. * t2 - 14596.24 * tm - 19.01402)), 0.);
-  double betaf = 1.3 * 1.42E-27 * pow(te, 0.5);
+  double eoi = fmaxr(de * doi * exp10(1381465. * t2 - 12328.69 * tm - 19.82621), 0.);
+  double eoii = fmaxr(de * doii * exp10(-2061075. * t2 - 14596.24 * tm - 19.01402), 0.);
+  double betaf = 1.3 * 1.42E-27 * sqrt(te);
   double hiicool = de * dhp * betaf;
-  double equil = (1.0455E-18 / pow(te, 0.63)) * (1. - exp(-pow((te * 1.E-5), 1.63))) * de * den + hiicool;
+  double equil = (1.0455E-18 / exp(0.63 * lte)) * (1. - exp(-exp(1.63 * (lte - kLn1e5)))) * de * den + hiicool;
   double fr = 0.;
   if (te >= 54770.) fr = 1.;
   if (te > 44770. && te < 54770.) {
@@ -72,8 +89,9 @@ __device__ __forceinline__ void d_atomic_core(double T, double y0, double dh, do
                                               double& t1)
 {
   const double xi = 1.e-4, boltzm = 1.3807e-16;
+  const double lT = log(T);
   double col = d_colf(T);
-  double rec = d_alpha(T);
+  double rec = d_alpha(lT);
   double a = rec + col;
   double b = -((2. + xi) * rec + (1. + xi) * col);
   double c = (1. + xi) * rec;
@@ -84,7 +102,7 @@ __device__ __forceinline__ void d_atomic_core(double T, double y0, double dh, do
   y1 = fminr(y1, 1.);
   y1 = fmaxr(y1, 0.0001);
   double dh0 = y1 * dh;
-  double al = d_aloss(y0, dh, dh0, T) / (dh * dh);
+  double al = d_aloss(y0, dh, dh0, T, lT) / (dh * dh);
   double tprime = 10.;
   ce = (2. * dh * al) / (3. * boltzm * T);
   t1 = tprime + (T - tprime) * exp(-ce * dt);
@@ -93,7 +111,6 @@ __device__ __forceinline__ void d_atomic_core(double T, double y0, double dh, do
   t1 = fmaxr(t1, tprime);
 }
 
-// src/coolingh.f90:171-259 (atomic) in FP64 on one cell's u
 template <int NEQ>
 __device__ __forceinline__ void d_atomic(const Phys<double>& ph, double dt, double* uu)
 {
