@@ -299,7 +299,7 @@ def batched_measure(args, plain_value: float, td=None, rank: int = 0, ws: int = 
     mine = shard_runs(nruns, ws, rank)
     nloc = len(mine)
     out, states = {}, {}
-    for name, prec, use_nn in (("fp32nn", 32, True), ("fp64", 64, False)):
+    for name, prec, use_nn in (("fp32nn", 32, True), ("fp32exact", 32, False), ("fp64", 64, False)):
         every = ensemble_members(count=nruns, precision=prec)
         mem = [every[r] for r in mine]
         for p, ic in mem:
@@ -348,6 +348,17 @@ def batched_measure(args, plain_value: float, td=None, rank: int = 0, ws: int = 
                             ens.totals(r)) for r in range(nloc)}
         rec["nbmax_max_run"] = max(ens.status(r)["nbmax"] for r in range(nloc))
         ens.close()
+    # the FP32 runs with the exact routine against the FP64 runs: what the
+    # precision alone costs
+    l1x = []
+    for r in range(nloc):
+        ia, ra, _ = states["fp64"][r]
+        ib, rb, _ = states["fp32exact"][r]
+        common, xa, xb = np.intersect1d(ia, ib, return_indices=True)
+        a, b = ra[xa], rb[xb].astype(np.float64)
+        l1x.append(float(np.abs(b - a)[:, 0].sum() / max(np.abs(a)[:, 0].sum(), 1e-300)))
+    l1x, _ = gather_runs(l1x, 0, td)
+    l1x = np.array(l1x)
     l1, same, fl1, drift = [], 0, [], []
     for r in range(nloc):
         ia, ra, ta = states["fp64"][r]
@@ -377,6 +388,9 @@ def batched_measure(args, plain_value: float, td=None, rank: int = 0, ws: int = 
         "scaling": "strong", "n_gpus": ws,
         "leaves": out["fp32nn"]["leaves"], "ratio_to_plain_fp64_value": v / plain_value,
         "fp32nn": out["fp32nn"], "fp64_exact_same_runs": out["fp64"],
+        "fp32_exact_same_runs": dict(out["fp32exact"], density_l1_vs_fp64_max=float(l1x.max()),
+                                     density_l1_vs_fp64_median=float(np.median(l1x))),
+        "network_gain_over_exact_cooling_fp32": v / out["fp32exact"]["value"],
         "density_l1_vs_fp64": {"max": float(l1.max()), "median": float(np.median(l1)),
                                "runs_over_1e-3": int((l1 > 1e-3).sum()), "runs_same_tree": same,
                                "note": "interior cells of the leaves both runs share, after the same step count"},
@@ -675,7 +689,9 @@ def run_ours(args, ws, rank, local):
                    "max_run_l1_per_field": batched["l1_vs_fp64_per_field"]["max_over_runs"],
                    "max_mass_drift": batched["fp64_totals_drift_vs_fp64_run"]["mass_max"],
                    "max_energy_drift": batched["fp64_totals_drift_vs_fp64_run"]["energy_max"],
-                   "served": batched["fp32nn"].get("cells_served_by_network")}
+                   "served": batched["fp32nn"].get("cells_served_by_network"),
+                   "fp32_exact_cooling_value": batched["fp32_exact_same_runs"]["value"],
+                   "network_gain_over_exact_cooling_fp32": batched["network_gain_over_exact_cooling_fp32"]}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,

@@ -20,3 +20,14 @@ def record(test: str, step: int, l1, dmax: float, nneq: int, **extra) -> None:
     row.update(extra)
     with open(path, "a") as f:
         f.write(json.dumps(row) + "\n")
+
+
+def record_value(test: str, **values) -> None:
+    """One JSON line of named figures (not a field comparison)."""
+    path = os.environ.get("W2D_PARITY_LOG")
+    if not path:
+        return
+    row = {"test": test}
+    row.update({k: float(v) for k, v in values.items()})
+    with open(path, "a") as f:
+        f.write(json.dumps(row) + "\n")

@@ -131,8 +131,13 @@ __host__ __device__ constexpr size_t smem_cool()
   return 128 + sizeof(R) * NEQ * W2D_CELLS + 64 * sizeof(double);
 }
 
+// Threads of the cooling kernel: one per cell 0..17 x 0..17 of a block
+// without its four corners (320), so the FP64 routine runs in one round;
+// the block statistics use the first 256 (warps 8 and 9 add neutral values).
+constexpr int W2D_COOL_THREADS = 320;
+
 template <typename R, int NEQ, bool P>
-__global__ void __launch_bounds__(W2D_THREADS, 2) k_cool(KArgs a, PhysArgs pa, double dt_s)
+__global__ void __launch_bounds__(W2D_COOL_THREADS, 2) k_cool(KArgs a, PhysArgs pa, double dt_s)
 {
   uint64_t* bar = reinterpret_cast<uint64_t*>(w2d_smem);
   R(*st)[W2D_W][W2D_W] = reinterpret_cast<R(*)[W2D_W][W2D_W]>(w2d_smem + 128);
@@ -156,9 +161,12 @@ __global__ void __launch_bounds__(W2D_THREADS, 2) k_cool(KArgs a, PhysArgs pa, d
     jet_interior_fn<R, NEQ>(st, a, b, u);
     __syncthreads();
   }
-  for (int c = tid; c < 18 * 18; c += W2D_THREADS) {
+  for (int t = tid; t < 320; t += W2D_COOL_THREADS) {
+    // the t-th of cells 0..17 x 0..17 without the corners c = 0, 17, 306, 323
+    int c = t + 1;
+    c += (c >= 17);
+    c += (c >= 306);
     const int i = c % 18, j = c / 18;
-    if ((i == 0 || i == 17) && (j == 0 || j == 17)) continue;
     double uu[NEQ];
 #pragma unroll
     for (int k = 0; k < NEQ; ++k) uu[k] = (double)st[k][j + 1][i + 1];

@@ -179,7 +179,7 @@ static cudaError_t cool_p(const KArgs& a, const PhysArgs& pa, double dt_s, cudaS
   constexpr size_t sm = smem_cool<R, NEQ>();
   cudaError_t e = smem_opt_in(k_cool<R, NEQ, P>, sm, done);
   if (e != cudaSuccess) return e;
-  k_cool<R, NEQ, P><<<launch_grid(a), W2D_THREADS, sm, st>>>(a, pa, dt_s);
+  k_cool<R, NEQ, P><<<launch_grid(a), W2D_COOL_THREADS, sm, st>>>(a, pa, dt_s);
   return cudaGetLastError();
 }
 template <int NEQ>
