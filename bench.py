@@ -274,6 +274,15 @@ def gather_runs(l1: list, same: int, td=None):
     return [x for g in gathered for x in g[0]], sum(g[1] for g in gathered)
 
 
+def leaf_keys(lp, icoord, ids):
+    """(level, ix, iy) of leaves packed in one integer: the same block of two
+    runs whose trees diverged carries different IDs (IDs follow the refine
+    order), so runs are compared leaf by leaf on these keys."""
+    import numpy as np
+    lev = lp[ids, 0].astype(np.int64)
+    return (lev << 48) | (icoord[ids, 0].astype(np.int64) << 24) | icoord[ids, 1].astype(np.int64)
+
+
 def batched_measure(args, plain_value: float, td=None, rank: int = 0, ws: int = 1):
     """The batched FP32 + learned-cooling path: the 256-run ensemble of
     Sedov-with-coolingh runs of uneven size, its surrogate trained on the
@@ -343,9 +352,13 @@ def batched_measure(args, plain_value: float, td=None, rank: int = 0, ws: int = 
         out[name] = rec
         # interiors of every conserved field (the FP32 state is exact in
         # float32) and the FP64 totals of every run
-        states[name] = {r: (ens.leaves(r), ens.blocks(r)[1][:, :, 2:18, 2:18].astype(np.float32 if prec == 32
-                                                                                    else np.float64),
-                            ens.totals(r)) for r in range(nloc)}
+        states[name] = {}
+        for r in range(nloc):
+            ids, blk = ens.blocks(r)
+            lp_r, _, ic_r = ens.tree(r)
+            states[name][r] = (leaf_keys(lp_r, ic_r, ids),
+                               blk[:, :, 2:18, 2:18].astype(np.float32 if prec == 32 else np.float64),
+                               ens.totals(r))
         rec["nbmax_max_run"] = max(ens.status(r)["nbmax"] for r in range(nloc))
         ens.close()
     # the FP32 runs with the exact routine against the FP64 runs: what the
@@ -393,7 +406,8 @@ def batched_measure(args, plain_value: float, td=None, rank: int = 0, ws: int = 
         "network_gain_over_exact_cooling_fp32": v / out["fp32exact"]["value"],
         "density_l1_vs_fp64": {"max": float(l1.max()), "median": float(np.median(l1)),
                                "runs_over_1e-3": int((l1 > 1e-3).sum()), "runs_same_tree": same,
-                               "note": "interior cells of the leaves both runs share, after the same step count"},
+                               "note": "interior cells of the leaves both runs share (the same level and icoord), "
+                                       "after the same step count"},
         "l1_vs_fp64_per_field": {
             "fields": ["rho", "rho vx", "rho vy", "E", "rho_HI", "tracer"][:fl1.shape[1]],
             "max_over_runs": [float(x) for x in fl1.max(axis=0)],
@@ -493,12 +507,13 @@ def variants_measure(args, nn_h):
                 res["fp64" if prec == 64 else "fp32nn"] = r
                 lp, lf, icd, ib = sim.tree()
                 ids = np.nonzero(lf)[0].astype(np.int32)
-                st[prec] = (ids, sim.ctx.get_blocks(ids)[:, 0, 2:18, 2:18])
+                st[prec] = (leaf_keys(lp, icd, ids), sim.ctx.get_blocks(ids)[:, 0, 2:18, 2:18])
                 sim.close()
             common, xa, xb = np.intersect1d(st[64][0], st[32][0], return_indices=True)
             a, b = st[64][1][xa], st[32][1][xb]
             res["density_l1_vs_fp64"] = float(np.abs(b - a).sum() / max(np.abs(a).sum(), 1e-300))
             res["same_tree"] = bool(len(common) == len(st[64][0]) == len(st[32][0]))
+            res["leaves_compared"] = int(len(common))
             res["timed_steps"] = steps
             res["warm_start"] = {"fp64_steps_from_ic": VARIANT_PRE_STEPS[name], "leaves": b0["nleaf"],
                                  "time_code_units": b0["time"], "untimed_s": pre_s}

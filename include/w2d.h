@@ -379,6 +379,10 @@ int w2d_ens_run_slots(W2dEns* ens, int run, int32_t* base, int32_t* cap);
 int w2d_ens_leaves(W2dEns* ens, int run, int32_t* ids, int32_t* n);
 /* w2d_totals of run `run` */
 int w2d_ens_totals(W2dEns* ens, int run, double* tot);
+/* as w2d_sim_tree (without innerbounds) for run `run`: lp (cap x 8,
+ * column-major), leaf (cap) and icoord (cap x 2, column-major) of its host
+ * tree, cap its capacity (w2d_ens_run_slots); arrays may be NULL */
+int w2d_ens_tree(W2dEns* ens, int run, int32_t* lp, int32_t* leaf, int32_t* icoord);
 int w2d_ens_set_amr(W2dEns* ens, int on);
 /* Host wall-clock ms per phase of w2d_ens_run: [0] leaf lists, [1] dt and
  * half-step launches with locatebounds + fill plans of the changed runs,

@@ -29,3 +29,11 @@ def compare_blocks(a: np.ndarray, b: np.ndarray, mask: np.ndarray):
     ref = np.abs(b)[:, :, mask]
     l1 = d.sum(axis=(0, 2)) / np.maximum(ref.sum(axis=(0, 2)), 1e-300)
     return float(d.max()) if d.size else 0.0, l1, int((a[:, :, mask] != b[:, :, mask]).sum())
+
+
+def leaf_keys(lp: np.ndarray, icoord: np.ndarray, ids: np.ndarray) -> np.ndarray:
+    """(level, ix, iy) of leaves packed in one integer.  Two runs whose trees
+    diverged give the same block different IDs (IDs follow the refine
+    order), so such runs are compared on these keys."""
+    lev = lp[ids, 0].astype(np.int64)
+    return (lev << 48) | (icoord[ids, 0].astype(np.int64) << 24) | icoord[ids, 1].astype(np.int64)

@@ -14,6 +14,8 @@ relative L1 of COOL_RTOL (the cooling routines use CUDA's exp, pow, log and
 log10 where the oracle uses glibc's; the adiabatic path is exact).  Both
 are also checked at their developed states (about 5.6k and 11k leaves),
 warm-started on both sides from the reference's BIN files of a device run.
+The FP32 path runs configuration 2 beside the FP64 oracle (density L1 and
+FP64 conserved totals).
 The measured figures go to W2D_PARITY_LOG when it is set.
 """
 import os
@@ -21,7 +23,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import compare_blocks, noncorner_mask
+from helpers import compare_blocks, leaf_keys, noncorner_mask
 from parity_log import record
 from walicxe2d_b200.params import config
 
@@ -151,3 +153,68 @@ def test_developed_state_fp64_vs_oracle(oracle_lib, tmp_path, name, pre, nsteps,
     worst = float(np.max(l1))
     assert np.all(l1 <= COOL_RTOL), (l1, dmax, n)
     assert worst >= 0.0
+
+
+def _root_grid_density(lp, icoord, ids, u, p):
+    """The leaves' interior densities averaged conservatively onto the
+    cells of the root level (nbroot_x*16 by nbroot_y*16): a measure of the
+    solution that does not depend on where each run refined."""
+    out = np.zeros((p.nbroot_y * 16, p.nbroot_x * 16))
+    for k, b in enumerate(ids):
+        f = 1 << (int(lp[b, 0]) - 1)            # leaf cells per root cell, per side
+        n = 16 // f
+        blk = u[k, 0, 2:18, 2:18].reshape(n, f, n, f).mean(axis=(1, 3))
+        y0, x0 = int(icoord[b, 1]) // f, int(icoord[b, 0]) // f
+        out[y0:y0 + n, x0:x0 + n] = blk
+    return out
+
+
+def test_config2_fp32_against_fp64_oracle(oracle_lib):
+    """The FP32 path (fluxes, slopes and updates in FP32; the CFL reduction
+    and the conserved totals in FP64) on configuration 2 at its own size
+    against the FP64 oracle, step for step.  In FP32 the refinement
+    decisions near the criterion's threshold flip, so the trees drift apart
+    (about a tenth of the leaves by step 150); the density is compared on
+    the root-level grid both meshes cover (conservative averages of the
+    leaves), relative L1 <= 1e-3 every 50 steps, and over the leaves both
+    trees share (matched by level and icoord) <= 1e-3 as well; the FP64 totals of mass and energy against
+    the oracle's (u dV over the leaf interiors) stay within 1e-5 and 1e-4."""
+    from walicxe2d_b200.api import Simulation
+    p, ic = config("sedov_amr")
+    o = oracle_lib.Oracle(p, ic, threads=THREADS)
+    o.startup()
+    p32 = p.copy()
+    p32.precision = 32
+    s = Simulation(p32, ic)
+    s.ctx.set_graphs(True)
+    worst = 0.0
+    for step in range(1, 301):
+        o.run(1)
+        s.run(1)
+        if step % 50:
+            continue
+        lp, lf, icd, _ = s.tree()
+        ids_d = np.nonzero(lf)[0].astype(np.int32)
+        ids_o = o.leaves()
+        ud = s.ctx.get_blocks(ids_d)
+        uo = o.u[ids_o]
+        gd = _root_grid_density(lp, icd, ids_d, ud, p)
+        go = _root_grid_density(o.lp, o.icoord, ids_o, uo, p)
+        l1 = float(np.abs(gd - go).sum() / np.abs(go).sum())
+        # leaves by (level, icoord): the same ID names other blocks once the trees diverge
+        common, xd, xo = np.intersect1d(leaf_keys(lp, icd, ids_d), leaf_keys(o.lp, o.icoord, ids_o),
+                                        return_indices=True)
+        l1c = float(np.abs(ud[xd, 0, 2:18, 2:18] - uo[xo, 0, 2:18, 2:18]).sum()
+                    / np.abs(uo[xo, 0, 2:18, 2:18]).sum())
+        lev = o.lp[ids_o, 0]
+        dv = o.dx[lev] * o.dy[lev]
+        tot_o = np.einsum("bkij,b->k", uo[:, :, 2:18, 2:18], dv)
+        tot_d = s.ctx.totals()
+        dm = abs(tot_d[0] - tot_o[0]) / abs(tot_o[0])
+        de = abs(tot_d[3] - tot_o[3]) / abs(tot_o[3])
+        record("config2_fp32", step, [l1], 0.0, 0, leaves=int(ids_o.size), common=int(common.size),
+               l1_shared_leaves=l1c, mass_rel=dm, energy_rel=de)
+        worst = max(worst, l1)
+        assert l1 <= 1e-3 and l1c <= 1e-3, (step, l1, l1c)
+        assert dm <= 1e-5 and de <= 1e-4, (step, dm, de)
+    assert worst > 0.0          # the FP32 path does round differently

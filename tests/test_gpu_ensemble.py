@@ -34,6 +34,11 @@ def _assert_same_run(ens, r, sim):
     ids = ens.leaves(r)
     lp, lf, ic, ib = sim.tree()
     np.testing.assert_array_equal(ids, np.nonzero(lf)[0].astype(np.int32))
+    lpe, lfe, ice = ens.tree(r)              # the run's own tree (w2d_ens_tree)
+    nb = sim.status()["nbmax"]
+    np.testing.assert_array_equal(lpe[1:nb + 1], lp[1:nb + 1])
+    np.testing.assert_array_equal(lfe[1:nb + 1], lf[1:nb + 1])
+    np.testing.assert_array_equal(ice[1:nb + 1], ic[1:nb + 1])
     st_e, st_s = ens.status(r), sim.status()
     assert st_e["time"] == st_s["time"] and st_e["nbmax"] == st_s["nbmax"], (st_e, st_s)
     _, ue = ens.blocks(r)

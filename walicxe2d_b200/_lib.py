@@ -36,6 +36,7 @@ SIGNATURES = {
     "w2d_get_primit": (_I, [_vp, _PI32, _I, _PD]),
     "w2d_totals": (_I, [_vp, _PD]),
     "w2d_ens_totals": (_I, [_vp, _I, _PD]),
+    "w2d_ens_tree": (_I, [_vp, _I, _PI32, _PI32, _PI32]),
     "w2d_timestep": (_I, [_vp, _PD]),
     "w2d_tstep": (_I, [_vp, _D, _D]),
     "w2d_criteria": (_I, [_vp, _PD]),

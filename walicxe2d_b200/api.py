@@ -472,6 +472,24 @@ class Ensemble:
         base, _ = self.slots(run)
         return ids, self.ctx.get_blocks(ids + base)
 
+    def tree(self, run: int):
+        """lp (cap+1, 8), leaf (cap+1,), icoord (cap+1, 2) of run `run`'s
+        tree, row 0 unused, IDs in the run's numbering (w2d_ens_tree)."""
+        _, cap = self.slots(run)
+        lp = np.zeros(8 * cap, np.int32)
+        lf = np.zeros(cap, np.int32)
+        ic = np.zeros(2 * cap, np.int32)
+        rc = self.L.w2d_ens_tree(self.h, run, _pi32(lp), _pi32(lf), _pi32(ic))
+        if rc:
+            raise _lib.W2dException(rc, None, "w2d_ens_tree")
+        lp2 = np.zeros((cap + 1, 8), np.int32)
+        lp2[1:] = lp.reshape(8, cap).T
+        ic2 = np.zeros((cap + 1, 2), np.int32)
+        ic2[1:] = ic.reshape(2, cap).T
+        lf2 = np.zeros(cap + 1, np.int32)
+        lf2[1:] = lf
+        return lp2, lf2, ic2
+
     def totals(self, run: int) -> np.ndarray:
         """FP64 conserved totals of run `run` (w2d_ens_totals)."""
         t = np.zeros(self.members[run][0].neq)

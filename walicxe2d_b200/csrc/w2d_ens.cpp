@@ -407,6 +407,12 @@ int w2d_ens_leaves(W2dEns* e, int run, int32_t* ids, int32_t* n)
   return W2D_OK;
 }
 
+int w2d_ens_tree(W2dEns* e, int run, int32_t* lp, int32_t* leaf, int32_t* icoord)
+{
+  if (!e || run < 0 || run >= (int)e->runs.size()) return W2D_ERR_ARG;
+  return w2d_sim_tree(&e->runs[run], lp, leaf, icoord, nullptr, nullptr);
+}
+
 int w2d_ens_totals(W2dEns* e, int run, double* tot)
 {
   if (!e || !tot || run < 0 || run >= (int)e->runs.size()) return W2D_ERR_ARG;
