@@ -140,19 +140,18 @@ template <int NEQ, typename R>
 __device__ __forceinline__ void hllc_star(const Phys<R>& ph, const R* q, R s, R smus, R sst,
                                           R den, R* ff)
 {
-  R uu[NEQ], uuk[NEQ];
-  R rhost = divr(q[0] * smus, s - sst);
-  R ek = R(0.5) * q[0] * (q[1] * q[1] + q[2] * q[2]) + ph.cv * q[3];
-  uuk[0] = rhost;
-  uuk[1] = rhost * sst;
-  uuk[2] = rhost * q[2];
-  uuk[3] = rhost * (divr(ek, q[0]) + (sst - q[1]) * (sst + divr(q[3], den * smus)));
+  // component by component (fewer values live at once), each term formed as
+  // primf, primu and the star state form it: F + s (U* - U)
+  const R rhost = divr(q[0] * smus, s - sst);
+  const R ek = R(0.5) * q[0] * (q[1] * q[1] + q[2] * q[2]) + ph.cv * q[3];
+  ff[0] = q[0] * q[1] + s * (rhost - q[0]);
+  ff[1] = (q[0] * q[1] * q[1] + q[3]) + s * (rhost * sst - q[0] * q[1]);
+  ff[2] = q[0] * q[1] * q[2] + s * (rhost * q[2] - q[0] * q[2]);
+  const R etot = R(0.5) * q[0] * (q[1] * q[1] + q[2] * q[2]) + ph.cv * q[3];
+  ff[3] = q[1] * (etot + q[3]) +
+          s * (rhost * (divr(ek, q[0]) + (sst - q[1]) * (sst + divr(q[3], den * smus))) - etot);
 #pragma unroll
-  for (int k = 4; k < NEQ; ++k) uuk[k] = divr(rhost * q[k], q[0]);
-  primf<NEQ>(ph, q, ff);
-  primu<NEQ>(ph, q, uu);
-#pragma unroll
-  for (int k = 0; k < NEQ; ++k) ff[k] = ff[k] + s * (uuk[k] - uu[k]);
+  for (int k = 4; k < NEQ; ++k) ff[k] = q[k] * q[1] + s * (divr(rhost * q[k], q[0]) - q[k]);
 }
 
 // HLL flux between ql and qr, src/hllfluxes.f90:118-124
