@@ -204,7 +204,7 @@ class ClockSampler:
 # ncu capture of the same workload (dram__bytes_read.sum +
 # dram__bytes_write.sum over the zones of the captured launch); traffic
 # grows with the zones a launch processes
-DRAM_BYTES_PER_ZONE = {("full_step", 64): 121.2, ("half_step", 64): 74.7, ("fill_I", 64): 42.8}
+DRAM_BYTES_PER_ZONE = {("full_step", 64): 117.5, ("half_step", 64): 74.9, ("fill_I", 64): 42.7}
 
 
 def _traffic_per_zone(kernel: str, precision: int):
