@@ -804,18 +804,36 @@ __device__ __forceinline__ bool full_leaf(const KArgs& a, const PhysArgs& pa, do
   const bool visc = lev >= (geo_nlevs(a, b) - 1);
   const R eta = R(a.eta);
 
+  // ghosts of the filled up gathered from the pool (box faces read the
+  // block's own interior there too): in FP32 while the tiles land; in FP64
+  // after them, with fewer values live across the wait (there the step's
+  // register pressure costs more than the copy's latency)
+  constexpr bool early = sizeof(R) == 4;
+  const int gf = tid / 32, gg = (tid / 16) % 2, gm = 1 + tid % 16;
+  R gv[NEQ];
+  unsigned gw = 0;
+  if constexpr (early) {
+    if (tid < 128) {
+      const int2 d = a.fd[li * 4 + gf];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) gw |= unsigned(ghost_value<R>(upool, bs, a, b, d, gf, gg, gm, k, gv[k])) << k;
+    }
+  }
   if (!wait_tiles_p<U>(bar, a.err, b, par)) return false;
-  // ghosts of the filled up gathered from the pool
-  // (box faces read the block's own interior there too)
   if (tid < 128) {
-    const int gf = tid / 32, gg = (tid / 16) % 2, gm = 1 + tid % 16;
-    const int2 d = a.fd[li * 4 + gf];
     int i, j;
     ghost_ij(gf, gg, gm, i, j);
+    if constexpr (early) {
 #pragma unroll
-    for (int k = 0; k < NEQ; ++k) {
-      R v;
-      if (ghost_value<R>(upool, bs, a, b, d, gf, gg, gm, k, v)) st[k][j + 1][i + 1] = v;
+      for (int k = 0; k < NEQ; ++k)
+        if (gw >> k & 1u) st[k][j + 1][i + 1] = gv[k];
+    } else {
+      const int2 d = a.fd[li * 4 + gf];
+#pragma unroll
+      for (int k = 0; k < NEQ; ++k) {
+        R v;
+        if (ghost_value<R>(upool, bs, a, b, d, gf, gg, gm, k, v)) st[k][j + 1][i + 1] = v;
+      }
     }
   }
   if (a.jet && a.jetblk[li]) jet_interior_fn<R, NEQ>(st, a, b, nullptr);
