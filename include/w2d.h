@@ -392,6 +392,78 @@ int w2d_ens_set_amr(W2dEns* ens, int on);
 #define W2D_ENS_NPHASES 8
 int w2d_ens_phase_ms(W2dEns* ens, double* ms, int reset);
 
+/* ---- One run partitioned by blocks over several GPUs ---------------------
+ * The reference's MPI build (-DMPIP): the leaves split between ranks in
+ * contiguous ranges of their Hilbert order (src/loadbalance.f90:5-240), the
+ * faces between ranks exchanged inside boundaryII / boundaryI
+ * (src/boundaryII.f90:516-1113, src/boundaryI.f90:398-857), dt reduced with
+ * mpi_allreduce(min) (src/timestep.f90:52), block data sent across ranks by
+ * refine / coarse (src/refine.f90:60-120, src/coarse.f90:200-345).
+ *
+ * Every rank keeps the whole block tree on the host and a pool of the full
+ * capacity on its GPU indexed by global block ID; its context steps only
+ * its own leaves.  Before the full step and before boundaryI each rank
+ * receives, whole, the neighbour blocks of its leaves that other ranks own
+ * (up, then u); dt is the minimum over ranks, the criteria maxima the
+ * maximum; refined sons stay with the parent's rank, a coarsened family
+ * gathers at its first son's rank; when the largest leaf count exceeds the
+ * mean by more than the balance tolerance (default 0.10) the leaves are
+ * re-split and moving blocks take their primitives and time-step partials
+ * with them.  A partitioned run equals the run on one GPU bit for bit (dt,
+ * tree, every interior and edge-ghost value), for any number of ranks.
+ *
+ * w2d_part_create: rank `rank` of nranks, one process per GPU (the current
+ * CUDA device), joined through NCCL (libnccl.so.2, loaded at run time, or
+ * the library W2D_NCCL_LIB names) from the 128-byte unique id that one rank
+ * obtained with w2d_part_nccl_id and passed to all.  Every wait for the
+ * other ranks is bounded (W2D_PART_TIMEOUT_S seconds, default 120): past
+ * it the communicator is aborted and the call returns W2D_ERR_TIMEOUT; the
+ * run cannot continue after that.  W2D_ERR_STATE: NCCL not found.
+ * w2d_part_create_local: all nranks ranks in this process on the current
+ * device, blocks moved by device copies between the ranks' buffers, the
+ * ranks stepped in lock step -- the same partition, exchanges and results,
+ * for checking a partition on one GPU.  The run must keep at least one
+ * leaf per rank (W2D_ERR_STATE otherwise). */
+typedef struct W2dPart W2dPart;
+int w2d_part_nccl_id(uint8_t* id, int bytes);
+int w2d_part_create(const W2dParams* p, const W2dInit* ic, int nranks, int rank, const uint8_t* nccl_id,
+                    W2dPart** out);
+int w2d_part_create_local(const W2dParams* p, const W2dInit* ic, int nranks, W2dPart** out);
+int w2d_part_destroy(W2dPart* part);
+/* nsteps steps of the main loop (timestep, tstep, admesh) on every rank */
+int w2d_part_run(W2dPart* part, int nsteps);
+/* as w2d_sim_status for the whole run (zone-updates of all ranks) */
+int w2d_part_status(W2dPart* part, double* time, double* dt, int64_t* steps,
+                    int32_t* nbmax, int32_t* nleaf, int64_t* zone_updates);
+/* ranks of the run, the first rank this object holds and how many;
+ * counters[4]: blocks sent as halo, blocks migrated, re-splits, exchanges */
+int w2d_part_info(W2dPart* part, int32_t* nranks, int32_t* first_rank, int32_t* nlocal, int64_t* counters);
+/* the global tree, as w2d_sim_tree (lp cap x 8 and icoord cap x 2,
+ * column-major; leaf cap) */
+int w2d_part_tree(W2dPart* part, int32_t* lp, int32_t* leaf, int32_t* icoord);
+/* owner[nb - 1]: the rank of leaf nb, -1 for other blocks (cap entries) */
+int w2d_part_owner(W2dPart* part, int32_t* owner);
+/* u of leaves held by this object's ranks (block-major, as w2d_get_blocks);
+ * W2D_ERR_ARG for a non-leaf or a leaf of a rank in another process */
+int w2d_part_get_blocks(W2dPart* part, const int32_t* ids, int n, double* u);
+int w2d_part_set_balance(W2dPart* part, double tol);
+/* w2d_sim_set_cooltab on every rank */
+int w2d_part_set_cooltab(W2dPart* part, const double* log_t, const double* neg_log_l, int n);
+/* the context of this object's k-th rank (0 .. nlocal-1) */
+W2dCtx* w2d_part_ctx(W2dPart* part, int k);
+/* The partition rules alone (host only, no device): w2d_part_split gives
+ * the Hilbert split of the leaves of a tree (lp, leaf, icoord as
+ * w2d_set_topology takes them; nx interior cells per block side) into
+ * owner[nb - 1]; w2d_part_halo the halo lists of rank `rank` for an
+ * innerbounds list (as w2d_set_bounds takes it) and an owner array:
+ * counts[k] blocks to send to rank k, counts[nranks + k] to receive from
+ * it, the IDs (ascending per peer) in ids, sends first, *nids in all
+ * (ids NULL: counts only). */
+int w2d_part_split(const int32_t* lp, int ld_lp, const int32_t* leaf, const int32_t* icoord, int ld_icoord,
+                   int nbmax, int nbroot_x, int nbroot_y, int nlevs, int nx, int nranks, int32_t* owner);
+int w2d_part_halo(const int32_t* innerbounds, int ld, int n, const int32_t* owner, int nbmax, int rank,
+                  int nranks, int32_t* counts, int32_t* ids, int cap_ids, int32_t* nids);
+
 /* ---- Launch shapes and step graphs (no counterpart in the reference) ------
  * The per-leaf kernels (half step, full step, boundaryI, cooling, block
  * statistics) run with one CTA per leaf or on a persistent grid of 2, 4 or

@@ -100,6 +100,22 @@ SIGNATURES = {
     "w2d_set_surrogate": (_I, [_vp, _vp]),
     "w2d_set_surrogate_tol": (_I, [_vp, _D]),
     "w2d_surrogate_counts": (_I, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "w2d_part_nccl_id": (_I, [C.POINTER(C.c_uint8), _I]),
+    "w2d_part_create": (_I, [C.POINTER(W2dParams), C.POINTER(W2dInit), _I, _I, C.POINTER(C.c_uint8),
+                             C.POINTER(_vp)]),
+    "w2d_part_create_local": (_I, [C.POINTER(W2dParams), C.POINTER(W2dInit), _I, C.POINTER(_vp)]),
+    "w2d_part_destroy": (_I, [_vp]),
+    "w2d_part_run": (_I, [_vp, _I]),
+    "w2d_part_status": (_I, [_vp, _PD, _PD, C.POINTER(C.c_int64), _PI32, _PI32, C.POINTER(C.c_int64)]),
+    "w2d_part_info": (_I, [_vp, _PI32, _PI32, _PI32, C.POINTER(C.c_int64)]),
+    "w2d_part_tree": (_I, [_vp, _PI32, _PI32, _PI32]),
+    "w2d_part_owner": (_I, [_vp, _PI32]),
+    "w2d_part_get_blocks": (_I, [_vp, _PI32, _I, _PD]),
+    "w2d_part_set_balance": (_I, [_vp, _D]),
+    "w2d_part_set_cooltab": (_I, [_vp, _PD, _PD, _I]),
+    "w2d_part_ctx": (_vp, [_vp, _I]),
+    "w2d_part_split": (_I, [_PI32, _I, _PI32, _PI32, _I, _I, _I, _I, _I, _I, _I, _PI32]),
+    "w2d_part_halo": (_I, [_PI32, _I, _I, _PI32, _I, _I, _I, _PI32, _PI32, _I, _PI32]),
 }
 
 _LIB = None

@@ -511,7 +511,7 @@ int half_step(W2dCtx* c, double dt, const double* dt_dev)
 
 // src/timestep.f90:7-61 as one reduction kernel; dt stays in device memory
 // and is copied, with the error word, to pinned memory behind it
-int ctx_dt_launch(W2dCtx* c)
+int ctx_dt_reduce(W2dCtx* c, double** dt_dev)
 {
   if (!c->have_topology) return set_error(c, W2D_ERR_STATE, 0, 0, 0, "w2d_set_topology first");
   int rc0 = ensure_leaf_list(c);
@@ -523,11 +523,22 @@ int ctx_dt_launch(W2dCtx* c)
                      c->p.cooling == W2D_COOLINGDMC, c->p.cfl, c->p.psc, c->p.tsc, c->d_dtwork, c->d_dtcount,
                      c->d_dt, c->st);
   });
-  if (rc) return rc;
+  if (dt_dev) *dt_dev = c->d_dt;
+  return rc;
+}
+
+int ctx_dt_publish(W2dCtx* c)
+{
   CK(cudaMemcpyAsync(c->h_small, c->d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CK(cudaMemcpyAsync(c->h_err, c->d_err, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
   if (!c->capturing) CK(cudaEventRecord(c->ev_dt, c->st));
   return W2D_OK;
+}
+
+int ctx_dt_launch(W2dCtx* c)
+{
+  int rc = ctx_dt_reduce(c, nullptr);
+  return rc ? rc : ctx_dt_publish(c);
 }
 
 int ctx_half_step(W2dCtx* c)
@@ -549,25 +560,36 @@ int ctx_dt_wait(W2dCtx* c, double* dt)
 // src/tstep.f90:49-126 after the half step: boundaryII (inside the full
 // step's gather), the full step with viscosity and u = up, boundaryI, then
 // calcprim or cooling
-int ctx_tstep_rest(W2dCtx* c, double time, double dt)
+// adiabatic runs without the jet: the full step computes the block
+// statistics of its new interior, fill I those of the filled faces; with
+// the jet its interior writes and the statistics follow in a second pass,
+// after every fill read of the interiors; with cooling, after cooling
+static int split_stats_of(const W2dCtx* c)
+{
+  return c->p.cooling == W2D_ADIABATIC && c->p.otherb != W2D_USERBC_JET;
+}
+
+int ctx_full_step(W2dCtx* c, double time, double dt)
 {
   int rc = tstep_ready(c);
   if (rc) return rc;
   PhysArgs pa = pargs(c);
-  KArgs a2 = kargs(c, c->d_fd2);
+  KArgs af = kargs(c, c->d_fd2);
+  set_jet_state(c, af, time);   // both fills impose the jet at tstep's time
+  af.split_stats = split_stats_of(c);
+  apply_shape(c, af, TK_FULL);
+  return launch_tk(c, TK_FULL, "full_step", [&] { return c->L->full(c->neq, af, pa, dt, c->st); });
+}
+
+int ctx_tstep_tail(W2dCtx* c, double time, double dt)
+{
+  int rc = tstep_ready(c);
+  if (rc) return rc;
+  PhysArgs pa = pargs(c);
   KArgs a1 = kargs(c, c->d_fd1);
-  set_jet_state(c, a2, time);   // both fills impose the jet at tstep's time
   set_jet_state(c, a1, time);
   const bool jet = a1.jet != 0;
-  // adiabatic runs without the jet: the full step computes the block
-  // statistics of its new interior, fill I those of the filled faces; with
-  // the jet its interior writes and the statistics follow in a second pass,
-  // after every fill read of the interiors; with cooling, after cooling
-  const int stats = c->p.cooling == W2D_ADIABATIC && !jet;
-  KArgs af = a2;
-  af.split_stats = stats;
-  apply_shape(c, af, TK_FULL);
-  if ((rc = launch_tk(c, TK_FULL, "full_step", [&] { return c->L->full(c->neq, af, pa, dt, c->st); }))) return rc;
+  const int stats = split_stats_of(c);
   KArgs ai = a1;
   ai.split_stats = stats;
   apply_shape(c, ai, TK_FILL1);
@@ -585,6 +607,32 @@ int ctx_tstep_rest(W2dCtx* c, double time, double dt)
     if ((rc = launch_tk(c, TK_COOL, "cooling", [&] { return c->L->cool(c->neq, ac, pa, dts, c->st); }))) return rc;
   }
   return W2D_OK;
+}
+
+int ctx_tstep_rest(W2dCtx* c, double time, double dt)
+{
+  int rc = ctx_full_step(c, time, dt);
+  return rc ? rc : ctx_tstep_tail(c, time, dt);
+}
+
+int ctx_pools(W2dCtx* c, CtxPools* o)
+{
+  if (!c || !o) return W2D_ERR_ARG;
+  o->u = c->d_u;
+  o->up = c->d_up;
+  o->prim = c->d_prim;
+  o->cfl = c->d_cfl;
+  o->dtcool = c->d_dtcool;
+  o->block_bytes = c->bs * c->elem;
+  o->stream = c->st;
+  o->device = c->device;
+  o->cap = c->cap;
+  return W2D_OK;
+}
+
+int ctx_fail(W2dCtx* c, int code, const char* what)
+{
+  return set_error(c, code, 0, 0, 0, "%s", what);
 }
 
 // ===========================================================================

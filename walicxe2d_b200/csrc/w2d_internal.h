@@ -19,6 +19,35 @@ int ctx_dt_launch(W2dCtx* c);                           // k_dt; dt and error wo
 int ctx_half_step(W2dCtx* c);                           // k_half, dt from device memory
 int ctx_dt_wait(W2dCtx* c, double* dt);                 // waits for the copy, checks the error word
 int ctx_tstep_rest(W2dCtx* c, double time, double dt);  // full step, boundaryI, prim/cooling
+// the same sequence with room for an exchange between its parts (a block
+// partition of one run over several GPUs):
+//   ctx_dt_launch  = ctx_dt_reduce (k_dt into device memory, *dt_dev its
+//                    address) + ctx_dt_publish (the copies behind it)
+//   ctx_tstep_rest = ctx_full_step (boundaryII inside the full step's
+//                    gather, full step, u = up) + ctx_tstep_tail (boundaryI,
+//                    prim/cooling)
+int ctx_dt_reduce(W2dCtx* c, double** dt_dev);
+int ctx_dt_publish(W2dCtx* c);
+int ctx_full_step(W2dCtx* c, double time, double dt);
+int ctx_tstep_tail(W2dCtx* c, double time, double dt);
+
+// the device arrays of a context's pool, for block exchanges between
+// contexts: slot b of u / up / prim starts at b * block_bytes, of cfl and
+// dtcool at element b
+struct CtxPools {
+  void* u;
+  void* up;
+  void* prim;
+  double* cfl;
+  double* dtcool;
+  size_t block_bytes;
+  void* stream;     // cudaStream_t
+  int device;
+  int cap;          // largest slot
+};
+int ctx_pools(W2dCtx* c, CtxPools* out);
+// records a failure of a caller above the context (w2d_last_error shows it)
+int ctx_fail(W2dCtx* c, int code, const char* what);
 
 // The refines (rq, nr quads) and coarsenings (cq, nc quads) of one admesh
 // pass in one launch; equal to w2d_refine(rq) followed by w2d_coarse(cq).
