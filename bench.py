@@ -25,8 +25,10 @@ Metric: zone-updates/s = sum over steps of (leaf blocks x 256) / time.
              the host cores, a bounded sample of the same workload
 
 --impl reference times that CPU implementation alone (rank 0 only).
-Several GPUs run independent replicas (the single AMR run does not shard):
-value = all ranks' zone-updates / the slowest rank's time.
+Several GPUs run independent replicas by default: value = all ranks'
+zone-updates / the slowest rank's time.  --partition instead splits the one
+run by blocks over the GPUs (NCCL halo exchanges; strong scaling) and
+prints that run's line.
 """
 from __future__ import annotations
 
@@ -737,6 +739,78 @@ def run_ours(args, ws, rank, local):
     return 0
 
 
+def run_partition(args, ws, rank, local):
+    """--partition: the same blast as ONE run split by blocks over the ws
+    GPUs (walicxe2d_b200.partition; NCCL between the ranks, a one-rank
+    communicator at ws = 1).  Strong scaling: value = the run's
+    zone-updates / the slowest rank's device time of the K steps."""
+    import datetime
+
+    import torch
+
+    from walicxe2d_b200.params import config
+    from walicxe2d_b200.partition import PartitionedRun, nccl_unique_id
+    torch.cuda.set_device(0)
+    td = None
+    if ws > 1:
+        import torch.distributed as td
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    p, ic = config("sedov_amr")
+    p.precision = args.precision
+    run = (PartitionedRun.from_process_group(p, ic) if td else PartitionedRun.nccl(p, ic, 0, 1, nccl_unique_id()))
+    ctx = run.contexts[0]
+    run.run(args.pre_steps + max(args.warmup, 3))
+
+    def barrier():
+        if td:
+            td.barrier()
+        torch.cuda.synchronize()
+
+    clk = ClockSampler(0).__enter__()
+    barrier()
+    ctx.sync()
+    st0, c0 = run.status(), run.counters()
+    clk.mark_start()
+    step_ms = []
+    for _ in range(args.steps):
+        ctx.flush_l2()
+        ctx.event_record(0)
+        run.run(1)
+        ctx.event_record(1)
+        step_ms.append(ctx.event_elapsed(0, 1))
+    ctx.sync()
+    time.sleep(0.06)
+    clk.__exit__()
+    st1, c1 = run.status(), run.counters()
+    barrier()
+    t_ms = sum(step_ms)
+    if td:
+        tmax = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
+        td.all_reduce(tmax, op=td.ReduceOp.MAX)
+        t_ms = float(tmax.item())
+    zu = st1["zone_updates"] - st0["zone_updates"]     # the whole run's, the same on every rank
+    own = int((run.owner() == rank).sum())
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": zu / (t_ms / 1000.0), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "impl": "partition",
+            "dtype": "f64" if args.precision == 64 else "f32", "data": "synthetic",
+            "config": {"workload": "sedov_amr as one run split by blocks over the GPUs",
+                       "parallelism": f"block partition x{ws}", "leaves_at_start": st0["nleaf"],
+                       "leaves_at_end": st1["nleaf"], "leaves_rank0_at_end": own,
+                       "l2": "flushed (256 MB write) before every timed step"},
+            "exchange_per_step": {k: (c1[k] - c0[k]) / args.steps for k in c1},
+            "clocks": clk.summary(),
+            "e2e": None,
+        }
+        print(json.dumps(line), flush=True)
+    run.close()
+    if td:
+        td.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -756,11 +830,15 @@ def main():
                          "(auto: timed both ways on the run, the faster kept)")
     ap.add_argument("--pre-steps", type=int, default=PRE_STEPS,
                     help="untimed steps before warm-up (smaller cases for profiling)")
+    ap.add_argument("--partition", action="store_true",
+                    help="one run split by blocks over the GPUs (strong scaling) instead of replicas")
     args = ap.parse_args()
     ws, rank, local = _dist_env()
     if args.impl == "reference":
         return run_reference(args, ws, rank)
     _pin_device(local, ws)
+    if args.partition:
+        return run_partition(args, ws, rank, local)
     return run_ours(args, ws, rank, local)
 
 

@@ -46,6 +46,17 @@ module w2d_iface
     character(kind=c_char) :: message(240)
   end type w2d_error
 
+  ! W2dInit of include/w2d.h: the set-up of the library's own main-loop
+  ! driver (basegrid and the initial conditions of src/initmain.f90)
+  type, bind(C) :: w2d_init
+    integer(c_int32_t) :: kind, init_levels, startup_admesh, pad_
+    real(c_double) :: rho0, p0
+    real(c_double) :: e_dep
+    real(c_double) :: xc, yc, rb
+    real(c_double) :: xh0
+    real(c_double) :: extra(8)
+  end type w2d_init
+
   interface
     ! ---- lifecycle (after the allocate()s of src/initmain.f90:76-81) ----
     integer(c_int) function w2d_create(p, ctx) bind(C, name="w2d_create")
@@ -253,6 +264,35 @@ module w2d_iface
       real(c_double), intent(in) :: dx(*), dy(*)
       real(c_double), intent(out) :: dt
     end function w2d_timestep_noalloc
+
+    ! ---- one run split by blocks over several GPUs (the -DMPIP build's
+    ! counterpart): rank 0 makes the NCCL id, mpi_bcast hands it to all,
+    ! every rank creates its part on its GPU and runs the main loop
+    integer(c_int) function w2d_part_nccl_id(id, bytes) bind(C, name="w2d_part_nccl_id")
+      import :: c_int, c_int8_t
+      integer(c_int8_t), intent(out) :: id(*)
+      integer(c_int), value :: bytes
+    end function w2d_part_nccl_id
+
+    integer(c_int) function w2d_part_create(p, ic, nranks, rank, nccl_id, part) bind(C, name="w2d_part_create")
+      import :: c_int, c_int8_t, c_ptr, w2d_params, w2d_init
+      type(w2d_params), intent(in) :: p
+      type(w2d_init), intent(in) :: ic
+      integer(c_int), value :: nranks, rank
+      integer(c_int8_t), intent(in) :: nccl_id(*)
+      type(c_ptr), intent(out) :: part
+    end function w2d_part_create
+
+    integer(c_int) function w2d_part_run(part, nsteps) bind(C, name="w2d_part_run")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: part
+      integer(c_int), value :: nsteps
+    end function w2d_part_run
+
+    integer(c_int) function w2d_part_destroy(part) bind(C, name="w2d_part_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: part
+    end function w2d_part_destroy
   end interface
 
   ! the host's one context (w2d_create in initmain)

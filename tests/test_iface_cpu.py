@@ -117,8 +117,9 @@ def _compatible(cparam, farg):
     if by_value:                  # any pointer may be passed as type(c_ptr), value
         return ft == "type(c_ptr)" and depth == 1
     want = {"int32_t": "integer(c_int32_t)", "int": "integer(c_int)", "double": "real(c_double)",
-            "W2dParams": "type(w2d_params)", "W2dError": "type(w2d_error)", "W2dCtx": "type(c_ptr)"}[base]
-    if base == "W2dCtx":
+            "uint8_t": "integer(c_int8_t)", "W2dParams": "type(w2d_params)", "W2dError": "type(w2d_error)",
+            "W2dInit": "type(w2d_init)", "W2dCtx": "type(c_ptr)", "W2dPart": "type(c_ptr)"}[base]
+    if base in ("W2dCtx", "W2dPart"):
         return ft == want and depth == 2
     return ft == want and depth == 1
 
@@ -144,8 +145,14 @@ def test_the_core_step_entry_points_are_bound():
         assert name in ff, name
 
 
+def test_the_partition_entry_points_are_bound():
+    ff = f90_functions()
+    for name in ("w2d_part_nccl_id", "w2d_part_create", "w2d_part_run", "w2d_part_destroy"):
+        assert name in ff, name
+
+
 def test_fortran_types_match_the_c_structs():
-    for ftype, cstruct in (("w2d_params", "W2dParams"), ("w2d_error", "W2dError")):
+    for ftype, cstruct in (("w2d_params", "W2dParams"), ("w2d_error", "W2dError"), ("w2d_init", "W2dInit")):
         f = f90_type(ftype)
         c = c_struct(cstruct)
         assert [(C_OF_F[t], n.lower(), k) for t, n, k in f] == [(t, n.lower(), k) for t, n, k in c], ftype
