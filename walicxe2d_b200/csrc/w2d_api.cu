@@ -548,6 +548,11 @@ int ctx_half_step(W2dCtx* c)
   return half_step(c, 0.0, c->d_dt);
 }
 
+int ctx_dt_query(W2dCtx* c)
+{
+  return (int)cudaEventQuery(c->ev_dt);
+}
+
 int ctx_dt_wait(W2dCtx* c, double* dt)
 {
   CK(cudaEventSynchronize(c->ev_dt));

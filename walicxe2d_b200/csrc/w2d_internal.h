@@ -28,6 +28,8 @@ int ctx_tstep_rest(W2dCtx* c, double time, double dt);  // full step, boundaryI,
 //                    prim/cooling)
 int ctx_dt_reduce(W2dCtx* c, double** dt_dev);
 int ctx_dt_publish(W2dCtx* c);
+// cudaEventQuery of the event ctx_dt_publish records (a cudaError_t value)
+int ctx_dt_query(W2dCtx* c);
 int ctx_full_step(W2dCtx* c, double time, double dt);
 int ctx_tstep_tail(W2dCtx* c, double time, double dt);
 

@@ -308,6 +308,7 @@ struct Rank {
   double* h_dt = nullptr;        // pinned: the local dt for the local transport
   std::vector<int32_t> rq, cq;   // this rank's refines and coarsenings of a pass
   int own = 0;                   // leaves owned
+  bool plan_stale = false;       // topology pushed, fill plans and halo lists not yet
 };
 
 }  // namespace w2dp
@@ -442,6 +443,14 @@ int nccl_fail(W2dPart* P, Rank* r, ncclResult_t e, const char* what)
   return ctx_fail(r->s->ctx, W2D_ERR_CUDA, m);
 }
 
+// the pause between two polls of a wait: none for its first 5 ms (a step
+// takes a fraction of a millisecond, and a sleep overshoots by tens of
+// microseconds), then 50 us
+void poll_pause(double t0)
+{
+  if (seconds_now() - t0 > 5e-3) std::this_thread::sleep_for(std::chrono::microseconds(50));
+}
+
 // a non-blocking communicator's call: until it is no longer in progress,
 // within the run's bound (then the communicator is aborted)
 int nccl_settle(W2dPart* P, Rank* r, ncclResult_t e, const char* what)
@@ -454,20 +463,21 @@ int nccl_settle(W2dPart* P, Rank* r, ncclResult_t e, const char* what)
       P->dead = true;
       return ctx_fail(r->s->ctx, W2D_ERR_TIMEOUT, "partition: NCCL call still in progress at the time limit");
     }
-    std::this_thread::sleep_for(std::chrono::microseconds(50));
+    poll_pause(t0);
     P->nc->CommGetAsyncError(P->comm, &e);
   }
   return e == ncclSuccess ? W2D_OK : nccl_fail(P, r, e, what);
 }
 
-// the stream work queued so far, waited for within the bound (a peer that
-// never joins a collective leaves its kernel waiting: the communicator is
-// then aborted, which ends it)
-int nccl_wait(W2dPart* P, Rank* r)
+// the stream work queued so far (or, with dt_only, the copy of dt behind
+// the dt reduction and its all-reduce), waited for within the bound (a peer
+// that never joins a collective leaves its kernel waiting: the communicator
+// is then aborted, which ends it)
+int nccl_wait(W2dPart* P, Rank* r, bool dt_only = false)
 {
   const double t0 = seconds_now();
   for (;;) {
-    const cudaError_t q = cudaStreamQuery(r->st);
+    const cudaError_t q = dt_only ? static_cast<cudaError_t>(ctx_dt_query(r->s->ctx)) : cudaStreamQuery(r->st);
     if (q == cudaSuccess) return W2D_OK;
     if (q != cudaErrorNotReady) return fail_cuda(r, q, "stream of the exchange");
     ncclResult_t e = ncclSuccess;
@@ -479,7 +489,7 @@ int nccl_wait(W2dPart* P, Rank* r)
       P->dead = true;
       return ctx_fail(r->s->ctx, W2D_ERR_TIMEOUT, "partition: exchange still running at the time limit");
     }
-    std::this_thread::sleep_for(std::chrono::microseconds(20));
+    poll_pause(t0);
   }
 }
 
@@ -623,7 +633,9 @@ int xchg_grad(W2dPart* P)
 
 // this rank's leaves to its context, the global innerbounds list for the
 // fill plans, and the halo lists of the new tree
-int push_rank_tree(W2dPart* P, Rank* r)
+// this rank's leaves to its context (the dt reduction and the half step
+// need nothing more)
+int push_rank_topology(W2dPart* P, Rank* r)
 {
   W2dSim* s = r->s;
   r->own = 0;
@@ -637,14 +649,31 @@ int push_rank_tree(W2dPart* P, Rank* r)
   int rc = w2d_set_topology(s->ctx, s->levbuf.data(), s->cap, r->mask.data(), s->icoord.data(), s->cap, s->nbmax,
                             s->dx.data(), s->dy.data());
   if (rc) return rc;
+  s->dirty = false;
+  r->plan_stale = true;
+  return W2D_OK;
+}
+
+// the global innerbounds list for the fill plans and the halo lists of the
+// new tree (host work that the device's dt reduction and half step overlap)
+int push_rank_bounds(W2dPart* P, Rank* r)
+{
+  W2dSim* s = r->s;
   w2dh::locatebounds(s);
-  if ((rc = w2d_set_bounds(s->ctx, s->ib.data(), s->nib, s->nib))) return rc;
+  int rc = w2d_set_bounds(s->ctx, s->ib.data(), s->nib, s->nib);
+  if (rc) return rc;
   if ((rc = halo_lists(s->ib.data(), s->nib, s->nib, P->owner.data(), s->nbmax, r->rank, P->nranks, r->halo.send,
                        r->halo.recv)))
     return ctx_fail(s->ctx, rc, "partition: innerbounds entry outside the tree");
   if ((rc = stage(r, r->halo, P->nranks))) return rc;
-  s->dirty = false;
+  r->plan_stale = false;
   return W2D_OK;
+}
+
+int push_rank_tree(W2dPart* P, Rank* r)
+{
+  int rc = push_rank_topology(P, r);
+  return rc ? rc : push_rank_bounds(P, r);
 }
 
 TreeView view_of(W2dSim* s)
@@ -698,21 +727,22 @@ void migration_lists(Rank* r, int nranks, const std::vector<int32_t>& blocks, co
 int phase_tree(W2dPart* P, Rank* r, double** d_dt)
 {
   int rc;
-  if (r->s->dirty && (rc = push_rank_tree(P, r))) return rc;
+  if (r->s->dirty && (rc = push_rank_topology(P, r))) return rc;
   return ctx_dt_reduce(r->s->ctx, d_dt);
 }
 
-int phase_half(Rank* r)
+int phase_half(W2dPart* P, Rank* r)
 {
   int rc = ctx_dt_publish(r->s->ctx);
-  return rc ? rc : ctx_half_step(r->s->ctx);
+  if (rc || (rc = ctx_half_step(r->s->ctx))) return rc;
+  return r->plan_stale ? push_rank_bounds(P, r) : W2D_OK;   // before the halo exchange that uses its lists
 }
 
 int phase_full(W2dPart* P, Rank* r)
 {
   double dt = 0.0;
   int rc;
-  if (!P->local && (rc = nccl_wait(P, r))) return rc;     // bounded, before the unbounded event wait
+  if (!P->local && (rc = nccl_wait(P, r, true))) return rc;   // bounded, before the unbounded event wait
   if ((rc = ctx_dt_wait(r->s->ctx, &dt))) return rc;
   r->s->dt = dt;
   r->s->time = r->s->time + dt;                               // src/main.f90:88
@@ -892,7 +922,7 @@ int part_step(W2dPart* P)
   for (size_t k = 0; k < P->ranks.size(); ++k)
     if ((rc = w2dp::phase_tree(P, P->ranks[k], &d_dt[k]))) return rc;
   if ((rc = w2dp::xchg_dt(P, d_dt))) return rc;                          // src/timestep.f90:52
-  if ((rc = each(P, [&](Rank* r) { return w2dp::phase_half(r); }))) return rc;
+  if ((rc = each(P, [&](Rank* r) { return w2dp::phase_half(P, r); }))) return rc;
   if ((rc = w2dp::xchg_blocks(P, &Rank::halo, false, true, false))) return rc;   // boundaryII's remote faces
   if ((rc = each(P, [&](Rank* r) { return w2dp::phase_full(P, r); }))) return rc;
   if ((rc = w2dp::xchg_blocks(P, &Rank::halo, true, false, false))) return rc;   // boundaryI's remote faces
