@@ -433,9 +433,11 @@ __device__ __forceinline__ bool wait_tiles(uint64_t* bar, int* err, int b)
 // then spill a few registers (about 60 and 110 bytes of spill loads) but
 // keep 4 CTAs (36 warps) per SM instead of 3, which measured 12% (half) and
 // 7% (full) faster: the FP64 pipe waits less on the long division and
-// square-root chains.  (The full step gathers its fill II ghosts after its
-// tiles have landed rather than during the copy: fewer values live across
-// the wait, half the spills, 1.7% faster.)
+// square-root chains.  (The FP64 full step gathers its fill II ghosts after
+// its tiles have landed rather than during the copy: fewer values live
+// across the wait, half the spills, 1.7% faster.)  In FP32, 5 and 6 CTAs
+// per SM (40 and 32 registers, 150-210 bytes of spill loads in the full
+// step) measured 3% and 13% slower on the 256-run ensemble than 4.
 template <typename R>
 __host__ __device__ constexpr int w2d_minb(bool)
 {
