@@ -71,6 +71,7 @@ struct XField {
   char* base;          // slot b starts at base + b * stride
   long long stride;
   int words;           // 8-byte words per slot
+  int off;             // first word of the field within an item
 };
 struct XSpec {
   XField f[4];
@@ -78,21 +79,32 @@ struct XSpec {
   int words;           // per item, sum over the fields
 };
 
-__global__ void __launch_bounds__(256) k_xpack(XSpec s, const int* __restrict__ ids, int n,
-                                               unsigned long long* __restrict__ buf, int unpack)
+// 8-byte words one CTA moves at a time: an exchange of a few tens of
+// blocks still spreads over many SMs (a 20x20 FP64 block of four fields is
+// 1,600 words, four slices)
+constexpr int kSliceWords = 512;
+
+// CTA unit u = item u / slices, words (u % slices) * kSliceWords ... of it;
+// the spec stays in parameter space (__grid_constant__, fields unrolled)
+__global__ void __launch_bounds__(256) k_xpack(const __grid_constant__ XSpec s, const int* __restrict__ ids, int n,
+                                               int slices, unsigned long long* __restrict__ buf, int unpack)
 {
-  for (int k = blockIdx.x; k < n; k += gridDim.x) {
+  const long long units = (long long)n * slices;
+  for (long long u = blockIdx.x; u < units; u += gridDim.x) {
+    const int k = (int)(u / slices), sl = (int)(u % slices);
     const long long b = ids[k];
     unsigned long long* m = buf + (size_t)k * s.words;
-    int off = 0;
-    for (int q = 0; q < s.nf; ++q) {
-      unsigned long long* p = reinterpret_cast<unsigned long long*>(s.f[q].base + b * s.f[q].stride);
-      const int w = s.f[q].words;
-      if (unpack)
-        for (int t = threadIdx.x; t < w; t += blockDim.x) p[t] = m[off + t];
-      else
-        for (int t = threadIdx.x; t < w; t += blockDim.x) m[off + t] = p[t];
-      off += w;
+    const int w0 = sl * kSliceWords, w1 = min(w0 + kSliceWords, s.words);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (q < s.nf) {
+        const int a = max(w0, s.f[q].off), e = min(w1, s.f[q].off + s.f[q].words);
+        unsigned long long* p = reinterpret_cast<unsigned long long*>(s.f[q].base + b * s.f[q].stride);
+        if (unpack)
+          for (int w = a + (int)threadIdx.x; w < e; w += blockDim.x) p[w - s.f[q].off] = m[w];
+        else
+          for (int w = a + (int)threadIdx.x; w < e; w += blockDim.x) m[w] = p[w - s.f[q].off];
+      }
     }
   }
 }
@@ -397,7 +409,7 @@ XSpec spec_of(const Rank* r, bool u, bool up, bool state)
   XSpec s{};
   const long long bb = (long long)r->pools.block_bytes;
   auto add = [&](void* base, long long stride, long long bytes) {
-    s.f[s.nf] = XField{static_cast<char*>(base), stride, (int)(bytes / 8)};
+    s.f[s.nf] = XField{static_cast<char*>(base), stride, (int)(bytes / 8), s.words};
     s.words += (int)(bytes / 8);
     s.nf++;
   };
@@ -414,8 +426,9 @@ XSpec spec_of(const Rank* r, bool u, bool up, bool state)
 int launch_xpack(Rank* r, const XSpec& s, const int* ids, size_t n, unsigned long long* buf, bool unpack)
 {
   if (n == 0) return W2D_OK;
-  const int grid = (int)std::min<size_t>(n, 4 * 148);
-  k_xpack<<<grid, 256, 0, r->st>>>(s, ids, (int)n, buf, unpack ? 1 : 0);
+  const int slices = (s.words + kSliceWords - 1) / kSliceWords;
+  const int grid = (int)std::min<size_t>(n * (size_t)slices, 8 * 148);
+  k_xpack<<<grid, 256, 0, r->st>>>(s, ids, (int)n, slices, buf, unpack ? 1 : 0);
   PK(r, cudaGetLastError());
   return W2D_OK;
 }
