@@ -50,6 +50,26 @@ PRE_STEPS = 250          # untimed evolution to a developed blast
 FALLBACK_HBM_GBS = 6650.0
 
 
+_JSON_OUT = None
+
+
+def _claim_stdout():
+    """The process's stdout (fd 1) goes to stderr for the rest of the run, so
+    that libraries writing there (NCCL prints its version banner on fd 1)
+    cannot add lines to the bench's output; the JSON line goes to the
+    original stdout."""
+    global _JSON_OUT
+    if _JSON_OUT is None:
+        sys.stdout.flush()
+        _JSON_OUT = os.fdopen(os.dup(1), "w")
+        os.dup2(2, 1)
+
+
+def emit(line: dict):
+    out = _JSON_OUT if _JSON_OUT is not None else sys.stdout
+    print(json.dumps(line), file=out, flush=True)
+
+
 def _dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -560,7 +580,7 @@ def run_reference(args, ws, rank):
                                    "no Fortran compiler)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
+    emit(line)
     return 0
 
 
@@ -732,7 +752,7 @@ def run_ours(args, ws, rank, local):
             "batched": batched,
             "configs_3_4": variants,
         }
-        print(json.dumps(line), flush=True)
+        emit(line)
     if dist:
         dist[1].destroy_process_group()
     sim.close()
@@ -804,7 +824,7 @@ def run_partition(args, ws, rank, local):
             "clocks": clk.summary(),
             "e2e": None,
         }
-        print(json.dumps(line), flush=True)
+        emit(line)
     run.close()
     if td:
         td.destroy_process_group()
@@ -833,6 +853,7 @@ def main():
     ap.add_argument("--partition", action="store_true",
                     help="one run split by blocks over the GPUs (strong scaling) instead of replicas")
     args = ap.parse_args()
+    _claim_stdout()
     ws, rank, local = _dist_env()
     if args.impl == "reference":
         return run_reference(args, ws, rank)

@@ -116,6 +116,7 @@ struct Nccl {
   void* h = nullptr;
   decltype(&ncclGetUniqueId) GetUniqueId = nullptr;
   decltype(&ncclCommInitRankConfig) CommInitRankConfig = nullptr;
+  decltype(&ncclCommFinalize) CommFinalize = nullptr;
   decltype(&ncclCommDestroy) CommDestroy = nullptr;
   decltype(&ncclCommAbort) CommAbort = nullptr;
   decltype(&ncclCommGetAsyncError) CommGetAsyncError = nullptr;
@@ -151,6 +152,7 @@ const Nccl* nccl()
   };
   sym(n.GetUniqueId, "ncclGetUniqueId");
   sym(n.CommInitRankConfig, "ncclCommInitRankConfig");
+  sym(n.CommFinalize, "ncclCommFinalize");
   sym(n.CommDestroy, "ncclCommDestroy");
   sym(n.CommAbort, "ncclCommAbort");
   sym(n.CommGetAsyncError, "ncclCommGetAsyncError");
@@ -516,8 +518,14 @@ int nccl_blocks(W2dPart* P, Rank* r, const Exchange& x, const XSpec& s)
   if (e != ncclSuccess) return nccl_fail(P, r, e, "ncclGroupStart");
   for (int k = 0; k < P->nranks; ++k) {
     const size_t ns = x.send[(size_t)k].size(), nr = x.recv[(size_t)k].size();
-    if (ns) P->nc->Send(r->d_sbuf + x.soff[(size_t)k] * s.words, ns * w, ncclChar, k, P->comm, r->st);
-    if (nr) P->nc->Recv(r->d_rbuf + x.roff[(size_t)k] * s.words, nr * w, ncclChar, k, P->comm, r->st);
+    if (ns) e = P->nc->Send(r->d_sbuf + x.soff[(size_t)k] * s.words, ns * w, ncclChar, k, P->comm, r->st);
+    if (e != ncclSuccess && e != ncclInProgress) break;
+    if (nr) e = P->nc->Recv(r->d_rbuf + x.roff[(size_t)k] * s.words, nr * w, ncclChar, k, P->comm, r->st);
+    if (e != ncclSuccess && e != ncclInProgress) break;
+  }
+  if (e != ncclSuccess && e != ncclInProgress) {
+    P->nc->GroupEnd();
+    return nccl_fail(P, r, e, "ncclSend / ncclRecv");
   }
   if ((rc = nccl_settle(P, r, P->nc->GroupEnd(), "block exchange"))) return rc;
   P->exchanges++;
@@ -1018,8 +1026,20 @@ void part_free(W2dPart* P)
   for (Rank* r : P->ranks)
     if (r) cudaStreamSynchronize(r->st);
   if (P->comm && P->nc) {
-    if (P->dead) P->nc->CommAbort(P->comm);
-    else P->nc->CommDestroy(P->comm);
+    if (!P->dead) {
+      // a non-blocking communicator: finalized (its last operations
+      // flushed, bounded) before it is destroyed; aborted otherwise
+      ncclResult_t e = P->nc->CommFinalize(P->comm);
+      const double t0 = w2dp::seconds_now();
+      while (e == ncclInProgress && w2dp::seconds_now() - t0 < P->timeout_s) {
+        w2dp::poll_pause(t0);
+        P->nc->CommGetAsyncError(P->comm, &e);
+      }
+      if (e == ncclSuccess) P->nc->CommDestroy(P->comm);
+      else P->nc->CommAbort(P->comm);
+    } else {
+      P->nc->CommAbort(P->comm);
+    }
   }
   for (Rank* r : P->ranks) free_rank(r);
   delete P;
