@@ -129,13 +129,19 @@ struct Nccl {
 };
 
 // W2D_NCCL_LIB names the library; else the one already loaded into the
-// process (PyTorch's), else the loader's search path
+// process (PyTorch's), else the loader's search path.  Resolved once per
+// process (a function-local static: thread-safe initialisation).
+Nccl load_nccl();
+
 const Nccl* nccl()
 {
-  static Nccl n;
-  static bool tried = false;
-  if (tried) return n.h ? &n : nullptr;
-  tried = true;
+  static const Nccl n = load_nccl();
+  return n.h ? &n : nullptr;
+}
+
+Nccl load_nccl()
+{
+  Nccl n;
   const char* env = getenv("W2D_NCCL_LIB");
   const char* names[] = {env, "libnccl.so.2", "libnccl.so"};
   for (const char* nm : names) {
@@ -144,7 +150,7 @@ const Nccl* nccl()
     if (!n.h) n.h = dlopen(nm, RTLD_NOW | RTLD_GLOBAL);
     if (n.h) break;
   }
-  if (!n.h) return nullptr;
+  if (!n.h) return n;
   bool ok = true;
   auto sym = [&](auto& fp, const char* name) {
     fp = reinterpret_cast<std::remove_reference_t<decltype(fp)>>(dlsym(n.h, name));
@@ -165,9 +171,8 @@ const Nccl* nccl()
   if (!ok) {
     dlclose(n.h);
     n.h = nullptr;
-    return nullptr;
   }
-  return &n;
+  return n;
 }
 
 double seconds_now()
