@@ -207,6 +207,8 @@ KArgs kargs(W2dCtx* c, const int2* fd)
   } else if (c->want_graphs && !a.jet) {   // a single run's step graphs: count and dt on the device
     a.nleaf_dev = c->d_nleaf;
     a.dt_dev = c->d_dt;
+  } else if (c->dt_on_device && !a.jet) {  // dt from the reduction's device copy (ctx_set_dt_on_device)
+    a.dt_dev = c->d_dt;
   }
   return a;
 }
@@ -546,6 +548,12 @@ int ctx_half_step(W2dCtx* c)
   int rc = tstep_ready(c, false);   // the half step reads no fill plan
   if (rc) return rc;
   return half_step(c, 0.0, c->d_dt);
+}
+
+int ctx_set_dt_on_device(W2dCtx* c, bool on)
+{
+  c->dt_on_device = on;
+  return W2D_OK;
 }
 
 int ctx_dt_query(W2dCtx* c)

@@ -74,6 +74,8 @@ struct W2dCtx {
   int* d_nleaf = nullptr;        // leaf count in device memory (ensembles)
   int* h_nleaf = nullptr;        // pinned
   bool want_graphs = false, capturing = false;
+  // kernels read dt from d_dt outside step graphs too (ctx_set_dt_on_device)
+  bool dt_on_device = false;
   cudaGraphExec_t gx_first = nullptr, gx_rest = nullptr;
   int64_t nlaunch_graph_first = 0, nlaunch_graph_rest = 0;
   // the fused step kernel (w2d_step.cuh), allocated by its first use: per

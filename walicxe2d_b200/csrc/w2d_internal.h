@@ -30,6 +30,12 @@ int ctx_dt_reduce(W2dCtx* c, double** dt_dev);
 int ctx_dt_publish(W2dCtx* c);
 // cudaEventQuery of the event ctx_dt_publish records (a cudaError_t value)
 int ctx_dt_query(W2dCtx* c);
+// the step's kernels (half step, full step, cooling) read dt from the
+// reduction's device copy, as inside step graphs, so that the host need
+// not wait for dt before it launches the full step (runs without the jet,
+// whose impose_jet reads the time on the host); the dt arguments of
+// ctx_full_step / ctx_tstep_tail are then unused
+int ctx_set_dt_on_device(W2dCtx* c, bool on);
 int ctx_full_step(W2dCtx* c, double time, double dt);
 int ctx_tstep_tail(W2dCtx* c, double time, double dt);
 

@@ -328,6 +328,7 @@ struct Rank {
   std::vector<int32_t> rq, cq;   // this rank's refines and coarsenings of a pass
   int own = 0;                   // leaves owned
   bool plan_stale = false;       // topology pushed, fill plans and halo lists not yet
+  bool dt_dev = false;           // kernels read dt on the device; the host reads it at the step's end
 };
 
 }  // namespace w2dp
@@ -764,15 +765,25 @@ int phase_half(W2dPart* P, Rank* r)
   return r->plan_stale ? push_rank_bounds(P, r) : W2D_OK;   // before the halo exchange that uses its lists
 }
 
-int phase_full(W2dPart* P, Rank* r)
+// the step's dt to the host: src/main.f90:88
+int take_dt(W2dPart* P, Rank* r)
 {
   double dt = 0.0;
   int rc;
   if (!P->local && (rc = nccl_wait(P, r, true))) return rc;   // bounded, before the unbounded event wait
   if ((rc = ctx_dt_wait(r->s->ctx, &dt))) return rc;
   r->s->dt = dt;
-  r->s->time = r->s->time + dt;                               // src/main.f90:88
-  return ctx_full_step(r->s->ctx, r->s->time, dt);
+  r->s->time = r->s->time + dt;
+  return W2D_OK;
+}
+
+int phase_full(W2dPart* P, Rank* r)
+{
+  // without the jet the kernels read dt on the device and the host takes
+  // it after the step (no wait here); impose_jet needs the time first
+  if (r->dt_dev) return ctx_full_step(r->s->ctx, 0.0, 0.0);
+  int rc = take_dt(P, r);
+  return rc ? rc : ctx_full_step(r->s->ctx, r->s->time, r->s->dt);
 }
 
 int phase_tail(W2dPart* P, Rank* r)
@@ -955,11 +966,18 @@ int part_step(W2dPart* P)
   if ((rc = each(P, [&](Rank* r) { return w2dp::phase_tail(P, r); }))) return rc;
   W2dSim* s0 = P->ranks[0]->s;
   P->zone_updates += (int64_t)s0->nbleafs * s0->p.nx * s0->p.ny;
+  if (!s0->amr) {   // nothing has waited for the step's kernels yet
+    rc = each(P, [&](Rank* r) {
+      int rc2 = P->local ? W2D_OK : w2dp::nccl_wait(P, r);
+      return rc2 ? rc2 : w2d_sync(r->s->ctx);
+    });
+    if (rc) return rc;
+  }
+  // the step's dt (copied to the host behind the reduction, long done)
+  if ((rc = each(P, [&](Rank* r) { return r->dt_dev ? w2dp::take_dt(P, r) : W2D_OK; }))) return rc;
   if (s0->amr) {
     if ((rc = w2dp::xchg_grad(P))) return rc;
     if ((rc = part_admesh(P))) return rc;
-  } else {
-    if ((rc = each(P, [&](Rank* r) { return w2d_sync(r->s->ctx); }))) return rc;
   }
   for (Rank* r : P->ranks) r->s->steps++;
   return W2D_OK;
@@ -999,6 +1017,8 @@ int new_rank(const W2dParams* p, const W2dInit* ic, int rank, Rank** out)
     return rc;
   }
   ctx_pools(r->s->ctx, &r->pools);
+  r->dt_dev = p->otherb != W2D_USERBC_JET;
+  ctx_set_dt_on_device(r->s->ctx, r->dt_dev);
   r->st = static_cast<cudaStream_t>(r->pools.stream);
   r->mask.assign((size_t)r->s->cap, 0);
   if (cudaMallocHost(&r->h_dt, sizeof(double)) != cudaSuccess) {
