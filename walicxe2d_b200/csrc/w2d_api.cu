@@ -640,7 +640,21 @@ int ctx_pools(W2dCtx* c, CtxPools* o)
   o->stream = c->st;
   o->device = c->device;
   o->cap = c->cap;
+  o->grad = c->d_grad;
+  o->leafflag = c->d_leafflag;
   return W2D_OK;
+}
+
+int ctx_err_fetch(W2dCtx* c)
+{
+  CK(cudaMemcpyAsync(c->h_err, c->d_err, 4 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  return W2D_OK;
+}
+
+int ctx_err_check(W2dCtx* c)
+{
+  tune_collect(c);
+  return check_device(c);
 }
 
 int ctx_fail(W2dCtx* c, int code, const char* what)

@@ -52,8 +52,15 @@ struct CtxPools {
   void* stream;     // cudaStream_t
   int device;
   int cap;          // largest slot
+  double* grad;     // criteria maximum per slot (the statistics write it)
+  int* leafflag;    // 1 for the slots of the leaf list of the last topology upload
 };
 int ctx_pools(W2dCtx* c, CtxPools* out);
+// the device error word queued for download behind the work so far, and
+// its check once the caller has waited for the stream (as sync_and_check
+// does in one call)
+int ctx_err_fetch(W2dCtx* c);
+int ctx_err_check(W2dCtx* c);
 // records a failure of a caller above the context (w2d_last_error shows it)
 int ctx_fail(W2dCtx* c, int code, const char* what);
 

@@ -109,6 +109,15 @@ __global__ void __launch_bounds__(256) k_xpack(const __grid_constant__ XSpec s, 
   }
 }
 
+// the criteria maxima of this rank's leaves, -1 for every other block, as
+// w2d_criteria hands them to the host: out[nb - 1] for nb = 1..nbmax
+__global__ void __launch_bounds__(256) k_mask_grad(const double* __restrict__ grad, const int* __restrict__ leafflag,
+                                                   int nbmax, double* __restrict__ out)
+{
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nbmax; q += gridDim.x * blockDim.x)
+    out[q] = leafflag[q + 1] ? grad[q + 1] : -1.0;
+}
+
 // ---------------------------------------------------------------------------
 // NCCL, resolved at run time (the library works without it for one GPU)
 
@@ -322,8 +331,8 @@ struct Rank {
   unsigned long long* d_sbuf = nullptr;
   unsigned long long* d_rbuf = nullptr;
   size_t sbuf_words = 0, rbuf_words = 0;
-  double* d_gradx = nullptr;     // criteria maxima for the all-reduce
-  size_t gradx_cap = 0;
+  double* d_gradx = nullptr;     // criteria maxima for the all-reduce (cap doubles)
+  double* h_gradx = nullptr;     // pinned: their download
   double* h_dt = nullptr;        // pinned: the local dt for the local transport
   std::vector<int32_t> rq, cq;   // this rank's refines and coarsenings of a pass
   int own = 0;                   // leaves owned
@@ -640,20 +649,16 @@ int xchg_grad(W2dPart* P)
       std::copy(g0.begin(), g0.begin() + nb, P->ranks[k]->s->grad.begin());
     return W2D_OK;
   }
+  // NCCL: the masked maxima (phase_tail) reduced in place on the device,
+  // one download, one bounded wait, then the device error word
   Rank* r = P->ranks[0];
-  if ((size_t)nb > r->gradx_cap) {
-    if (r->d_gradx) cudaFree(r->d_gradx);
-    r->d_gradx = nullptr;
-    r->gradx_cap = 0;
-    PK(r, cudaMalloc(&r->d_gradx, sizeof(double) * (size_t)r->s->cap));
-    r->gradx_cap = (size_t)r->s->cap;
-  }
-  if (nb == 0) return W2D_OK;
-  PK(r, cudaMemcpyAsync(r->d_gradx, r->s->grad.data(), sizeof(double) * (size_t)nb, cudaMemcpyHostToDevice, r->st));
-  int rc = nccl_allreduce(P, r, r->d_gradx, (size_t)nb, ncclMax);
+  int rc = nb > 0 ? nccl_allreduce(P, r, r->d_gradx, (size_t)nb, ncclMax) : W2D_OK;
   if (rc) return rc;
-  PK(r, cudaMemcpyAsync(r->s->grad.data(), r->d_gradx, sizeof(double) * (size_t)nb, cudaMemcpyDeviceToHost, r->st));
-  return nccl_wait(P, r);
+  if (nb > 0)
+    PK(r, cudaMemcpyAsync(r->h_gradx, r->d_gradx, sizeof(double) * (size_t)nb, cudaMemcpyDeviceToHost, r->st));
+  if ((rc = ctx_err_fetch(r->s->ctx)) || (rc = nccl_wait(P, r))) return rc;
+  std::copy(r->h_gradx, r->h_gradx + nb, r->s->grad.begin());
+  return ctx_err_check(r->s->ctx);
 }
 
 // ---- tree and plans --------------------------------------------------------
@@ -786,13 +791,26 @@ int phase_full(W2dPart* P, Rank* r)
   return rc ? rc : ctx_full_step(r->s->ctx, r->s->time, r->s->dt);
 }
 
+// this rank's criteria maxima, -1 for the blocks it does not hold as leaves:
+// on the host (local transport: w2d_criteria), or formed on the device for
+// the all-reduce there (NCCL; xchg_grad downloads the result)
+int prepare_grad(W2dPart* P, Rank* r)
+{
+  if (P->local) return w2d_criteria(r->s->ctx, r->s->grad.data());
+  const int nb = r->s->nbmax;
+  if (nb > 0) {
+    k_mask_grad<<<std::min((nb + 255) / 256, 4 * 148), 256, 0, r->st>>>(r->pools.grad, r->pools.leafflag, nb,
+                                                                          r->d_gradx);
+    PK(r, cudaGetLastError());
+  }
+  return W2D_OK;
+}
+
 int phase_tail(W2dPart* P, Rank* r)
 {
   int rc = ctx_tstep_tail(r->s->ctx, r->s->time, r->s->dt);
   if (rc) return rc;
-  if (!r->s->amr) return W2D_OK;
-  if (!P->local && (rc = nccl_wait(P, r))) return rc;
-  return w2d_criteria(r->s->ctx, r->s->grad.data());        // -1 for the leaves of other ranks
+  return r->s->amr ? prepare_grad(P, r) : W2D_OK;
 }
 
 // admesh's integer part from the combined criteria (the same on every rank),
@@ -945,7 +963,7 @@ int part_criteria_admesh(W2dPart* P)
   int rc = each(P, [&](Rank* r) {
     int rc2;
     if (r->s->dirty && (rc2 = w2dp::push_rank_tree(P, r))) return rc2;
-    return w2d_criteria(r->s->ctx, r->s->grad.data());
+    return w2dp::prepare_grad(P, r);
   });
   if (rc) return rc;
   if ((rc = w2dp::xchg_grad(P))) return rc;
@@ -994,6 +1012,7 @@ void free_rank(Rank* r)
   if (r->d_sbuf) cudaFree(r->d_sbuf);
   if (r->d_rbuf) cudaFree(r->d_rbuf);
   if (r->d_gradx) cudaFree(r->d_gradx);
+  if (r->h_gradx) cudaFreeHost(r->h_gradx);
   if (r->h_dt) cudaFreeHost(r->h_dt);
   if (r->s) w2d_sim_destroy(r->s);
   delete r;
@@ -1021,7 +1040,9 @@ int new_rank(const W2dParams* p, const W2dInit* ic, int rank, Rank** out)
   ctx_set_dt_on_device(r->s->ctx, r->dt_dev);
   r->st = static_cast<cudaStream_t>(r->pools.stream);
   r->mask.assign((size_t)r->s->cap, 0);
-  if (cudaMallocHost(&r->h_dt, sizeof(double)) != cudaSuccess) {
+  if (cudaMallocHost(&r->h_dt, sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&r->d_gradx, sizeof(double) * ((size_t)r->s->cap + 1)) != cudaSuccess ||
+      cudaMallocHost(&r->h_gradx, sizeof(double) * ((size_t)r->s->cap + 1)) != cudaSuccess) {
     free_rank(r);
     return W2D_ERR_NOMEM;
   }
