@@ -13,7 +13,11 @@ kernel of one process ever waits on another's.  Everything above those
 calls is the code that runs with NCCL.
 
 Each rank's run must equal the one-GPU run bit for bit: dt every step, the
-tree, and every interior and edge-ghost value of the leaves the rank owns.
+tree, and every interior and edge-ghost value of the leaves the rank owns
+(coolingdmc included: the processes and the one-GPU run evaluate it with
+the same device code).  The DMC jet covers the ranks that wait for dt on
+the host before the full step (impose_jet reads the time there) and the
+migration of the primitives coolingdmc stores.
 """
 import multiprocessing as mp
 import os
@@ -30,6 +34,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 STANDIN = os.path.join(ROOT, "tests", "nccl_standin", "libnccl_standin.so")
 
 
+def _dmc_table():
+    rows = np.loadtxt(os.path.join(ROOT, "tests", "golden", "coolingDMC.tab"))
+    return rows[:, 0], rows[:, 1]
+
+
 def _rank(rank, n, ident, name, steps, tol, q):
     try:
         os.environ["W2D_NCCL_LIB"] = STANDIN
@@ -39,6 +48,8 @@ def _rank(rank, n, ident, name, steps, tol, q):
         r = PartitionedRun.nccl(p, ic, rank, n, ident)
         if tol is not None:
             r.set_balance(tol)
+        if name.endswith("dmc"):
+            r.set_cooltab(*_dmc_table())
         dts = []
         for _ in range(steps):
             r.run(1)
@@ -55,7 +66,7 @@ def _rank(rank, n, ident, name, steps, tol, q):
 
 @pytest.mark.timeout(600)
 @pytest.mark.parametrize("name,n,steps,tol", [("sedov_amr_small", 2, 100, None), ("sedov_amr_small", 3, 80, 0.0),
-                                               ("snr_small", 2, 60, 0.05)])
+                                               ("snr_small", 2, 60, 0.05), ("jet_small_dmc", 2, 60, 0.0)])
 def test_nccl_ranks_as_processes_equal_one_gpu(name, n, steps, tol):
     assert os.path.exists(STANDIN), "build() compiles tests/nccl_standin"
     ident = f"w2dstandin-test-{os.getpid()}-{time.time_ns()}".encode().ljust(128, b"\0")
@@ -81,6 +92,8 @@ def test_nccl_ranks_as_processes_equal_one_gpu(name, n, steps, tol):
     p, ic = config(name)
     s = Simulation(p, ic)
     s.set_tree_mode("host")
+    if name.endswith("dmc"):
+        s.set_cooltab(*_dmc_table())
     dts = []
     for _ in range(steps):
         s.run(1)
