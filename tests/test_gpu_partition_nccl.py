@@ -117,3 +117,66 @@ def test_nccl_ranks_as_processes_equal_one_gpu(name, n, steps, tol):
     if tol == 0.0:
         assert any(res[k][9]["rebalances"] > 0 and res[k][9]["migrated"] > 0 for k in range(n))
     s.close()
+
+
+def _rank_leaves(rank, ident, q):
+    """Rank 1 takes 20 steps and leaves; rank 0 takes the same 20, then a
+    21st that must fail within the bounded waits."""
+    try:
+        os.environ["W2D_NCCL_LIB"] = STANDIN
+        os.environ["W2D_STANDIN_TIMEOUT_S"] = "3"
+        os.environ["W2D_PART_TIMEOUT_S"] = "10"
+        from walicxe2d_b200.partition import PartitionedRun
+        p, ic = config("sedov_amr_small")
+        r = PartitionedRun.nccl(p, ic, rank, 2, ident)
+        r.run(20)
+        if rank == 1:
+            r.close()
+            q.put((rank, "left"))
+            return
+        t0 = time.time()
+        try:
+            r.run(1)
+            q.put((rank, "no error"))
+            return
+        except Exception as e:
+            msg, waited = str(e), time.time() - t0
+        try:
+            r.run(1)
+            again = "ran"
+        except Exception as e2:
+            again = str(e2)
+        r.close()
+        q.put((rank, "failed", msg, waited, again))
+    except Exception as e:
+        q.put((rank, "unexpected " + repr(e)))
+
+
+@pytest.mark.timeout(300)
+def test_a_rank_that_leaves_ends_the_others_next_step_with_an_error():
+    """Failure detection without a GPU fault: the peer stops between steps,
+    the survivor's next exchange gives up on the host within its bound and
+    the call reports it; the run then refuses further steps and closes."""
+    assert os.path.exists(STANDIN), "build() compiles tests/nccl_standin"
+    ident = f"w2dstandin-leave-{os.getpid()}-{time.time_ns()}".encode().ljust(128, b"\0")
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_rank_leaves, args=(k, ident, q)) for k in range(2)]
+    for pr in procs:
+        pr.start()
+    res = {}
+    try:
+        for _ in range(2):
+            item = q.get(timeout=240)
+            res[item[0]] = item
+    finally:
+        for pr in procs:
+            pr.join(60)
+            if pr.is_alive():
+                pr.kill()
+    assert res[1][1] == "left", res[1]
+    assert res[0][1] == "failed", res[0]
+    _, _, msg, waited, again = res[0]
+    assert "partition" in msg, msg
+    assert waited < 30, waited
+    assert again != "ran" and "status 7" in again, again   # W2D_ERR_STATE: the run is over
